@@ -1,0 +1,300 @@
+/*
+ * pt.h — C ABI of libpt, the sm_100a wavefront path tracer.
+ *
+ * Plain C: fixed-width integers, plain pointers and sizes, no C++ or torch
+ * types.  Every entry point returns 0 on success or a negative PT_E* code;
+ * the message of the last failure on a context is pt_last_error(ctx).
+ * Nothing throws across this boundary and no kernel traps: device-side
+ * failures (queue overflow, step caps) raise a device flag that the host
+ * reads after the stream synchronises and turns into PT_E_DEVICE.
+ *
+ * A context owns one CUDA stream and the device copy of one scene.  A
+ * context is used by one host thread at a time; several contexts may live
+ * side by side (also on different devices).
+ *
+ * Each entry point names the reference interface it replaces
+ * (gracejinsotrue/PBRT-renderer-, path within that project).
+ */
+#ifndef PT_H
+#define PT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PT_ABI_VERSION 1
+
+/* ---- status codes ---------------------------------------------------- */
+#define PT_OK 0
+#define PT_E_INVALID (-1)     /* bad argument (null pointer, size, enum)   */
+#define PT_E_CUDA (-2)        /* a CUDA runtime call failed                */
+#define PT_E_NOMEM (-3)       /* device or host allocation failed          */
+#define PT_E_NOSCENE (-4)     /* render/trace before pt_upload_scene       */
+#define PT_E_DEVICE (-5)      /* a kernel raised the device error flag     */
+#define PT_E_UNSUPPORTED (-6) /* feature not built into this library       */
+
+/* ---- material types: include/bsdf.h:48-57 (BSDFGPUData::Type) -------- */
+#define PT_MAT_DIFFUSE 0
+#define PT_MAT_MIRROR 1
+#define PT_MAT_DIELECTRIC 2
+#define PT_MAT_MICROFACET 3
+#define PT_MAT_DISNEY 4
+#define PT_MAT_HAIR 5
+#define PT_MAT_SUBSURFACE 6
+
+#define PT_NO_TEXTURE 0xFFFFFFFFu
+
+/*
+ * pt_material — one record per mesh, the GPUMaterial layout of
+ * shaders/Common.hlsli:55-89 (36 x 4 bytes = 144 bytes, same field order).
+ * Field aliasing follows the reference plugins: hair stores beta_m in
+ * `roughness`, the cuticle tilt in degrees in `alpha` and eta in `intIOR`
+ * (src/cpu/hair.cpp:389-403); subsurface stores the mean free path in
+ * `subsurface`, g in `anisotropic` and its tint in sheen/sheenTint/clearcoat
+ * (src/cpu/subsurface.cpp:69-90).
+ * The caller fills type, colours, parameters, isEmitter/radiance and the
+ * index/vertex ranges; pt_upload_scene fills surfaceArea, emitterCdfOffset
+ * and emitterSelectionProb the way src/gpu/DXRApp_Scene.cpp:172-299 does.
+ */
+typedef struct pt_material {
+    uint32_t type;
+    float albedo[3];
+    float intIOR;
+    float extIOR;
+    float alpha;
+    uint32_t isEmitter;
+    float radiance[3];
+    uint32_t indexOffset;  /* first index of this mesh in pt_scene_desc.indices */
+    uint32_t vertexOffset; /* added to this mesh's (local) indices              */
+    uint32_t indexCount;   /* 3 x triangle count                               */
+    uint32_t vertexCount;
+    float surfaceArea;
+    uint32_t emitterCdfOffset;
+    uint32_t albedoTexIndex;
+    uint32_t normalTexIndex;
+    uint32_t roughnessTexIndex;
+    uint32_t metallicTexIndex;
+    uint32_t specularTexIndex;
+    uint32_t subsurfaceTexIndex;
+    uint32_t alphaTexIndex;
+    float roughness;
+    float metallic;
+    float specular;
+    float specularTint;
+    float sheen;
+    float sheenTint;
+    float subsurface;
+    float clearcoat;
+    float clearcoatGloss;
+    float anisotropic;
+    float betaN;
+    float emitterSelectionProb;
+} pt_material;
+
+/* GPUVolume flags: shaders/Common.hlsli:121-139 */
+#define PT_VOLUME_HETEROGENEOUS 0x1u
+
+/*
+ * pt_volume — one participating medium (shaders/Common.hlsli:124-139).
+ * density_grid indexes pt_scene_desc.grids (PT_NO_TEXTURE for none); the
+ * 4^3-brick majorant grid of src/gpu/DXRApp_Scene.cpp:625-641 is built by
+ * the library on the device.
+ */
+typedef struct pt_volume {
+    float vmin[3];
+    float vmax[3];
+    float sigma_a[3];
+    float sigma_s[3];
+    float phase_g;
+    uint32_t flags;
+    uint32_t density_grid;
+} pt_volume;
+
+/* Dense float32 density grid, x fastest (src/gpu/DXRApp_Scene.cpp:531-545). */
+typedef struct pt_grid {
+    uint32_t w, h, d;
+    const float *data;
+} pt_grid;
+
+/*
+ * pt_scene_desc — the flattened scene CreateSceneBuffers uploads
+ * (src/gpu/DXRApp_Scene.cpp:172-451).  Arrays are host memory owned by the
+ * caller; pt_upload_scene copies them.  `indices` are local to each mesh
+ * (the mesh's vertexOffset is added), exactly like the reference buffers.
+ * normals / texcoords / tangents may be NULL (zero-filled like the
+ * reference).  The envmap is RGB float32, W x H, row 0 = top (theta = 0).
+ */
+typedef struct pt_scene_desc {
+    uint32_t num_vertices;
+    const float *positions; /* 3 x num_vertices */
+    const float *normals;   /* 3 x num_vertices or NULL */
+    const float *texcoords; /* 2 x num_vertices or NULL (already V-flipped) */
+    const float *tangents;  /* 3 x num_vertices or NULL (hair strands) */
+    uint32_t num_indices;
+    const uint32_t *indices;
+    uint32_t num_meshes;
+    const pt_material *materials;
+    uint32_t env_width, env_height;
+    const float *env_rgb; /* 3 x W x H */
+    float env_scale;
+    float ev_compensation;
+    uint32_t num_volumes;
+    const pt_volume *volumes;
+    uint32_t num_grids;
+    const pt_grid *grids;
+} pt_scene_desc;
+
+/* Camera constants of shaders/Common.hlsli:31-51, built as
+ * src/gpu/DXRApp_Camera.cpp:23-112 does (lower-left corner + image plane). */
+typedef struct pt_camera {
+    float pos[3];
+    float llc[3];
+    float horizontal[3];
+    float vertical[3];
+    float lens_radius;
+    float focal_distance;
+} pt_camera;
+
+/* Sample generators of shaders/RNG.hlsli:226-274. */
+#define PT_RNG_SOBOL_OWEN 0 /* USE_SOBOL=1 (the reference default) */
+#define PT_RNG_PCG_HASH 1   /* USE_SOBOL=0 white-noise PCG stream  */
+
+/* Envmap light sampling. */
+#define PT_ENV_CDF 0   /* 2D CDF inversion of shaders/Envmap.hlsli:58-101 (same mapping) */
+#define PT_ENV_ALIAS 1 /* Walker alias table from FP64 prefix sums (same pdf) */
+
+typedef struct pt_render_params {
+    uint32_t width, height;
+    uint32_t spp;           /* samples per pixel rendered by this call            */
+    uint32_t sample_offset; /* first sample index (the reference's frameCount)    */
+    uint32_t max_depth;     /* MAX_BOUNCES (shaders/Common.hlsli:151-153)         */
+    uint32_t rng_kind;      /* PT_RNG_*                                           */
+    uint32_t env_sampling;  /* PT_ENV_*                                           */
+    uint32_t wave_paths;    /* paths in flight per wave (0 = library default)    */
+    pt_camera camera;
+} pt_render_params;
+
+/* Film: per pixel Σ(L, 1) as RGBA float32 (shaders/Shaders.hlsl:632-634)
+ * plus the Kahan compensation of the same shape.  location 0 = host
+ * memory (copied in and out by the call), 1 = device memory of ctx's device. */
+#define PT_MEM_HOST 0
+#define PT_MEM_DEVICE 1
+typedef struct pt_film {
+    uint32_t width, height;
+    float *sum;  /* 4 x W x H */
+    float *comp; /* 4 x W x H */
+    uint32_t location;
+} pt_film;
+
+typedef struct pt_stats {
+    uint64_t paths;
+    uint64_t extension_rays;
+    uint64_t shadow_rays;
+    uint64_t waves;
+    uint64_t bounces; /* wavefront iterations launched */
+    float ms_total;   /* device time of the render, CUDA events */
+    float ms_extend;  /* closest-hit traversal kernels */
+    float ms_shadow;  /* any-hit traversal kernels */
+    float ms_shade;   /* everything else */
+} pt_stats;
+
+typedef struct pt_ctx pt_ctx;
+
+/* ---- context ------------------------------------------------------------
+ * Replaces DXRApp construction + OnInit (src/gpu/DXRApp.cpp:44-79). */
+int pt_create(pt_ctx **out, int device);
+int pt_destroy(pt_ctx *ctx);
+const char *pt_last_error(const pt_ctx *ctx);
+int pt_abi_version(void);
+
+/* ---- scene --------------------------------------------------------------
+ * Replaces CreateAccelerationStructure + CreateSceneBuffers + SetupVolumes
+ * + BuildEnvmapDistribution (src/gpu/DXRApp_Scene.cpp:37-493,
+ * src/gpu/DXRApp_Textures.cpp:281-389): copies the scene, builds the LBVH
+ * and its 8-wide compressed form, the emitter CDFs, the envmap CDFs and
+ * alias table, and the volume majorant grids on the device. */
+int pt_upload_scene(pt_ctx *ctx, const pt_scene_desc *scene);
+
+/* ---- render ---------------------------------------------------------------
+ * Replaces OnRender/DispatchRays of RayGen once per spp
+ * (src/gpu/DXRApp.cpp:84-118, shaders/Shaders.hlsl:25-651): renders
+ * params->spp samples per pixel starting at params->sample_offset and adds
+ * them into film.  stats may be NULL. */
+int pt_render(pt_ctx *ctx, const pt_render_params *params, pt_film *film, pt_stats *stats);
+
+/* ---- parity entry points (batched, device or host arrays) ----------------
+ * wi, wo: local-frame directions, 3 floats each; h: hair offset per query
+ * (may be NULL = 0).  Replace MaterialEval / MaterialPdf / MaterialSample
+ * (shaders/Material.hlsli:18-194), which the Nori plugins expose as
+ * BSDF::eval / pdf / sample (include/bsdf.h:111-139).
+ * mat_index selects per-query materials from `materials` (may be NULL =
+ * material 0 for all).  For sample, `u` holds PT_SAMPLE_DIMS uniforms per
+ * query consumed in the order the shader's NextFloat calls make.  All
+ * pointers are host memory unless location == PT_MEM_DEVICE. */
+#define PT_SAMPLE_DIMS 4
+int pt_bsdf_eval_batch(pt_ctx *ctx, const pt_material *materials, uint32_t num_materials,
+                       const uint32_t *mat_index, const float *wi, const float *wo,
+                       const float *h, size_t n, float *f_out, float *pdf_out, uint32_t location);
+int pt_bsdf_sample_batch(pt_ctx *ctx, const pt_material *materials, uint32_t num_materials,
+                         const uint32_t *mat_index, const float *wi, const float *u,
+                         const float *h, size_t n, float *wo_out, float *weight_out,
+                         float *pdf_out, uint32_t location);
+
+/* Henyey-Greenstein eval/sample (shaders/Volume.hlsl:31-65).  wo: travel
+ * direction (3 floats), u: 2 uniforms per query; outputs the sampled
+ * direction and pdf. */
+int pt_phase_sample_batch(pt_ctx *ctx, const float *g, const float *wo, const float *u, size_t n,
+                          float *wi_out, float *pdf_out, uint32_t location);
+
+/* Envmap sample / pdf / eval against the uploaded scene
+ * (shaders/Envmap.hlsli:15-135).  u: 2 uniforms per query. */
+int pt_env_sample_batch(pt_ctx *ctx, uint32_t env_sampling, const float *u, size_t n,
+                        float *dir_out, float *radiance_out, float *pdf_out, uint32_t location);
+int pt_env_pdf_batch(pt_ctx *ctx, uint32_t env_sampling, const float *dir, size_t n, float *pdf_out,
+                     float *radiance_out, uint32_t location);
+/* Device copies of the envmap marginal (H+1) and conditional (H*(W+1)) CDFs. */
+int pt_env_read_cdf(pt_ctx *ctx, float *marginal, float *conditional);
+
+/* Owen-scrambled Sobol / PCG sample generator (shaders/RNG.hlsli:184-274):
+ * out[i*dims + d] = NextFloat for pixel pixel_ids[i], sample sample_ids[i],
+ * dimensions 0..dims-1, frame size width x height. */
+int pt_rng_batch(pt_ctx *ctx, uint32_t rng_kind, const uint32_t *pixel_ids, const uint32_t *sample_ids,
+                 size_t n, uint32_t dims, uint32_t width, uint32_t height, float *out,
+                 uint32_t location);
+
+/* ---- acceleration structure (topology parity + ray queries) --------------
+ * Replaces the BLAS/TLAS build (src/gpu/DXRApp_Scene.cpp:37-170) with the
+ * LBVH of the uploaded scene.  morton_out: one 30-bit code per triangle in
+ * global triangle order (may be NULL); sorted_prims_out: triangle ids in
+ * LBVH leaf order; nodes_out: (n-1) internal nodes x 2 child links
+ * (a link >= 0 is an internal node, ~link a leaf slot).  Host memory. */
+int pt_bvh_info(pt_ctx *ctx, uint32_t *num_triangles, uint32_t *num_wide_nodes);
+int pt_bvh_read(pt_ctx *ctx, uint32_t *morton_out, uint32_t *sorted_prims_out, int32_t *nodes_out);
+
+/* pt_hit: the HitPayload of shaders/Common.hlsli:158-166 (t, instance =
+ * mesh id, primitive id local to the mesh, barycentrics). */
+typedef struct pt_hit {
+    float t;
+    uint32_t mesh;
+    uint32_t prim;
+    float u, v;
+    uint32_t hit;
+} pt_hit;
+
+/* rays: n x 8 floats (ox, oy, oz, tmin, dx, dy, dz, tmax).
+ * Closest hit (TraceClosestInline, shaders/RayQueryTrace.hlsli:36-81) and
+ * occlusion (TraceShadowInline, shaders/RayQueryTrace.hlsli:88-129;
+ * occluded_out = 1 when an opaque surface blocks, transmission_out = the
+ * product of (1 - Fr) over mirror/dielectric surfaces crossed, 3 floats). */
+int pt_trace_closest(pt_ctx *ctx, const float *rays, size_t n, pt_hit *out, uint32_t location);
+int pt_trace_shadow(pt_ctx *ctx, const float *rays, size_t n, uint32_t *occluded_out,
+                    float *transmission_out, uint32_t location);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PT_H */

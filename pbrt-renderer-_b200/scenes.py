@@ -1,0 +1,344 @@
+"""Seeded synthetic workloads for the path tracer.
+
+The reference measures on its own scene files, whose large assets are absent
+(envmaps, hair, density grids); these generators stand in for them with the
+shapes, sizes and value distributions of the benchmark configurations:
+
+* ``cornell``        — 12-triangle room + icosphere (subdiv 3, 1280 tris,
+                       Disney roughness 0.5) + one quad light of radiance 17.
+* ``disney_spheres`` — n x n UV spheres of 20,480 triangles each with Disney
+                       parameters drawn U[0,1] (roughness U[0.05,1]) and a
+                       procedural sky + sun HDR envmap (peak 5e4).
+* ``hair_volume``    — camera-facing hair ribbons (Chiang BCSDF) inside an
+                       fBm density grid (heterogeneous medium).
+
+Every array is float32 / uint32 and every draw comes from
+``numpy.random.default_rng(seed)``.
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import (PT_MAT_DIFFUSE, PT_MAT_DISNEY, PT_MAT_HAIR, PT_NO_TEXTURE, PT_VOLUME_HETEROGENEOUS, Scene,
+               make_material, pt_camera, pt_volume)
+
+
+# ---------------------------------------------------------------------------
+# camera: the lower-left-corner / image-plane form of CameraConstants
+# (src/gpu/DXRApp_Camera.cpp:84-112) from a look-at and a vertical fov.
+# ---------------------------------------------------------------------------
+def look_at_camera(origin, target, up, fov_y_deg, aspect, lens_radius=0.0, focal_distance=1.0) -> pt_camera:
+    o = np.asarray(origin, np.float64)
+    f = np.asarray(target, np.float64) - o
+    f /= np.linalg.norm(f)
+    r = np.cross(f, np.asarray(up, np.float64))
+    r /= np.linalg.norm(r)
+    u = np.cross(r, f)
+    half_h = math.tan(math.radians(fov_y_deg) * 0.5)
+    half_w = half_h * aspect
+    llc = o + f - half_w * r - half_h * u
+    c = pt_camera()
+    c.pos[:] = o.astype(np.float32)
+    c.llc[:] = llc.astype(np.float32)
+    c.horizontal[:] = (2 * half_w * r).astype(np.float32)
+    c.vertical[:] = (2 * half_h * u).astype(np.float32)
+    c.lens_radius = lens_radius
+    c.focal_distance = focal_distance
+    return c
+
+
+# ---------------------------------------------------------------------------
+# meshes
+# ---------------------------------------------------------------------------
+def icosphere(subdiv: int):
+    t = (1.0 + 5 ** 0.5) / 2.0
+    v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+         (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    v = [np.array(p, np.float64) / np.linalg.norm(p) for p in v]
+    f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6),
+         (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10),
+         (8, 6, 7), (9, 8, 1)]
+    for _ in range(subdiv):
+        cache = {}
+
+        def mid(a, b):
+            k = (min(a, b), max(a, b))
+            if k not in cache:
+                p = v[a] + v[b]
+                v.append(p / np.linalg.norm(p))
+                cache[k] = len(v) - 1
+            return cache[k]
+
+        nf = []
+        for a, b, c in f:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        f = nf
+    return np.array(v, np.float64), np.array(f, np.uint32)
+
+
+def uv_sphere(slices: int, rings: int):
+    """UV sphere with 2 * slices * (rings - 1) triangles (pole fans + quads)."""
+    verts = [(0.0, 1.0, 0.0)]
+    for i in range(1, rings):
+        th = math.pi * i / rings
+        for j in range(slices):
+            ph = 2 * math.pi * j / slices
+            verts.append((math.sin(th) * math.cos(ph), math.cos(th), math.sin(th) * math.sin(ph)))
+    verts.append((0.0, -1.0, 0.0))
+    v = np.array(verts, np.float64)
+    bot = len(verts) - 1
+    faces = []
+    ring = lambda i, j: 1 + (i - 1) * slices + (j % slices)
+    for j in range(slices):
+        faces.append((0, ring(1, j + 1), ring(1, j)))
+    for i in range(1, rings - 1):
+        for j in range(slices):
+            a, b, c, d = ring(i, j), ring(i, j + 1), ring(i + 1, j), ring(i + 1, j + 1)
+            faces.append((a, b, d))
+            faces.append((a, d, c))
+    for j in range(slices):
+        faces.append((bot, ring(rings - 1, j), ring(rings - 1, j + 1)))
+    return v, np.array(faces, np.uint32)
+
+
+class _Builder:
+    def __init__(self):
+        self.pos, self.nrm, self.uv, self.tan, self.idx, self.mats = [], [], [], [], [], []
+        self.nv = 0
+        self.ni = 0
+
+    def add(self, pos, faces, mat, normals=None, uvs=None, tangents=None):
+        pos = np.asarray(pos, np.float32)
+        faces = np.asarray(faces, np.uint32).reshape(-1)
+        mat.vertexOffset, mat.vertexCount = self.nv, len(pos)
+        mat.indexOffset, mat.indexCount = self.ni, len(faces)
+        self.pos.append(pos)
+        self.nrm.append(np.zeros_like(pos) if normals is None else np.asarray(normals, np.float32))
+        self.uv.append(np.zeros((len(pos), 2), np.float32) if uvs is None else np.asarray(uvs, np.float32))
+        self.tan.append(np.zeros_like(pos) if tangents is None else np.asarray(tangents, np.float32))
+        self.idx.append(faces)
+        self.mats.append(mat)
+        self.nv += len(pos)
+        self.ni += len(faces)
+
+    def scene(self, **kw) -> Scene:
+        return Scene(np.concatenate(self.pos), np.concatenate(self.idx), self.mats, normals=np.concatenate(self.nrm),
+                     texcoords=np.concatenate(self.uv), tangents=np.concatenate(self.tan), **kw)
+
+
+def _quad(p0, p1, p2, p3):
+    return np.array([p0, p1, p2, p3], np.float32), np.array([[0, 1, 2], [0, 2, 3]], np.uint32)
+
+
+def _flat_normals(pos, faces):
+    p = np.asarray(pos, np.float64)
+    f = np.asarray(faces).reshape(-1, 3)
+    n = np.cross(p[f[0, 1]] - p[f[0, 0]], p[f[0, 2]] - p[f[0, 0]])
+    n /= np.linalg.norm(n)
+    return np.tile(n.astype(np.float32), (len(p), 1))
+
+
+# ---------------------------------------------------------------------------
+# configuration 1: Cornell-style box
+# ---------------------------------------------------------------------------
+def cornell(width=256, height=256, subdiv=3):
+    """Closed 12-triangle room (white 0.73, red 0.65, green 0.12 walls), a Disney
+    icosphere (roughness 0.5) and a downward quad light of radiance 17."""
+    b = _Builder()
+    white = make_material(PT_MAT_DIFFUSE, (0.73, 0.73, 0.73))
+    red = make_material(PT_MAT_DIFFUSE, (0.65, 0.05, 0.05))
+    green = make_material(PT_MAT_DIFFUSE, (0.12, 0.45, 0.15))
+    # room x in [-1,1], y in [0,2], z in [-1,1]; faces wound to face inward
+    walls_w = []
+    walls_w.append(_quad((-1, 0, -1), (1, 0, -1), (1, 0, 1), (-1, 0, 1)))    # floor (+y)
+    walls_w.append(_quad((-1, 2, -1), (-1, 2, 1), (1, 2, 1), (1, 2, -1)))    # ceiling (-y)
+    walls_w.append(_quad((-1, 0, -1), (-1, 2, -1), (1, 2, -1), (1, 0, -1)))  # back (+z)
+    walls_w.append(_quad((-1, 0, 1), (1, 0, 1), (1, 2, 1), (-1, 2, 1)))      # front (-z)
+    pw = np.concatenate([w[0] for w in walls_w])
+    fw = np.concatenate([w[1] + 4 * i for i, w in enumerate(walls_w)])
+    nw = np.concatenate([_flat_normals(w[0], w[1]) for w in walls_w])
+    b.add(pw, fw, white, normals=nw)
+    pl, fl = _quad((-1, 0, -1), (-1, 0, 1), (-1, 2, 1), (-1, 2, -1))       # left (+x), red
+    b.add(pl, fl, red, normals=_flat_normals(pl, fl))
+    pr, fr = _quad((1, 0, -1), (1, 2, -1), (1, 2, 1), (1, 0, 1))           # right (-x), green
+    b.add(pr, fr, green, normals=_flat_normals(pr, fr))
+    # light: 0.5 x 0.5 quad just under the ceiling, normal -y
+    y = 1.98
+    pq, fq = _quad((-0.25, y, -0.25), (0.25, y, -0.25), (0.25, y, 0.25), (-0.25, y, 0.25))
+    light = make_material(PT_MAT_DIFFUSE, (0.0, 0.0, 0.0), radiance=(17.0, 17.0, 17.0))
+    b.add(pq, fq, light, normals=_flat_normals(pq, fq))
+    v, f = icosphere(subdiv)
+    sph = make_material(PT_MAT_DISNEY, (0.8, 0.6, 0.4), roughness=0.5)
+    c, r = np.array([0.0, 0.55, -0.1]), 0.55
+    b.add(v * r + c, f, sph, normals=v)
+    scene = b.scene()
+    cam = look_at_camera((0.0, 1.0, 0.95), (0.0, 0.9, -1.0), (0, 1, 0), 62.0, width / height)
+    return scene, cam
+
+
+# ---------------------------------------------------------------------------
+# configuration 2: Disney sphere grid under a procedural sky
+# ---------------------------------------------------------------------------
+def sky_envmap(width=2048, height=1024, sun_peak=5.0e4, sun_elev_deg=35.0, sun_azim_deg=60.0, sun_sigma_deg=0.6):
+    """Equirectangular RGB float32 envmap (row 0 = zenith, y-up convention of
+    shaders/Envmap.hlsli:15-24): sky gradient above the horizon, dark ground
+    below, and a Gaussian sun lobe of the given peak radiance."""
+    y = (np.arange(height) + 0.5) / height
+    x = (np.arange(width) + 0.5) / width
+    theta = np.pi * y[:, None]
+    phi = 2 * np.pi * x[None, :]
+    d = np.stack([np.sin(theta) * np.cos(phi), np.cos(theta) * np.ones_like(phi), np.sin(theta) * np.sin(phi)], -1)
+    up = np.clip(d[..., 1], -1, 1)
+    zen = np.array([0.25, 0.45, 1.0])
+    hor = np.array([1.0, 0.95, 0.9])
+    gnd = np.array([0.12, 0.10, 0.08])
+    t = np.clip(up, 0, 1)[..., None] ** 0.5
+    sky = hor * (1 - t) + zen * t
+    env = np.where(up[..., None] > 0, sky * 1.5, gnd)
+    el, az = math.radians(sun_elev_deg), math.radians(sun_azim_deg)
+    s = np.array([math.cos(el) * math.cos(az), math.sin(el), math.cos(el) * math.sin(az)])
+    ang = np.arccos(np.clip((d * s).sum(-1), -1, 1))
+    sig = math.radians(sun_sigma_deg)
+    env = env + sun_peak * np.exp(-0.5 * (ang / sig) ** 2)[..., None] * np.array([1.0, 0.95, 0.85])
+    return env.astype(np.float32)
+
+
+def disney_spheres(width=1280, height=720, grid=8, slices=128, rings=81, seed=0, env_w=2048, env_h=1024):
+    rng = np.random.default_rng(seed)
+    b = _Builder()
+    v, f = uv_sphere(slices, rings)
+    spacing = 2.5
+    off = (grid - 1) * spacing / 2
+    for i in range(grid):
+        for j in range(grid):
+            m = make_material(PT_MAT_DISNEY, tuple(rng.uniform(0, 1, 3)))
+            m.roughness = float(rng.uniform(0.05, 1.0))
+            m.metallic, m.specular, m.specularTint = (float(x) for x in rng.uniform(0, 1, 3))
+            m.sheen, m.sheenTint, m.subsurface = (float(x) for x in rng.uniform(0, 1, 3))
+            m.clearcoat, m.clearcoatGloss = (float(x) for x in rng.uniform(0, 1, 2))
+            c = np.array([i * spacing - off, 1.0, j * spacing - off])
+            b.add(v + c, f, m, normals=v)
+    env = sky_envmap(env_w, env_h)
+    scene = b.scene(env_rgb=env, env_scale=1.0)
+    ext = off + 2.0
+    cam = look_at_camera((0.0, 1.15 * ext + 3.0, 1.6 * ext + 4.0), (0.0, 0.5, 0.0), (0, 1, 0), 40.0, width / height)
+    return scene, cam
+
+
+# ---------------------------------------------------------------------------
+# configuration 3: hair ribbons in a heterogeneous medium
+# ---------------------------------------------------------------------------
+def eumelanin_to_color(eu, beta_n):
+    """Colour whose Chiang-Eq.-9 inversion (shaders/Hair.hlsli:125-133) gives the
+    PBRT eumelanin absorption sigma_a = eu * (0.419, 0.697, 1.37)."""
+    sa = eu * np.array([0.419, 0.697, 1.37])
+    bn = beta_n
+    den = 5.969 - 0.215 * bn + 2.532 * bn ** 2 - 10.73 * bn ** 3 + 5.574 * bn ** 4 + 0.245 * bn ** 5
+    return np.exp(-np.sqrt(sa) * den)
+
+
+def fbm_grid(n=128, seed=0, octaves=5):
+    rng = np.random.default_rng(seed)
+    out = np.zeros((n, n, n), np.float64)
+    amp, total = 1.0, 0.0
+    for o in range(octaves):
+        r = 4 * 2 ** o
+        lat = rng.uniform(0, 1, (r + 1, r + 1, r + 1))
+        c = np.linspace(0, r, n, endpoint=False) + 0.5 * r / n
+        i0 = np.floor(c).astype(int)
+        t = c - i0
+        i0 = np.clip(i0, 0, r - 1)
+        t = t * t * (3 - 2 * t)
+
+        def interp(a, ax):
+            a0 = np.take(a, i0, axis=ax)
+            a1 = np.take(a, i0 + 1, axis=ax)
+            sh = [1, 1, 1]
+            sh[ax] = n
+            tt = t.reshape(sh)
+            return a0 * (1 - tt) + a1 * tt
+
+        out += amp * interp(interp(interp(lat, 0), 1), 2)
+        total += amp
+        amp *= 0.5
+    out /= total
+    # sphere falloff + contrast, density in [0, 1]
+    g = (np.arange(n) + 0.5) / n * 2 - 1
+    rr = np.sqrt(g[:, None, None] ** 2 + g[None, :, None] ** 2 + g[None, None, :] ** 2)
+    d = np.clip((out - 0.45) * 3.0, 0, 1) * np.clip(1.2 - rr, 0, 1)
+    return d.astype(np.float32)
+
+
+def hair_volume(width=1024, height=1024, strands=20000, segments=32, seed=0, grid_n=128, g=0.3):
+    rng = np.random.default_rng(seed)
+    b = _Builder()
+    cam_pos = np.array([0.0, 0.0, 4.0])
+    # strands: roots on a unit sphere cap, gently curved downward
+    roots = rng.normal(size=(strands, 3))
+    roots /= np.linalg.norm(roots, axis=1, keepdims=True)
+    roots[:, 1] = np.abs(roots[:, 1])
+    length = rng.uniform(0.6, 1.2, strands)
+    width_h = 0.004
+    eu = rng.uniform(0.1, 8.0, strands)
+    s = np.linspace(0, 1, segments + 1)
+    ribbons_pos, ribbons_uv, ribbons_tan, faces = [], [], [], []
+    # one mesh per eumelanin band keeps the material count small
+    bands = 8
+    band_of = np.minimum((eu - 0.1) / (7.9 / bands), bands - 1).astype(int)
+    for band in range(bands):
+        ids = np.nonzero(band_of == band)[0]
+        if len(ids) == 0:
+            continue
+        P, UV, T, F = [], [], [], []
+        nv = 0
+        for k in ids:
+            r0 = roots[k]
+            out = r0 + np.array([0, -0.3, 0])
+            pts = r0[None, :] + (s[:, None] * length[k]) * (out / np.linalg.norm(out))[None, :]
+            pts[:, 1] -= 0.5 * (s * length[k]) ** 2
+            tang = np.gradient(pts, axis=0)
+            tang /= np.linalg.norm(tang, axis=1, keepdims=True)
+            view = cam_pos[None, :] - pts
+            side = np.cross(tang, view)
+            side /= np.linalg.norm(side, axis=1, keepdims=True) + 1e-12
+            left, right = pts - side * width_h, pts + side * width_h
+            for i in range(segments + 1):
+                P += [left[i], right[i]]
+                UV += [(s[i], 0.0), (s[i], 1.0)]   # UV.y = (h + 1) / 2 across the ribbon
+                T += [tang[i], tang[i]]
+            for i in range(segments):
+                a = nv + 2 * i
+                F += [(a, a + 1, a + 3), (a, a + 3, a + 2)]
+            nv += 2 * (segments + 1)
+        eu_mid = 0.1 + (band + 0.5) * 7.9 / bands
+        col = eumelanin_to_color(eu_mid, 0.3)
+        m = make_material(PT_MAT_HAIR, tuple(col))
+        m.roughness, m.betaN, m.alpha, m.intIOR = 0.3, 0.3, 2.0, 1.55
+        b.add(np.array(P), np.array(F), m, uvs=np.array(UV), tangents=np.array(T))
+    dens = fbm_grid(grid_n, seed)
+    vol = pt_volume()
+    vol.vmin[:] = (-1.6, -1.6, -1.6)
+    vol.vmax[:] = (1.6, 1.6, 1.6)
+    vol.sigma_a[:] = (0.2, 0.2, 0.2)
+    vol.sigma_s[:] = (1.8, 1.8, 1.8)   # albedo 0.9
+    vol.phase_g = g
+    vol.flags = PT_VOLUME_HETEROGENEOUS
+    vol.density_grid = 0
+    env = sky_envmap(512, 256, sun_peak=2.0e3)
+    scene = b.scene(env_rgb=env, volumes=[vol], grids=[dens])
+    cam = look_at_camera(tuple(cam_pos), (0, 0.2, 0), (0, 1, 0), 45.0, width / height)
+    return scene, cam
+
+
+def sample_directions(n, seed, upper=False):
+    """Uniform unit vectors (upper hemisphere if `upper`), float32."""
+    rng = np.random.default_rng(seed)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    if upper:
+        d[:, 2] = np.abs(d[:, 2])
+    return d.astype(np.float32)
