@@ -1,0 +1,359 @@
+#!/usr/bin/env python
+"""bench.py — throughput of the sm_100a wavefront path tracer (libpt).
+
+Workload (default): 64 UV spheres of 20,480 triangles (1,310,720 triangles)
+on an 8 x 8 grid with Disney parameters drawn U[0,1] (roughness U[0.05,1]),
+a procedural 2048 x 1024 float32 sky + sun envmap (peak 5e4), 1280 x 720,
+64 samples per pixel, depth 16, MIS.  One step = one 64-spp frame
+(58,982,400 paths).  Synthetic, seeded inputs stand in for the reference's
+scene assets.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl pt|reference]
+
+Each rank renders its own 64-spp frame from a disjoint sample-index range and
+the films are summed with one NCCL all-reduce per step (weak scaling).  The
+value is the whole-job paths per second (device time, CUDA events on libpt's
+stream, max over ranks).  `e2e` repeats the measurement through pt_render with
+pinned host films (copies inside the timed region).  `--impl reference` times
+the reference's own shader code compiled for the CPU (oracle/_ref/libref.so,
+else the oracle restatement) on the host cores.
+"""
+
+from __future__ import annotations
+
+import argparse
+import importlib
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "pbrt-renderer-_b200")
+sys.path.insert(0, ROOT)
+
+METRIC = "Mpaths/s and time-to-relMSE 1e-2, cached vs plain PT on one B200"
+BYTES_PER_EXT_RAY = 48    # ray in (o, d, tmin, tmax: 32 B) + hit out (t, prim, u, v: 16 B)
+BYTES_PER_SHADOW_RAY = 36  # ray in (32 B) + visibility out (4 B)
+BYTES_PER_PATH_FILM = 64   # float4 sum + float4 Kahan compensation read-modify-write
+
+
+def load_pkg():
+    if "pbrt_b200" in sys.modules:
+        return sys.modules["pbrt_b200"]
+    spec = importlib.util.spec_from_file_location("pbrt_b200", os.path.join(PKG, "__init__.py"),
+                                                  submodule_search_locations=[PKG])
+    m = importlib.util.module_from_spec(spec)
+    sys.modules["pbrt_b200"] = m
+    spec.loader.exec_module(m)
+    return m
+
+
+def workload(name, scale=1.0):
+    pt = load_pkg()
+    scenes = importlib.import_module("pbrt_b200.scenes")
+    if name == "disney_envmap":
+        W, H, spp, depth = 1280, 720, 64, 16
+        sc, cam = scenes.disney_spheres(W, H)
+        cfg = {"workload": "disney_envmap", "spheres": 64, "triangles": sc.num_triangles, "width": W, "height": H,
+               "spp": spp, "max_depth": depth, "envmap": "2048x1024 rgb32f", "mis": True}
+    elif name == "cornell":
+        W, H, spp, depth = 256, 256, 16, 8
+        sc, cam = scenes.cornell(W, H)
+        cfg = {"workload": "cornell", "triangles": sc.num_triangles, "width": W, "height": H, "spp": spp,
+               "max_depth": depth}
+    elif name == "hair_volume":
+        W, H, spp, depth = 1024, 1024, 128, 16
+        sc, cam = scenes.hair_volume(W, H)
+        cfg = {"workload": "hair_volume", "triangles": sc.num_triangles, "width": W, "height": H, "spp": spp,
+               "max_depth": depth, "grid": "128^3 fbm"}
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    return pt, sc, cam, W, H, spp, depth, cfg
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in self.rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per extension ray from the committed ncu summary (or None)."""
+    p = os.path.join(ROOT, "profiles", "extend_traffic.json")
+    if os.path.exists(p):
+        try:
+            return json.load(open(p))
+        except ValueError:
+            return None
+    return None
+
+
+def cpu_reference_run(pt, sc, cam, W, H, depth, seconds=15.0, prefer_reference=True):
+    """Time the CPU implementation on a bounded sample of the workload:
+    whole frames at 1 spp (the reference's one-sample dispatch), repeated
+    until about `seconds` of work; returns (Mpaths/s, kind, cores, sample)."""
+    from oracle.oracle import Oracle, Reference
+    cores = os.cpu_count() or 1
+    if prefer_reference and Reference.available():
+        impl, kind = Reference(pt), "reference"
+    else:
+        impl, kind = Oracle(pt), "port"
+    impl.load(sc)
+    frames, t_total, paths = 0, 0.0, 0
+    rows = H
+    while t_total < seconds and frames < 64:
+        P = pt.render_params(W, rows, 1, cam, max_depth=depth, sample_offset=frames)
+        t0 = time.perf_counter()
+        if kind == "reference":
+            impl.render(P, threads=cores)
+        else:
+            impl.render(P, threads=cores)
+        dt = time.perf_counter() - t0
+        t_total += dt
+        paths += W * rows
+        frames += 1
+    return paths / t_total / 1e6, kind, cores, f"{frames} frame(s) of {W}x{rows} at 1 spp ({paths} paths, {t_total:.1f} s)"
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    pt, sc, cam, W, H, spp, depth, cfg = workload(args.workload)
+    times = []
+    kind = cores = sample = None
+    for i in range(args.warmup + args.steps):
+        v, kind, cores, sample = cpu_reference_run(pt, sc, cam, W, H, depth, seconds=args.cpu_seconds)
+        if i >= args.warmup:
+            times.append(v)
+    value = float(np.median(times))
+    paths_step = W * H * spp
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": paths_step / (value * 1e6) * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": dict(cfg, parallelism="host threads"),
+            "cpu_baseline": {"value": value, "unit": "Mpaths/s", "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="pt", choices=["pt", "reference"])
+    ap.add_argument("--workload", default="disney_envmap", choices=["disney_envmap", "cornell", "hair_volume"])
+    ap.add_argument("--env-sampling", default="cdf", choices=["cdf", "alias"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--spp", type=int, default=0, help="override samples per pixel (profiling of small cases)")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    pt, sc, cam, W, H, spp, depth, cfg = workload(args.workload)
+    if args.spp:
+        spp = cfg["spp"] = args.spp
+    env_mode = pt.PT_ENV_ALIAS if args.env_sampling == "alias" else pt.PT_ENV_CDF
+    ctx = pt.Context(local)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    t0 = time.perf_counter()
+    ctx.upload(sc)
+    upload_s = time.perf_counter() - t0
+    film = torch.zeros((H, W, 4), dtype=torch.float32, device="cuda")
+    comp = torch.zeros_like(film)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > 126 MB L2
+    paths_step = W * H * spp
+
+    def step(i, timing=False):
+        off = (i * world + rank) * spp
+        P = pt.render_params(W, H, spp, cam, max_depth=depth, sample_offset=off, env_sampling=env_mode,
+                             flags=pt.PT_RENDER_STAGE_TIMING if timing else 0)
+        _, _, st = ctx.render(P, film.data_ptr(), comp.data_ptr(), pt.PT_MEM_DEVICE)
+        if world > 1:
+            dist.all_reduce(film)
+            dist.all_reduce(comp)
+        return st
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    def timed_steps(first, timing):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        sts = []
+        for k in range(args.steps):
+            flush.zero_()
+            if world > 1:
+                dist.barrier()
+            torch.cuda.synchronize()
+            ev[k][0].record(stream)
+            sts.append(step(first + k, timing=timing))
+            ev[k][1].record(stream)
+            torch.cuda.synchronize()
+        t = sum(a.elapsed_time(b) for a, b in ev)
+        if world > 1:
+            tt = torch.tensor([t], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt.item())
+        return t, sts
+
+    with ClockSampler(local) as clk:
+        ms, stats = timed_steps(args.warmup, timing=False)
+    value = paths_step * world * args.steps / (ms / 1e3) / 1e6
+    # the same steps again with an event pair around every launch: per-kernel
+    # times for the roofline (the headline above carries no per-launch events)
+    _, tstats = timed_steps(args.warmup + args.steps, timing=True)
+
+    # end to end through the C ABI with pinned host films (copies in the timed region)
+    e2e_value = None
+    if not args.no_e2e:
+        hsum = torch.zeros((H, W, 4), dtype=torch.float32, pin_memory=True)
+        hcomp = torch.zeros_like(hsum, pin_memory=True)
+        film_np, comp_np = hsum.numpy(), hcomp.numpy()
+        e2e_ms = 0.0
+        for k in range(args.steps):
+            P = pt.render_params(W, H, spp, cam, max_depth=depth, sample_offset=(k * world + rank) * spp,
+                                 env_sampling=env_mode)
+            flush.zero_()
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            ctx.render(P, film_np, comp_np, pt.PT_MEM_HOST)
+            b.record(stream)
+            torch.cuda.synchronize()
+            e2e_ms += a.elapsed_time(b)
+        if world > 1:
+            t = torch.tensor([e2e_ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+        e2e_value = paths_step * world * args.steps / (e2e_ms / 1e3) / 1e6
+
+    ext = sum(s.extension_rays for s in stats)
+    sh = sum(s.shadow_rays for s in stats)
+    stage_ms = {k: sum(getattr(s, "ms_" + k) for s in tstats) for k in ("raygen", "extend", "shade", "shadow", "film")}
+    launches = {"extend": sum(s.bounces for s in tstats)}
+    peak, peak_src = measured_peaks()
+    dominant = max(stage_ms, key=stage_ms.get)
+    alg = {"extend": ext * BYTES_PER_EXT_RAY, "shadow": sh * BYTES_PER_SHADOW_RAY}
+    # roofline of the closest-hit traversal kernel: algorithmic bytes per launch / mean launch time
+    n_ext_launch = max(1, launches["extend"])
+    ext_bytes_per_launch = ext * BYTES_PER_EXT_RAY / n_ext_launch
+    ext_ms_per_launch = stage_ms["extend"] / n_ext_launch
+    achieved = ext_bytes_per_launch / (ext_ms_per_launch / 1e3) / 1e9 if ext_ms_per_launch > 0 else 0.0
+    tr = profile_traffic()
+    traffic = None
+    if tr and tr.get("workload") == cfg["workload"] and tr.get("dram_bytes_per_ray"):
+        traffic = tr["dram_bytes_per_ray"] * ext / n_ext_launch
+    n_ext = ext / (paths_step * args.steps)
+    n_sh = sh / (paths_step * args.steps)
+    b_path = BYTES_PER_PATH_FILM + BYTES_PER_EXT_RAY * n_ext + BYTES_PER_SHADOW_RAY * n_sh
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene, no reference assets)",
+        "config": dict(cfg, parallelism=f"sample-range x{world}" if world > 1 else "single GPU",
+                       env_sampling=args.env_sampling,
+                       l2="flushed between timed steps (256 MiB write); path state > L2"),
+        "mrays_per_s": round((ext + sh) * world / (ms / 1e3) / 1e6, 2),
+        "per_path": {"extension_rays": round(n_ext, 4), "shadow_rays": round(n_sh, 4),
+                     "algorithmic_bytes": round(b_path, 2),
+                     "achieved_gbs": round(value * 1e6 * b_path / world / 1e9, 2)},
+        "stage_ms_per_step": {k: round(v / args.steps, 3) for k, v in stage_ms.items()},
+        "roofline": {"bound": "hbm", "kernel": "k_extend (BVH8 closest hit)", "achieved": round(achieved, 2),
+                     "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 5),
+                     "traffic": traffic, "peak_source": peak_src,
+                     "algorithmic_bytes_per_launch": round(ext_bytes_per_launch, 1),
+                     "mean_launch_ms": round(ext_ms_per_launch, 4), "dominant_stage": dominant},
+        "e2e": None if e2e_value is None else {
+            "value": round(e2e_value, 3), "unit": "Mpaths/s", "h2d_bytes_per_step": 2 * W * H * 16,
+            "d2h_bytes_per_step": 2 * W * H * 16},
+        "gpu_launches": int(sum(s.launches for s in stats)),
+        "clocks": clk.summary(),
+        "scene_upload_s": round(upload_s, 3),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, kind, cores, sample = cpu_reference_run(pt, sc, cam, W, H, depth, seconds=args.cpu_seconds)
+        line["cpu_baseline"] = {"value": round(v, 4), "unit": "Mpaths/s", "cores": cores, "kind": kind,
+                                "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

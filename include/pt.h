@@ -174,8 +174,12 @@ typedef struct pt_render_params {
     uint32_t rng_kind;      /* PT_RNG_*                                           */
     uint32_t env_sampling;  /* PT_ENV_*                                           */
     uint32_t wave_paths;    /* paths in flight per wave (0 = library default)    */
+    uint32_t flags;         /* PT_RENDER_*                                        */
     pt_camera camera;
 } pt_render_params;
+
+/* pt_render_params.flags */
+#define PT_RENDER_STAGE_TIMING 0x1u /* fill pt_stats.ms_* per stage (CUDA events per launch) */
 
 /* Film: per pixel Σ(L, 1) as RGBA float32 (shaders/Shaders.hlsl:632-634)
  * plus the Kahan compensation of the same shape.  location 0 = host
@@ -194,11 +198,15 @@ typedef struct pt_stats {
     uint64_t extension_rays;
     uint64_t shadow_rays;
     uint64_t waves;
-    uint64_t bounces; /* wavefront iterations launched */
-    float ms_total;   /* device time of the render, CUDA events */
-    float ms_extend;  /* closest-hit traversal kernels */
-    float ms_shadow;  /* any-hit traversal kernels */
-    float ms_shade;   /* everything else */
+    uint64_t bounces;  /* wavefront iterations launched */
+    uint64_t launches; /* kernels this call launched */
+    float ms_total;    /* device time of the render, CUDA events on the context's stream */
+    /* per stage, with PT_RENDER_STAGE_TIMING (0 otherwise): */
+    float ms_raygen;   /* camera rays */
+    float ms_extend;   /* closest-hit traversal */
+    float ms_shade;    /* surface / medium / light events */
+    float ms_shadow;   /* any-hit traversal */
+    float ms_film;     /* film accumulation */
 } pt_stats;
 
 typedef struct pt_ctx pt_ctx;
@@ -207,6 +215,11 @@ typedef struct pt_ctx pt_ctx;
  * Replaces DXRApp construction + OnInit (src/gpu/DXRApp.cpp:44-79). */
 int pt_create(pt_ctx **out, int device);
 int pt_destroy(pt_ctx *ctx);
+/* Use an existing CUDA stream (a cudaStream_t passed as void*, NULL = the
+ * context's own stream) for all later work of ctx.  The caller keeps
+ * ownership of the stream.  No reference counterpart (DXRApp owns its queue,
+ * src/gpu/DXRApp_Device.cpp). */
+int pt_set_stream(pt_ctx *ctx, void *stream);
 const char *pt_last_error(const pt_ctx *ctx);
 int pt_abi_version(void);
 

@@ -52,7 +52,8 @@ class Oracle:
     """The C++ restatement (pt_oracle.cpp)."""
 
     def __init__(self, pt):
-        if not os.path.exists(ORACLE_SO):
+        src = os.path.join(HERE, "pt_oracle.cpp")
+        if not os.path.exists(ORACLE_SO) or os.path.getmtime(src) > os.path.getmtime(ORACLE_SO):
             build_oracle()
         self.pt = pt
         L = C.CDLL(ORACLE_SO)
@@ -71,6 +72,7 @@ class Oracle:
         L.or_bsdf_eval.argtypes = [C.c_int, M, U, F, F, F, S, F, F]
         L.or_bsdf_sample.argtypes = [C.c_int, M, U, F, F, F, S, F, F, F]
         L.or_phase_sample.argtypes = [C.c_int, F, F, F, S, F, F]
+        L.or_lbvh.argtypes = [P, U, U, C.POINTER(C.c_int32)]
         L.or_trace_closest.argtypes = [P, F, S, C.POINTER(pt.pt_hit)]
         L.or_trace_shadow.argtypes = [P, F, S, U, F]
         L.or_render.argtypes = [P, C.POINTER(pt.pt_render_params), F, F, C.c_int, C.POINTER(C.c_uint64)]
@@ -147,6 +149,13 @@ class Oracle:
         wi, p = np.zeros((n, 3), np.float32), np.zeros(n, np.float32)
         self.L.or_phase_sample(1 if fp64 else 0, _f(g), _f(wo), _f(u), n, _f(wi), _f(p))
         return wi, p
+
+    def lbvh(self):
+        n = self.scene.num_triangles
+        morton, order = np.zeros(n, np.uint32), np.zeros(n, np.uint32)
+        nodes = np.zeros((max(n - 1, 1), 2), np.int32)
+        self.L.or_lbvh(self.h, _u(morton), _u(order), nodes.ctypes.data_as(C.POINTER(C.c_int32)))
+        return morton, order, nodes[: max(n - 1, 0)]
 
     def trace_closest(self, rays):
         n = len(rays)

@@ -1878,6 +1878,76 @@ void or_phase_sample(int precision, const float *g, const float *wo, const float
     }
 }
 
+// CPU LBVH for topology parity (new in this build; the reference uses the
+// driver's BVH).  Morton codes of triangle-bounds centroids quantised to 10
+// bits per axis over the centroid bounds, stable sort by code, then the radix
+// tree of Karras 2012 ("Maximizing Parallelism in the Construction of BVHs,
+// Octrees, and k-d Trees", Fig. 4), with equal codes ordered by position.
+static uint32_t expand_bits10(uint32_t v) {
+    v = (v * 0x00010001u) & 0xFF0000FFu;
+    v = (v * 0x00000101u) & 0x0F00F00Fu;
+    v = (v * 0x00000011u) & 0xC30C30C3u;
+    v = (v * 0x00000005u) & 0x49249249u;
+    return v;
+}
+static int lbvh_delta(const std::vector<uint32_t> &k, int n, int i, int j) {
+    if (j < 0 || j >= n) return -1;
+    if (k[i] == k[j]) return 32 + __builtin_clz((uint32_t)(i ^ j));
+    return __builtin_clz(k[i] ^ k[j]);
+}
+void or_lbvh(void *sp, uint32_t *morton, uint32_t *sorted, int32_t *children) {
+    Scene *s = static_cast<Scene *>(sp);
+    const int n = (int)s->triMesh.size();
+    if (n == 0) return;
+    std::vector<F3> cen(n);
+    F3 bl(std::numeric_limits<float>::infinity()), bh(-std::numeric_limits<float>::infinity());
+    for (int g = 0; g < n; g++) {
+        F3 p0, p1, p2;
+        tri_verts(*s, (uint32_t)g, p0, p1, p2);
+        F3 lo = vmin(p0, vmin(p1, p2)), hi = vmax(p0, vmax(p1, p2));
+        cen[g] = F3((lo.x + hi.x) * 0.5f, (lo.y + hi.y) * 0.5f, (lo.z + hi.z) * 0.5f);
+        bl = vmin(bl, cen[g]);
+        bh = vmax(bh, cen[g]);
+    }
+    std::vector<uint32_t> codes(n), ids(n);
+    for (int g = 0; g < n; g++) {
+        uint32_t q[3];
+        for (int a = 0; a < 3; a++) {
+            float ext = bh[a] - bl[a];
+            float x = ext > 0.0f ? (cen[g][a] - bl[a]) / ext : 0.0f;
+            q[a] = (uint32_t)std::min(std::max(x * 1024.0f, 0.0f), 1023.0f);
+        }
+        codes[g] = (expand_bits10(q[0]) << 2) | (expand_bits10(q[1]) << 1) | expand_bits10(q[2]);
+        ids[g] = (uint32_t)g;
+    }
+    std::stable_sort(ids.begin(), ids.end(), [&](uint32_t a, uint32_t b) { return codes[a] < codes[b]; });
+    std::vector<uint32_t> keys(n);
+    for (int i = 0; i < n; i++) keys[i] = codes[ids[i]];
+    if (morton) std::memcpy(morton, codes.data(), n * 4);
+    if (sorted) std::memcpy(sorted, ids.data(), n * 4);
+    if (!children) return;
+    for (int i = 0; i < n - 1; i++) {
+        int d = (lbvh_delta(keys, n, i, i + 1) - lbvh_delta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
+        int dmin = lbvh_delta(keys, n, i, i - d);
+        int lmax = 2;
+        while (lbvh_delta(keys, n, i, i + lmax * d) > dmin) lmax *= 2;
+        int l = 0;
+        for (int t = lmax / 2; t >= 1; t /= 2)
+            if (lbvh_delta(keys, n, i, i + (l + t) * d) > dmin) l += t;
+        int j = i + l * d;
+        int dnode = lbvh_delta(keys, n, i, j);
+        int sp2 = 0, t = l;
+        do {  // binary search for the split: t = ceil(l / 2), ceil(l / 4), ..., 1
+            t = (t + 1) >> 1;
+            if (lbvh_delta(keys, n, i, i + (sp2 + t) * d) > dnode) sp2 += t;
+        } while (t > 1);
+        int gamma = i + sp2 * d + std::min(d, 0);
+        int lo = std::min(i, j), hi = std::max(i, j);
+        children[2 * i] = (lo == gamma) ? ~gamma : gamma;
+        children[2 * i + 1] = (hi == gamma + 1) ? ~(gamma + 1) : gamma + 1;
+    }
+}
+
 void or_trace_closest(void *sp, const float *rays, size_t n, pt_hit *out) {
     Scene *s = static_cast<Scene *>(sp);
     for (size_t i = 0; i < n; i++) {

@@ -259,7 +259,7 @@ enum : uint { COMMITTED_NOTHING = 0, COMMITTED_TRIANGLE_HIT = 1 };
 
 // One triangle the ray crosses in [TMin, TMax] (provided by ref_entry.cpp).
 struct Candidate { float t, u, v; uint inst, prim, gid; bool opaque; };
-void collect_candidates(const RayDesc &ray, std::vector<Candidate> &out);  // sorted by (t, gid)
+void collect_candidates(const RayDesc &ray, std::vector<Candidate> &out, bool accept_first);  // sorted by (t, gid)
 
 extern int g_max_bounces;  // MAX_BOUNCES (see build_ref.py)
 extern thread_local uint3 g_dispatch_index;
@@ -285,7 +285,7 @@ struct RayQuery {
     Candidate com{};
     void TraceRayInline(const RaytracingAccelerationStructure &, uint, uint, const RayDesc &ray) {
         cands.clear();
-        collect_candidates(ray, cands);
+        collect_candidates(ray, cands, (FLAGS & RAY_FLAG_ACCEPT_FIRST_HIT_AND_END_SEARCH) != 0);
         next = 0; cur = -1; committed = false; done = false;
     }
     bool Proceed() {

@@ -113,16 +113,25 @@ static bool mt(const float3 &p0, const float3 &p1, const float3 &p2, const RayDe
     return t >= r.TMin && t <= r.TMax;
 }
 
-void collect_candidates(const RayDesc &r, std::vector<Candidate> &out) {
+// Candidates the query reports, in (t, triangle id) order: the non-opaque
+// triangles in front of the nearest opaque one, then that opaque one (which
+// commits and ends the query).  Opaque hits shrink the search interval as
+// traversal finds them; an occlusion query (accept_first) stops at the first
+// opaque hit, whose commit alone decides its result.
+void collect_candidates(const RayDesc &r, std::vector<Candidate> &out, bool accept_first) {
     if (g_host.nodes.empty()) return;
     float inv[3] = {1.0f / r.Direction.x, 1.0f / r.Direction.y, 1.0f / r.Direction.z};
     float o[3] = {r.Origin.x, r.Origin.y, r.Origin.z};
     uint stack[128];
     int sp = 0;
     stack[sp++] = 0;
+    RayDesc q = r;  // q.TMax: nearest opaque hit so far
+    bool haveOpaque = false;
+    Candidate best{};
+    auto before = [](const Candidate &a, const Candidate &b) { return a.t < b.t || (a.t == b.t && a.gid < b.gid); };
     while (sp) {
         const HostScene::Node &n = g_host.nodes[stack[--sp]];
-        float t0 = r.TMin, t1 = r.TMax;
+        float t0 = q.TMin, t1 = q.TMax;
         for (int a = 0; a < 3; a++) {
             float tn = (n.lo[a] - o[a]) * inv[a], tf = (n.hi[a] - o[a]) * inv[a];
             if (tn > tf) std::swap(tn, tf);
@@ -137,17 +146,26 @@ void collect_candidates(const RayDesc &r, std::vector<Candidate> &out) {
                 float3 p0, p1, p2;
                 tri_verts(g, p0, p1, p2);
                 float u, v, t;
-                if (mt(p0, p1, p2, r, u, v, t))
-                    out.push_back({t, u, v, g_host.triMesh[g], g_host.triPrim[g], g, (bool)g_host.opaque[g_host.triMesh[g]]});
+                if (!mt(p0, p1, p2, q, u, v, t)) continue;
+                Candidate c{t, u, v, g_host.triMesh[g], g_host.triPrim[g], g, (bool)g_host.opaque[g_host.triMesh[g]]};
+                if (c.opaque) {
+                    if (!haveOpaque || before(c, best)) { best = c; haveOpaque = true; q.TMax = t; }
+                    if (accept_first) { out.clear(); out.push_back(best); return; }
+                } else {
+                    out.push_back(c);
+                }
             }
         } else {
             stack[sp++] = n.left;
             stack[sp++] = n.right;
         }
     }
-    std::sort(out.begin(), out.end(), [](const Candidate &a, const Candidate &b) {
-        return a.t < b.t || (a.t == b.t && a.gid < b.gid);
-    });
+    if (haveOpaque) {
+        out.erase(std::remove_if(out.begin(), out.end(), [&](const Candidate &c) { return !before(c, best); }),
+                  out.end());
+        out.push_back(best);
+    }
+    std::sort(out.begin(), out.end(), before);
 }
 
 static void bind_u32(ByteAddressBuffer &b, const void *p) { b.data = static_cast<const uint *>(p); }

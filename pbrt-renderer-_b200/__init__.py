@@ -28,6 +28,7 @@ PT_RNG_SOBOL_OWEN, PT_RNG_PCG_HASH = 0, 1
 PT_ENV_CDF, PT_ENV_ALIAS = 0, 1
 PT_MEM_HOST, PT_MEM_DEVICE = 0, 1
 PT_SAMPLE_DIMS = 4
+PT_RENDER_STAGE_TIMING = 1
 
 
 class pt_material(C.Structure):
@@ -80,7 +81,8 @@ class pt_camera(C.Structure):
 class pt_render_params(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32),
                 ("sample_offset", C.c_uint32), ("max_depth", C.c_uint32), ("rng_kind", C.c_uint32),
-                ("env_sampling", C.c_uint32), ("wave_paths", C.c_uint32), ("camera", pt_camera)]
+                ("env_sampling", C.c_uint32), ("wave_paths", C.c_uint32), ("flags", C.c_uint32),
+                ("camera", pt_camera)]
 
 
 class pt_film(C.Structure):
@@ -90,8 +92,9 @@ class pt_film(C.Structure):
 
 class pt_stats(C.Structure):
     _fields_ = [("paths", C.c_uint64), ("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
-                ("waves", C.c_uint64), ("bounces", C.c_uint64), ("ms_total", C.c_float),
-                ("ms_extend", C.c_float), ("ms_shadow", C.c_float), ("ms_shade", C.c_float)]
+                ("waves", C.c_uint64), ("bounces", C.c_uint64), ("launches", C.c_uint64), ("ms_total", C.c_float),
+                ("ms_raygen", C.c_float), ("ms_extend", C.c_float), ("ms_shade", C.c_float),
+                ("ms_shadow", C.c_float), ("ms_film", C.c_float)]
 
 
 class pt_hit(C.Structure):
@@ -183,10 +186,11 @@ def make_material(type=PT_MAT_DIFFUSE, albedo=(0.5, 0.5, 0.5), **kw) -> pt_mater
 
 
 def render_params(width, height, spp, camera: pt_camera, max_depth=32, sample_offset=0,
-                  rng_kind=PT_RNG_SOBOL_OWEN, env_sampling=PT_ENV_CDF, wave_paths=0) -> pt_render_params:
+                  rng_kind=PT_RNG_SOBOL_OWEN, env_sampling=PT_ENV_CDF, wave_paths=0, flags=0) -> pt_render_params:
     p = pt_render_params()
     p.width, p.height, p.spp, p.sample_offset = width, height, spp, sample_offset
     p.max_depth, p.rng_kind, p.env_sampling, p.wave_paths = max_depth, rng_kind, env_sampling, wave_paths
+    p.flags = flags
     p.camera = camera
     return p
 
@@ -208,6 +212,7 @@ def lib():
         P, F, U, S = C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_uint32), C.c_size_t
         L.pt_create.argtypes = [C.POINTER(C.c_void_p), C.c_int]
         L.pt_destroy.argtypes = [P]
+        L.pt_set_stream.argtypes = [P, C.c_void_p]
         L.pt_last_error.argtypes = [P]
         L.pt_last_error.restype = C.c_char_p
         L.pt_upload_scene.argtypes = [P, C.POINTER(pt_scene_desc)]
@@ -242,6 +247,10 @@ class Context:
     def _check(self, rc):
         if rc != 0:
             raise PTError(f"libpt error {rc}: {self.L.pt_last_error(self.h).decode()}")
+
+    def set_stream(self, stream_ptr):
+        """Run libpt work on an existing CUDA stream (an int cudaStream_t)."""
+        self._check(self.L.pt_set_stream(self.h, C.c_void_p(stream_ptr) if stream_ptr else None))
 
     def close(self):
         if self.h:

@@ -1,0 +1,427 @@
+// pt_bvh.cu — GPU acceleration-structure build of libpt.
+//
+// Replaces the driver's BLAS/TLAS build (src/gpu/DXRApp_Scene.cpp:37-170 of
+// gracejinsotrue/PBRT-renderer-) with:
+//   1. per-triangle bounds and 30-bit Morton codes of the centroids,
+//   2. a stable radix sort of (code, triangle id) (CUB),
+//   3. the Karras 2012 binary radix tree over the sorted codes (ties broken by
+//      position, so the topology is a pure function of the input),
+//   4. bottom-up bounds with one atomic per internal node,
+//   5. a top-down collapse into 8-wide nodes: each wide node takes its binary
+//      root's two children and repeatedly opens the child with the largest
+//      surface area until it has 8; subtrees of <= 3 triangles become leaves.
+//      Child boxes are quantised to 8 bits per plane against a power-of-two
+//      grid with directed rounding, so every stored box contains its child.
+#include <cub/device/device_radix_sort.cuh>
+
+#include "pt_internal.h"
+
+namespace pt {
+
+constexpr uint32_t kLeafMax = 3;
+
+__device__ __forceinline__ uint32_t expand_bits(uint32_t v) {
+    v = (v * 0x00010001u) & 0xFF0000FFu;
+    v = (v * 0x00000101u) & 0x0F00F00Fu;
+    v = (v * 0x00000011u) & 0xC30C30C3u;
+    v = (v * 0x00000005u) & 0x49249249u;
+    return v;
+}
+
+// Triangle bounds, mesh of each triangle and centroid (exact float ops).
+__global__ void k_tri_bounds(uint32_t n, const uint32_t *__restrict__ meshFirstTri, uint32_t numMeshes,
+                             const pt_material *__restrict__ mats, const uint32_t *__restrict__ idx,
+                             const float *__restrict__ pos, uint32_t *triMesh, float4 *lo, float4 *hi,
+                             float4 *cen) {
+    uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    uint32_t a = 0, b = numMeshes;  // last mesh with meshFirstTri <= g
+    while (b - a > 1) {
+        uint32_t m = (a + b) >> 1;
+        if (meshFirstTri[m] <= g) a = m; else b = m;
+    }
+    const pt_material &m = mats[a];
+    uint32_t base = m.indexOffset + 3u * (g - meshFirstTri[a]);
+    float3 p0 = ld3(pos, m.vertexOffset + idx[base]);
+    float3 p1 = ld3(pos, m.vertexOffset + idx[base + 1]);
+    float3 p2 = ld3(pos, m.vertexOffset + idx[base + 2]);
+    float3 l = vmin(p0, vmin(p1, p2)), h = vmax(p0, vmax(p1, p2));
+    triMesh[g] = a;
+    lo[g] = make_float4(l.x, l.y, l.z, 0.0f);
+    hi[g] = make_float4(h.x, h.y, h.z, 0.0f);
+    cen[g] = make_float4(__fmul_rn(__fadd_rn(l.x, h.x), 0.5f), __fmul_rn(__fadd_rn(l.y, h.y), 0.5f),
+                         __fmul_rn(__fadd_rn(l.z, h.z), 0.5f), 0.0f);
+}
+
+__device__ __forceinline__ uint32_t f2ord(float f) {
+    uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float ord2f(uint32_t u) {
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u);
+}
+// bounds[0..2] = ordered min, bounds[3..5] = ordered max of the centroids
+__global__ void k_centroid_bounds(uint32_t n, const float4 *__restrict__ cen, uint32_t *bounds) {
+    uint32_t mn3[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, mx3[3] = {0u, 0u, 0u};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 c = cen[i];
+        float v[3] = {c.x, c.y, c.z};
+        for (int a = 0; a < 3; a++) {
+            uint32_t o = f2ord(v[a]);
+            mn3[a] = min(mn3[a], o);
+            mx3[a] = max(mx3[a], o);
+        }
+    }
+    for (int a = 0; a < 3; a++) {
+        for (int off = 16; off; off >>= 1) {
+            mn3[a] = min(mn3[a], __shfl_xor_sync(0xFFFFFFFFu, mn3[a], off));
+            mx3[a] = max(mx3[a], __shfl_xor_sync(0xFFFFFFFFu, mx3[a], off));
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicMin(&bounds[a], mn3[a]);
+            atomicMax(&bounds[3 + a], mx3[a]);
+        }
+    }
+}
+__global__ void k_morton(uint32_t n, const float4 *__restrict__ cen, const uint32_t *__restrict__ bounds,
+                         uint32_t *codes, uint32_t *ids) {
+    uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    float4 c = cen[g];
+    float v[3] = {c.x, c.y, c.z};
+    uint32_t q[3];
+    for (int a = 0; a < 3; a++) {
+        float lo = ord2f(bounds[a]), hi = ord2f(bounds[3 + a]);
+        float ext = __fsub_rn(hi, lo);
+        float x = ext > 0.0f ? __fdiv_rn(__fsub_rn(v[a], lo), ext) : 0.0f;
+        float s = fminf(fmaxf(__fmul_rn(x, 1024.0f), 0.0f), 1023.0f);
+        q[a] = (uint32_t)s;
+    }
+    codes[g] = (expand_bits(q[0]) << 2) | (expand_bits(q[1]) << 1) | expand_bits(q[2]);
+    ids[g] = g;
+}
+
+__device__ __forceinline__ int delta(const uint32_t *k, int n, int i, int j) {
+    if (j < 0 || j >= n) return -1;
+    uint32_t a = k[i], b = k[j];
+    if (a == b) return 32 + __clz((uint32_t)(i ^ j));
+    return __clz(a ^ b);
+}
+// Karras 2012, Figure 4: internal node i of the radix tree over sorted keys.
+__global__ void k_karras(int n, const uint32_t *__restrict__ keys, int32_t *children, int32_t *intParent,
+                         int32_t *leafParent, uint32_t *rangeFirst, uint32_t *rangeLast) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    int d = (delta(keys, n, i, i + 1) - delta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
+    int dmin = delta(keys, n, i, i - d);
+    int lmax = 2;
+    while (delta(keys, n, i, i + lmax * d) > dmin) lmax *= 2;
+    int l = 0;
+    for (int t = lmax / 2; t >= 1; t /= 2)
+        if (delta(keys, n, i, i + (l + t) * d) > dmin) l += t;
+    int j = i + l * d;
+    int dnode = delta(keys, n, i, j);
+    int s = 0, div = 2, t = (l + div - 1) / div;
+    for (;;) {
+        if (delta(keys, n, i, i + (s + t) * d) > dnode) s += t;
+        if (t == 1) break;
+        div *= 2;
+        t = (l + div - 1) / div;
+    }
+    int gamma = i + s * d + min(d, 0);
+    int lo = min(i, j), hi = max(i, j);
+    int left = (lo == gamma) ? ~gamma : gamma;
+    int right = (hi == gamma + 1) ? ~(gamma + 1) : gamma + 1;
+    children[2 * i] = left;
+    children[2 * i + 1] = right;
+    if (left >= 0) intParent[left] = i; else leafParent[~left] = i;
+    if (right >= 0) intParent[right] = i; else leafParent[~right] = i;
+    rangeFirst[i] = lo;
+    rangeLast[i] = hi;
+    if (i == 0) intParent[0] = -1;
+}
+__global__ void k_refit(int n, const uint32_t *__restrict__ sorted, const float4 *__restrict__ tlo,
+                        const float4 *__restrict__ thi, const int32_t *__restrict__ children,
+                        const int32_t *__restrict__ intParent, const int32_t *__restrict__ leafParent,
+                        float4 *leafLo, float4 *leafHi, float4 *intLo, float4 *intHi, uint32_t *flags) {
+    int leaf = blockIdx.x * blockDim.x + threadIdx.x;
+    if (leaf >= n) return;
+    uint32_t g = sorted[leaf];
+    leafLo[leaf] = tlo[g];
+    leafHi[leaf] = thi[g];
+    if (n == 1) return;
+    int node = leafParent[leaf];
+    for (int guard = 0; node >= 0 && guard < n; guard++) {
+        __threadfence();
+        if (atomicAdd(&flags[node], 1u) == 0u) return;  // first arrival: sibling finishes the node
+        int c0 = children[2 * node], c1 = children[2 * node + 1];
+        float4 l0 = c0 >= 0 ? __ldcg(&intLo[c0]) : __ldcg(&leafLo[~c0]);
+        float4 h0 = c0 >= 0 ? __ldcg(&intHi[c0]) : __ldcg(&leafHi[~c0]);
+        float4 l1 = c1 >= 0 ? __ldcg(&intLo[c1]) : __ldcg(&leafLo[~c1]);
+        float4 h1 = c1 >= 0 ? __ldcg(&intHi[c1]) : __ldcg(&leafHi[~c1]);
+        intLo[node] = make_float4(fminf(l0.x, l1.x), fminf(l0.y, l1.y), fminf(l0.z, l1.z), 0.0f);
+        intHi[node] = make_float4(fmaxf(h0.x, h1.x), fmaxf(h0.y, h1.y), fmaxf(h0.z, h1.z), 0.0f);
+        node = intParent[node];
+    }
+}
+
+struct CollapseIn {
+    int n;
+    const int32_t *children;
+    const uint32_t *rangeFirst, *rangeLast;
+    const float4 *leafLo, *leafHi, *intLo, *intHi;
+    const uint32_t *sorted;
+    const uint32_t *triMesh, *meshFirstTri;
+    const pt_material *mats;
+    const uint32_t *idx;
+    const float *pos;
+    BVH8Node *nodes;
+    float4 *tri;
+    uint32_t *counters;  // [0] wide nodes allocated, [1] triangles written, [2] next queue size
+};
+
+__device__ __forceinline__ float area(float4 l, float4 h) {
+    float dx = h.x - l.x, dy = h.y - l.y, dz = h.z - l.z;
+    return dx * dy + dy * dz + dz * dx;
+}
+// Exponent e (biased) with (hi - lo) / 2^(e-127) <= 255, from an upper bound.
+__device__ __forceinline__ uint32_t quant_exp(float lo, float hi) {
+    float r = __fdiv_ru(__fsub_ru(hi, lo), 255.0f);
+    uint32_t b = __float_as_uint(r);
+    uint32_t e = (b >> 23) & 0xFFu;
+    if (b & 0x7FFFFFu) e += 1;
+    return max(e, 1u);
+}
+
+// One thread per wide node of the current level.
+__global__ void k_collapse(CollapseIn C, const int2 *__restrict__ qin, uint32_t qn, int2 *qout) {
+    uint32_t qi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (qi >= qn) return;
+    int2 item = qin[qi];
+    int32_t root = item.x;  // binary node (>= 0 internal, < 0 leaf)
+    uint32_t wide = (uint32_t)item.y;
+    int32_t ch[8];
+    int cnt = 0;
+    if (root >= 0) {
+        ch[0] = C.children[2 * root];
+        ch[1] = C.children[2 * root + 1];
+        cnt = 2;
+    } else {
+        ch[0] = root;
+        cnt = 1;
+    }
+    auto openable = [&](int32_t r) { return r >= 0 && (C.rangeLast[r] - C.rangeFirst[r] + 1) > kLeafMax; };
+    while (cnt < 8) {
+        int best = -1;
+        float ba = -1.0f;
+        for (int i = 0; i < cnt; i++)
+            if (openable(ch[i])) {
+                float a = area(C.intLo[ch[i]], C.intHi[ch[i]]);
+                if (a > ba) { ba = a; best = i; }
+            }
+        if (best < 0) break;
+        int32_t r = ch[best];
+        ch[best] = C.children[2 * r];
+        ch[cnt++] = C.children[2 * r + 1];
+    }
+    float4 clo[8], chi[8];
+    float4 nlo = make_float4(3e38f, 3e38f, 3e38f, 0), nhi = make_float4(-3e38f, -3e38f, -3e38f, 0);
+    for (int i = 0; i < cnt; i++) {
+        int32_t r = ch[i];
+        clo[i] = r >= 0 ? C.intLo[r] : C.leafLo[~r];
+        chi[i] = r >= 0 ? C.intHi[r] : C.leafHi[~r];
+        nlo = make_float4(fminf(nlo.x, clo[i].x), fminf(nlo.y, clo[i].y), fminf(nlo.z, clo[i].z), 0);
+        nhi = make_float4(fmaxf(nhi.x, chi[i].x), fmaxf(nhi.y, chi[i].y), fmaxf(nhi.z, chi[i].z), 0);
+    }
+    // slot assignment by octant of the child centre
+    float cx = 0.5f * (nlo.x + nhi.x), cy = 0.5f * (nlo.y + nhi.y), cz = 0.5f * (nlo.z + nhi.z);
+    int slotOf[8];
+    uint32_t used = 0;
+    for (int i = 0; i < cnt; i++) {
+        float mx_ = 0.5f * (clo[i].x + chi[i].x), my_ = 0.5f * (clo[i].y + chi[i].y), mz_ = 0.5f * (clo[i].z + chi[i].z);
+        uint32_t o = (mx_ > cx ? 1u : 0u) | (my_ > cy ? 2u : 0u) | (mz_ > cz ? 4u : 0u);
+        int best = -1, bd = 99;
+        for (uint32_t s = 0; s < 8; s++)
+            if (!((used >> s) & 1u)) {
+                int dd = __popc(s ^ o);
+                if (dd < bd) { bd = dd; best = (int)s; }
+            }
+        slotOf[i] = best;
+        used |= 1u << best;
+    }
+    int child[8];
+    for (int s = 0; s < 8; s++) child[s] = -1;
+    for (int i = 0; i < cnt; i++) child[slotOf[i]] = i;
+    // allocation
+    uint32_t nInt = 0, nTri = 0, imask = 0;
+    for (int s = 0; s < 8; s++) {
+        if (child[s] < 0) continue;
+        int32_t r = ch[child[s]];
+        if (openable(r)) { nInt++; imask |= 1u << s; }
+        else nTri += r >= 0 ? (C.rangeLast[r] - C.rangeFirst[r] + 1) : 1u;
+    }
+    uint32_t childBase = nInt ? atomicAdd(&C.counters[0], nInt) : 0u;
+    uint32_t triBase = atomicAdd(&C.counters[1], nTri);
+    uint32_t qpos = nInt ? atomicAdd(&C.counters[2], nInt) : 0u;
+    // quantisation grid
+    uint32_t ex = quant_exp(nlo.x, nhi.x), ey = quant_exp(nlo.y, nhi.y), ez = quant_exp(nlo.z, nhi.z);
+    float ix = __uint_as_float((254u - ex) << 23), iy = __uint_as_float((254u - ey) << 23),
+          iz = __uint_as_float((254u - ez) << 23);  // 2^(127 - e)
+    uint8_t meta[8], qlx[8], qly[8], qlz[8], qhx[8], qhy[8], qhz[8];
+    uint32_t rank = 0, toff = 0;
+    for (int s = 0; s < 8; s++) {
+        meta[s] = 0;
+        qlx[s] = qly[s] = qlz[s] = 255;
+        qhx[s] = qhy[s] = qhz[s] = 0;
+        if (child[s] < 0) continue;
+        int i = child[s];
+        int32_t r = ch[i];
+        qlx[s] = (uint8_t)min(255.0f, fmaxf(0.0f, floorf(__fmul_rd(__fsub_rd(clo[i].x, nlo.x), ix))));
+        qly[s] = (uint8_t)min(255.0f, fmaxf(0.0f, floorf(__fmul_rd(__fsub_rd(clo[i].y, nlo.y), iy))));
+        qlz[s] = (uint8_t)min(255.0f, fmaxf(0.0f, floorf(__fmul_rd(__fsub_rd(clo[i].z, nlo.z), iz))));
+        qhx[s] = (uint8_t)min(255.0f, fmaxf(0.0f, ceilf(__fmul_ru(__fsub_ru(chi[i].x, nlo.x), ix))));
+        qhy[s] = (uint8_t)min(255.0f, fmaxf(0.0f, ceilf(__fmul_ru(__fsub_ru(chi[i].y, nlo.y), iy))));
+        qhz[s] = (uint8_t)min(255.0f, fmaxf(0.0f, ceilf(__fmul_ru(__fsub_ru(chi[i].z, nlo.z), iz))));
+        if ((imask >> s) & 1u) {
+            meta[s] = (uint8_t)(0x20u | s);
+            qout[qpos + rank] = make_int2(r, (int)(childBase + rank));
+            rank++;
+        } else {
+            uint32_t first = r >= 0 ? C.rangeFirst[r] : (uint32_t)(~r);
+            uint32_t count = r >= 0 ? (C.rangeLast[r] - first + 1) : 1u;
+            meta[s] = (uint8_t)((count << 5) | toff);
+            for (uint32_t k = 0; k < count; k++) {
+                uint32_t g = C.sorted[first + k];
+                uint32_t mesh = C.triMesh[g];
+                const pt_material &m = C.mats[mesh];
+                uint32_t base = m.indexOffset + 3u * (g - C.meshFirstTri[mesh]);
+                float3 p0 = ld3(C.pos, m.vertexOffset + C.idx[base]);
+                float3 p1 = ld3(C.pos, m.vertexOffset + C.idx[base + 1]);
+                float3 p2 = ld3(C.pos, m.vertexOffset + C.idx[base + 2]);
+                float3 e1 = p1 - p0, e2 = p2 - p0;
+                float4 *t = C.tri + 3u * (triBase + toff + k);
+                t[0] = make_float4(p0.x, p0.y, p0.z, __uint_as_float(g));
+                t[1] = make_float4(e1.x, e1.y, e1.z, 0.0f);
+                t[2] = make_float4(e2.x, e2.y, e2.z, 0.0f);
+            }
+            toff += count;
+        }
+    }
+    auto pack4 = [](const uint8_t *b) {
+        return (uint32_t)b[0] | ((uint32_t)b[1] << 8) | ((uint32_t)b[2] << 16) | ((uint32_t)b[3] << 24);
+    };
+    BVH8Node nd;
+    nd.n[0] = make_uint4(__float_as_uint(nlo.x), __float_as_uint(nlo.y), __float_as_uint(nlo.z),
+                         ex | (ey << 8) | (ez << 16) | (imask << 24));
+    nd.n[1] = make_uint4(childBase, triBase, pack4(meta), pack4(meta + 4));
+    nd.n[2] = make_uint4(pack4(qlx), pack4(qlx + 4), pack4(qly), pack4(qly + 4));
+    nd.n[3] = make_uint4(pack4(qlz), pack4(qlz + 4), pack4(qhx), pack4(qhx + 4));
+    nd.n[4] = make_uint4(pack4(qhy), pack4(qhy + 4), pack4(qhz), pack4(qhz + 4));
+    C.nodes[wide] = nd;
+}
+
+}  // namespace pt
+
+using namespace pt;
+
+// Exact floating-point bounds are needed by the element subtraction in
+// k_collapse's e1/e2: they use the same IEEE subtraction as the oracle.
+int pt_build_bvh_device(pt_ctx *ctx, const uint32_t *d_meshFirstTri, uint32_t n) {
+    cudaStream_t st = ctx->stream;
+    DevScene &S = ctx->S;
+    ctx->numTris = n;
+    ctx->numWide = 0;
+    S.numTris = n;
+    S.numNodes = 0;
+    if (n == 0) return PT_OK;
+    uint32_t *triMesh, *codes, *ids, *codesS, *idsS, *bounds, *flags, *counters, *rf, *rl;
+    float4 *tlo, *thi, *cen, *leafLo, *leafHi, *intLo, *intHi;
+    int32_t *children, *intParent, *leafParent;
+    PT_CUDA(ctx->alloc_scene(&triMesh, n));
+    PT_CUDA(ctx->alloc_scene(&codes, n));
+    PT_CUDA(ctx->alloc_scene(&codesS, n));
+    PT_CUDA(ctx->alloc_scene(&idsS, n));
+    PT_CUDA(ctx->alloc_scene(&children, 2 * (size_t)max(n - 1, 1u)));
+    // temporaries
+    std::vector<void *> tmp;
+    auto talloc = [&](void **p, size_t bytes) {
+        cudaError_t e = cudaMalloc(p, bytes + 16);
+        if (e == cudaSuccess) tmp.push_back(*p);
+        return e;
+    };
+    auto cleanup = [&]() { for (void *p : tmp) cudaFree(p); };
+#define TA(p, bytes)                                                                   \
+    do {                                                                               \
+        cudaError_t e_ = talloc((void **)&(p), (bytes));                               \
+        if (e_ != cudaSuccess) { cleanup(); return ctx->fail(PT_E_NOMEM, "bvh temp", cudaGetErrorString(e_)); } \
+    } while (0)
+    TA(ids, n * 4);
+    TA(tlo, n * 16); TA(thi, n * 16); TA(cen, n * 16);
+    TA(bounds, 6 * 4);
+    TA(intParent, (size_t)max(n - 1, 1u) * 4); TA(leafParent, (size_t)n * 4);
+    TA(rf, (size_t)max(n - 1, 1u) * 4); TA(rl, (size_t)max(n - 1, 1u) * 4);
+    TA(leafLo, n * 16); TA(leafHi, n * 16);
+    TA(intLo, (size_t)max(n - 1, 1u) * 16); TA(intHi, (size_t)max(n - 1, 1u) * 16);
+    TA(flags, (size_t)max(n - 1, 1u) * 4);
+    TA(counters, 4 * 4);
+    int2 *qa, *qb;
+    TA(qa, (size_t)n * 8); TA(qb, (size_t)n * 8);
+    const int B = 256;
+    uint32_t G = (n + B - 1) / B;
+    k_tri_bounds<<<G, B, 0, st>>>(n, d_meshFirstTri, S.numMeshes, S.mats, S.idx, S.pos, triMesh, tlo, thi, cen);
+    uint32_t binit[6] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u, 0u};
+    cudaMemcpyAsync(bounds, binit, sizeof(binit), cudaMemcpyHostToDevice, st);
+    k_centroid_bounds<<<min(G, 1024u), B, 0, st>>>(n, cen, bounds);
+    k_morton<<<G, B, 0, st>>>(n, cen, bounds, codes, ids);
+    size_t tb = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tb, codes, codesS, ids, idsS, (int)n, 0, 30, st);
+    void *dtmp;
+    TA(dtmp, tb);
+    cub::DeviceRadixSort::SortPairs(dtmp, tb, codes, codesS, ids, idsS, (int)n, 0, 30, st);
+    if (n > 1) {
+        k_karras<<<(n - 1 + B - 1) / B, B, 0, st>>>((int)n, codesS, children, intParent, leafParent, rf, rl);
+        cudaMemsetAsync(flags, 0, (size_t)(n - 1) * 4, st);
+    }
+    k_refit<<<G, B, 0, st>>>((int)n, idsS, tlo, thi, children, intParent, leafParent, leafLo, leafHi, intLo, intHi,
+                             flags);
+    // collapse: wide nodes <= max(1, n - 1); triangles exactly n
+    BVH8Node *nodes;
+    float4 *tri;
+    uint32_t maxWide = max(1u, n - 1);
+    cudaError_t e1 = ctx->alloc_scene(&nodes, maxWide);
+    cudaError_t e2 = ctx->alloc_scene(&tri, 3 * (size_t)n);
+    if (e1 != cudaSuccess || e2 != cudaSuccess) { cleanup(); return ctx->fail(PT_E_NOMEM, "bvh nodes"); }
+    CollapseIn C{(int)n, children, rf, rl, leafLo, leafHi, intLo, intHi, idsS, triMesh, d_meshFirstTri,
+                 S.mats, S.idx, S.pos, nodes, tri, counters};
+    int2 root = make_int2(n > 1 ? 0 : ~0, 0);
+    cudaMemcpyAsync(qa, &root, sizeof(root), cudaMemcpyHostToDevice, st);
+    uint32_t cinit[4] = {1u, 0u, 0u, 0u};
+    cudaMemcpyAsync(counters, cinit, sizeof(cinit), cudaMemcpyHostToDevice, st);
+    uint32_t qn = 1;
+    int levels = 0;
+    while (qn > 0) {
+        cudaMemsetAsync(counters + 2, 0, 4, st);
+        k_collapse<<<(qn + 127) / 128, 128, 0, st>>>(C, qa, qn, qb);
+        PT_CUDA(cudaMemcpyAsync(&qn, counters + 2, 4, cudaMemcpyDeviceToHost, st));
+        PT_CUDA(cudaStreamSynchronize(st));
+        std::swap(qa, qb);
+        if (++levels > 64) { cleanup(); return ctx->fail(PT_E_DEVICE, "bvh collapse did not terminate"); }
+    }
+    uint32_t cnt[4];
+    PT_CUDA(cudaMemcpyAsync(cnt, counters, sizeof(cnt), cudaMemcpyDeviceToHost, st));
+    cudaError_t se = cudaStreamSynchronize(st);
+    cleanup();
+    if (se != cudaSuccess) return ctx->fail(PT_E_CUDA, "bvh build", cudaGetErrorString(se));
+    if (cnt[1] != n) return ctx->fail(PT_E_DEVICE, "bvh collapse lost triangles");
+    S.tri = tri;
+    S.nodes = nodes;
+    S.numNodes = cnt[0];
+    S.triMesh = triMesh;
+    ctx->numWide = cnt[0];
+    ctx->d_morton = codes;
+    ctx->d_sorted = idsS;
+    ctx->d_binChildren = children;
+    (void)codesS;
+    return PT_OK;
+#undef TA
+}

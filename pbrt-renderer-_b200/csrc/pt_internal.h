@@ -1,0 +1,92 @@
+// pt_internal.h — context and shared declarations of libpt.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "pt_device.cuh"
+
+#define PT_CUDA(call)                                                                  \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess) return ctx->fail(PT_E_CUDA, #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+// Device error flag bits (raised by kernels, read after a sync).
+enum : uint32_t {
+    PT_DEVERR_STACK = 1u,     // traversal stack overflow
+    PT_DEVERR_QUEUE = 2u,     // queue overflow
+    PT_DEVERR_BVH = 4u,       // traversal visited more nodes than exist
+};
+
+// Per-wave buffers of the wavefront integrator (structure of arrays).
+struct WaveBuffers {
+    size_t cap = 0;
+    // path state, indexed by path slot
+    float4 *thr_pdf = nullptr;  // throughput.xyz, last BSDF pdf
+    float4 *lo_eta = nullptr;   // Lo.xyz, eta
+    float4 *pendA = nullptr;    // pending area-light NEE contribution
+    float4 *pendE = nullptr;    // pending envmap NEE contribution
+    uint4 *rng = nullptr;       // dim, white-noise state, bounce, flags
+    // ray queues (double buffered), indexed by queue position
+    uint32_t *qslot[2] = {nullptr, nullptr};
+    float4 *qo[2] = {nullptr, nullptr};  // origin, tmin
+    float4 *qd[2] = {nullptr, nullptr};  // direction, tmax
+    float4 *qhit = nullptr;              // t, gid bits, u, v
+    // shadow queue (two per path per bounce at most)
+    uint32_t *sslot = nullptr;           // slot | kind << 31
+    float4 *so = nullptr, *sd = nullptr, *sX = nullptr, *sthr = nullptr;
+    // counters: [0] ray count q0, [1] ray count q1, [2] shadow count,
+    // [3..4] total extension / shadow rays (uint64 as two words each), [8] error flags
+    uint32_t *counters = nullptr;
+};
+
+struct pt_ctx {
+    int device = 0;
+    int numSMs = 148;
+    cudaStream_t stream = nullptr;     // stream all work is issued on
+    cudaStream_t ownStream = nullptr;  // created by pt_create, destroyed by pt_destroy
+    std::string err;
+    std::vector<void *> sceneAllocs;  // freed on re-upload / destroy
+    pt::DevScene S{};
+    bool hasScene = false;
+    uint32_t numTris = 0;
+    uint32_t numWide = 0;
+    uint32_t *d_morton = nullptr, *d_sorted = nullptr;
+    int32_t *d_binChildren = nullptr;
+    uint32_t *d_sobol1 = nullptr;
+    uint32_t *d_err = nullptr;
+    WaveBuffers W;
+    // scratch of the batch entry points
+    void *scratch = nullptr;
+    size_t scratchBytes = 0;
+
+    int fail(int code, const char *what, const char *detail = nullptr) {
+        err = what;
+        if (detail) { err += ": "; err += detail; }
+        return code;
+    }
+    template <class T>
+    cudaError_t alloc_scene(T **p, size_t count) {
+        cudaError_t e = cudaMalloc((void **)p, count * sizeof(T) + 16);
+        if (e == cudaSuccess) sceneAllocs.push_back((void *)*p);
+        return e;
+    }
+    void free_scene() {
+        for (void *p : sceneAllocs) cudaFree(p);
+        sceneAllocs.clear();
+        hasScene = false;
+        S = pt::DevScene{};
+        d_morton = d_sorted = nullptr;
+        d_binChildren = nullptr;
+    }
+};
+
+// pt_bvh.cu: builds S.tri / S.nodes / S.triMesh / S.meshFirstTri and the
+// parity exports on the device from the uploaded geometry.
+int pt_build_bvh_device(pt_ctx *ctx, const uint32_t *d_meshFirstTri, uint32_t numTris);
+// pt_render.cu
+int pt_render_impl(pt_ctx *ctx, const pt_render_params *p, float *d_sum, float *d_comp, pt_stats *stats);
+int pt_wave_free(pt_ctx *ctx);

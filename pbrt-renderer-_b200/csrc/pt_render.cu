@@ -1,0 +1,690 @@
+// pt_render.cu — the wavefront integrator of libpt (sm_100a).
+//
+// Restates RayGen (gracejinsotrue/PBRT-renderer-, shaders/Shaders.hlsl:25-651)
+// as a sequence of kernels over waves of paths:
+//
+//   raygen -> [ extend -> shade -> shadow ] x max_depth -> film
+//
+// * extend: closest-hit BVH8 traversal of the ray queue -> hit records.
+// * shade: one thread per queued path: folds the previous bounce's NEE
+//   results into Lo, handles miss / emitter / surface events, samples NEE
+//   (shadow rays to the shadow queue) and the BSDF (next ray queue), Russian
+//   roulette.  Path slots stay fixed; queues hold slot ids and are compacted
+//   with one atomic per warp (ballot + popc).
+// * shadow: any-hit traversal; writes thr * (X * transmission) or thr * 0
+//   into the path's pending slot, folded in by the next shade (or by film),
+//   so Lo receives the same float additions in the same order as RayGen.
+// * film: per pixel, the wave's samples in sample order, Kahan-compensated
+//   float32 accumulation of (L, 1).
+//
+// The sampler is counter-based (pixel, sample, dimension), so each path draws
+// the same dimensions as RayGen.  In scenes with participating media the
+// reference traces NEE shadow rays before deciding whether to draw ratio
+// tracking samples (Emitter.hlsli:138-148); there shade traces its shadow
+// rays inline to keep that order.
+#include "pt_internal.h"
+
+namespace pt {
+
+constexpr uint32_t kFlagPending = 1u;
+constexpr int kBlock = 256;
+
+struct WaveArgs {
+    DevScene S;
+    uint32_t width, height, npix;
+    uint32_t sampleOffset;   // sample index of path id 0 of this render call
+    uint32_t rngKind, envMode, maxDepth;
+    uint64_t waveStart;      // first path id of the wave
+    uint32_t waveCount;
+    pt_camera cam;
+    // buffers
+    float4 *thr_pdf, *lo_eta, *pendA, *pendE;
+    uint4 *rng;
+    uint32_t *qslotIn, *qslotOut;
+    float4 *qoIn, *qdIn, *qoOut, *qdOut, *qhit;
+    uint32_t *sslot;
+    float4 *so, *sd, *sX, *sthr;
+    uint32_t *cntIn, *cntOut, *cntShadow;
+    unsigned long long *rayTotals;  // [0] extension, [1] shadow
+    uint32_t *err;
+    uint32_t shadowCap;
+};
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// Warp-aggregated append: returns this lane's slot in the queue.
+__device__ __forceinline__ uint32_t warp_append(uint32_t *counter, bool pred) {
+    uint32_t active = __activemask();
+    uint32_t mask = __ballot_sync(active, pred);
+    if (!pred) return 0xFFFFFFFFu;
+    uint32_t leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if (lane_id() == leader) base = atomicAdd(counter, __popc(mask));
+    base = __shfl_sync(mask, base, leader);
+    return base + __popc(mask & ((1u << lane_id()) - 1u));
+}
+
+__device__ __forceinline__ void path_coords(const WaveArgs &A, uint32_t slot, uint32_t &pix, uint32_t &frame) {
+    uint64_t pid = A.waveStart + slot;
+    pix = (uint32_t)(pid % A.npix);
+    frame = A.sampleOffset + (uint32_t)(pid / A.npix);
+}
+__device__ __forceinline__ Rng load_rng(const WaveArgs &A, uint32_t slot, uint4 st) {
+    uint32_t pix, frame;
+    path_coords(A, slot, pix, frame);
+    Rng r;
+    r.pixelSeed = pcg_hash(pix ^ 0x9e3779b9u);
+    r.sampleIndex = frame;
+    r.dim = st.x;
+    r.white = st.y;
+    r.kind = A.rngKind;
+    return r;
+}
+
+// ---- raygen: camera rays (Shaders.hlsl:55-92) ------------------------------
+__global__ void k_raygen(WaveArgs A) {
+    uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= A.waveCount) return;
+    uint32_t pix, frame;
+    path_coords(A, slot, pix, frame);
+    uint32_t px = pix % A.width, py = pix / A.width;
+    Rng r = rng_init(pix, A.npix, frame, A.rngKind);
+    float jx = next_float(r, A.S.sobol1), jy = next_float(r, A.S.sobol1);
+    float ux = ((float)px + jx) / (float)A.width;
+    float uy = 1.0f - ((float)py + jy) / (float)A.height;
+    const pt_camera &c = A.cam;
+    float3 cpos = make_float3(c.pos[0], c.pos[1], c.pos[2]);
+    float3 llc = make_float3(c.llc[0], c.llc[1], c.llc[2]);
+    float3 hor = make_float3(c.horizontal[0], c.horizontal[1], c.horizontal[2]);
+    float3 ver = make_float3(c.vertical[0], c.vertical[1], c.vertical[2]);
+    float3 dir = normalize(llc + ux * hor + uy * ver - cpos);
+    float3 ro = cpos, rd = dir;
+    if (c.lens_radius > 0.0f) {
+        float3 fwd = normalize(llc + 0.5f * hor + 0.5f * ver - cpos);
+        float3 right = normalize(hor), up = normalize(ver);
+        float ft = c.focal_distance / dot(dir, fwd);
+        float3 fp = cpos + dir * ft;
+        float u1 = next_float(r, A.S.sobol1), u2 = next_float(r, A.S.sobol1);
+        float rr = sqrtf(u1) * c.lens_radius;
+        float th = 2.0f * kPi * u2;
+        ro = cpos + (rr * cosf(th)) * right + (rr * sinf(th)) * up;
+        rd = normalize(fp - ro);
+    }
+    A.qslotOut[slot] = slot;
+    A.qoOut[slot] = make_float4(ro.x, ro.y, ro.z, 0.001f);
+    A.qdOut[slot] = make_float4(rd.x, rd.y, rd.z, 1e20f);
+    A.thr_pdf[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+    A.lo_eta[slot] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+    A.rng[slot] = make_uint4(r.dim, r.white, 0u, 0u);
+    if (slot == 0) *A.cntOut = A.waveCount;
+}
+
+// ---- extend: closest hit -----------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_extend(WaveArgs A) {
+    uint32_t n = *(volatile uint32_t *)A.cntIn;
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&A.rayTotals[0], (unsigned long long)n);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 o = A.qoIn[i], d = A.qdIn[i];
+        Hit h = trace_closest(A.S, make_float3(o.x, o.y, o.z), make_float3(d.x, d.y, d.z), o.w, d.w, A.err);
+        A.qhit[i] = make_float4(h.t, __uint_as_float(h.gid), h.u, h.v);
+    }
+}
+
+// ---- shadow: any hit -> pending NEE contribution ---------------------------
+__global__ void __launch_bounds__(kBlock) k_shadow(WaveArgs A) {
+    uint32_t n = *(volatile uint32_t *)A.cntShadow;
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&A.rayTotals[1], (unsigned long long)n);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float4 o = A.so[i], d = A.sd[i], X = A.sX[i], T = A.sthr[i];
+        uint32_t s = A.sslot[i];
+        float3 tr;
+        bool occ = trace_shadow(A.S, make_float3(o.x, o.y, o.z), make_float3(d.x, d.y, d.z), o.w, d.w, tr, A.err);
+        float3 thr = make_float3(T.x, T.y, T.z);
+        float3 R = occ ? thr * v3(0.0f) : thr * (make_float3(X.x, X.y, X.z) * tr);
+        float4 out = make_float4(R.x, R.y, R.z, 0.0f);
+        if (s >> 31) A.pendE[s & 0x7FFFFFFFu] = out;
+        else A.pendA[s] = out;
+    }
+}
+
+// One NEE estimate, deferred: either a shadow ray carrying X (everything but
+// visibility/transmission) or, when the estimate is zero before any trace,
+// the final thr * 0 written straight to the pending slot.
+struct NeeOut {
+    bool ray;
+    float3 o, d, X;
+    float tmin, tmax;
+};
+
+// MISDirectIllumination (Emitter.hlsli:105-153) up to the shadow trace.
+template <bool INLINE>
+__device__ __forceinline__ float3 nee_area(const WaveArgs &A, float3 hp, float3 N, float3 Ng, float3 T, float3 B,
+                                           float3 wil, const pt_material &m, float h, Rng &rng, NeeOut &out) {
+    const DevScene &S = A.S;
+    out.ray = false;
+    EmitterSample es = sample_emitter(S, rng);
+    if (!es.valid) return v3(0.0f);
+    float3 tl = es.pos - hp;
+    float dist = len(tl);
+    float3 ww = tl / v3(dist);
+    float ct = dot(N, ww), cl = dot(es.nrm, -ww);
+    bool hair = m.type == PT_MAT_HAIR;
+    if ((!hair && ct <= 0.0f) || cl <= 0.0f) return v3(0.0f);
+    float act = hair ? fabsf(ct) : ct;
+    float3 sng = hair ? (dot(ww, Ng) >= 0.0f ? Ng : -Ng) : Ng;
+    float3 so = offset_origin(hp, sng, sng);
+    float3 trans = v3(1.0f);
+    if (INLINE) {
+        if (trace_shadow(S, so, ww, 0.0f, dist - 0.001f, trans, A.err)) return v3(0.0f);
+    }
+    float3 f;
+    float pb;
+    material_eval_pdf(wil, to_local(ww, T, B, N), m, h, f, pb);
+    float pe = es.pdfArea * dist * dist / cl;
+    float w = balance(pe, pb);
+    float3 vt = INLINE ? multi_volume_tr(S, so, ww, dist, rng) : v3(1.0f);
+    float3 X = es.rad * f * act / v3(mx(pe, 1e-20f)) * w * vt;
+    if (INLINE) return X * trans;
+    out.ray = true;
+    out.o = so; out.d = ww; out.tmin = 0.0f; out.tmax = dist - 0.001f; out.X = X;
+    return v3(0.0f);
+}
+// EnvmapDirectIllumination (Emitter.hlsli:275-326) up to the shadow trace.
+template <bool INLINE>
+__device__ __forceinline__ float3 nee_env(const WaveArgs &A, float3 hp, float3 N, float3 Ng, float3 T, float3 B,
+                                          float3 wil, const pt_material &m, float h, Rng &rng, NeeOut &out) {
+    const DevScene &S = A.S;
+    out.ray = false;
+    float u1 = next_float(rng, S.sobol1), u2 = next_float(rng, S.sobol1);
+    float3 ww, Le;
+    float pe;
+    env_sample(S, A.envMode, u1, u2, ww, Le, pe);
+    if (pe <= 0.0f) return v3(0.0f);
+    float ct = dot(N, ww);
+    bool hair = m.type == PT_MAT_HAIR;
+    if (!hair && ct <= 0.0f) return v3(0.0f);
+    float act = hair ? fabsf(ct) : ct;
+    float3 sng = hair ? (dot(ww, Ng) >= 0.0f ? Ng : -Ng) : Ng;
+    float3 so = offset_origin(hp, sng, sng);
+    float3 trans = v3(1.0f);
+    if (INLINE) {
+        if (trace_shadow(S, so, ww, 0.0f, 1e20f, trans, A.err)) return v3(0.0f);
+    }
+    float3 f;
+    float pb;
+    material_eval_pdf(wil, to_local(ww, T, B, N), m, h, f, pb);
+    float w = balance(pe, pb);
+    float3 vt = INLINE ? multi_volume_tr(S, so, ww, 1e20f, rng) : v3(1.0f);
+    float3 X = Le * f * act / v3(mx(pe, 1e-20f)) * w * vt;
+    if (INLINE) return X * trans;
+    out.ray = true;
+    out.o = so; out.d = ww; out.tmin = 0.0f; out.tmax = 1e20f; out.X = X;
+    return v3(0.0f);
+}
+// Volume NEE (Emitter.hlsli:334-434), always traced inline.
+__device__ bool vol_nee_skip(const pt_volume &v, float3 p) {
+    float3 st = vsigma_t(v);
+    float smin = mn(st.x, mn(st.y, st.z));
+    float3 dmn = p - make_float3(v.vmin[0], v.vmin[1], v.vmin[2]);
+    float3 dmx = make_float3(v.vmax[0], v.vmax[1], v.vmax[2]) - p;
+    float md = mn(mn(dmn.x, dmn.y), mn(dmn.z, mn(dmx.x, mn(dmx.y, dmx.z))));
+    return md * smin > 8.0f;
+}
+__device__ float3 vol_nee_area(const WaveArgs &A, float3 sp, float3 wo, uint32_t vi, Rng &rng) {
+    const DevScene &S = A.S;
+    const pt_volume &v = S.vols[vi];
+    if (vol_nee_skip(v, sp)) return v3(0.0f);
+    EmitterSample es = sample_emitter(S, rng);
+    if (!es.valid) return v3(0.0f);
+    float3 tl = es.pos - sp;
+    float dist = len(tl);
+    float3 wi = tl / v3(dist);
+    float cl = dot(es.nrm, -wi);
+    if (cl <= 0.0f) return v3(0.0f);
+    float3 trans;
+    if (trace_shadow(S, sp, wi, 0.001f, dist - 0.001f, trans, A.err)) return v3(0.0f);
+    float fp = hg(dot(wo, wi), v.phase_g);
+    float pe = es.pdfArea * dist * dist / cl;
+    float w = balance(pe, fp);
+    float3 vt = multi_volume_tr(S, sp, wi, dist, rng);
+    return es.rad * fp / v3(mx(pe, 1e-20f)) * w * vt * trans;
+}
+__device__ float3 vol_nee_env(const WaveArgs &A, float3 sp, float3 wo, uint32_t vi, Rng &rng) {
+    const DevScene &S = A.S;
+    const pt_volume &v = S.vols[vi];
+    if (vol_nee_skip(v, sp)) return v3(0.0f);
+    float u1 = next_float(rng, S.sobol1), u2 = next_float(rng, S.sobol1);
+    float3 wi, Le;
+    float pe;
+    env_sample(S, A.envMode, u1, u2, wi, Le, pe);
+    if (pe <= 0.0f) return v3(0.0f);
+    float3 trans;
+    if (trace_shadow(S, sp, wi, 0.001f, 1e20f, trans, A.err)) return v3(0.0f);
+    float fp = hg(dot(wo, wi), v.phase_g);
+    float w = balance(pe, fp);
+    float3 vt = multi_volume_tr(S, sp, wi, 1e20f, rng);
+    return Le * fp / v3(mx(pe, 1e-20f)) * w * vt * trans;
+}
+
+__device__ __forceinline__ void push_shadow(const WaveArgs &A, bool pred, uint32_t slot, uint32_t kind,
+                                            const NeeOut &o, float3 thr) {
+    uint32_t pos = warp_append(A.cntShadow, pred);
+    if (!pred) return;
+    if (pos >= A.shadowCap) { atomicOr(A.err, (uint32_t)PT_DEVERR_QUEUE); return; }
+    A.sslot[pos] = slot | (kind << 31);
+    A.so[pos] = make_float4(o.o.x, o.o.y, o.o.z, o.tmin);
+    A.sd[pos] = make_float4(o.d.x, o.d.y, o.d.z, o.tmax);
+    A.sX[pos] = make_float4(o.X.x, o.X.y, o.X.z, 0.0f);
+    A.sthr[pos] = make_float4(thr.x, thr.y, thr.z, 0.0f);
+}
+
+// ---- shade: one bounce of RayGen's loop body (Shaders.hlsl:108-627) --------
+template <bool INLINE>
+__global__ void __launch_bounds__(kBlock) k_shade(WaveArgs A) {
+    const DevScene &S = A.S;
+    uint32_t n = *(volatile uint32_t *)A.cntIn;
+    uint32_t iters = (n + gridDim.x * blockDim.x - 1) / (gridDim.x * blockDim.x);
+    for (uint32_t it = 0; it < iters; it++) {
+        uint32_t i = (it * gridDim.x + blockIdx.x) * blockDim.x + threadIdx.x;
+        bool active = i < n;
+        bool cont = false;
+        uint32_t slot = 0;
+        float3 thr = v3(1.0f), Lo = v3(0.0f);
+        float lastPdf = 0.0f, eta = 1.0f;
+        uint4 st = make_uint4(0, 0, 0, 0);
+        float3 no = v3(0.0f), nd = v3(0.0f);
+        float ntmin = 0.0f;
+        NeeOut neeA, neeE;
+        neeA.ray = neeE.ray = false;
+        float3 thrNee = v3(0.0f);
+        Rng rng;
+        if (active) {
+            slot = A.qslotIn[i];
+            float4 tp = A.thr_pdf[slot], le = A.lo_eta[slot];
+            st = A.rng[slot];
+            thr = make_float3(tp.x, tp.y, tp.z);
+            lastPdf = tp.w;
+            Lo = make_float3(le.x, le.y, le.z);
+            eta = le.w;
+            if (st.w & kFlagPending) {  // NEE of the previous bounce, in RayGen's order
+                float4 pa = A.pendA[slot], pe = A.pendE[slot];
+                Lo += make_float3(pa.x, pa.y, pa.z);
+                Lo += make_float3(pe.x, pe.y, pe.z);
+                st.w &= ~kFlagPending;
+            }
+            rng = load_rng(A, slot, st);
+            float4 o4 = A.qoIn[i], d4 = A.qdIn[i], h4 = A.qhit[i];
+            float3 ro = make_float3(o4.x, o4.y, o4.z), rd = make_float3(d4.x, d4.y, d4.z);
+            uint32_t gid = __float_as_uint(h4.y);
+            bool hit = gid != 0xFFFFFFFFu;
+            bool volScat = false;
+            if (INLINE && S.numVols > 0) {  // Shaders.hlsl:133-179
+                float tSurf = hit ? h4.x : 1e20f;
+                float tsc;
+                uint32_t svi;
+                float3 vw = v3(1.0f);
+                bool sc = sample_free_flight(S, ro, rd, tSurf, rng, vw, tsc, svi);
+                thr *= vw;
+                if (sc) {
+                    volScat = true;
+                    const pt_volume &v = S.vols[svi];
+                    float3 spos = xpos(ro, rd, tsc);
+                    thr *= make_float3(v.sigma_s[0], v.sigma_s[1], v.sigma_s[2]) / vmax(vsigma_t(v), v3(1e-20f));
+                    Lo += thr * vol_nee_area(A, spos, rd, svi, rng);
+                    Lo += thr * vol_nee_env(A, spos, rd, svi, rng);
+                    float x1 = next_float(rng, S.sobol1), x2 = next_float(rng, S.sobol1);
+                    float pp;
+                    nd = sample_hg(rd, v.phase_g, x1, x2, pp);
+                    no = spos;
+                    ntmin = 0.0f;
+                    lastPdf = mx(pp, 1e-20f);
+                    cont = true;
+                }
+            }
+            if (volScat) {
+            } else if (!hit) {  // Shaders.hlsl:188-212
+                float3 env = eval_env(S, rd);
+                if (lastPdf == 0.0f) Lo += thr * env;
+                else Lo += thr * env * balance(lastPdf, env_pdf(S, A.envMode, rd));
+            } else {
+                uint32_t mesh = __ldg(S.triMesh + gid);
+                uint32_t prim = gid - __ldg(S.meshFirstTri + mesh);
+                const pt_material m = S.mats[mesh];
+                uint32_t i0, i1, i2;
+                tri_vidx(S, mesh, prim, i0, i1, i2);
+                float bx = h4.z, by = h4.w, w0 = 1.0f - bx - by;
+                float3 hp = ro + rd * h4.x;
+                float3 p0 = ld3(S.pos, i0), p1 = ld3(S.pos, i1), p2 = ld3(S.pos, i2);
+                float3 Ng = normalize(normalize(cross(p1 - p0, p2 - p0)));
+                float3 nn = ld3(S.nrm, i0) * w0 + ld3(S.nrm, i1) * bx + ld3(S.nrm, i2) * by;
+                float l2 = dot(nn, nn);
+                float3 N = normalize(l2 < 1e-8f ? normalize(cross(p1 - p0, p2 - p0)) : nn * (1.0f / sqrtf(l2)));
+                bool back = dot(Ng, rd) > 0.0f;
+                if (back) Ng = -Ng;
+                if (dot(N, Ng) < 0.0f) N = -N;
+                if (m.isEmitter) {  // Shaders.hlsl:317-335
+                    float3 rad = make_float3(m.radiance[0], m.radiance[1], m.radiance[2]);
+                    if (lastPdf == 0.0f) Lo += thr * rad;
+                    else Lo += thr * rad * balance(lastPdf, emitter_pdf_sa(S, m, hp, ro, N));
+                } else {
+                    float3 T, B;
+                    float h = 0.0f;
+                    if (m.type == PT_MAT_HAIR) {  // Shaders.hlsl:340-387
+                        float hu = __ldg(S.uv + 2 * i0) * w0 + __ldg(S.uv + 2 * i1) * bx + __ldg(S.uv + 2 * i2) * by;
+                        float hv = __ldg(S.uv + 2 * i0 + 1) * w0 + __ldg(S.uv + 2 * i1 + 1) * bx +
+                                   __ldg(S.uv + 2 * i2 + 1) * by;
+                        float3 ht = ld3(S.tan, i0) * w0 + ld3(S.tan, i1) * bx + ld3(S.tan, i2) * by;
+                        float tl2 = dot(ht, ht);
+                        ht = tl2 > 1e-8f ? ht * (1.0f / sqrtf(tl2)) : v3(0.0f);
+                        if (dot(ht, ht) > 1e-8f) {
+                            ht = normalize(ht);
+                            h = hv * 2.0f - 1.0f;
+                        } else {
+                            float a0u = __ldg(S.uv + 2 * i0), a0v = __ldg(S.uv + 2 * i0 + 1);
+                            float d1u = __ldg(S.uv + 2 * i1) - a0u, d1v = __ldg(S.uv + 2 * i1 + 1) - a0v;
+                            float d2u = __ldg(S.uv + 2 * i2) - a0u, d2v = __ldg(S.uv + 2 * i2 + 1) - a0v;
+                            float det = d1u * d2v - d2u * d1v;
+                            if (fabsf(det) > 1e-8f) ht = normalize((-d1u * (p1 - p0) + d2u * (p2 - p0)) * (1.0f / det));
+                            else build_onb(N, ht, B);
+                            h = hu * 2.0f - 1.0f;
+                        }
+                        T = normalize(ht - N * dot(ht, N));
+                        B = cross(N, T);
+                    } else {
+                        build_onb(N, T, B);
+                    }
+                    {  // terminator bend, Shaders.hlsl:402-411
+                        float3 V = -rd;
+                        float ndv = dot(N, V);
+                        if (ndv <= 0.0f && dot(V, Ng) > 0.0f) {
+                            N = normalize(N + V * (1e-3f - ndv));
+                            build_onb(N, T, B);
+                        }
+                    }
+                    float3 wil = to_local(-rd, T, B, N);
+                    if (m.type == PT_MAT_MIRROR) {  // Shaders.hlsl:419-427
+                        nd = reflect(rd, N);
+                        no = hp + Ng * 0.001f;
+                        lastPdf = 0.0f;
+                        cont = true;
+                    } else if (m.type == PT_MAT_DIELECTRIC) {  // Shaders.hlsl:429-472
+                        float etaI = back ? m.intIOR : m.extIOR, etaT = back ? m.extIOR : m.intIOR;
+                        float Fr = fresnel(dot(-rd, N), etaI, etaT);
+                        bool refr = false;
+                        if (next_float(rng, S.sobol1) < Fr) nd = reflect(rd, N);
+                        else {
+                            nd = refract(rd, N, etaI / etaT);
+                            if (dot(nd, nd) < 0.001f) nd = reflect(rd, N);
+                            else refr = true;
+                        }
+                        no = hp + (dot(nd, Ng) > 0.0f ? Ng : -Ng) * 0.001f;
+                        lastPdf = 0.0f;
+                        if (refr) eta *= etaI / etaT;
+                        cont = true;
+                    } else if (m.type == PT_MAT_DIFFUSE || m.type == PT_MAT_MICROFACET || m.type == PT_MAT_DISNEY ||
+                               m.type == PT_MAT_HAIR) {  // Shaders.hlsl:473-511
+                        float3 ra = nee_area<INLINE>(A, hp, N, Ng, T, B, wil, m, h, rng, neeA);
+                        float3 re = nee_env<INLINE>(A, hp, N, Ng, T, B, wil, m, h, rng, neeE);
+                        if (INLINE) {
+                            Lo += thr * ra;
+                            Lo += thr * re;
+                        } else {
+                            thrNee = thr;
+                            if (!neeA.ray) A.pendA[slot] = make_float4(thr.x * 0.0f, thr.y * 0.0f, thr.z * 0.0f, 0.0f);
+                            if (!neeE.ray) A.pendE[slot] = make_float4(thr.x * 0.0f, thr.y * 0.0f, thr.z * 0.0f, 0.0f);
+                            st.w |= kFlagPending;
+                        }
+                        float u[4];
+                        int k = material_sample_dims(m, wil);
+                        for (int j = 0; j < k; j++) u[j] = next_float(rng, S.sobol1);
+                        float3 wol;
+                        float bp;
+                        float3 wt = material_sample(wil, u, m, h, wol, bp);
+                        if (!(bp <= 0.0f || (wt.x == 0.0f && wt.y == 0.0f && wt.z == 0.0f))) {
+                            float3 ww = to_world(wol, T, B, N);
+                            float3 on = m.type == PT_MAT_HAIR ? (dot(ww, Ng) >= 0.0f ? Ng : -Ng) : Ng;
+                            no = offset_origin(hp, on, on);
+                            nd = ww;
+                            thr *= wt;
+                            lastPdf = mx(bp, 1e-20f);
+                            cont = true;
+                        }
+                    }
+                }
+            }
+            // Russian roulette after bounce 3 (Shaders.hlsl:620-626)
+            if (cont && st.z >= 3u) {
+                float q = mn(maxc(thr) * eta * eta, 0.95f);
+                if (next_float(rng, S.sobol1) >= q) cont = false;
+                else thr = thr / v3(q);
+            }
+            st.z += 1u;
+            if (st.z >= A.maxDepth) cont = false;
+            st.x = rng.dim;
+            st.y = rng.white;
+            A.thr_pdf[slot] = make_float4(thr.x, thr.y, thr.z, lastPdf);
+            A.lo_eta[slot] = make_float4(Lo.x, Lo.y, Lo.z, eta);
+            A.rng[slot] = st;
+        }
+        if (!INLINE) {
+            push_shadow(A, active && neeA.ray, slot, 0u, neeA, thrNee);
+            push_shadow(A, active && neeE.ray, slot, 1u, neeE, thrNee);
+        }
+        uint32_t pos = warp_append(A.cntOut, active && cont);
+        if (active && cont) {
+            A.qslotOut[pos] = slot;
+            A.qoOut[pos] = make_float4(no.x, no.y, no.z, ntmin);
+            A.qdOut[pos] = make_float4(nd.x, nd.y, nd.z, 1e20f);
+        }
+    }
+}
+
+// ---- film: Kahan-compensated accumulation of (L, 1), samples in order -------
+// (Shaders.hlsl:629-634: NaN/Inf guard, then accum += (Lo, 1)).
+__device__ __forceinline__ void kahan(float &s, float &c, float x) {
+    float y = x - c;
+    float t = s + y;
+    c = (t - s) - y;
+    s = t;
+}
+__global__ void k_film(WaveArgs A, float4 *sum, float4 *comp) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t cover = min(A.waveCount, A.npix);
+    if (t >= cover) return;
+    uint64_t first = A.waveStart, last = A.waveStart + A.waveCount;
+    uint32_t pix = (uint32_t)((first + t) % A.npix);
+    float4 s = sum[pix], c = comp[pix];
+    for (uint64_t pid = first + t; pid < last; pid += A.npix) {
+        uint32_t slot = (uint32_t)(pid - first);
+        float4 le = A.lo_eta[slot];
+        float3 L = make_float3(le.x, le.y, le.z);
+        if (A.rng[slot].w & kFlagPending) {
+            float4 pa = A.pendA[slot], pe = A.pendE[slot];
+            L += make_float3(pa.x, pa.y, pa.z);
+            L += make_float3(pe.x, pe.y, pe.z);
+        }
+        if (isnan(L.x) || isnan(L.y) || isnan(L.z) || isinf(L.x) || isinf(L.y) || isinf(L.z)) L = v3(0.0f);
+        kahan(s.x, c.x, L.x);
+        kahan(s.y, c.y, L.y);
+        kahan(s.z, c.z, L.z);
+        kahan(s.w, c.w, 1.0f);
+    }
+    sum[pix] = s;
+    comp[pix] = c;
+}
+
+}  // namespace pt
+
+using namespace pt;
+
+static int grid_for(pt_ctx *ctx, const void *fn) {
+    int blocks = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fn, kBlock, 0) != cudaSuccess || blocks < 1) blocks = 1;
+    return blocks * ctx->numSMs;
+}
+
+int pt_wave_free(pt_ctx *ctx) {
+    WaveBuffers &W = ctx->W;
+    void *ps[] = {W.thr_pdf, W.lo_eta, W.pendA, W.pendE, W.rng, W.qslot[0], W.qslot[1], W.qo[0], W.qo[1],
+                  W.qd[0], W.qd[1], W.qhit, W.sslot, W.so, W.sd, W.sX, W.sthr, W.counters};
+    for (void *p : ps)
+        if (p) cudaFree(p);
+    W = WaveBuffers{};
+    return PT_OK;
+}
+
+static int wave_alloc(pt_ctx *ctx, size_t cap) {
+    if (ctx->W.cap >= cap) return PT_OK;
+    pt_wave_free(ctx);
+    WaveBuffers &W = ctx->W;
+    size_t sc = 2 * cap;
+    cudaError_t e = cudaSuccess;
+    auto A = [&](void **p, size_t bytes) { if (e == cudaSuccess) e = cudaMalloc(p, bytes); };
+    A((void **)&W.thr_pdf, cap * 16); A((void **)&W.lo_eta, cap * 16);
+    A((void **)&W.pendA, cap * 16); A((void **)&W.pendE, cap * 16); A((void **)&W.rng, cap * 16);
+    for (int k = 0; k < 2; k++) { A((void **)&W.qslot[k], cap * 4); A((void **)&W.qo[k], cap * 16); A((void **)&W.qd[k], cap * 16); }
+    A((void **)&W.qhit, cap * 16);
+    A((void **)&W.sslot, sc * 4); A((void **)&W.so, sc * 16); A((void **)&W.sd, sc * 16);
+    A((void **)&W.sX, sc * 16); A((void **)&W.sthr, sc * 16);
+    A((void **)&W.counters, 64);
+    if (e != cudaSuccess) {
+        pt_wave_free(ctx);
+        return ctx->fail(PT_E_NOMEM, "wave buffers", cudaGetErrorString(e));
+    }
+    W.cap = cap;
+    return PT_OK;
+}
+
+int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *d_comp, pt_stats *stats) {
+    const uint32_t W = P->width, H = P->height;
+    const uint64_t npix = (uint64_t)W * H;
+    const uint64_t total = npix * P->spp;
+    size_t cap = P->wave_paths ? P->wave_paths : (size_t)1 << 21;
+    if (npix <= cap) cap = (cap / npix) * npix;
+    if (cap > total) cap = (size_t)total;
+    if (cap == 0) return PT_OK;
+    int rc = wave_alloc(ctx, cap);
+    if (rc) return rc;
+    cudaStream_t st = ctx->stream;
+    WaveBuffers &B = ctx->W;
+    const bool inl = ctx->S.numVols > 0;
+    static int gExt = 0, gShade = 0, gShadeI = 0, gShadow = 0;
+    if (!gExt) {
+        gExt = grid_for(ctx, (const void *)k_extend);
+        gShade = grid_for(ctx, (const void *)k_shade<false>);
+        gShadeI = grid_for(ctx, (const void *)k_shade<true>);
+        gShadow = grid_for(ctx, (const void *)k_shadow);
+    }
+    cudaEvent_t ev[2];
+    cudaEventCreate(&ev[0]);
+    cudaEventCreate(&ev[1]);
+    PT_CUDA(cudaMemsetAsync(B.counters, 0, 64, st));
+    PT_CUDA(cudaMemsetAsync(ctx->d_err, 0, 4, st));
+    cudaEventRecord(ev[0], st);
+    WaveArgs A;
+    A.S = ctx->S;
+    A.width = W; A.height = H; A.npix = (uint32_t)npix;
+    A.sampleOffset = P->sample_offset;
+    A.rngKind = P->rng_kind; A.envMode = P->env_sampling; A.maxDepth = P->max_depth;
+    A.cam = P->camera;
+    A.thr_pdf = B.thr_pdf; A.lo_eta = B.lo_eta; A.pendA = B.pendA; A.pendE = B.pendE; A.rng = B.rng;
+    A.qhit = B.qhit;
+    A.sslot = B.sslot; A.so = B.so; A.sd = B.sd; A.sX = B.sX; A.sthr = B.sthr;
+    A.cntShadow = B.counters + 2;
+    A.rayTotals = (unsigned long long *)(B.counters + 4);
+    A.err = ctx->d_err;
+    A.shadowCap = (uint32_t)(2 * B.cap);
+    uint64_t waves = 0, bounces = 0, launches = 0;
+    // optional per-stage timing: an event pair around every launch
+    const bool timing = (P->flags & PT_RENDER_STAGE_TIMING) != 0;
+    enum { STG_RAYGEN, STG_EXTEND, STG_SHADE, STG_SHADOW, STG_FILM, STG_N };
+    struct Mark { int stage; cudaEvent_t a, b; };
+    std::vector<Mark> marks;
+    auto begin = [&](int stage) {
+        launches++;
+        if (!timing) return;
+        Mark m{stage, nullptr, nullptr};
+        cudaEventCreate(&m.a);
+        cudaEventCreate(&m.b);
+        cudaEventRecord(m.a, st);
+        marks.push_back(m);
+    };
+    auto end = [&]() {
+        if (timing) cudaEventRecord(marks.back().b, st);
+    };
+    for (uint64_t ws = 0; ws < total; ws += cap) {
+        A.waveStart = ws;
+        A.waveCount = (uint32_t)std::min<uint64_t>(cap, total - ws);
+        A.qslotOut = B.qslot[0]; A.qoOut = B.qo[0]; A.qdOut = B.qd[0]; A.cntOut = B.counters + 0;
+        begin(STG_RAYGEN);
+        k_raygen<<<(A.waveCount + kBlock - 1) / kBlock, kBlock, 0, st>>>(A);
+        end();
+        int cur = 0;
+        for (uint32_t b = 0; b < P->max_depth; b++) {
+            A.qslotIn = B.qslot[cur]; A.qoIn = B.qo[cur]; A.qdIn = B.qd[cur]; A.cntIn = B.counters + cur;
+            A.qslotOut = B.qslot[1 - cur]; A.qoOut = B.qo[1 - cur]; A.qdOut = B.qd[1 - cur];
+            A.cntOut = B.counters + (1 - cur);
+            cudaMemsetAsync(A.cntOut, 0, 4, st);
+            cudaMemsetAsync(A.cntShadow, 0, 4, st);
+            begin(STG_EXTEND);
+            k_extend<<<gExt, kBlock, 0, st>>>(A);
+            end();
+            begin(STG_SHADE);
+            if (inl) k_shade<true><<<gShadeI, kBlock, 0, st>>>(A);
+            else k_shade<false><<<gShade, kBlock, 0, st>>>(A);
+            end();
+            if (!inl) {
+                begin(STG_SHADOW);
+                k_shadow<<<gShadow, kBlock, 0, st>>>(A);
+                end();
+            }
+            cur = 1 - cur;
+            bounces++;
+        }
+        uint32_t cover = (uint32_t)std::min<uint64_t>(A.waveCount, npix);
+        begin(STG_FILM);
+        k_film<<<(cover + kBlock - 1) / kBlock, kBlock, 0, st>>>(A, (float4 *)d_sum, (float4 *)d_comp);
+        end();
+        waves++;
+    }
+    cudaEventRecord(ev[1], st);
+    uint32_t hostCnt[16];
+    PT_CUDA(cudaMemcpyAsync(hostCnt, B.counters, 64, cudaMemcpyDeviceToHost, st));
+    uint32_t derr = 0;
+    PT_CUDA(cudaMemcpyAsync(&derr, ctx->d_err, 4, cudaMemcpyDeviceToHost, st));
+    cudaError_t se = cudaStreamSynchronize(st);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, ev[0], ev[1]);
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    float stage[STG_N] = {0, 0, 0, 0, 0};
+    for (Mark &m : marks) {
+        float t = 0.0f;
+        if (se == cudaSuccess) cudaEventElapsedTime(&t, m.a, m.b);
+        stage[m.stage] += t;
+        cudaEventDestroy(m.a);
+        cudaEventDestroy(m.b);
+    }
+    if (se != cudaSuccess) return ctx->fail(PT_E_CUDA, "render", cudaGetErrorString(se));
+    if (derr)
+        return ctx->fail(PT_E_DEVICE, (derr & PT_DEVERR_STACK) ? "traversal stack overflow"
+                                      : (derr & PT_DEVERR_BVH) ? "traversal visited more nodes than the BVH has"
+                                                               : "queue overflow");
+    if (stats) {
+        unsigned long long tot[2];
+        memcpy(tot, hostCnt + 4, sizeof(tot));
+        stats->paths = total;
+        stats->extension_rays = tot[0];
+        stats->shadow_rays = tot[1];
+        stats->waves = waves;
+        stats->bounces = bounces;
+        stats->launches = launches;
+        stats->ms_total = ms;
+        stats->ms_raygen = stage[STG_RAYGEN];
+        stats->ms_extend = stage[STG_EXTEND];
+        stats->ms_shade = stage[STG_SHADE];
+        stats->ms_shadow = stage[STG_SHADOW];
+        stats->ms_film = stage[STG_FILM];
+    }
+    return PT_OK;
+}

@@ -1,0 +1,259 @@
+"""libpt (CUDA, through the C ABI) against the CPU oracle.
+
+Integer work (sample stream, Morton codes, radix-tree topology, envmap CDF
+tables) must be bit-exact.  Float work is compared per element against the
+oracle's float32 result, with the error of both stated against the oracle's
+FP64 evaluation, on 1M seeded direction pairs per material type:
+
+* relative difference GPU vs float32 oracle <= 1e-5 for >= 99 % of pairs and
+  <= 5e-5 for >= 99.9 % (floor 1e-6 of the median magnitude);
+* the GPU is never less accurate than the float32 oracle: its error against
+  FP64 is within 4x the oracle's own error + 1e-5 relative for >= 99.9 % of
+  pairs, and its 99.9th-percentile error against FP64 is at most 1.25x the
+  oracle's.
+
+Cancellation in the reference formulas (e.g. pow(1 - cos, 5), GTR1 at low
+gloss) puts the float32 oracle itself ~2e-5 from FP64 at the 99.9th
+percentile for the Disney BSDF, which is why the 1e-5 bar is stated at p99.
+BSDF *sampling* maps uniforms to a direction first; near-delta lobes amplify
+direction rounding into the value, so sampling is checked as (a) direction
+parity against FP64 and (b) value parity at the GPU's own direction.
+"""
+
+import numpy as np
+import pytest
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+N_PAIRS = 1 << 20
+
+
+def random_materials(pt, rng, kind, count):
+    mats = []
+    for _ in range(count):
+        m = pt.make_material(kind, tuple(rng.uniform(0.05, 1.0, 3)))
+        if kind == pt.PT_MAT_DISNEY:
+            m.roughness = rng.uniform(0.05, 1.0)
+            m.metallic, m.specular, m.specularTint = rng.uniform(0, 1, 3)
+            m.sheen, m.sheenTint, m.subsurface = rng.uniform(0, 1, 3)
+            m.clearcoat, m.clearcoatGloss = rng.uniform(0, 1, 2)
+        elif kind == pt.PT_MAT_MICROFACET:
+            m.alpha = rng.uniform(0.05, 0.8)
+        elif kind == pt.PT_MAT_HAIR:
+            m.roughness, m.betaN = rng.uniform(0.2, 0.6), rng.uniform(0.2, 0.6)
+            m.alpha, m.intIOR = 2.0, 1.55
+        mats.append(m)
+    return mats
+
+
+def parity_stats(gpu, o32, o64, floor):
+    d = rel_err(gpu, o32, floor)
+    e_gpu = np.abs(gpu.astype(np.float64) - o64)
+    e_or = np.abs(o32.astype(np.float64) - o64)
+    bound = 4.0 * e_or + 1e-5 * np.maximum(np.abs(o64), floor)
+    return {"p99": float(np.quantile(d, 0.99)), "p999": float(np.quantile(d, 0.999)), "max": float(d.max()),
+            "frac_within_bound": float((e_gpu <= bound).mean()),
+            "gpu_vs_fp64_p999": float(np.quantile(e_gpu / np.maximum(np.abs(o64), floor), 0.999)),
+            "oracle_vs_fp64_p999": float(np.quantile(e_or / np.maximum(np.abs(o64), floor), 0.999))}
+
+
+def assert_parity(st):
+    assert st["p99"] <= 1e-5 and st["p999"] <= 5e-5, st
+    assert st["frac_within_bound"] >= 0.999, st
+    assert st["gpu_vs_fp64_p999"] <= 1.25 * st["oracle_vs_fp64_p999"] + 1e-6, st
+
+
+def test_sample_stream_bit_exact(ctx, oracle):
+    rng = np.random.default_rng(1)
+    pix = rng.integers(0, 1280 * 720, 200000).astype(np.uint32)
+    smp = rng.integers(0, 1 << 16, 200000).astype(np.uint32)
+    for kind in (0, 1):
+        a = ctx.rng(kind, pix, smp, 16, 1280, 720)
+        b = oracle.rng(kind, pix, smp, 16, 1280, 720)
+        assert np.array_equal(a, b), kind
+
+
+@pytest.mark.parametrize("kind_name", ["DIFFUSE", "MICROFACET", "DISNEY", "HAIR"])
+def test_bsdf_eval_parity(kind_name, pt, scenes, ctx, oracle):
+    kind = getattr(pt, "PT_MAT_" + kind_name)
+    rng = np.random.default_rng(17)
+    mats = random_materials(pt, rng, kind, 64)
+    wi = scenes.sample_directions(N_PAIRS, 21, upper=kind != pt.PT_MAT_HAIR)
+    wo = scenes.sample_directions(N_PAIRS, 22, upper=kind != pt.PT_MAT_HAIR)
+    mi = rng.integers(0, len(mats), N_PAIRS).astype(np.uint32)
+    h = rng.uniform(-0.95, 0.95, N_PAIRS).astype(np.float32)
+    fg, pg = ctx.bsdf_eval(mats, mi, wi, wo, h)
+    f32, p32 = oracle.bsdf_eval(mats, mi, wi, wo, h)
+    f64, p64 = oracle.bsdf_eval(mats, mi, wi, wo, h, fp64=True)
+    scale_f = float(np.quantile(np.abs(f64), 0.5)) + 1e-12
+    scale_p = float(np.quantile(np.abs(p64), 0.5)) + 1e-12
+    sf = parity_stats(fg, f32, f64, 1e-6 * scale_f)
+    sp = parity_stats(pg, p32, p64, 1e-6 * scale_p)
+    print(kind_name, "f", sf, "pdf", sp)
+    assert_parity(sf)
+    assert_parity(sp)
+
+
+@pytest.mark.parametrize("kind_name", ["DIFFUSE", "MICROFACET", "DISNEY", "HAIR"])
+def test_bsdf_sample_parity(kind_name, pt, scenes, ctx, oracle):
+    kind = getattr(pt, "PT_MAT_" + kind_name)
+    rng = np.random.default_rng(29)
+    mats = random_materials(pt, rng, kind, 64)
+    n = N_PAIRS
+    wi = scenes.sample_directions(n, 31, upper=kind != pt.PT_MAT_HAIR)
+    u = rng.uniform(0, 1, (n, 4)).astype(np.float32)
+    mi = rng.integers(0, len(mats), n).astype(np.uint32)
+    h = rng.uniform(-0.95, 0.95, n).astype(np.float32)
+    wog, wtg, pg = ctx.bsdf_sample(mats, mi, wi, u, h)
+    wo32, _, _ = oracle.bsdf_sample(mats, mi, wi, u, h)
+    wo64, _, _ = oracle.bsdf_sample(mats, mi, wi, u, h, fp64=True)
+    # (a) directions: the GPU's distance to the FP64 direction vs the oracle's
+    valid = (pg > 0) & np.isfinite(wo64).all(1)
+    e_gpu = np.abs(wog - wo64).max(1)
+    e_or = np.abs(wo32 - wo64).max(1)
+    same_lobe = e_gpu < 1e-2  # a lobe/branch pick flipped by rounding of u
+    assert same_lobe[valid].mean() > 0.9995, same_lobe[valid].mean()
+    ok = e_gpu <= 4 * e_or + 2e-6
+    assert ok[valid & same_lobe].mean() > 0.999, ok[valid & same_lobe].mean()
+    # (b) values at the GPU's direction: weight = f |cos| / pdf (albedo for diffuse)
+    f_o, p_o = oracle.bsdf_eval(mats, mi, wi, wog, h)
+    f_d, p_d = oracle.bsdf_eval(mats, mi, wi, wog, h, fp64=True)
+    sel = valid & (p_o > 0) & (p_d > 0)
+    cos_o = np.abs(wog[:, 2:3]).astype(np.float64)
+    if kind == pt.PT_MAT_DIFFUSE:
+        alb = np.array([list(m.albedo) for m in mats], np.float64)[mi]
+        w_o32, w_o64 = alb.astype(np.float32), alb
+    else:
+        w_o32 = (f_o * cos_o / p_o[:, None]).astype(np.float32)
+        w_o64 = f_d.astype(np.float64) * cos_o / p_d[:, None].astype(np.float64)
+    sw = parity_stats(wtg[sel], w_o32[sel], w_o64[sel], 1e-6)
+    sp = parity_stats(pg[sel], p_o[sel], p_d[sel].astype(np.float64), 1e-6 * float(np.median(np.abs(p_d[sel]))))
+    print(kind_name, "weight", sw, "pdf", sp)
+    assert_parity(sw)
+    assert_parity(sp)
+
+
+def test_phase_sample_parity(ctx, oracle, scenes):
+    n = N_PAIRS
+    rng = np.random.default_rng(41)
+    g = rng.choice(np.array([0.0, 0.3, 0.8, -0.5], np.float32), n)
+    wo = scenes.sample_directions(n, 42)
+    u = rng.uniform(0, 1, (n, 2)).astype(np.float32)
+    wg, pg = ctx.phase_sample(g, wo, u)
+    w32, p32 = oracle.phase_sample(g, wo, u)
+    w64, p64 = oracle.phase_sample(g, wo, u, fp64=True)
+    e_gpu = np.abs(wg - w64).max(1)
+    e_or = np.abs(w32 - w64).max(1)
+    assert (e_gpu <= 4 * e_or + 2e-6).mean() > 0.999
+    assert float(np.quantile(e_gpu, 0.999)) <= 1.25 * float(np.quantile(e_or, 0.999)) + 1e-6
+    sp = parity_stats(pg, p32, p64, 1e-6)
+    assert_parity(sp)
+
+
+@pytest.fixture(scope="module")
+def sky_scene(scenes):
+    return scenes.disney_spheres(64, 48, grid=2, slices=32, rings=17, env_w=512, env_h=256)
+
+
+def test_envmap_tables_bit_exact(ctx, oracle, sky_scene):
+    sc, _ = sky_scene
+    ctx.upload(sc)
+    oracle.load(sc)
+    mg, cg = ctx.env_cdf()
+    mo, co = oracle.env_cdf()
+    assert np.array_equal(mg, mo) and np.array_equal(cg, co)
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_envmap_sample_pdf_parity(mode, ctx, oracle, sky_scene):
+    sc, _ = sky_scene
+    ctx.upload(sc)
+    oracle.load(sc)
+    u = np.random.default_rng(43).uniform(0, 1, (N_PAIRS, 2)).astype(np.float32)
+    dg, rg, pg = ctx.env_sample(mode, u)
+    do, ro, po = oracle.env_sample(mode, u)
+    assert np.abs(dg - do).max() < 1e-5
+    assert float(np.quantile(rel_err(pg, po, 1e-6), 0.999)) <= 1e-5
+    assert float(np.quantile(rel_err(rg, ro, 1e-6), 0.999)) <= 1e-5
+    pg2, rg2 = ctx.env_pdf(mode, do)
+    po2, ro2 = oracle.env_pdf(mode, do)
+    assert float(np.quantile(rel_err(pg2, po2, 1e-6), 0.999)) <= 1e-5
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_envmap_sampler_distribution(mode, pt, ctx, scenes):
+    """Sampled texels follow lum * sin(theta) (the density both tables encode):
+    per-texel counts against expectation, z-scores over texels with >= 200
+    expected samples."""
+    env = scenes.sky_envmap(64, 32, sun_peak=40.0, sun_sigma_deg=8.0)
+    m = pt.make_material(pt.PT_MAT_DIFFUSE)
+    tri = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32)
+    m.vertexCount, m.indexCount = 3, 3
+    ctx.upload(pt.Scene(tri, np.array([0, 1, 2]), [m], env_rgb=env))
+    n = 1 << 22
+    u = np.random.default_rng(44 + mode).uniform(0, 1, (n, 2)).astype(np.float32)
+    d, _, _ = ctx.env_sample(mode, u)
+    phi = np.mod(np.arctan2(d[:, 2], d[:, 0]), 2 * np.pi)
+    th = np.arccos(np.clip(d[:, 1], -1, 1))
+    H, W = env.shape[:2]
+    x = np.minimum((phi / (2 * np.pi) * W).astype(int), W - 1)
+    y = np.minimum((th / np.pi * H).astype(int), H - 1)
+    cnt = np.bincount(y * W + x, minlength=W * H).astype(np.float64)
+    lum = 0.2126 * env[..., 0] + 0.7152 * env[..., 1] + 0.0722 * env[..., 2]
+    w = lum * np.sin(np.pi * (np.arange(H) + 0.5) / H)[:, None]
+    exp = (w / w.sum()).reshape(-1) * n
+    sel = exp >= 200
+    z = (cnt[sel] - exp[sel]) / np.sqrt(exp[sel])
+    assert np.abs(z).max() < 6.0 and np.mean(z ** 2) < 1.3, (np.abs(z).max(), np.mean(z ** 2))
+
+
+def test_bvh_topology_bit_exact(ctx, oracle, scenes):
+    sc, _ = scenes.disney_spheres(32, 32, grid=3, slices=48, rings=25, env_w=16, env_h=8)
+    ctx.upload(sc)
+    oracle.load(sc)
+    mg, og, ng, nwide = ctx.bvh()
+    mo, oo, no = oracle.lbvh()
+    assert np.array_equal(mg, mo)
+    assert np.array_equal(og, oo)
+    assert np.array_equal(ng, no)
+    assert 0 < nwide < sc.num_triangles
+
+
+@pytest.mark.parametrize("which", ["spheres", "cornell", "hair"])
+def test_trace_parity(which, ctx, oracle, scenes):
+    if which == "spheres":
+        sc, _ = scenes.disney_spheres(32, 32, grid=3, slices=48, rings=25, env_w=16, env_h=8)
+        lo, hi = -6.0, 6.0
+    elif which == "cornell":
+        sc, _ = scenes.cornell(32, 32)
+        lo, hi = -1.0, 2.0
+    else:
+        sc, _ = scenes.hair_volume(32, 32, strands=400, segments=8, grid_n=16)
+        lo, hi = -1.5, 1.5
+    ctx.upload(sc)
+    oracle.load(sc)
+    rng = np.random.default_rng(47)
+    n = 200000
+    o = rng.uniform(lo, hi, (n, 3)).astype(np.float32)
+    d = scenes.sample_directions(n, 48)
+    rays = np.zeros((n, 8), np.float32)
+    rays[:, 0:3], rays[:, 3], rays[:, 4:7], rays[:, 7] = o, 0.0, d, 1e20
+    hg = ctx.trace_closest(rays)
+    ho = oracle.trace_closest(rays)
+    same_hit = hg["hit"] == ho["hit"]
+    both = (hg["hit"] == 1) & (ho["hit"] == 1)
+    same_prim = (hg["mesh"] == ho["mesh"]) & (hg["prim"] == ho["prim"])
+    # disagreements only where the oracle's barycentrics are within 1e-6 of an edge
+    # (or the hit distances tie), i.e. the ray grazes a shared edge or vertex
+    edge = np.minimum(np.minimum(ho["u"], ho["v"]), 1 - ho["u"] - ho["v"]) < 1e-4
+    bad = ~(same_hit & (~both | same_prim))
+    assert (bad & ~edge).sum() <= max(2, n // 100000), int((bad & ~edge).sum())
+    tt = both & same_prim
+    assert np.abs(hg["t"][tt] - ho["t"][tt]).max() <= 1e-4 * max(1.0, float(np.abs(ho["t"][tt]).max()))
+    # shadow rays: occlusion within the closest-hit distance
+    rays[:, 7] = np.where(ho["hit"] == 1, ho["t"] * 0.5, 10.0)
+    og, _ = ctx.trace_shadow(rays)
+    oo, _ = oracle.trace_shadow(rays)
+    assert (og != oo).mean() < 1e-3
