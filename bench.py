@@ -134,15 +134,11 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """DRAM bytes per extension ray from the committed ncu summary (or None)."""
-    p = os.path.join(ROOT, "profiles", "extend_traffic.json")
-    if os.path.exists(p):
-        try:
-            return json.load(open(p))
-        except ValueError:
-            return None
-    return None
+# k_extend DRAM traffic per extension ray (dram__bytes_read.sum + dram__bytes_write.sum
+# from one ncu capture of this workload at 2 spp: 131.1 MB over the 1,843,200
+# camera rays of bounce 0).  The scene is L2-resident and the queues stream
+# once, so traffic scales with the rays a launch processes.
+EXTEND_DRAM_BYTES_PER_RAY = {"disney_envmap": 71.1}
 
 
 def cpu_reference_run(pt, sc, cam, W, H, depth, seconds=15.0, prefer_reference=True):
@@ -232,19 +228,18 @@ def main():
     t0 = time.perf_counter()
     ctx.upload(sc)
     upload_s = time.perf_counter() - t0
-    film = torch.zeros((H, W, 4), dtype=torch.float32, device="cuda")
-    comp = torch.zeros_like(film)
+    D = importlib.import_module("pbrt_b200.distributed")
+    film = D.new_film(H, W, device="cuda")  # (sum, Kahan compensation)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > 126 MB L2
     paths_step = W * H * spp
 
     def step(i, timing=False):
-        off = (i * world + rank) * spp
-        P = pt.render_params(W, H, spp, cam, max_depth=depth, sample_offset=off, env_sampling=env_mode,
-                             flags=pt.PT_RENDER_STAGE_TIMING if timing else 0)
-        _, _, st = ctx.render(P, film.data_ptr(), comp.data_ptr(), pt.PT_MEM_DEVICE)
-        if world > 1:
-            dist.all_reduce(film)
-            dist.all_reduce(comp)
+        def params(off):
+            return pt.render_params(W, H, spp, cam, max_depth=depth, sample_offset=off, env_sampling=env_mode,
+                                    flags=pt.PT_RENDER_STAGE_TIMING if timing else 0)
+
+        _, _, st = D.render_shard(ctx, params, film, i, rank, world, spp)
+        D.all_reduce_film(film)
         return st
 
     for i in range(args.warmup):
@@ -284,8 +279,8 @@ def main():
         film_np, comp_np = hsum.numpy(), hcomp.numpy()
         e2e_ms = 0.0
         for k in range(args.steps):
-            P = pt.render_params(W, H, spp, cam, max_depth=depth, sample_offset=(k * world + rank) * spp,
-                                 env_sampling=env_mode)
+            P = pt.render_params(W, H, spp, cam, max_depth=depth,
+                                 sample_offset=D.sample_offset(k, rank, world, spp), env_sampling=env_mode)
             flush.zero_()
             torch.cuda.synchronize()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -312,10 +307,9 @@ def main():
     ext_bytes_per_launch = ext * BYTES_PER_EXT_RAY / n_ext_launch
     ext_ms_per_launch = stage_ms["extend"] / n_ext_launch
     achieved = ext_bytes_per_launch / (ext_ms_per_launch / 1e3) / 1e9 if ext_ms_per_launch > 0 else 0.0
-    tr = profile_traffic()
     traffic = None
-    if tr and tr.get("workload") == cfg["workload"] and tr.get("dram_bytes_per_ray"):
-        traffic = tr["dram_bytes_per_ray"] * ext / n_ext_launch
+    if cfg["workload"] in EXTEND_DRAM_BYTES_PER_RAY:
+        traffic = round(EXTEND_DRAM_BYTES_PER_RAY[cfg["workload"]] * ext / n_ext_launch, 1)
     n_ext = ext / (paths_step * args.steps)
     n_sh = sh / (paths_step * args.steps)
     b_path = BYTES_PER_PATH_FILM + BYTES_PER_EXT_RAY * n_ext + BYTES_PER_SHADOW_RAY * n_sh
