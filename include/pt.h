@@ -35,6 +35,7 @@ extern "C" {
 #define PT_E_NOSCENE (-4)     /* render/trace before pt_upload_scene       */
 #define PT_E_DEVICE (-5)      /* a kernel raised the device error flag     */
 #define PT_E_UNSUPPORTED (-6) /* feature not built into this library       */
+#define PT_E_LIMIT (-7)       /* request larger than a fixed-size buffer   */
 
 /* ---- material types: include/bsdf.h:48-57 (BSDFGPUData::Type) -------- */
 #define PT_MAT_DIFFUSE 0
@@ -251,6 +252,29 @@ int pt_render(pt_ctx *ctx, const pt_render_params *params, pt_film *film, pt_sta
 int pt_bsdf_eval_batch(pt_ctx *ctx, const pt_material *materials, uint32_t num_materials,
                        const uint32_t *mat_index, const float *wi, const float *wo,
                        const float *h, size_t n, float *f_out, float *pdf_out, uint32_t location);
+/* pt_bsdf_eval_batch without any allocation and without a context; no
+ * counterpart in the reference.  For callers that must not allocate device
+ * memory (cudaFree synchronises the whole device, stalling a render running
+ * on another stream; or all device memory was reserved up front).  Host
+ * arrays are staged through one fixed 3 MiB array in the library's static
+ * device memory, so with PT_MEM_HOST at most PT_NOALLOC_MAX_QUERIES queries
+ * and PT_NOALLOC_MAX_MATERIALS materials per call (PT_E_LIMIT otherwise);
+ * PT_MEM_DEVICE arrays are used in place and have no limit.
+ * - Runs on the calling thread's current device and on `stream` (a
+ *   cudaStream_t; NULL = the default stream); returns after the stream
+ *   synchronises.
+ * - The first call on a device looks up the array's device address (with
+ *   that device current) and keeps it; make that first call before any
+ *   stream capture.
+ * - The array is one per device and process: calls that overlap in time on
+ *   the same device (other threads or streams) race on it.  Serialise them.
+ * Errors are status codes only (no context to hold a message). */
+#define PT_NOALLOC_MAX_QUERIES 65536u
+#define PT_NOALLOC_MAX_MATERIALS 256u
+int pt_bsdf_eval_batch_noalloc(void *stream, const pt_material *materials, uint32_t num_materials,
+                               const uint32_t *mat_index, const float *wi, const float *wo,
+                               const float *h, size_t n, float *f_out, float *pdf_out,
+                               uint32_t location);
 int pt_bsdf_sample_batch(pt_ctx *ctx, const pt_material *materials, uint32_t num_materials,
                          const uint32_t *mat_index, const float *wi, const float *u,
                          const float *h, size_t n, float *wo_out, float *weight_out,

@@ -1,5 +1,6 @@
 // pt_api.cu — the C ABI of libpt (include/pt.h).
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -636,6 +637,81 @@ int pt_bsdf_eval_batch(pt_ctx *ctx, const pt_material *materials, uint32_t nm, c
                                                          (float *)s.dev(2), (float *)s.dev(3), (float *)s.dev(4), n,
                                                          (float *)s.dev(5), (float *)s.dev(6));
     return s.finish();
+}
+
+// ---- BSDF evaluation without any allocation ---------------------------------
+// pt_bsdf_eval_batch stages host arrays through a context's scratch, which
+// grows with cudaMalloc/cudaFree, and needs a context, whose creation
+// allocates.  Some callers cannot allow that: a plugin that queries BSDFs on
+// the side while a render keeps another stream of the same device busy
+// (cudaFree synchronises the whole device and would stall that render), or a
+// host that reserved its device memory up front and must not fail a query
+// on an allocation later.  This variant stages through one fixed array in
+// the module's static device memory instead, and runs the same kernel.
+//
+// Layout of the array, every part 256-byte aligned: materials, then
+// mat_index, wi, wo, h, f, pdf for PT_NOALLOC_MAX_QUERIES queries.
+// Nothing in it has to start at zero: each call overwrites the inputs it
+// uses, the kernel reads an optional input only when the caller passed it,
+// and it writes every output element below n before anything reads it.
+namespace {
+constexpr size_t kNaMat = (PT_NOALLOC_MAX_MATERIALS * sizeof(pt_material) + 255) & ~(size_t)255;
+constexpr size_t kNaU32 = (PT_NOALLOC_MAX_QUERIES * 4 + 255) & ~(size_t)255;
+constexpr size_t kNaF3 = (PT_NOALLOC_MAX_QUERIES * 12 + 255) & ~(size_t)255;
+constexpr size_t kNaOffMi = kNaMat;
+constexpr size_t kNaOffWi = kNaOffMi + kNaU32;
+constexpr size_t kNaOffWo = kNaOffWi + kNaF3;
+constexpr size_t kNaOffH = kNaOffWo + kNaF3;
+constexpr size_t kNaOffF = kNaOffH + kNaU32;
+constexpr size_t kNaOffPdf = kNaOffF + kNaF3;
+constexpr size_t kNaBytes = kNaOffPdf + kNaU32;  // 3,182,592 bytes
+static_assert(kNaBytes == 3182592, "static staging size");
+constexpr int kNaMaxDevices = 64;
+std::atomic<char *> g_noallocAddr[kNaMaxDevices];  // per device ordinal, set on first use
+}  // namespace
+static __device__ __align__(256) unsigned char g_noallocStage[kNaBytes];
+
+int pt_bsdf_eval_batch_noalloc(void *stream, const pt_material *materials, uint32_t nm, const uint32_t *mi,
+                               const float *wi, const float *wo, const float *h, size_t n, float *f, float *pdf,
+                               uint32_t loc) {
+    if (!materials || !nm || !wi || !wo || !f || !pdf) return PT_E_INVALID;
+    if (loc != PT_MEM_HOST && loc != PT_MEM_DEVICE) return PT_E_INVALID;
+    if (loc == PT_MEM_HOST && (n > PT_NOALLOC_MAX_QUERIES || nm > PT_NOALLOC_MAX_MATERIALS)) return PT_E_LIMIT;
+    if (!n) return PT_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (loc == PT_MEM_DEVICE) {  // arrays used in place: no staging at all
+        k_bsdf_eval<<<blocks_for(n), 256, 0, st>>>(materials, nm, mi, wi, wo, h, n, f, pdf);
+        if (cudaGetLastError() != cudaSuccess) return PT_E_CUDA;
+        return cudaStreamSynchronize(st) == cudaSuccess ? PT_OK : PT_E_CUDA;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return PT_E_CUDA;
+    if (dev < 0 || dev >= kNaMaxDevices) return PT_E_INVALID;
+    // First call on a device: look up where the array lives on it (with that
+    // device current).  Two threads racing here store the same address.
+    char *base = g_noallocAddr[dev].load(std::memory_order_acquire);
+    if (!base) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noallocStage) != cudaSuccess || !p) return PT_E_CUDA;
+        base = (char *)p;
+        g_noallocAddr[dev].store(base, std::memory_order_release);
+    }
+    auto h2d = [&](size_t off, const void *src, size_t bytes) {
+        return cudaMemcpyAsync(base + off, src, bytes, cudaMemcpyHostToDevice, st) == cudaSuccess;
+    };
+    if (!h2d(0, materials, nm * sizeof(pt_material)) || (mi && !h2d(kNaOffMi, mi, n * 4)) ||
+        !h2d(kNaOffWi, wi, n * 12) || !h2d(kNaOffWo, wo, n * 12) || (h && !h2d(kNaOffH, h, n * 4)))
+        return PT_E_CUDA;
+    k_bsdf_eval<<<blocks_for(n), 256, 0, st>>>((const pt_material *)base, nm,
+                                                mi ? (const uint32_t *)(base + kNaOffMi) : nullptr,
+                                                (const float *)(base + kNaOffWi), (const float *)(base + kNaOffWo),
+                                                h ? (const float *)(base + kNaOffH) : nullptr, n,
+                                                (float *)(base + kNaOffF), (float *)(base + kNaOffPdf));
+    if (cudaGetLastError() != cudaSuccess) return PT_E_CUDA;
+    if (cudaMemcpyAsync(f, base + kNaOffF, n * 12, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyAsync(pdf, base + kNaOffPdf, n * 4, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        return PT_E_CUDA;
+    return cudaStreamSynchronize(st) == cudaSuccess ? PT_OK : PT_E_CUDA;
 }
 
 int pt_bsdf_sample_batch(pt_ctx *ctx, const pt_material *materials, uint32_t nm, const uint32_t *mi, const float *wi,
