@@ -154,7 +154,7 @@ def cpu_reference_run(pt, sc, cam, W, H, depth, seconds=15.0, prefer_reference=T
     impl.load(sc)
     frames, t_total, paths = 0, 0.0, 0
     rows = H
-    while t_total < seconds and frames < 64:
+    while t_total < seconds and frames < 1024:
         P = pt.render_params(W, rows, 1, cam, max_depth=depth, sample_offset=frames)
         t0 = time.perf_counter()
         if kind == "reference":
@@ -203,6 +203,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--spp", type=int, default=0, help="override samples per pixel (profiling of small cases)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--wave-paths", type=int, default=0, help="paths in flight per wave (0 = library default)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -236,15 +237,13 @@ def main():
     def step(i, timing=False):
         def params(off):
             return pt.render_params(W, H, spp, cam, max_depth=depth, sample_offset=off, env_sampling=env_mode,
+                                    wave_paths=args.wave_paths,
                                     flags=pt.PT_RENDER_STAGE_TIMING if timing else 0)
 
         _, _, st = D.render_shard(ctx, params, film, i, rank, world, spp)
         D.all_reduce_film(film)
         return st
 
-    for i in range(args.warmup):
-        step(i)
-    torch.cuda.synchronize()
     def timed_steps(first, timing):
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
         sts = []
@@ -257,19 +256,25 @@ def main():
             sts.append(step(first + k, timing=timing))
             ev[k][1].record(stream)
             torch.cuda.synchronize()
-        t = sum(a.elapsed_time(b) for a, b in ev)
+        per = [a.elapsed_time(b) for a, b in ev]
+        t = sum(per)
         if world > 1:
             tt = torch.tensor([t], device="cuda")
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
             t = float(tt.item())
-        return t, sts
+        return t, sts, per
 
+    # the clock sampler starts with the warm-up (its start-up stays out of the
+    # timed steps) and keeps sampling through them
     with ClockSampler(local) as clk:
-        ms, stats = timed_steps(args.warmup, timing=False)
+        for i in range(args.warmup):
+            step(i)
+        torch.cuda.synchronize()
+        ms, stats, per_step = timed_steps(args.warmup, timing=False)
     value = paths_step * world * args.steps / (ms / 1e3) / 1e6
     # the same steps again with an event pair around every launch: per-kernel
     # times for the roofline (the headline above carries no per-launch events)
-    _, tstats = timed_steps(args.warmup + args.steps, timing=True)
+    _, tstats, _ = timed_steps(args.warmup + args.steps, timing=True)
 
     # end to end through the C ABI with pinned host films (copies in the timed region)
     e2e_value = None
@@ -280,7 +285,8 @@ def main():
         e2e_ms = 0.0
         for k in range(args.steps):
             P = pt.render_params(W, H, spp, cam, max_depth=depth,
-                                 sample_offset=D.sample_offset(k, rank, world, spp), env_sampling=env_mode)
+                                 sample_offset=D.sample_offset(k, rank, world, spp), env_sampling=env_mode,
+                                 wave_paths=args.wave_paths)
             flush.zero_()
             torch.cuda.synchronize()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -315,7 +321,8 @@ def main():
     b_path = BYTES_PER_PATH_FILM + BYTES_PER_EXT_RAY * n_ext + BYTES_PER_SHADOW_RAY * n_sh
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
+        "ms_steps": [round(x, 3) for x in per_step], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene, no reference assets)",
         "config": dict(cfg, parallelism=f"sample-range x{world}" if world > 1 else "single GPU",
                        env_sampling=args.env_sampling,

@@ -367,6 +367,7 @@ int pt_upload_scene(pt_ctx *ctx, const pt_scene_desc *d) {
     std::vector<uint32_t> meshFirstTri(std::max(1u, d->num_meshes), 0);
     uint32_t numTris = 0;
     bool hasGlass = false;
+    uint32_t clsMask = 1u << CLS_MISS;  // shading classes the scene can produce
     for (uint32_t m = 0; m < d->num_meshes; m++) {
         const pt_material &pm = mats[m];
         if (pm.type > PT_MAT_SUBSURFACE) return ctx->fail(PT_E_INVALID, "unknown material type");
@@ -382,6 +383,7 @@ int pt_upload_scene(pt_ctx *ctx, const pt_scene_desc *d) {
         meshFirstTri[m] = numTris;
         numTris += pm.indexCount / 3;
         hasGlass |= pm.type == PT_MAT_MIRROR || pm.type == PT_MAT_DIELECTRIC;
+        if (pm.indexCount) clsMask |= 1u << shade_class(true, pm.isEmitter != 0, pm.type);
     }
     for (uint32_t v = 0; v < d->num_volumes; v++) {
         const pt_volume &vol = d->volumes[v];
@@ -581,6 +583,7 @@ int pt_upload_scene(pt_ctx *ctx, const pt_scene_desc *d) {
         S.vols = dvols; S.dens = ddens; S.maj = dmaj;
     }
     PT_CUDA(cudaStreamSynchronize(st));
+    ctx->clsMask = clsMask;
     ctx->hasScene = true;
     return PT_OK;
 }

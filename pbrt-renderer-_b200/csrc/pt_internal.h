@@ -21,6 +21,32 @@ enum : uint32_t {
     PT_DEVERR_BVH = 4u,       // traversal visited more nodes than exist
 };
 
+// Shading classes: the closest-hit kernel sorts each path into one of these
+// queues and one shading kernel per class present in the scene runs with its
+// material type fixed at compile time.
+enum ShadeClass : int {
+    CLS_ANY = -1,  // no classification (scenes with media: the medium decides first)
+    CLS_MISS = 0,
+    CLS_EMIT = 1,     // emitter hit (any material type)
+    CLS_DELTA = 2,    // mirror, dielectric
+    CLS_DIFFUSE = 3,
+    CLS_MICRO = 4,
+    CLS_DISNEY = 5,
+    CLS_HAIR = 6,
+    CLS_N = 7
+};
+__host__ __device__ inline int shade_class(bool hit, bool emitter, uint32_t type) {
+    if (!hit) return CLS_MISS;
+    if (emitter) return CLS_EMIT;
+    switch (type) {
+        case PT_MAT_MIRROR: case PT_MAT_DIELECTRIC: return CLS_DELTA;
+        case PT_MAT_DIFFUSE: return CLS_DIFFUSE;
+        case PT_MAT_MICROFACET: return CLS_MICRO;
+        case PT_MAT_DISNEY: return CLS_DISNEY;
+        default: return CLS_HAIR;  // upload admits no other type
+    }
+}
+
 // Per-wave buffers of the wavefront integrator (structure of arrays).
 struct WaveBuffers {
     size_t cap = 0;
@@ -35,11 +61,12 @@ struct WaveBuffers {
     float4 *qo[2] = {nullptr, nullptr};  // origin, tmin
     float4 *qd[2] = {nullptr, nullptr};  // direction, tmax
     float4 *qhit = nullptr;              // t, gid bits, u, v
+    uint32_t *cls = nullptr;             // CLS_N queues of ray-queue positions, cap each
     // shadow queue (two per path per bounce at most)
     uint32_t *sslot = nullptr;           // slot | kind << 31
     float4 *so = nullptr, *sd = nullptr, *sX = nullptr, *sthr = nullptr;
     // counters: [0] ray count q0, [1] ray count q1, [2] shadow count,
-    // [3..4] total extension / shadow rays (uint64 as two words each), [8] error flags
+    // [4..7] total extension / shadow rays (two uint64), [8..14] class queue counts
     uint32_t *counters = nullptr;
 };
 
@@ -52,6 +79,7 @@ struct pt_ctx {
     std::vector<void *> sceneAllocs;  // freed on re-upload / destroy
     pt::DevScene S{};
     bool hasScene = false;
+    uint32_t clsMask = 0;  // bit c: shading class c occurs in the scene
     uint32_t numTris = 0;
     uint32_t numWide = 0;
     uint32_t *d_morton = nullptr, *d_sorted = nullptr;

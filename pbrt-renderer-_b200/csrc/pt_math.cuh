@@ -51,6 +51,19 @@ PT_HD float mx(float a, float b) { return a > b ? a : b; }
 PT_HD float clampf(float x, float a, float b) { return mn(mx(x, a), b); }
 PT_HD float sat(float x) { return clampf(x, 0.0f, 1.0f); }
 
+// Round-to-nearest products and sums that the compiler may not fuse into an
+// FMA: for expressions that cancel (the HG denominator near |g| -> 1), where
+// a fused product shifts the result by many ulps against the unfused order.
+#if defined(__CUDA_ARCH__)
+PT_HD float rmul(float a, float b) { return __fmul_rn(a, b); }
+PT_HD float radd(float a, float b) { return __fadd_rn(a, b); }
+PT_HD float rsub(float a, float b) { return __fsub_rn(a, b); }
+#else
+PT_HD float rmul(float a, float b) { return a * b; }
+PT_HD float radd(float a, float b) { return a + b; }
+PT_HD float rsub(float a, float b) { return a - b; }
+#endif
+
 PT_HD float3 v3(float a) { return make_float3(a, a, a); }
 PT_HD float3 v3(float a, float b, float c) { return make_float3(a, b, c); }
 PT_HD float3 operator+(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
@@ -480,8 +493,12 @@ PT_HD float3 hair_sample_dir(float3 wi, const float *u, const pt_material &m, co
 // ---------------------------------------------------------------------------
 // Material dispatch (shaders/Material.hlsli:18-194)
 // ---------------------------------------------------------------------------
-PT_HD void material_eval_pdf(float3 wi, float3 wo, const pt_material &m, float h, float3 &f, float &pdf) {
-    switch (m.type) {
+// The dispatchers take the material type as an explicit key: a kernel that
+// serves one material class passes a compile-time constant and keeps only
+// that branch.
+PT_HD void material_eval_pdf_t(uint32_t type, float3 wi, float3 wo, const pt_material &m, float h, float3 &f,
+                               float &pdf) {
+    switch (type) {
         case PT_MAT_DIFFUSE:
             if (wi.z <= 0.0f || wo.z <= 0.0f) { f = v3(0.0f); pdf = 0.0f; }
             else { f = albedo(m) * kInvPi; pdf = wo.z * kInvPi; }
@@ -505,18 +522,23 @@ PT_HD void material_eval_pdf(float3 wi, float3 wo, const pt_material &m, float h
             pdf = 0.0f;
     }
 }
+PT_HD void material_eval_pdf(float3 wi, float3 wo, const pt_material &m, float h, float3 &f, float &pdf) {
+    material_eval_pdf_t(m.type, wi, wo, m, h, f, pdf);
+}
 // Number of NextFloat draws MaterialSample makes for this material and wi.
-PT_HD int material_sample_dims(const pt_material &m, float3 wi) {
-    switch (m.type) {
+PT_HD int material_sample_dims_t(uint32_t type, float3 wi) {
+    switch (type) {
         case PT_MAT_DIFFUSE: case PT_MAT_MICROFACET: return wi.z <= 0.0f ? 0 : 2;
         case PT_MAT_DISNEY: return wi.z <= 0.0f ? 0 : 3;
         case PT_MAT_HAIR: return 4;
         default: return 0;
     }
 }
+PT_HD int material_sample_dims(const pt_material &m, float3 wi) { return material_sample_dims_t(m.type, wi); }
 // MaterialSample with its uniforms supplied: returns f*cos/pdf, sets wo, pdf.
-PT_HD float3 material_sample(float3 wi, const float *u, const pt_material &m, float h, float3 &wo, float &pdf) {
-    switch (m.type) {
+PT_HD float3 material_sample_t(uint32_t type, float3 wi, const float *u, const pt_material &m, float h, float3 &wo,
+                               float &pdf) {
+    switch (type) {
         case PT_MAT_DIFFUSE:
             if (wi.z <= 0.0f) { wo = v3(0.0f, 0.0f, 1.0f); pdf = 0.0f; return v3(0.0f); }
             wo = cos_hemi(u[0], u[1]);
@@ -571,21 +593,25 @@ PT_HD float3 material_sample(float3 wi, const float *u, const pt_material &m, fl
             return v3(0.0f);
     }
 }
+PT_HD float3 material_sample(float3 wi, const float *u, const pt_material &m, float h, float3 &wo, float &pdf) {
+    return material_sample_t(m.type, wi, u, m, h, wo, pdf);
+}
 
 // ---------------------------------------------------------------------------
 // Henyey-Greenstein (shaders/Volume.hlsl:31-65)
 // ---------------------------------------------------------------------------
 PT_HD float hg(float c, float g) {
-    float g2 = g * g;
-    float den = 1.0f + g2 - 2.0f * g * c;
-    return (1.0f / (4.0f * kPi)) * (1.0f - g2) / (den * sqrtf(mx(den, 1e-8f)));
+    float g2 = rmul(g, g);
+    float den = rsub(radd(1.0f, g2), rmul(2.0f * g, c));
+    return rmul(1.0f / (4.0f * kPi), 1.0f - g2) / rmul(den, sqrtf(mx(den, 1e-8f)));
 }
 PT_HD float3 sample_hg(float3 wo, float g, float xi1, float xi2, float &pdf) {
     float c;
-    if (fabsf(g) < 1e-3f) c = 1.0f - 2.0f * xi1;
+    if (fabsf(g) < 1e-3f) c = rsub(1.0f, 2.0f * xi1);
     else {
-        float sq = (1.0f - g * g) / (1.0f + g - 2.0f * g * xi1);
-        c = clampf((1.0f + g * g - sq * sq) / (2.0f * g), -1.0f, 1.0f);
+        float g2 = rmul(g, g);
+        float sq = (1.0f - g2) / rsub(radd(1.0f, g), rmul(2.0f * g, xi1));
+        c = clampf(rsub(radd(1.0f, g2), rmul(sq, sq)) / (2.0f * g), -1.0f, 1.0f);
     }
     float s = sqrtf(mx(0.0f, 1.0f - c * c));
     float phi = 2.0f * kPi * xi2;

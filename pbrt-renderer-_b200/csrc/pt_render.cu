@@ -45,6 +45,8 @@ struct WaveArgs {
     uint32_t *sslot;
     float4 *so, *sd, *sX, *sthr;
     uint32_t *cntIn, *cntOut, *cntShadow;
+    uint32_t *cls, *cntCls;  // shading-class queues (CLS_N x clsStride) and their counts
+    uint32_t clsStride;
     unsigned long long *rayTotals;  // [0] extension, [1] shadow
     uint32_t *err;
     uint32_t shadowCap;
@@ -119,7 +121,19 @@ __global__ void k_raygen(WaveArgs A) {
     if (slot == 0) *A.cntOut = A.waveCount;
 }
 
-// ---- extend: closest hit -----------------------------------------------------
+// Append queue position i to the queue of class c: lanes with the same class
+// share one atomic (match_any + popc).
+__device__ __forceinline__ void class_append(const WaveArgs &A, int c, uint32_t i) {
+    uint32_t peers = __match_any_sync(__activemask(), c);
+    uint32_t leader = __ffs(peers) - 1;
+    uint32_t base = 0;
+    if (lane_id() == leader) base = atomicAdd(A.cntCls + c, __popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    A.cls[(size_t)c * A.clsStride + base + __popc(peers & ((1u << lane_id()) - 1u))] = i;
+}
+
+// ---- extend: closest hit (+ sort into shading classes) -----------------------
+template <bool CLASSIFY>
 __global__ void __launch_bounds__(kBlock) k_extend(WaveArgs A) {
     uint32_t n = *(volatile uint32_t *)A.cntIn;
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&A.rayTotals[0], (unsigned long long)n);
@@ -127,6 +141,17 @@ __global__ void __launch_bounds__(kBlock) k_extend(WaveArgs A) {
         float4 o = A.qoIn[i], d = A.qdIn[i];
         Hit h = trace_closest(A.S, make_float3(o.x, o.y, o.z), make_float3(d.x, d.y, d.z), o.w, d.w, A.err);
         A.qhit[i] = make_float4(h.t, __uint_as_float(h.gid), h.u, h.v);
+        if (CLASSIFY) {
+            bool hit = h.gid != 0xFFFFFFFFu;
+            bool emitter = false;
+            uint32_t type = 0;
+            if (hit) {
+                const pt_material *m = A.S.mats + __ldg(A.S.triMesh + h.gid);
+                type = __ldg(&m->type);
+                emitter = __ldg(&m->isEmitter) != 0u;
+            }
+            class_append(A, shade_class(hit, emitter, type), i);
+        }
     }
 }
 
@@ -159,7 +184,8 @@ struct NeeOut {
 // MISDirectIllumination (Emitter.hlsli:105-153) up to the shadow trace.
 template <bool INLINE>
 __device__ __forceinline__ float3 nee_area(const WaveArgs &A, float3 hp, float3 N, float3 Ng, float3 T, float3 B,
-                                           float3 wil, const pt_material &m, float h, Rng &rng, NeeOut &out) {
+                                           float3 wil, uint32_t type, const pt_material &m, float h, Rng &rng,
+                                           NeeOut &out) {
     const DevScene &S = A.S;
     out.ray = false;
     EmitterSample es = sample_emitter(S, rng);
@@ -168,7 +194,7 @@ __device__ __forceinline__ float3 nee_area(const WaveArgs &A, float3 hp, float3 
     float dist = len(tl);
     float3 ww = tl / v3(dist);
     float ct = dot(N, ww), cl = dot(es.nrm, -ww);
-    bool hair = m.type == PT_MAT_HAIR;
+    bool hair = type == PT_MAT_HAIR;
     if ((!hair && ct <= 0.0f) || cl <= 0.0f) return v3(0.0f);
     float act = hair ? fabsf(ct) : ct;
     float3 sng = hair ? (dot(ww, Ng) >= 0.0f ? Ng : -Ng) : Ng;
@@ -179,7 +205,7 @@ __device__ __forceinline__ float3 nee_area(const WaveArgs &A, float3 hp, float3 
     }
     float3 f;
     float pb;
-    material_eval_pdf(wil, to_local(ww, T, B, N), m, h, f, pb);
+    material_eval_pdf_t(type, wil, to_local(ww, T, B, N), m, h, f, pb);
     float pe = es.pdfArea * dist * dist / cl;
     float w = balance(pe, pb);
     float3 vt = INLINE ? multi_volume_tr(S, so, ww, dist, rng) : v3(1.0f);
@@ -192,7 +218,8 @@ __device__ __forceinline__ float3 nee_area(const WaveArgs &A, float3 hp, float3 
 // EnvmapDirectIllumination (Emitter.hlsli:275-326) up to the shadow trace.
 template <bool INLINE>
 __device__ __forceinline__ float3 nee_env(const WaveArgs &A, float3 hp, float3 N, float3 Ng, float3 T, float3 B,
-                                          float3 wil, const pt_material &m, float h, Rng &rng, NeeOut &out) {
+                                          float3 wil, uint32_t type, const pt_material &m, float h, Rng &rng,
+                                          NeeOut &out) {
     const DevScene &S = A.S;
     out.ray = false;
     float u1 = next_float(rng, S.sobol1), u2 = next_float(rng, S.sobol1);
@@ -201,7 +228,7 @@ __device__ __forceinline__ float3 nee_env(const WaveArgs &A, float3 hp, float3 N
     env_sample(S, A.envMode, u1, u2, ww, Le, pe);
     if (pe <= 0.0f) return v3(0.0f);
     float ct = dot(N, ww);
-    bool hair = m.type == PT_MAT_HAIR;
+    bool hair = type == PT_MAT_HAIR;
     if (!hair && ct <= 0.0f) return v3(0.0f);
     float act = hair ? fabsf(ct) : ct;
     float3 sng = hair ? (dot(ww, Ng) >= 0.0f ? Ng : -Ng) : Ng;
@@ -212,7 +239,7 @@ __device__ __forceinline__ float3 nee_env(const WaveArgs &A, float3 hp, float3 N
     }
     float3 f;
     float pb;
-    material_eval_pdf(wil, to_local(ww, T, B, N), m, h, f, pb);
+    material_eval_pdf_t(type, wil, to_local(ww, T, B, N), m, h, f, pb);
     float w = balance(pe, pb);
     float3 vt = INLINE ? multi_volume_tr(S, so, ww, 1e20f, rng) : v3(1.0f);
     float3 X = Le * f * act / v3(mx(pe, 1e-20f)) * w * vt;
@@ -278,15 +305,26 @@ __device__ __forceinline__ void push_shadow(const WaveArgs &A, bool pred, uint32
     A.sthr[pos] = make_float4(thr.x, thr.y, thr.z, 0.0f);
 }
 
+// Material type served by a surface shading class.
+__host__ __device__ constexpr uint32_t class_type(int c) {
+    return c == CLS_DIFFUSE ? PT_MAT_DIFFUSE : c == CLS_MICRO ? PT_MAT_MICROFACET
+                                             : c == CLS_DISNEY ? PT_MAT_DISNEY : PT_MAT_HAIR;
+}
+
 // ---- shade: one bounce of RayGen's loop body (Shaders.hlsl:108-627) --------
-template <bool INLINE>
+// CLS == CLS_ANY: every path of the ray queue, events dispatched at run time
+// (media scenes).  Otherwise the paths of one shading class, whose event and
+// material type are then compile-time facts: each class gets a small kernel.
+template <bool INLINE, int CLS>
 __global__ void __launch_bounds__(kBlock) k_shade(WaveArgs A) {
     const DevScene &S = A.S;
-    uint32_t n = *(volatile uint32_t *)A.cntIn;
+    uint32_t n = CLS == CLS_ANY ? *(volatile uint32_t *)A.cntIn : *(volatile uint32_t *)(A.cntCls + CLS);
     uint32_t iters = (n + gridDim.x * blockDim.x - 1) / (gridDim.x * blockDim.x);
     for (uint32_t it = 0; it < iters; it++) {
-        uint32_t i = (it * gridDim.x + blockIdx.x) * blockDim.x + threadIdx.x;
-        bool active = i < n;
+        uint32_t q = (it * gridDim.x + blockIdx.x) * blockDim.x + threadIdx.x;
+        bool active = q < n;
+        uint32_t i = q;
+        if (CLS != CLS_ANY && active) i = A.cls[(size_t)(CLS < 0 ? 0 : CLS) * A.clsStride + q];
         bool cont = false;
         uint32_t slot = 0;
         float3 thr = v3(1.0f), Lo = v3(0.0f);
@@ -342,14 +380,15 @@ __global__ void __launch_bounds__(kBlock) k_shade(WaveArgs A) {
                 }
             }
             if (volScat) {
-            } else if (!hit) {  // Shaders.hlsl:188-212
+            } else if (CLS == CLS_MISS || (CLS == CLS_ANY && !hit)) {  // Shaders.hlsl:188-212
                 float3 env = eval_env(S, rd);
                 if (lastPdf == 0.0f) Lo += thr * env;
                 else Lo += thr * env * balance(lastPdf, env_pdf(S, A.envMode, rd));
-            } else {
+            } else if (CLS != CLS_MISS) {
                 uint32_t mesh = __ldg(S.triMesh + gid);
                 uint32_t prim = gid - __ldg(S.meshFirstTri + mesh);
                 const pt_material m = S.mats[mesh];
+                const uint32_t type = CLS >= CLS_DIFFUSE ? class_type(CLS) : m.type;
                 uint32_t i0, i1, i2;
                 tri_vidx(S, mesh, prim, i0, i1, i2);
                 float bx = h4.z, by = h4.w, w0 = 1.0f - bx - by;
@@ -362,14 +401,14 @@ __global__ void __launch_bounds__(kBlock) k_shade(WaveArgs A) {
                 bool back = dot(Ng, rd) > 0.0f;
                 if (back) Ng = -Ng;
                 if (dot(N, Ng) < 0.0f) N = -N;
-                if (m.isEmitter) {  // Shaders.hlsl:317-335
+                if (CLS == CLS_EMIT || (CLS == CLS_ANY && m.isEmitter)) {  // Shaders.hlsl:317-335
                     float3 rad = make_float3(m.radiance[0], m.radiance[1], m.radiance[2]);
                     if (lastPdf == 0.0f) Lo += thr * rad;
                     else Lo += thr * rad * balance(lastPdf, emitter_pdf_sa(S, m, hp, ro, N));
-                } else {
+                } else if (CLS != CLS_EMIT) {
                     float3 T, B;
                     float h = 0.0f;
-                    if (m.type == PT_MAT_HAIR) {  // Shaders.hlsl:340-387
+                    if (type == PT_MAT_HAIR) {  // Shaders.hlsl:340-387
                         float hu = __ldg(S.uv + 2 * i0) * w0 + __ldg(S.uv + 2 * i1) * bx + __ldg(S.uv + 2 * i2) * by;
                         float hv = __ldg(S.uv + 2 * i0 + 1) * w0 + __ldg(S.uv + 2 * i1 + 1) * bx +
                                    __ldg(S.uv + 2 * i2 + 1) * by;
@@ -402,12 +441,12 @@ __global__ void __launch_bounds__(kBlock) k_shade(WaveArgs A) {
                         }
                     }
                     float3 wil = to_local(-rd, T, B, N);
-                    if (m.type == PT_MAT_MIRROR) {  // Shaders.hlsl:419-427
+                    if (type == PT_MAT_MIRROR) {  // Shaders.hlsl:419-427
                         nd = reflect(rd, N);
                         no = hp + Ng * 0.001f;
                         lastPdf = 0.0f;
                         cont = true;
-                    } else if (m.type == PT_MAT_DIELECTRIC) {  // Shaders.hlsl:429-472
+                    } else if (type == PT_MAT_DIELECTRIC) {  // Shaders.hlsl:429-472
                         float etaI = back ? m.intIOR : m.extIOR, etaT = back ? m.extIOR : m.intIOR;
                         float Fr = fresnel(dot(-rd, N), etaI, etaT);
                         bool refr = false;
@@ -421,10 +460,11 @@ __global__ void __launch_bounds__(kBlock) k_shade(WaveArgs A) {
                         lastPdf = 0.0f;
                         if (refr) eta *= etaI / etaT;
                         cont = true;
-                    } else if (m.type == PT_MAT_DIFFUSE || m.type == PT_MAT_MICROFACET || m.type == PT_MAT_DISNEY ||
-                               m.type == PT_MAT_HAIR) {  // Shaders.hlsl:473-511
-                        float3 ra = nee_area<INLINE>(A, hp, N, Ng, T, B, wil, m, h, rng, neeA);
-                        float3 re = nee_env<INLINE>(A, hp, N, Ng, T, B, wil, m, h, rng, neeE);
+                    } else if (CLS != CLS_DELTA &&
+                               (type == PT_MAT_DIFFUSE || type == PT_MAT_MICROFACET || type == PT_MAT_DISNEY ||
+                                type == PT_MAT_HAIR)) {  // Shaders.hlsl:473-511
+                        float3 ra = nee_area<INLINE>(A, hp, N, Ng, T, B, wil, type, m, h, rng, neeA);
+                        float3 re = nee_env<INLINE>(A, hp, N, Ng, T, B, wil, type, m, h, rng, neeE);
                         if (INLINE) {
                             Lo += thr * ra;
                             Lo += thr * re;
@@ -435,14 +475,14 @@ __global__ void __launch_bounds__(kBlock) k_shade(WaveArgs A) {
                             st.w |= kFlagPending;
                         }
                         float u[4];
-                        int k = material_sample_dims(m, wil);
+                        int k = material_sample_dims_t(type, wil);
                         for (int j = 0; j < k; j++) u[j] = next_float(rng, S.sobol1);
                         float3 wol;
                         float bp;
-                        float3 wt = material_sample(wil, u, m, h, wol, bp);
+                        float3 wt = material_sample_t(type, wil, u, m, h, wol, bp);
                         if (!(bp <= 0.0f || (wt.x == 0.0f && wt.y == 0.0f && wt.z == 0.0f))) {
                             float3 ww = to_world(wol, T, B, N);
-                            float3 on = m.type == PT_MAT_HAIR ? (dot(ww, Ng) >= 0.0f ? Ng : -Ng) : Ng;
+                            float3 on = type == PT_MAT_HAIR ? (dot(ww, Ng) >= 0.0f ? Ng : -Ng) : Ng;
                             no = offset_origin(hp, on, on);
                             nd = ww;
                             thr *= wt;
@@ -526,12 +566,20 @@ static int grid_for(pt_ctx *ctx, const void *fn) {
 int pt_wave_free(pt_ctx *ctx) {
     WaveBuffers &W = ctx->W;
     void *ps[] = {W.thr_pdf, W.lo_eta, W.pendA, W.pendE, W.rng, W.qslot[0], W.qslot[1], W.qo[0], W.qo[1],
-                  W.qd[0], W.qd[1], W.qhit, W.sslot, W.so, W.sd, W.sX, W.sthr, W.counters};
+                  W.qd[0], W.qd[1], W.qhit, W.cls, W.sslot, W.so, W.sd, W.sX, W.sthr, W.counters};
     for (void *p : ps)
         if (p) cudaFree(p);
     W = WaveBuffers{};
     return PT_OK;
 }
+
+// Bytes of wave state per path slot: 5 float4/uint4 of path state, two ray
+// queues (slot + origin + direction), the hit buffer, one entry in each
+// shading-class queue, and two shadow-queue
+// entries (slot + origin + direction + contribution + throughput).
+constexpr size_t kWaveBytesPerPath = 5 * 16 + 2 * (4 + 16 + 16) + 16 + 4 * CLS_N + 2 * (4 + 4 * 16);
+constexpr size_t kMaxWavePaths = (size_t)1 << 30;  // queue indices stay 32-bit (shadow queue: 2 per path)
+static_assert(kWaveBytesPerPath == 332, "wave state layout");
 
 static int wave_alloc(pt_ctx *ctx, size_t cap) {
     if (ctx->W.cap >= cap) return PT_OK;
@@ -544,6 +592,7 @@ static int wave_alloc(pt_ctx *ctx, size_t cap) {
     A((void **)&W.pendA, cap * 16); A((void **)&W.pendE, cap * 16); A((void **)&W.rng, cap * 16);
     for (int k = 0; k < 2; k++) { A((void **)&W.qslot[k], cap * 4); A((void **)&W.qo[k], cap * 16); A((void **)&W.qd[k], cap * 16); }
     A((void **)&W.qhit, cap * 16);
+    A((void **)&W.cls, cap * 4 * CLS_N);
     A((void **)&W.sslot, sc * 4); A((void **)&W.so, sc * 16); A((void **)&W.sd, sc * 16);
     A((void **)&W.sX, sc * 16); A((void **)&W.sthr, sc * 16);
     A((void **)&W.counters, 64);
@@ -559,7 +608,18 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
     const uint32_t W = P->width, H = P->height;
     const uint64_t npix = (uint64_t)W * H;
     const uint64_t total = npix * P->spp;
-    size_t cap = P->wave_paths ? P->wave_paths : (size_t)1 << 21;
+    // Default wave: the whole render when its state fits in half of the free
+    // device memory.  Each bounce of a wave ends with a latency-bound tail (a
+    // few slow traversals), so fewer, larger waves amortise it; 59 M paths of
+    // a 1280 x 720 x 64 frame take ~18 GB.
+    size_t cap = P->wave_paths;
+    if (!cap) {
+        size_t freeB = 0, totalB = 0;
+        if (cudaMemGetInfo(&freeB, &totalB) != cudaSuccess) freeB = (size_t)4 << 30;
+        size_t fit = (freeB / 2 + (ctx->W.cap ? ctx->W.cap * kWaveBytesPerPath : 0) / 2) / kWaveBytesPerPath;
+        cap = (size_t)std::min<uint64_t>(total, std::min<size_t>(fit, kMaxWavePaths));
+        cap = std::max<size_t>(cap, (size_t)1 << 16);
+    }
     if (npix <= cap) cap = (cap / npix) * npix;
     if (cap > total) cap = (size_t)total;
     if (cap == 0) return PT_OK;
@@ -568,12 +628,18 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
     cudaStream_t st = ctx->stream;
     WaveBuffers &B = ctx->W;
     const bool inl = ctx->S.numVols > 0;
-    static int gExt = 0, gShade = 0, gShadeI = 0, gShadow = 0;
+    using Kernel = void (*)(WaveArgs);
+    static const Kernel kShadeCls[CLS_N] = {k_shade<false, CLS_MISS>,    k_shade<false, CLS_EMIT>,
+                                            k_shade<false, CLS_DELTA>,   k_shade<false, CLS_DIFFUSE>,
+                                            k_shade<false, CLS_MICRO>,   k_shade<false, CLS_DISNEY>,
+                                            k_shade<false, CLS_HAIR>};
+    static int gExt = 0, gExtC = 0, gShadeI = 0, gShadow = 0, gCls[CLS_N];
     if (!gExt) {
-        gExt = grid_for(ctx, (const void *)k_extend);
-        gShade = grid_for(ctx, (const void *)k_shade<false>);
-        gShadeI = grid_for(ctx, (const void *)k_shade<true>);
+        gExt = grid_for(ctx, (const void *)k_extend<false>);
+        gExtC = grid_for(ctx, (const void *)k_extend<true>);
+        gShadeI = grid_for(ctx, (const void *)k_shade<true, CLS_ANY>);
         gShadow = grid_for(ctx, (const void *)k_shadow);
+        for (int c = 0; c < CLS_N; c++) gCls[c] = grid_for(ctx, (const void *)kShadeCls[c]);
     }
     cudaEvent_t ev[2];
     cudaEventCreate(&ev[0]);
@@ -591,6 +657,9 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
     A.qhit = B.qhit;
     A.sslot = B.sslot; A.so = B.so; A.sd = B.sd; A.sX = B.sX; A.sthr = B.sthr;
     A.cntShadow = B.counters + 2;
+    A.cntCls = B.counters + 8;
+    A.cls = B.cls;
+    A.clsStride = (uint32_t)B.cap;
     A.rayTotals = (unsigned long long *)(B.counters + 4);
     A.err = ctx->d_err;
     A.shadowCap = (uint32_t)(2 * B.cap);
@@ -626,13 +695,25 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
             A.cntOut = B.counters + (1 - cur);
             cudaMemsetAsync(A.cntOut, 0, 4, st);
             cudaMemsetAsync(A.cntShadow, 0, 4, st);
-            begin(STG_EXTEND);
-            k_extend<<<gExt, kBlock, 0, st>>>(A);
-            end();
-            begin(STG_SHADE);
-            if (inl) k_shade<true><<<gShadeI, kBlock, 0, st>>>(A);
-            else k_shade<false><<<gShade, kBlock, 0, st>>>(A);
-            end();
+            if (inl) {
+                begin(STG_EXTEND);
+                k_extend<false><<<gExt, kBlock, 0, st>>>(A);
+                end();
+                begin(STG_SHADE);
+                k_shade<true, CLS_ANY><<<gShadeI, kBlock, 0, st>>>(A);
+                end();
+            } else {
+                cudaMemsetAsync(A.cntCls, 0, CLS_N * sizeof(uint32_t), st);
+                begin(STG_EXTEND);
+                k_extend<true><<<gExtC, kBlock, 0, st>>>(A);
+                end();
+                for (int c = 0; c < CLS_N; c++) {
+                    if (!((ctx->clsMask >> c) & 1u)) continue;
+                    begin(STG_SHADE);
+                    kShadeCls[c]<<<gCls[c], kBlock, 0, st>>>(A);
+                    end();
+                }
+            }
             if (!inl) {
                 begin(STG_SHADOW);
                 k_shadow<<<gShadow, kBlock, 0, st>>>(A);

@@ -71,6 +71,31 @@ uint32_t nori_materials(void *scene, pt_material *out, uint32_t maxCount) {
     return (uint32_t)mats.size();
 }
 
+// One flattened scene array (no GPU needed): which = 0 positions, 1 normals,
+// 2 texcoords, 3 tangents (floats), 4 indices (u32), 5 envmap RGB (floats),
+// 6 envmap width.  Copies into out when it is not NULL; returns the element
+// count (the width for 6).
+uint64_t nori_flat(void *scene, int which, void *out) {
+    const Scene *s = static_cast<const Scene *>(scene);
+    std::vector<float> pos, nrm, uv, tan, env;
+    std::vector<uint32_t> idx;
+    std::vector<pt_material> mats;
+    std::vector<pt_volume> vols;
+    std::vector<std::vector<float>> grids;
+    std::vector<pt_grid> gd;
+    uint32_t w, h;
+    flattenScene(s, pos, nrm, uv, tan, idx, mats, env, w, h, vols, grids, gd);
+    const std::vector<float> *f[] = {&pos, &nrm, &uv, &tan, nullptr, &env};
+    if (which == 6) return w;
+    if (which == 4) {
+        if (out) std::memcpy(out, idx.data(), idx.size() * 4);
+        return idx.size();
+    }
+    if (which < 0 || which > 5) return 0;
+    if (out) std::memcpy(out, f[which]->data(), f[which]->size() * 4);
+    return f[which]->size();
+}
+
 // Render spp samples from sample_offset with the scene's GPU integrator into
 // host films (4 x W x H floats each; added to).  Returns 0 or -1 (err set).
 int nori_render(void *scene, uint32_t spp, uint32_t sample_offset, float *sum, float *comp, pt_stats *stats,

