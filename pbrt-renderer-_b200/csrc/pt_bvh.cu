@@ -282,14 +282,17 @@ __global__ void k_collapse(CollapseIn C, const int2 *__restrict__ qin, uint32_t 
         qhx[s] = (uint8_t)min(255.0f, fmaxf(0.0f, ceilf(__fmul_ru(__fsub_ru(chi[i].x, nlo.x), ix))));
         qhy[s] = (uint8_t)min(255.0f, fmaxf(0.0f, ceilf(__fmul_ru(__fsub_ru(chi[i].y, nlo.y), iy))));
         qhz[s] = (uint8_t)min(255.0f, fmaxf(0.0f, ceilf(__fmul_ru(__fsub_ru(chi[i].z, nlo.z), iz))));
+        // meta = (hit bits << 5) | bit position: an internal child sets bit
+        // 24 + slot, a leaf sets one bit per triangle from its offset up
+        // (< 24: at most 8 leaves of kLeafMax <= 3 triangles).
         if ((imask >> s) & 1u) {
-            meta[s] = (uint8_t)(0x20u | s);
+            meta[s] = (uint8_t)(0x20u | 24u | s);
             qout[qpos + rank] = make_int2(r, (int)(childBase + rank));
             rank++;
         } else {
             uint32_t first = r >= 0 ? C.rangeFirst[r] : (uint32_t)(~r);
             uint32_t count = r >= 0 ? (C.rangeLast[r] - first + 1) : 1u;
-            meta[s] = (uint8_t)((count << 5) | toff);
+            meta[s] = (uint8_t)((((1u << count) - 1u) << 5) | toff);
             for (uint32_t k = 0; k < count; k++) {
                 uint32_t g = C.sorted[first + k];
                 uint32_t mesh = C.triMesh[g];

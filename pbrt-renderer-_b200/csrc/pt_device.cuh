@@ -25,10 +25,12 @@ struct DevGrid {
 //   n4 = (qhi.y[0..3], qhi.y[4..7], qhi.z[0..3], qhi.z[4..7])
 // Child i's box is p + [qlo_i, qhi_i] * 2^(e - 127) per axis.  imask bit i:
 // child i is an internal node (index child_base + rank of i among internal
-// children); otherwise meta[i] = 0 (empty) or (count << 5) | offset: a leaf of
-// `count` (1..3) triangles at tri_base + offset.  Child slots follow the
-// octant of the child's centre within the node, so visiting slot (k ^ oct)
-// for k = 0..7 is near-to-far for rays of octant oct.
+// children).  meta[i] = (bits << 5) | position, one formula for every child:
+// a hit ORs bits << position into the node's hit mask.  Internal child:
+// bits 1 at position 24 + i; leaf of c (1..3) triangles at tri_base + offset:
+// bits 2^c - 1 at position offset (< 24); empty slot: 0.  Child slots follow
+// the octant of the child's centre within the node, so visiting slot
+// (k ^ oct) for k = 0..7 is near-to-far for rays of octant oct.
 struct BVH8Node { uint4 n[5]; };
 
 struct DevScene {
@@ -529,15 +531,19 @@ __device__ __forceinline__ void intersect_node(const DevScene &S, uint32_t ni, c
     uint4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2), n3 = __ldg(np + 3), n4 = __ldg(np + 4);
     float px = __uint_as_float(n0.x), py = __uint_as_float(n0.y), pz = __uint_as_float(n0.z);
     uint32_t ex = n0.w & 0xFFu, ey = (n0.w >> 8) & 0xFFu, ez = (n0.w >> 16) & 0xFFu;
-    uint32_t imask = n0.w >> 24;
     float sx = __uint_as_float(ex << 23) * r.idir.x;
     float sy = __uint_as_float(ey << 23) * r.idir.y;
     float sz = __uint_as_float(ez << 23) * r.idir.z;
     float ox = (px - r.o.x) * r.idir.x, oy = (py - r.o.y) * r.idir.y, oz = (pz - r.o.z) * r.idir.z;
     gBase = n1.x;
     tBase = n1.y;
-    gImask = imask;
-    uint32_t gh = 0, th = 0;
+    gImask = n0.w >> 24;
+    // internal children (meta bits 3 and 4 set: position >= 24) take their
+    // position XOR the ray octant, four meta bytes at a time
+    uint32_t oct4 = r.oct * 0x01010101u;
+    uint32_t ma = n1.z ^ (((n1.z >> 3) & (n1.z >> 4) & 0x01010101u) * 7u & oct4);
+    uint32_t mb = n1.w ^ (((n1.w >> 3) & (n1.w >> 4) & 0x01010101u) * 7u & oct4);
+    uint32_t hits = 0;
     // near/far plane words per axis by ray sign
     uint32_t lxa = n2.x, lxb = n2.y, hxa = n3.z, hxb = n3.w;
     uint32_t lya = n2.z, lyb = n2.w, hya = n4.x, hyb = n4.y;
@@ -556,62 +562,118 @@ __device__ __forceinline__ void intersect_node(const DevScene &S, uint32_t ni, c
         float tfz = fmaf(byte_as_float(i < 4 ? hza : hzb, sel), sz, oz);
         float t0 = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
         float t1 = fminf(fminf(tfx, tfy), fminf(tfz, tmax));
-        uint32_t meta = byte_of(i < 4 ? n1.z : n1.w, sel);
-        bool hit = t0 <= t1 * 1.00000024f;
-        if ((imask >> i) & 1u) {
-            if (hit) gh |= 1u << (i ^ r.oct);
-        } else if (meta != 0u && hit) {
-            th |= ((1u << (meta >> 5)) - 1u) << (meta & 31u);
-        }
+        uint32_t meta = byte_of(i < 4 ? ma : mb, sel);
+        if (t0 <= t1 * 1.00000024f) hits |= (meta >> 5) << (meta & 31u);
     }
-    gHits = gh;
-    tHits = th;
+    gHits = hits >> 24;
+    tHits = hits & 0x00FFFFFFu;
 }
 
-// Closest hit (TraceClosestInline semantics for opaque geometry).  Returns
-// false and sets *err on stack overflow.
+// Resumable traversal state: the kernels with per-lane ray replacement run
+// it one node at a time; trace_closest / trace_shadow run it to the end.
+// The node stack is a separate object: indexed at run time, it lives in
+// local memory, and must not drag the scalar state there with it.
+struct Trav {
+    RayPre r;
+    float tmin, tmax;
+    uint32_t gBase, gImask, gHits, tBase, tHits;
+    uint32_t visits;
+    int sp;
+};
+struct TravStack {
+    uint32_t base[kTraversalStack], mask[kTraversalStack];
+};
+__device__ __forceinline__ void trav_init(Trav &T, const DevScene &S, float3 o, float3 d, float tmin, float tmax) {
+    T.r = ray_pre(o, d);
+    T.tmin = tmin;
+    T.tmax = tmax;
+    T.sp = 0;
+    T.visits = 1;
+    T.gHits = T.tHits = 0;
+    if (S.numNodes) intersect_node(S, 0, T.r, tmin, tmax, T.gBase, T.gImask, T.gHits, T.tBase, T.tHits);
+}
+// Next node: pop the nearest pending child (from this node or the stack) and
+// intersect it.  Returns false when nothing is left (or on an error, which
+// is flagged in *err).
+__device__ __forceinline__ bool trav_next_node(Trav &T, TravStack &K, const DevScene &S, float tmax, uint32_t *err) {
+    if (T.gHits == 0) {
+        if (T.sp == 0) return false;
+        --T.sp;
+        T.gBase = K.base[T.sp];
+        T.gImask = K.mask[T.sp] >> 8;
+        T.gHits = K.mask[T.sp] & 0xFFu;
+    }
+    uint32_t k = __ffs(T.gHits) - 1;
+    T.gHits &= T.gHits - 1;
+    uint32_t slot = k ^ T.r.oct;
+    uint32_t child = T.gBase + __popc(T.gImask & ((1u << slot) - 1u));
+    if (++T.visits > S.numNodes || child >= S.numNodes) {
+        if (err) atomicOr(err, 4u);
+        return false;
+    }
+    if (T.gHits) {
+        if (T.sp == kTraversalStack) {
+            if (err) atomicOr(err, 1u);
+            return false;
+        }
+        K.base[T.sp] = T.gBase;
+        K.mask[T.sp] = (T.gImask << 8) | T.gHits;
+        ++T.sp;
+    }
+    intersect_node(S, child, T.r, T.tmin, tmax, T.gBase, T.gImask, T.gHits, T.tBase, T.tHits);
+    return true;
+}
+// Closest-hit step: the current node's triangles, then the next node.
+// Returns true when the traversal has finished.
+__device__ __forceinline__ bool trav_step_closest(Trav &T, TravStack &K, const DevScene &S, Hit &h, uint32_t *err) {
+    while (T.tHits) {
+        uint32_t j = __ffs(T.tHits) - 1;
+        T.tHits &= T.tHits - 1;
+        const float4 *tp = S.tri + 3u * (T.tBase + j);
+        float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+        float t, u, v;
+        if (tri_test(T.r.o, T.r.d, a, b, c, T.tmin, h.t, t, u, v)) {
+            uint32_t g = __float_as_uint(a.w);
+            if (t < h.t || (t == h.t && g < h.gid)) { h.t = t; h.u = u; h.v = v; h.gid = g; }
+        }
+    }
+    return !trav_next_node(T, K, S, h.t, err);
+}
+// Any-hit step (shadow rays).  Sets `occluded` and returns true at the first
+// opaque hit; mirror/dielectric hits multiply `trans` by (1 - Fr).
+__device__ __forceinline__ bool trav_step_shadow(Trav &T, TravStack &K, const DevScene &S, float3 &trans,
+                                                 bool &occluded, uint32_t *err) {
+    while (T.tHits) {
+        uint32_t j = __ffs(T.tHits) - 1;
+        T.tHits &= T.tHits - 1;
+        const float4 *tp = S.tri + 3u * (T.tBase + j);
+        float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+        float t, u, v;
+        if (tri_test(T.r.o, T.r.d, a, b, c, T.tmin, T.tmax, t, u, v)) {
+            uint32_t g = __float_as_uint(a.w);
+            if (!S.hasGlass) { occluded = true; return true; }
+            uint32_t mesh = __ldg(S.triMesh + g);
+            const pt_material &m = S.mats[mesh];
+            if (m.type != PT_MAT_MIRROR && m.type != PT_MAT_DIELECTRIC) { occluded = true; return true; }
+            float3 Ng = normalize(cross(make_float3(b.x, b.y, b.z), make_float3(c.x, c.y, c.z)));
+            float Fr = fresnel(fabsf(dot(T.r.d, Ng)), m.extIOR, m.intIOR);
+            trans = trans * (1.0f - Fr);
+        }
+    }
+    return !trav_next_node(T, K, S, T.tmax, err);
+}
+
+// Closest hit (TraceClosestInline semantics for opaque geometry).  Sets *err
+// on stack overflow or a runaway visit count.
 __device__ __forceinline__ Hit trace_closest(const DevScene &S, float3 o, float3 d, float tmin, float tmax,
                                              uint32_t *err) {
     Hit h;
     h.t = tmax; h.u = 0.0f; h.v = 0.0f; h.gid = 0xFFFFFFFFu;
     if (S.numNodes == 0) return h;
-    RayPre r = ray_pre(o, d);
-    uint32_t stBase[kTraversalStack], stMask[kTraversalStack];
-    int sp = 0;
-    uint32_t visits = 1;
-    uint32_t gBase, gImask, gHits, tBase, tHits;
-    intersect_node(S, 0, r, tmin, h.t, gBase, gImask, gHits, tBase, tHits);
-    for (;;) {
-        while (tHits) {
-            uint32_t j = __ffs(tHits) - 1;
-            tHits &= tHits - 1;
-            const float4 *tp = S.tri + 3u * (tBase + j);
-            float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
-            float t, u, v;
-            if (tri_test(o, d, a, b, c, tmin, h.t, t, u, v)) {
-                uint32_t g = __float_as_uint(a.w);
-                if (t < h.t || (t == h.t && g < h.gid)) { h.t = t; h.u = u; h.v = v; h.gid = g; }
-            }
-        }
-        if (gHits == 0) {
-            if (sp == 0) break;
-            --sp;
-            gBase = stBase[sp];
-            gImask = stMask[sp] >> 8;
-            gHits = stMask[sp] & 0xFFu;
-        }
-        uint32_t k = __ffs(gHits) - 1;
-        gHits &= gHits - 1;
-        uint32_t slot = k ^ r.oct;
-        uint32_t child = gBase + __popc(gImask & ((1u << slot) - 1u));
-        if (++visits > S.numNodes || child >= S.numNodes) { if (err) atomicOr(err, 4u); break; }
-        if (gHits) {
-            if (sp == kTraversalStack) { if (err) atomicOr(err, 1u); break; }
-            stBase[sp] = gBase;
-            stMask[sp] = (gImask << 8) | gHits;
-            ++sp;
-        }
-        intersect_node(S, child, r, tmin, h.t, gBase, gImask, gHits, tBase, tHits);
+    Trav T;
+    TravStack K;
+    trav_init(T, S, o, d, tmin, tmax);
+    while (!trav_step_closest(T, K, S, h, err)) {
     }
     return h;
 }
@@ -623,51 +685,13 @@ __device__ __forceinline__ bool trace_shadow(const DevScene &S, float3 o, float3
                                              float3 &trans, uint32_t *err) {
     trans = v3(1.0f);
     if (S.numNodes == 0) return false;
-    RayPre r = ray_pre(o, d);
-    uint32_t stBase[kTraversalStack], stMask[kTraversalStack];
-    int sp = 0;
-    uint32_t visits = 1;
-    uint32_t gBase, gImask, gHits, tBase, tHits;
-    intersect_node(S, 0, r, tmin, tmax, gBase, gImask, gHits, tBase, tHits);
-    for (;;) {
-        while (tHits) {
-            uint32_t j = __ffs(tHits) - 1;
-            tHits &= tHits - 1;
-            const float4 *tp = S.tri + 3u * (tBase + j);
-            float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
-            float t, u, v;
-            if (tri_test(o, d, a, b, c, tmin, tmax, t, u, v)) {
-                uint32_t g = __float_as_uint(a.w);
-                if (!S.hasGlass) return true;
-                uint32_t mesh = __ldg(S.triMesh + g);
-                const pt_material &m = S.mats[mesh];
-                if (m.type != PT_MAT_MIRROR && m.type != PT_MAT_DIELECTRIC) return true;
-                float3 Ng = normalize(cross(make_float3(b.x, b.y, b.z), make_float3(c.x, c.y, c.z)));
-                float Fr = fresnel(fabsf(dot(d, Ng)), m.extIOR, m.intIOR);
-                trans = trans * (1.0f - Fr);
-            }
-        }
-        if (gHits == 0) {
-            if (sp == 0) break;
-            --sp;
-            gBase = stBase[sp];
-            gImask = stMask[sp] >> 8;
-            gHits = stMask[sp] & 0xFFu;
-        }
-        uint32_t k = __ffs(gHits) - 1;
-        gHits &= gHits - 1;
-        uint32_t slot = k ^ r.oct;
-        uint32_t child = gBase + __popc(gImask & ((1u << slot) - 1u));
-        if (++visits > S.numNodes || child >= S.numNodes) { if (err) atomicOr(err, 4u); break; }
-        if (gHits) {
-            if (sp == kTraversalStack) { if (err) atomicOr(err, 1u); break; }
-            stBase[sp] = gBase;
-            stMask[sp] = (gImask << 8) | gHits;
-            ++sp;
-        }
-        intersect_node(S, child, r, tmin, tmax, gBase, gImask, gHits, tBase, tHits);
+    Trav T;
+    TravStack K;
+    trav_init(T, S, o, d, tmin, tmax);
+    bool occ = false;
+    while (!trav_step_shadow(T, K, S, trans, occ, err)) {
     }
-    return false;
+    return occ;
 }
 
 }  // namespace pt

@@ -5,12 +5,15 @@
 //
 //   raygen -> [ extend -> shade -> shadow ] x max_depth -> film
 //
-// * extend: closest-hit BVH8 traversal of the ray queue -> hit records.
-// * shade: one thread per queued path: folds the previous bounce's NEE
-//   results into Lo, handles miss / emitter / surface events, samples NEE
-//   (shadow rays to the shadow queue) and the BSDF (next ray queue), Russian
-//   roulette.  Path slots stay fixed; queues hold slot ids and are compacted
-//   with one atomic per warp (ballot + popc).
+// * extend: closest-hit BVH8 traversal of the ray queue -> hit records, and
+//   each path's queue position into the queue of its shading class (miss,
+//   emitter, delta, diffuse, microfacet, Disney, hair).
+// * shade: one kernel per shading class present in the scene, its material
+//   type fixed at compile time; one thread per path: folds the previous
+//   bounce's NEE results into Lo, handles the miss / emitter / surface event,
+//   samples NEE (shadow rays to the shadow queue) and the BSDF (next ray
+//   queue), Russian roulette.  Path slots stay fixed; queues hold slot ids
+//   and are compacted with one atomic per warp (ballot + popc).
 // * shadow: any-hit traversal; writes thr * (X * transmission) or thr * 0
 //   into the path's pending slot, folded in by the next shade (or by film),
 //   so Lo receives the same float additions in the same order as RayGen.
@@ -66,9 +69,25 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t *counter, bool pred) {
     return base + __popc(mask & ((1u << lane_id()) - 1u));
 }
 
+// Pixel of position p of the path order.  Positions run over 8 x 4 pixel
+// tiles (one warp's paths cover one tile: compact bundles of camera rays),
+// tiles row by row; pixels right of the last full tile column or below the
+// last full tile row follow in row-major order.  A bijection on [0, W*H).
+__device__ __forceinline__ uint32_t tile_pixel(const WaveArgs &A, uint32_t p) {
+    const uint32_t W = A.width, Wt = A.width / 8u, Ht = A.height / 4u;
+    const uint32_t full = 32u * Wt * Ht;
+    if (p < full) {
+        uint32_t t = p >> 5, w = p & 31u;
+        return ((t / Wt) * 4u + (w >> 3)) * W + (t % Wt) * 8u + (w & 7u);
+    }
+    uint32_t q = p - full, rw = W - 8u * Wt;
+    if (q < 4u * Ht * rw) return (q / rw) * W + 8u * Wt + q % rw;
+    q -= 4u * Ht * rw;
+    return (4u * Ht + q / W) * W + q % W;
+}
 __device__ __forceinline__ void path_coords(const WaveArgs &A, uint32_t slot, uint32_t &pix, uint32_t &frame) {
     uint64_t pid = A.waveStart + slot;
-    pix = (uint32_t)(pid % A.npix);
+    pix = tile_pixel(A, (uint32_t)(pid % A.npix));
     frame = A.sampleOffset + (uint32_t)(pid / A.npix);
 }
 __device__ __forceinline__ Rng load_rng(const WaveArgs &A, uint32_t slot, uint4 st) {
@@ -134,37 +153,45 @@ __device__ __forceinline__ void class_append(const WaveArgs &A, int c, uint32_t 
 
 // ---- extend: closest hit (+ sort into shading classes) -----------------------
 template <bool CLASSIFY>
+__device__ __forceinline__ void finish_extend(const WaveArgs &A, uint32_t i, const Hit &h) {
+    A.qhit[i] = make_float4(h.t, __uint_as_float(h.gid), h.u, h.v);
+    if (CLASSIFY) {
+        bool hit = h.gid != 0xFFFFFFFFu;
+        bool emitter = false;
+        uint32_t type = 0;
+        if (hit) {
+            const pt_material *m = A.S.mats + __ldg(A.S.triMesh + h.gid);
+            type = __ldg(&m->type);
+            emitter = __ldg(&m->isEmitter) != 0u;
+        }
+        class_append(A, shade_class(hit, emitter, type), i);
+    }
+}
+template <bool CLASSIFY>
 __global__ void __launch_bounds__(kBlock) k_extend(WaveArgs A) {
-    uint32_t n = *(volatile uint32_t *)A.cntIn;
+    // grid-stride over the queue in order: the 32 rays of a warp are
+    // neighbours in the queue (coherent traversal), and the class queues and
+    // the next ray queue keep that order for the kernels that follow
+    const uint32_t n = *(volatile uint32_t *)A.cntIn;
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&A.rayTotals[0], (unsigned long long)n);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float4 o = A.qoIn[i], d = A.qdIn[i];
         Hit h = trace_closest(A.S, make_float3(o.x, o.y, o.z), make_float3(d.x, d.y, d.z), o.w, d.w, A.err);
-        A.qhit[i] = make_float4(h.t, __uint_as_float(h.gid), h.u, h.v);
-        if (CLASSIFY) {
-            bool hit = h.gid != 0xFFFFFFFFu;
-            bool emitter = false;
-            uint32_t type = 0;
-            if (hit) {
-                const pt_material *m = A.S.mats + __ldg(A.S.triMesh + h.gid);
-                type = __ldg(&m->type);
-                emitter = __ldg(&m->isEmitter) != 0u;
-            }
-            class_append(A, shade_class(hit, emitter, type), i);
-        }
+        finish_extend<CLASSIFY>(A, i, h);
     }
 }
 
 // ---- shadow: any hit -> pending NEE contribution ---------------------------
 __global__ void __launch_bounds__(kBlock) k_shadow(WaveArgs A) {
-    uint32_t n = *(volatile uint32_t *)A.cntShadow;
+    const uint32_t n = *(volatile uint32_t *)A.cntShadow;
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&A.rayTotals[1], (unsigned long long)n);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        float4 o = A.so[i], d = A.sd[i], X = A.sX[i], T = A.sthr[i];
-        uint32_t s = A.sslot[i];
+        float4 o = A.so[i], d = A.sd[i];
         float3 tr;
         bool occ = trace_shadow(A.S, make_float3(o.x, o.y, o.z), make_float3(d.x, d.y, d.z), o.w, d.w, tr, A.err);
-        float3 thr = make_float3(T.x, T.y, T.z);
+        float4 X = A.sX[i], Th = A.sthr[i];
+        uint32_t s = A.sslot[i];
+        float3 thr = make_float3(Th.x, Th.y, Th.z);
         float3 R = occ ? thr * v3(0.0f) : thr * (make_float3(X.x, X.y, X.z) * tr);
         float4 out = make_float4(R.x, R.y, R.z, 0.0f);
         if (s >> 31) A.pendE[s & 0x7FFFFFFFu] = out;
@@ -532,7 +559,7 @@ __global__ void k_film(WaveArgs A, float4 *sum, float4 *comp) {
     uint32_t cover = min(A.waveCount, A.npix);
     if (t >= cover) return;
     uint64_t first = A.waveStart, last = A.waveStart + A.waveCount;
-    uint32_t pix = (uint32_t)((first + t) % A.npix);
+    uint32_t pix = tile_pixel(A, (uint32_t)((first + t) % A.npix));
     float4 s = sum[pix], c = comp[pix];
     for (uint64_t pid = first + t; pid < last; pid += A.npix) {
         uint32_t slot = (uint32_t)(pid - first);
