@@ -141,6 +141,55 @@ def measured_peaks():
 EXTEND_DRAM_BYTES_PER_RAY = {"disney_envmap": 71.1}
 
 
+REF_SPP = 4096        # reference image: plain path tracing, samples [0, 4096)
+TTQ_TARGET = 1e-2     # relMSE bar
+TTQ_OFFSET = 1 << 20  # progressive renders draw samples from here on (independent of the reference)
+
+
+def relmse(x, ref):
+    """mean((x - ref)^2 / (ref^2 + 1e-2)) over pixels and RGB, the relMSE of
+    the reference's comparison tool (validation_tests/compare_exr.py:102)."""
+    return float(((x - ref) ** 2 / (ref ** 2 + 1e-2)).mean())
+
+
+def time_to_relmse(pt, ctx, stream, W, H, cam, depth, env_mode, chunk):
+    """Device time for plain path tracing to reach relMSE <= 1e-2 against a
+    4096-spp render of the same scene: progressive accumulation (the
+    reference's frame-by-frame accumulation) at 1, 2, 4, ... spp, timed with
+    CUDA events per render call; the first point at or below the bar gives
+    the time.  The radiance-cache form is not built (cached: null)."""
+    import torch
+
+    D = importlib.import_module("pbrt_b200.distributed")
+    ref = D.new_film(H, W, device="cuda")
+    for k in range(REF_SPP // chunk):
+        P = pt.render_params(W, H, chunk, cam, max_depth=depth, sample_offset=k * chunk, env_sampling=env_mode)
+        ctx.render(P, ref[0].data_ptr(), ref[1].data_ptr(), pt.PT_MEM_DEVICE)
+    ref_img = D.resolve(ref)
+    film = D.new_film(H, W, device="cuda")
+    done, total_ms, curve, reached = 0, 0.0, [], None
+    add = 1
+    while done < REF_SPP // 4:
+        P = pt.render_params(W, H, add, cam, max_depth=depth, sample_offset=TTQ_OFFSET + done, env_sampling=env_mode)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        ctx.render(P, film[0].data_ptr(), film[1].data_ptr(), pt.PT_MEM_DEVICE)
+        b.record(stream)
+        torch.cuda.synchronize()
+        total_ms += a.elapsed_time(b)
+        done += add
+        e = relmse(D.resolve(film), ref_img)
+        curve.append([done, round(e, 6), round(total_ms / 1e3, 5)])
+        if e <= TTQ_TARGET:
+            reached = (done, total_ms / 1e3)
+            break
+        add = done  # double the sample count
+    return {"target": TTQ_TARGET, "reference_spp": REF_SPP, "plain": {
+        "seconds": None if reached is None else round(reached[1], 5),
+        "spp": None if reached is None else reached[0], "curve": curve}, "cached": None}
+
+
 def cpu_reference_run(pt, sc, cam, W, H, depth, seconds=15.0, prefer_reference=True):
     """Time the CPU implementation on a bounded sample of the workload:
     whole frames at 1 spp (the reference's one-sample dispatch), repeated
@@ -204,6 +253,7 @@ def main():
     ap.add_argument("--spp", type=int, default=0, help="override samples per pixel (profiling of small cases)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--wave-paths", type=int, default=0, help="paths in flight per wave (0 = library default)")
+    ap.add_argument("--no-ttq", action="store_true", help="skip the time-to-relMSE measurement")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -344,6 +394,8 @@ def main():
         "clocks": clk.summary(),
         "scene_upload_s": round(upload_s, 3),
     }
+    if world == 1 and not args.no_ttq:
+        line["time_to_relmse"] = time_to_relmse(pt, ctx, stream, W, H, cam, depth, env_mode, max(spp, 64))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, kind, cores, sample = cpu_reference_run(pt, sc, cam, W, H, depth, seconds=args.cpu_seconds)
         line["cpu_baseline"] = {"value": round(v, 4), "unit": "Mpaths/s", "cores": cores, "kind": kind,

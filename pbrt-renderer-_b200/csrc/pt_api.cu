@@ -332,6 +332,7 @@ int pt_destroy(pt_ctx *ctx) {
     if (!ctx) return PT_E_INVALID;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    pt_graph_free(ctx);
     ctx->free_scene();
     pt_wave_free(ctx);
     if (ctx->scratch) cudaFree(ctx->scratch);

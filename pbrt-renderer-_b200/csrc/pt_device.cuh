@@ -516,10 +516,23 @@ __device__ __forceinline__ RayPre ray_pre(float3 o, float3 d) {
 __device__ __forceinline__ uint32_t byte_of(uint32_t w, uint32_t i) { return (w >> (8u * i)) & 0xFFu; }
 // Byte `i` of w as a float, exactly (float)byte: one byte permute builds the
 // bits of 2^23 + byte (exponent 0x4B, byte in the low mantissa bits) and an
-// exact subtraction removes 2^23.  Keeps the 48 decodes per node on the ALU
-// and FMA pipes instead of the conversion unit.
+// exact subtraction removes 2^23.  Runs on the ALU and FMA pipes instead of
+// the conversion unit.
 __device__ __forceinline__ float byte_as_float(uint32_t w, uint32_t i) {
     return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u | i)) - 8388608.0f;
+}
+
+// Three-input float max / min (PTX 8.8, sm_100): the same value as two
+// chained fmaxf / fminf in one ALU instruction.
+__device__ __forceinline__ float fmax3(float a, float b, float c) {
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+__device__ __forceinline__ float fmin3(float a, float b, float c) {
+    float d;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
 }
 
 // Intersect the 8 children of node `ni`: internal hits (in near-to-far visit
@@ -554,14 +567,17 @@ __device__ __forceinline__ void intersect_node(const DevScene &S, uint32_t ni, c
 #pragma unroll
     for (uint32_t i = 0; i < 8; i++) {
         uint32_t sel = i & 3u;
-        float tnx = fmaf(byte_as_float(i < 4 ? lxa : lxb, sel), sx, ox);
-        float tfx = fmaf(byte_as_float(i < 4 ? hxa : hxb, sel), sx, ox);
-        float tny = fmaf(byte_as_float(i < 4 ? lya : lyb, sel), sy, oy);
-        float tfy = fmaf(byte_as_float(i < 4 ? hya : hyb, sel), sy, oy);
+        // x and y planes through the conversion unit, z through byte_as_float:
+        // both exact; the split balances the ALU, FMA and XU pipes (measured
+        // on B200: all-ALU and all-XU decodes are both slower)
+        float tnx = fmaf((float)byte_of(i < 4 ? lxa : lxb, sel), sx, ox);
+        float tfx = fmaf((float)byte_of(i < 4 ? hxa : hxb, sel), sx, ox);
+        float tny = fmaf((float)byte_of(i < 4 ? lya : lyb, sel), sy, oy);
+        float tfy = fmaf((float)byte_of(i < 4 ? hya : hyb, sel), sy, oy);
         float tnz = fmaf(byte_as_float(i < 4 ? lza : lzb, sel), sz, oz);
         float tfz = fmaf(byte_as_float(i < 4 ? hza : hzb, sel), sz, oz);
-        float t0 = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
-        float t1 = fminf(fminf(tfx, tfy), fminf(tfz, tmax));
+        float t0 = fmax3(tnx, tny, fmaxf(tnz, tmin));
+        float t1 = fmin3(tfx, tfy, fminf(tfz, tmax));
         uint32_t meta = byte_of(i < 4 ? ma : mb, sel);
         if (t0 <= t1 * 1.00000024f) hits |= (meta >> 5) << (meta & 31u);
     }

@@ -70,6 +70,19 @@ struct WaveBuffers {
     uint32_t *counters = nullptr;
 };
 
+// A render's launch sequence captured as a CUDA graph, with the configuration
+// it was captured for (everything baked into its launches).  The sample
+// offset is not baked: the kernels read it from device memory.
+struct RenderGraph {
+    cudaGraphExec_t exec = nullptr;
+    uint32_t width = 0, height = 0, spp = 0, maxDepth = 0, rngKind = 0, envSampling = 0;
+    pt_camera cam{};
+    size_t cap = 0;
+    const void *sum = nullptr, *comp = nullptr;
+    uint64_t sceneGen = 0, waveGen = 0;
+    uint64_t launches = 0;
+};
+
 struct pt_ctx {
     int device = 0;
     int numSMs = 148;
@@ -85,8 +98,10 @@ struct pt_ctx {
     uint32_t *d_morton = nullptr, *d_sorted = nullptr;
     int32_t *d_binChildren = nullptr;
     uint32_t *d_sobol1 = nullptr;
-    uint32_t *d_err = nullptr;
+    uint32_t *d_err = nullptr;  // [0] device error flags, [1] sample offset of the running render
     WaveBuffers W;
+    RenderGraph graph;
+    uint64_t sceneGen = 1, waveGen = 1;  // bumped when scene / wave buffers are replaced
     // scratch of the batch entry points
     void *scratch = nullptr;
     size_t scratchBytes = 0;
@@ -103,6 +118,7 @@ struct pt_ctx {
         return e;
     }
     void free_scene() {
+        sceneGen++;
         for (void *p : sceneAllocs) cudaFree(p);
         sceneAllocs.clear();
         hasScene = false;
@@ -118,3 +134,4 @@ int pt_build_bvh_device(pt_ctx *ctx, const uint32_t *d_meshFirstTri, uint32_t nu
 // pt_render.cu
 int pt_render_impl(pt_ctx *ctx, const pt_render_params *p, float *d_sum, float *d_comp, pt_stats *stats);
 int pt_wave_free(pt_ctx *ctx);
+void pt_graph_free(pt_ctx *ctx);

@@ -35,7 +35,7 @@ constexpr int kBlock = 256;
 struct WaveArgs {
     DevScene S;
     uint32_t width, height, npix;
-    uint32_t sampleOffset;   // sample index of path id 0 of this render call
+    const uint32_t *sampleOffset;  // -> sample index of path id 0 of this render call
     uint32_t rngKind, envMode, maxDepth;
     uint64_t waveStart;      // first path id of the wave
     uint32_t waveCount;
@@ -88,7 +88,7 @@ __device__ __forceinline__ uint32_t tile_pixel(const WaveArgs &A, uint32_t p) {
 __device__ __forceinline__ void path_coords(const WaveArgs &A, uint32_t slot, uint32_t &pix, uint32_t &frame) {
     uint64_t pid = A.waveStart + slot;
     pix = tile_pixel(A, (uint32_t)(pid % A.npix));
-    frame = A.sampleOffset + (uint32_t)(pid / A.npix);
+    frame = __ldg(A.sampleOffset) + (uint32_t)(pid / A.npix);
 }
 __device__ __forceinline__ Rng load_rng(const WaveArgs &A, uint32_t slot, uint4 st) {
     uint32_t pix, frame;
@@ -605,7 +605,10 @@ int pt_wave_free(pt_ctx *ctx) {
 // shading-class queue, and two shadow-queue
 // entries (slot + origin + direction + contribution + throughput).
 constexpr size_t kWaveBytesPerPath = 5 * 16 + 2 * (4 + 16 + 16) + 16 + 4 * CLS_N + 2 * (4 + 4 * 16);
-constexpr size_t kMaxWavePaths = (size_t)1 << 30;  // queue indices stay 32-bit (shadow queue: 2 per path)
+// Default wave cap: 2^26 paths (~22 GB of state).  Larger renders run as
+// several waves, whose tails are small at this size, instead of regrowing the
+// buffers (a free + malloc of tens of GB that would stall the render).
+constexpr size_t kMaxWavePaths = (size_t)1 << 26;
 static_assert(kWaveBytesPerPath == 332, "wave state layout");
 
 static int wave_alloc(pt_ctx *ctx, size_t cap) {
@@ -628,17 +631,117 @@ static int wave_alloc(pt_ctx *ctx, size_t cap) {
         return ctx->fail(PT_E_NOMEM, "wave buffers", cudaGetErrorString(e));
     }
     W.cap = cap;
+    ctx->waveGen++;
     return PT_OK;
+}
+
+namespace {
+using Kernel = void (*)(WaveArgs);
+const Kernel kShadeCls[CLS_N] = {k_shade<false, CLS_MISS>,  k_shade<false, CLS_EMIT>,    k_shade<false, CLS_DELTA>,
+                                 k_shade<false, CLS_DIFFUSE>, k_shade<false, CLS_MICRO>, k_shade<false, CLS_DISNEY>,
+                                 k_shade<false, CLS_HAIR>};
+int gExt = 0, gExtC = 0, gShadeI = 0, gShadow = 0, gCls[CLS_N];
+
+enum { STG_RAYGEN, STG_EXTEND, STG_SHADE, STG_SHADOW, STG_FILM, STG_N };
+struct Mark { int stage; cudaEvent_t a, b; };
+
+// Issues one render's work on a stream: directly (optionally with an event
+// pair around every launch), or into a stream capture.
+struct Enqueue {
+    cudaStream_t st;
+    bool timing;
+    std::vector<Mark> marks;
+    uint64_t launches = 0;
+    void begin(int stage) {
+        launches++;
+        if (!timing) return;
+        Mark m{stage, nullptr, nullptr};
+        cudaEventCreate(&m.a);
+        cudaEventCreate(&m.b);
+        cudaEventRecord(m.a, st);
+        marks.push_back(m);
+    }
+    void end() {
+        if (timing) cudaEventRecord(marks.back().b, st);
+    }
+};
+
+void enqueue_render(const pt_ctx *ctx, Enqueue &E, WaveArgs A, const pt_render_params *P, size_t cap, uint64_t total,
+                    uint64_t npix, float *d_sum, float *d_comp) {
+    const WaveBuffers &B = ctx->W;
+    const bool inl = ctx->S.numVols > 0;
+    cudaStream_t st = E.st;
+    cudaMemsetAsync(B.counters, 0, 64, st);
+    cudaMemsetAsync(ctx->d_err, 0, 4, st);
+    for (uint64_t ws = 0; ws < total; ws += cap) {
+        A.waveStart = ws;
+        A.waveCount = (uint32_t)std::min<uint64_t>(cap, total - ws);
+        A.qslotOut = B.qslot[0]; A.qoOut = B.qo[0]; A.qdOut = B.qd[0]; A.cntOut = B.counters + 0;
+        E.begin(STG_RAYGEN);
+        k_raygen<<<(A.waveCount + kBlock - 1) / kBlock, kBlock, 0, st>>>(A);
+        E.end();
+        int cur = 0;
+        for (uint32_t b = 0; b < P->max_depth; b++) {
+            A.qslotIn = B.qslot[cur]; A.qoIn = B.qo[cur]; A.qdIn = B.qd[cur]; A.cntIn = B.counters + cur;
+            A.qslotOut = B.qslot[1 - cur]; A.qoOut = B.qo[1 - cur]; A.qdOut = B.qd[1 - cur];
+            A.cntOut = B.counters + (1 - cur);
+            cudaMemsetAsync(A.cntOut, 0, 4, st);
+            cudaMemsetAsync(A.cntShadow, 0, 4, st);
+            if (inl) {
+                E.begin(STG_EXTEND);
+                k_extend<false><<<gExt, kBlock, 0, st>>>(A);
+                E.end();
+                E.begin(STG_SHADE);
+                k_shade<true, CLS_ANY><<<gShadeI, kBlock, 0, st>>>(A);
+                E.end();
+            } else {
+                cudaMemsetAsync(A.cntCls, 0, CLS_N * sizeof(uint32_t), st);
+                E.begin(STG_EXTEND);
+                k_extend<true><<<gExtC, kBlock, 0, st>>>(A);
+                E.end();
+                for (int c = 0; c < CLS_N; c++) {
+                    if (!((ctx->clsMask >> c) & 1u)) continue;
+                    E.begin(STG_SHADE);
+                    kShadeCls[c]<<<gCls[c], kBlock, 0, st>>>(A);
+                    E.end();
+                }
+                E.begin(STG_SHADOW);
+                k_shadow<<<gShadow, kBlock, 0, st>>>(A);
+                E.end();
+            }
+            cur = 1 - cur;
+        }
+        uint32_t cover = (uint32_t)std::min<uint64_t>(A.waveCount, npix);
+        E.begin(STG_FILM);
+        k_film<<<(cover + kBlock - 1) / kBlock, kBlock, 0, st>>>(A, (float4 *)d_sum, (float4 *)d_comp);
+        E.end();
+    }
+}
+
+__global__ void k_set_u32(uint32_t *p, uint32_t v) { *p = v; }
+
+bool graph_matches(const pt_ctx *ctx, const pt_render_params *P, size_t cap, const float *sum, const float *comp) {
+    const RenderGraph &G = ctx->graph;
+    return G.exec && G.width == P->width && G.height == P->height && G.spp == P->spp && G.maxDepth == P->max_depth &&
+           G.rngKind == P->rng_kind && G.envSampling == P->env_sampling && G.cap == cap && G.sum == sum &&
+           G.comp == comp && G.sceneGen == ctx->sceneGen && G.waveGen == ctx->waveGen &&
+           memcmp(&G.cam, &P->camera, sizeof(pt_camera)) == 0;
+}
+}  // namespace
+
+void pt_graph_free(pt_ctx *ctx) {
+    if (ctx->graph.exec) cudaGraphExecDestroy(ctx->graph.exec);
+    ctx->graph = RenderGraph{};
 }
 
 int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *d_comp, pt_stats *stats) {
     const uint32_t W = P->width, H = P->height;
     const uint64_t npix = (uint64_t)W * H;
     const uint64_t total = npix * P->spp;
-    // Default wave: the whole render when its state fits in half of the free
-    // device memory.  Each bounce of a wave ends with a latency-bound tail (a
-    // few slow traversals), so fewer, larger waves amortise it; 59 M paths of
-    // a 1280 x 720 x 64 frame take ~18 GB.
+    // Default wave: the whole render, up to kMaxWavePaths and half of the
+    // free device memory.  Each bounce of a wave ends with a latency-bound
+    // tail (a few slow traversals), so fewer, larger waves amortise it; the
+    // 59 M paths of a 1280 x 720 x 64 frame take ~20 GB.
     size_t cap = P->wave_paths;
     if (!cap) {
         size_t freeB = 0, totalB = 0;
@@ -654,13 +757,6 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
     if (rc) return rc;
     cudaStream_t st = ctx->stream;
     WaveBuffers &B = ctx->W;
-    const bool inl = ctx->S.numVols > 0;
-    using Kernel = void (*)(WaveArgs);
-    static const Kernel kShadeCls[CLS_N] = {k_shade<false, CLS_MISS>,    k_shade<false, CLS_EMIT>,
-                                            k_shade<false, CLS_DELTA>,   k_shade<false, CLS_DIFFUSE>,
-                                            k_shade<false, CLS_MICRO>,   k_shade<false, CLS_DISNEY>,
-                                            k_shade<false, CLS_HAIR>};
-    static int gExt = 0, gExtC = 0, gShadeI = 0, gShadow = 0, gCls[CLS_N];
     if (!gExt) {
         gExt = grid_for(ctx, (const void *)k_extend<false>);
         gExtC = grid_for(ctx, (const void *)k_extend<true>);
@@ -668,16 +764,10 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
         gShadow = grid_for(ctx, (const void *)k_shadow);
         for (int c = 0; c < CLS_N; c++) gCls[c] = grid_for(ctx, (const void *)kShadeCls[c]);
     }
-    cudaEvent_t ev[2];
-    cudaEventCreate(&ev[0]);
-    cudaEventCreate(&ev[1]);
-    PT_CUDA(cudaMemsetAsync(B.counters, 0, 64, st));
-    PT_CUDA(cudaMemsetAsync(ctx->d_err, 0, 4, st));
-    cudaEventRecord(ev[0], st);
     WaveArgs A;
     A.S = ctx->S;
     A.width = W; A.height = H; A.npix = (uint32_t)npix;
-    A.sampleOffset = P->sample_offset;
+    A.sampleOffset = ctx->d_err + 1;
     A.rngKind = P->rng_kind; A.envMode = P->env_sampling; A.maxDepth = P->max_depth;
     A.cam = P->camera;
     A.thr_pdf = B.thr_pdf; A.lo_eta = B.lo_eta; A.pendA = B.pendA; A.pendE = B.pendE; A.rng = B.rng;
@@ -690,70 +780,50 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
     A.rayTotals = (unsigned long long *)(B.counters + 4);
     A.err = ctx->d_err;
     A.shadowCap = (uint32_t)(2 * B.cap);
-    uint64_t waves = 0, bounces = 0, launches = 0;
-    // optional per-stage timing: an event pair around every launch
+    const uint64_t waves = (total + cap - 1) / cap;
+    // Without per-launch timing the render replays a CUDA graph of its launch
+    // sequence, captured on the first call with this configuration: no host
+    // gaps between the ~100 launches of a render.
     const bool timing = (P->flags & PT_RENDER_STAGE_TIMING) != 0;
-    enum { STG_RAYGEN, STG_EXTEND, STG_SHADE, STG_SHADOW, STG_FILM, STG_N };
-    struct Mark { int stage; cudaEvent_t a, b; };
-    std::vector<Mark> marks;
-    auto begin = [&](int stage) {
-        launches++;
-        if (!timing) return;
-        Mark m{stage, nullptr, nullptr};
-        cudaEventCreate(&m.a);
-        cudaEventCreate(&m.b);
-        cudaEventRecord(m.a, st);
-        marks.push_back(m);
-    };
-    auto end = [&]() {
-        if (timing) cudaEventRecord(marks.back().b, st);
-    };
-    for (uint64_t ws = 0; ws < total; ws += cap) {
-        A.waveStart = ws;
-        A.waveCount = (uint32_t)std::min<uint64_t>(cap, total - ws);
-        A.qslotOut = B.qslot[0]; A.qoOut = B.qo[0]; A.qdOut = B.qd[0]; A.cntOut = B.counters + 0;
-        begin(STG_RAYGEN);
-        k_raygen<<<(A.waveCount + kBlock - 1) / kBlock, kBlock, 0, st>>>(A);
-        end();
-        int cur = 0;
-        for (uint32_t b = 0; b < P->max_depth; b++) {
-            A.qslotIn = B.qslot[cur]; A.qoIn = B.qo[cur]; A.qdIn = B.qd[cur]; A.cntIn = B.counters + cur;
-            A.qslotOut = B.qslot[1 - cur]; A.qoOut = B.qo[1 - cur]; A.qdOut = B.qd[1 - cur];
-            A.cntOut = B.counters + (1 - cur);
-            cudaMemsetAsync(A.cntOut, 0, 4, st);
-            cudaMemsetAsync(A.cntShadow, 0, 4, st);
-            if (inl) {
-                begin(STG_EXTEND);
-                k_extend<false><<<gExt, kBlock, 0, st>>>(A);
-                end();
-                begin(STG_SHADE);
-                k_shade<true, CLS_ANY><<<gShadeI, kBlock, 0, st>>>(A);
-                end();
-            } else {
-                cudaMemsetAsync(A.cntCls, 0, CLS_N * sizeof(uint32_t), st);
-                begin(STG_EXTEND);
-                k_extend<true><<<gExtC, kBlock, 0, st>>>(A);
-                end();
-                for (int c = 0; c < CLS_N; c++) {
-                    if (!((ctx->clsMask >> c) & 1u)) continue;
-                    begin(STG_SHADE);
-                    kShadeCls[c]<<<gCls[c], kBlock, 0, st>>>(A);
-                    end();
-                }
-            }
-            if (!inl) {
-                begin(STG_SHADOW);
-                k_shadow<<<gShadow, kBlock, 0, st>>>(A);
-                end();
-            }
-            cur = 1 - cur;
-            bounces++;
+    bool useGraph = !timing;
+    if (useGraph && !graph_matches(ctx, P, cap, d_sum, d_comp)) {
+        pt_graph_free(ctx);
+        Enqueue E{ctx->ownStream, false, {}, 0};
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        bool ok = cudaStreamBeginCapture(ctx->ownStream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+        if (ok) {
+            enqueue_render(ctx, E, A, P, cap, total, npix, d_sum, d_comp);
+            ok = cudaStreamEndCapture(ctx->ownStream, &g) == cudaSuccess && g;
         }
-        uint32_t cover = (uint32_t)std::min<uint64_t>(A.waveCount, npix);
-        begin(STG_FILM);
-        k_film<<<(cover + kBlock - 1) / kBlock, kBlock, 0, st>>>(A, (float4 *)d_sum, (float4 *)d_comp);
-        end();
-        waves++;
+        ok = ok && cudaGraphInstantiate(&exec, g, 0) == cudaSuccess;
+        if (g) cudaGraphDestroy(g);
+        if (ok) {
+            RenderGraph &G = ctx->graph;
+            G.exec = exec;
+            G.width = W; G.height = H; G.spp = P->spp; G.maxDepth = P->max_depth;
+            G.rngKind = P->rng_kind; G.envSampling = P->env_sampling; G.cam = P->camera;
+            G.cap = cap; G.sum = d_sum; G.comp = d_comp;
+            G.sceneGen = ctx->sceneGen; G.waveGen = ctx->waveGen;
+            G.launches = E.launches;
+        } else {  // capture unavailable: issue the launches directly
+            cudaGetLastError();
+            useGraph = false;
+        }
+    }
+    cudaEvent_t ev[2];
+    cudaEventCreate(&ev[0]);
+    cudaEventCreate(&ev[1]);
+    cudaEventRecord(ev[0], st);
+    k_set_u32<<<1, 1, 0, st>>>(ctx->d_err + 1, P->sample_offset);
+    Enqueue E{st, timing, {}, 0};
+    uint64_t launches = 1;
+    if (useGraph) {
+        PT_CUDA(cudaGraphLaunch(ctx->graph.exec, st));
+        launches += ctx->graph.launches;
+    } else {
+        enqueue_render(ctx, E, A, P, cap, total, npix, d_sum, d_comp);
+        launches += E.launches;
     }
     cudaEventRecord(ev[1], st);
     uint32_t hostCnt[16];
@@ -766,7 +836,7 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
     cudaEventDestroy(ev[0]);
     cudaEventDestroy(ev[1]);
     float stage[STG_N] = {0, 0, 0, 0, 0};
-    for (Mark &m : marks) {
+    for (Mark &m : E.marks) {
         float t = 0.0f;
         if (se == cudaSuccess) cudaEventElapsedTime(&t, m.a, m.b);
         stage[m.stage] += t;
@@ -785,7 +855,7 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
         stats->extension_rays = tot[0];
         stats->shadow_rays = tot[1];
         stats->waves = waves;
-        stats->bounces = bounces;
+        stats->bounces = waves * P->max_depth;
         stats->launches = launches;
         stats->ms_total = ms;
         stats->ms_raygen = stage[STG_RAYGEN];

@@ -110,6 +110,24 @@ def test_deterministic_and_split_invariant(pt, scenes, ctx):
     assert np.array_equal(a, w)
 
 
+@pytest.mark.parametrize("name", ["cornell", "spheres"])
+def test_graph_replay_matches_direct_launches(name, pt, scenes, ctx):
+    """Renders replay a captured CUDA graph of their launches; with per-launch
+    timing they issue the launches directly.  Same films, bit for bit, also
+    when one graph is replayed with another sample offset."""
+    make, W, H, depth = SCENES[name]
+    sc, cam = make(scenes)
+    ctx.upload(sc)
+    for off in (0, 7, 1000):
+        P = pt.render_params(W, H, 3, cam, max_depth=depth, sample_offset=off)
+        Pt = pt.render_params(W, H, 3, cam, max_depth=depth, sample_offset=off, flags=pt.PT_RENDER_STAGE_TIMING)
+        g, cg, sg = ctx.render(P)
+        d, cd, sd = ctx.render(Pt)
+        assert np.array_equal(g, d) and np.array_equal(cg, cd), off
+        assert sg.extension_rays == sd.extension_rays and sg.launches == sd.launches
+        assert sd.ms_extend > 0 and sg.ms_extend == 0
+
+
 def test_pcg_sampler_parity(pt, scenes, ctx, oracle):
     sc, cam = scenes.cornell(48, 48)
     ctx.upload(sc)
