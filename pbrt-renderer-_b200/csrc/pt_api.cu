@@ -316,6 +316,8 @@ int pt_create(pt_ctx **out, int device) {
     ctx->numSMs = prop.multiProcessorCount;
     if (cudaStreamCreateWithFlags(&ctx->ownStream, cudaStreamNonBlocking) != cudaSuccess) return bail(PT_E_CUDA);
     ctx->stream = ctx->ownStream;
+    if (cudaEventCreate(&ctx->ev[0]) != cudaSuccess || cudaEventCreate(&ctx->ev[1]) != cudaSuccess)
+        return bail(PT_E_CUDA);
     uint32_t tab[1024];
     for (uint32_t k = 0; k < 4; k++)
         for (uint32_t b = 0; b < 256; b++) tab[256 * k + b] = ptm::sobol1_loop(b << (8 * k));
@@ -338,6 +340,8 @@ int pt_destroy(pt_ctx *ctx) {
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->d_sobol1) cudaFree(ctx->d_sobol1);
     if (ctx->d_err) cudaFree(ctx->d_err);
+    for (cudaEvent_t e : ctx->ev)
+        if (e) cudaEventDestroy(e);
     if (ctx->ownStream) cudaStreamDestroy(ctx->ownStream);
     delete ctx;
     return PT_OK;

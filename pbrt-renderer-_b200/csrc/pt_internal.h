@@ -88,6 +88,7 @@ struct pt_ctx {
     int numSMs = 148;
     cudaStream_t stream = nullptr;     // stream all work is issued on
     cudaStream_t ownStream = nullptr;  // created by pt_create, destroyed by pt_destroy
+    cudaEvent_t ev[2] = {nullptr, nullptr};  // brackets each render (stats.ms_total)
     std::string err;
     std::vector<void *> sceneAllocs;  // freed on re-upload / destroy
     pt::DevScene S{};

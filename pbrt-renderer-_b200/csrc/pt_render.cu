@@ -342,8 +342,18 @@ __host__ __device__ constexpr uint32_t class_type(int c) {
 // CLS == CLS_ANY: every path of the ray queue, events dispatched at run time
 // (media scenes).  Otherwise the paths of one shading class, whose event and
 // material type are then compile-time facts: each class gets a small kernel.
+// Resident blocks per SM the shading kernels are compiled for.  The Disney
+// kernel is latency-bound: 3 blocks (80 registers, a few spills) beat 2
+// blocks (112 registers, none) by 7 % on B200.  The others get the count
+// their register use gives anyway (a bound makes the compiler spend up to it).
+template <int CLS>
+struct ShadeBlocks {
+    static constexpr int value = CLS == CLS_MISS ? 5 : (CLS == CLS_EMIT || CLS == CLS_DELTA) ? 4
+                                                     : CLS == CLS_DISNEY ? 3 : 2;
+};
+
 template <bool INLINE, int CLS>
-__global__ void __launch_bounds__(kBlock) k_shade(WaveArgs A) {
+__global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveArgs A) {
     const DevScene &S = A.S;
     uint32_t n = CLS == CLS_ANY ? *(volatile uint32_t *)A.cntIn : *(volatile uint32_t *)(A.cntCls + CLS);
     uint32_t iters = (n + gridDim.x * blockDim.x - 1) / (gridDim.x * blockDim.x);
@@ -742,13 +752,19 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
     // free device memory.  Each bounce of a wave ends with a latency-bound
     // tail (a few slow traversals), so fewer, larger waves amortise it; the
     // 59 M paths of a 1280 x 720 x 64 frame take ~20 GB.
+    // The free-memory query runs only when the buffers would have to grow: it
+    // is a driver call that can block on other clients of the driver.
     size_t cap = P->wave_paths;
     if (!cap) {
-        size_t freeB = 0, totalB = 0;
-        if (cudaMemGetInfo(&freeB, &totalB) != cudaSuccess) freeB = (size_t)4 << 30;
-        size_t fit = (freeB / 2 + (ctx->W.cap ? ctx->W.cap * kWaveBytesPerPath : 0) / 2) / kWaveBytesPerPath;
-        cap = (size_t)std::min<uint64_t>(total, std::min<size_t>(fit, kMaxWavePaths));
-        cap = std::max<size_t>(cap, (size_t)1 << 16);
+        size_t want = (size_t)std::min<uint64_t>(total, kMaxWavePaths);
+        if (want <= ctx->W.cap) {
+            cap = want;
+        } else {
+            size_t freeB = 0, totalB = 0;
+            if (cudaMemGetInfo(&freeB, &totalB) != cudaSuccess) freeB = (size_t)4 << 30;
+            size_t fit = (freeB / 2 + ctx->W.cap * kWaveBytesPerPath / 2) / kWaveBytesPerPath;
+            cap = std::max<size_t>(std::min(want, fit), std::min<size_t>(want, (size_t)1 << 16));
+        }
     }
     if (npix <= cap) cap = (cap / npix) * npix;
     if (cap > total) cap = (size_t)total;
@@ -811,9 +827,7 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
             useGraph = false;
         }
     }
-    cudaEvent_t ev[2];
-    cudaEventCreate(&ev[0]);
-    cudaEventCreate(&ev[1]);
+    cudaEvent_t *ev = ctx->ev;
     cudaEventRecord(ev[0], st);
     k_set_u32<<<1, 1, 0, st>>>(ctx->d_err + 1, P->sample_offset);
     Enqueue E{st, timing, {}, 0};
@@ -833,8 +847,6 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
     cudaError_t se = cudaStreamSynchronize(st);
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, ev[0], ev[1]);
-    cudaEventDestroy(ev[0]);
-    cudaEventDestroy(ev[1]);
     float stage[STG_N] = {0, 0, 0, 0, 0};
     for (Mark &m : E.marks) {
         float t = 0.0f;
