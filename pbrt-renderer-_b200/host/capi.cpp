@@ -96,6 +96,18 @@ uint64_t nori_flat(void *scene, int which, void *out) {
     return f[which]->size();
 }
 
+// Write W x H x 3 floats (top row first) as an uncompressed OpenEXR file.
+// Returns 0 or -1 (err set).
+int nori_write_exr(const char *path, int width, int height, const float *rgb, char *err, size_t errlen) {
+    try {
+        writeEXR(path ? path : "", width, height, rgb);
+        return 0;
+    } catch (const std::exception &e) {
+        seterr(err, errlen, e.what());
+        return -1;
+    }
+}
+
 // Render spp samples from sample_offset with the scene's GPU integrator into
 // host films (4 x W x H floats each; added to).  Returns 0 or -1 (err set).
 int nori_render(void *scene, uint32_t spp, uint32_t sample_offset, float *sum, float *comp, pt_stats *stats,

@@ -1,5 +1,6 @@
-// nori_render — render a Nori XML scene on the GPU and write a PFM image.
-//   nori_render scene.xml [spp] [out.pfm]
+// nori_render — render a Nori XML scene on the GPU and write the linear HDR
+// mean image: OpenEXR when the output name ends in .exr, PFM otherwise.
+//   nori_render scene.xml [spp] [out.exr|out.pfm]
 #include <cstdio>
 #include <cstdlib>
 #include <string>
@@ -8,7 +9,7 @@
 
 int main(int argc, char **argv) {
     if (argc < 2) {
-        std::fprintf(stderr, "usage: %s scene.xml [spp] [out.pfm]\n", argv[0]);
+        std::fprintf(stderr, "usage: %s scene.xml [spp] [out.exr|out.pfm]\n", argv[0]);
         return 2;
     }
     try {
@@ -21,11 +22,16 @@ int main(int argc, char **argv) {
         gi->preprocess(scene);
         nori::RenderResult r = gi->render(spp);
         std::vector<float> img = r.mean();
-        FILE *f = std::fopen(out.c_str(), "wb");
-        if (!f) throw nori::NoriException("cannot write " + out);
-        std::fprintf(f, "PF\n%d %d\n-1.0\n", r.width, r.height);
-        for (int y = r.height - 1; y >= 0; y--) std::fwrite(&img[(size_t)y * r.width * 3], 4, (size_t)r.width * 3, f);
-        std::fclose(f);
+        if (out.size() > 4 && out.compare(out.size() - 4, 4, ".exr") == 0) {
+            nori::writeEXR(out, r.width, r.height, img.data());
+        } else {
+            FILE *f = std::fopen(out.c_str(), "wb");
+            if (!f) throw nori::NoriException("cannot write " + out);
+            std::fprintf(f, "PF\n%d %d\n-1.0\n", r.width, r.height);
+            for (int y = r.height - 1; y >= 0; y--)
+                std::fwrite(&img[(size_t)y * r.width * 3], 4, (size_t)r.width * 3, f);
+            std::fclose(f);
+        }
         std::printf("%s: %dx%d, %u spp, %.2f ms on the GPU (%.1f Mpaths/s)\n", out.c_str(), r.width, r.height, spp,
                     r.stats.ms_total, r.stats.paths / (r.stats.ms_total * 1e3));
         return 0;

@@ -449,6 +449,8 @@ protected:
 
 // ---- loading -------------------------------------------------------------------------------
 NoriObject *loadFromXML(const std::string &filename);
+// Linear HDR image as an uncompressed OpenEXR file (rgb: W*H*3, top row first).
+void writeEXR(const std::string &path, int width, int height, const float *rgb);
 
 // Flatten a scene the way src/gpu/DXRApp_Scene.cpp:172-493 and
 // src/gpu/DXRApp_Textures.cpp:181-275 do (shared with GPUIntegrator).

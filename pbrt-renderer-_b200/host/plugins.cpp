@@ -676,6 +676,97 @@ public:
     }
 };
 
+// ---- hair strands (src/cpu/hair.cpp:43-322) -----------------------------------------------------
+// A Cem Yuksel HAIR file (128-byte little-endian header "HAIR", strand and
+// point counts, a flag word selecting the optional arrays, defaults; then
+// the arrays: segments u16 per strand, points 3 x f32, thickness f32,
+// transparency f32, colour 3 x f32 per point) tessellated into tubes of
+// `sides` vertices per ring.  The vertex layout is the one the hair shading
+// reads: UV = (position along the strand, (h + 1) / 2) with h = -cos(angle
+// around the tube), tangent = strand direction at the ring.
+class HairMesh : public Mesh {
+public:
+    explicit HairMesh(const PropertyList &propList) {
+        std::string filename = resolvePath(propList.getString("filename"));
+        int sides = propList.getInteger("sides", 6);
+        float radiusScale = propList.getFloat("radiusScale", 1.0f);
+        int maxStrands = propList.getInteger("maxStrands", -1);
+        Transform trafo = propList.getTransform("toWorld", Transform());
+        if (sides < 3) throw NoriException("hair: \"sides\" must be at least 3");
+        std::ifstream f(filename, std::ios::binary);
+        if (!f) throw NoriException("hair: cannot open \"" + filename + "\"");
+        unsigned char hdr[128];
+        f.read(reinterpret_cast<char *>(hdr), 128);
+        if (!f || std::memcmp(hdr, "HAIR", 4) != 0) throw NoriException("hair: \"" + filename + "\" is not a HAIR file");
+        auto u32 = [&](int o) { uint32_t v; std::memcpy(&v, hdr + o, 4); return v; };
+        auto f32 = [&](int o) { float v; std::memcpy(&v, hdr + o, 4); return v; };
+        const uint32_t numStrands = u32(4), numPoints = u32(8), flags = u32(12), defSegs = u32(16);
+        const float defThickness = f32(20);
+        if (!(flags & 2u)) throw NoriException("hair: \"" + filename + "\" has no points array");
+        std::vector<uint16_t> segs;
+        if (flags & 1u) {
+            segs.resize(numStrands);
+            f.read(reinterpret_cast<char *>(segs.data()), (std::streamsize)numStrands * 2);
+        }
+        std::vector<float> pts((size_t)numPoints * 3), thick;
+        f.read(reinterpret_cast<char *>(pts.data()), (std::streamsize)pts.size() * 4);
+        if (flags & 4u) {
+            thick.resize(numPoints);
+            f.read(reinterpret_cast<char *>(thick.data()), (std::streamsize)numPoints * 4);
+        }
+        if (!f) throw NoriException("hair: \"" + filename + "\" is truncated");
+        // strand point ranges; the counts must add up to numPoints
+        std::vector<std::pair<uint32_t, uint32_t>> strands;  // (first point, point count)
+        uint64_t at = 0;
+        for (uint32_t s = 0; s < numStrands; s++) {
+            uint32_t n = (segs.empty() ? defSegs : segs[s]) + 1u;
+            strands.push_back({(uint32_t)at, n});
+            at += n;
+        }
+        if (at != numPoints) throw NoriException("hair: \"" + filename + "\": strand point counts do not add up");
+        if (maxStrands > 0 && (uint32_t)maxStrands < numStrands) strands.resize((size_t)maxStrands);
+        auto P = [&](uint32_t i) { return trafo.point(Vec3(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2])); };
+        const float kTwoPi = 6.28318530717958647692f;
+        for (const auto &st : strands) {
+            const uint32_t first = st.first, n = st.second;
+            if (n < 2) continue;
+            const uint32_t ring0 = (uint32_t)(m_V.size() / 3);
+            for (uint32_t p = 0; p < n; p++) {
+                Vec3 c = P(first + p);
+                m_bbox.expandBy(c);
+                Vec3 t = p == 0 ? P(first + 1) - P(first) : p == n - 1 ? P(first + p) - P(first + p - 1)
+                                                                     : P(first + p + 1) - P(first + p - 1);
+                t = t.normalized();
+                Vec3 ref = std::abs(t.x()) < 0.9f ? Vec3(1.0f, 0.0f, 0.0f) : Vec3(0.0f, 1.0f, 0.0f);
+                Vec3 b = t.cross(ref).normalized();
+                Vec3 nr = t.cross(b).normalized();
+                float radius = (thick.empty() ? defThickness : thick[first + p]) * 0.5f * radiusScale;
+                float along = (float)p / (float)(n - 1);
+                for (int k = 0; k < sides; k++) {
+                    float ang = kTwoPi * (float)k / (float)sides;
+                    Vec3 radial = b * std::cos(ang) + nr * std::sin(ang);
+                    Vec3 v = c + radial * radius;
+                    Vec3 nn = radial.normalized();
+                    float h = -std::cos(ang);
+                    for (int a = 0; a < 3; a++) { m_V.push_back(v[a]); m_N.push_back(nn[a]); m_T.push_back(t[a]); }
+                    m_UV.push_back(along);
+                    m_UV.push_back((h + 1.0f) * 0.5f);
+                }
+                if (p > 0) {  // two triangles per quad between this ring and the previous one
+                    uint32_t prev = ring0 + (p - 1) * (uint32_t)sides, cur = ring0 + p * (uint32_t)sides;
+                    for (uint32_t k = 0; k < (uint32_t)sides; k++) {
+                        uint32_t k1 = (k + 1) % (uint32_t)sides;
+                        uint32_t tri[6] = {prev + k, prev + k1, cur + k1, prev + k, cur + k1, cur + k};
+                        m_F.insert(m_F.end(), tri, tri + 6);
+                    }
+                }
+            }
+        }
+        if (m_F.empty()) throw NoriException("hair: \"" + filename + "\" has no strand with two points");
+        m_name = filename;
+    }
+};
+
 // ---- scene (src/cpu/scene.cpp) ------------------------------------------------------------------
 Scene::Scene(const PropertyList &p) {
     m_envmap = p.getString("envmap", "textures/white_furnace.hdr");
@@ -740,6 +831,7 @@ NORI_REGISTER_CLASS(GaussianFilter, "gaussian")
 NORI_REGISTER_CLASS(PerspectiveCamera, "perspective")
 NORI_REGISTER_CLASS(Independent, "independent")
 NORI_REGISTER_CLASS(WavefrontOBJ, "obj")
+NORI_REGISTER_CLASS(HairMesh, "hair")
 NORI_REGISTER_CLASS(Scene, "scene")
 
 }  // namespace nori

@@ -19,8 +19,10 @@ def write_hdr(path, rgb):
     with open(path, "wb") as f:
         f.write(b"#?RADIANCE\nFORMAT=32-bit_rle_rgbe\n\n")
         f.write(f"-Y {H} +X {W}\n".encode())
+        # shared exponent e from frexp (max = f * 2^e, f in [0.5, 1)): mantissas
+        # rgb * 256 / 2^e < 256, so 1.0 is stored exactly as 128 at e = 1
         m = rgb.max(-1)
-        e = np.where(m > 1e-32, np.ceil(np.log2(np.maximum(m, 1e-32))), -128).astype(np.int32)
+        _, e = np.frexp(np.maximum(m, 1e-32))
         sc = np.where(m > 1e-32, 256.0 / np.exp2(e), 0.0)
         q = np.clip(np.floor(rgb * sc[..., None]), 0, 255).astype(np.uint8)
         ex = np.where(m > 1e-32, e + 128, 0).astype(np.uint8)
@@ -194,6 +196,156 @@ def test_xml_render_matches_direct_scene(nori, pt, scenes, scene_dir):
     d, _, _ = ctx.render(pt.render_params(W, H, 4, cam, max_depth=8))
     ctx.close()
     assert np.array_equal(s, d), np.abs(s - d).max()
+    nori.nori_free(h)
+
+
+def write_hair(path, strands, thickness=None, default_thickness=0.1, default_segments=None):
+    """A HAIR file (Cem Yuksel's format): 128-byte header, then the segment
+    counts (u16 per strand, omitted when all strands have default_segments),
+    points (3 x f32), optional thickness (f32 per point)."""
+    import struct
+
+    flags = 2 | (0 if default_segments is not None else 1) | (4 if thickness is not None else 0)
+    npts = sum(len(s) for s in strands)
+    hdr = struct.pack("<4sIIIIff3f", b"HAIR", len(strands), npts, flags, default_segments or 0,
+                      default_thickness, 1.0, 1.0, 1.0, 1.0)
+    hdr += b"\0" * (128 - len(hdr))
+    with open(path, "wb") as f:
+        f.write(hdr)
+        if default_segments is None:
+            f.write(np.array([len(s) - 1 for s in strands], np.uint16).tobytes())
+        f.write(np.concatenate([np.asarray(s, np.float32).reshape(-1) for s in strands]).tobytes())
+        if thickness is not None:
+            f.write(np.asarray(thickness, np.float32).tobytes())
+
+
+def wavy_strands(n=40, segs=10, seed=3):
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        x0, y0 = rng.uniform(-2, 2), rng.uniform(-0.5, 0.5)
+        z = np.linspace(-4, 4, segs + 1)
+        out.append(np.stack([x0 + 0.3 * np.sin(z * 1.5 + k), y0 + 0 * z, z], 1))
+    return out
+
+
+HAIR_XML = """<scene>
+  <integrator type="path_mis"/>
+  <camera type="perspective">
+    <float name="fov" value="55"/>
+    <transform name="toWorld"><lookat target="0, 0, 0" origin="0, 12, 0" up="0, 0, 1"/></transform>
+    <integer name="height" value="48"/><integer name="width" value="64"/>
+  </camera>
+  <sampler type="independent"><integer name="sampleCount" value="64"/></sampler>
+  <mesh type="hair">
+    <string name="filename" value="strands.hair"/>
+    <integer name="sides" value="{sides}"/>
+    <float name="radiusScale" value="{scale}"/>
+    <bsdf type="hair_bsdf">
+      <color name="color" value="1.0 1.0 1.0"/>
+      <float name="beta_m" value="0.2"/><float name="beta_n" value="0.3"/>
+      <float name="alpha" value="2.0"/><float name="eta" value="1.55"/>
+    </bsdf>
+  </mesh>
+</scene>
+"""
+
+
+@pytest.fixture(scope="module")
+def hair_dir(tmp_path_factory):
+    d = tmp_path_factory.mktemp("hair_scene")
+    strands = wavy_strands()
+    thick = np.concatenate([np.linspace(0.12, 0.04, len(s)) for s in strands])
+    write_hair(d / "strands.hair", strands, thickness=thick)
+    (d / "textures").mkdir()
+    write_hdr(d / "textures" / "white_furnace.hdr", np.ones((2, 2, 3), np.float32))  # the scene's default envmap
+    (d / "scene.xml").write_text(HAIR_XML.format(sides=6, scale=1.0))
+    return d, strands, thick
+
+
+def test_hair_tessellation(nori, pt, hair_dir):
+    d, strands, thick = hair_dir
+    h, err = load(nori, d / "scene.xml")
+    assert h, err
+    S = 6
+    nv = sum(len(s) for s in strands) * S
+    nt = sum(len(s) - 1 for s in strands) * 2 * S
+    info = (C.c_uint32 * 8)()
+    nori.nori_info(h, info)
+    assert info[4] == nt and info[7] == 32  # path_mis default depth
+    pos, nrm, uv, tan = (flat(nori, h, k).reshape(-1, w) for k, w in ((0, 3), (1, 3), (2, 2), (3, 3)))
+    assert len(pos) == nv and len(tan) == nv
+    centres = np.concatenate(strands).repeat(S, 0)
+    radii = np.repeat(thick * 0.5, S)
+    # ring vertices lie at the strand radius around the control point, normals radial
+    off = pos - centres
+    assert np.allclose(np.linalg.norm(off, axis=1), radii, rtol=1e-5, atol=1e-6)
+    assert np.allclose(nrm * radii[:, None], off, atol=1e-5)
+    # unit tangents, orthogonal to the radial direction
+    assert np.allclose(np.linalg.norm(tan, axis=1), 1.0, atol=1e-5)
+    assert np.abs((tan * nrm).sum(1)).max() < 1e-5
+    # UV: position along the strand, (h + 1) / 2 with h = -cos(2 pi k / S)  (stored unflipped for hair)
+    k = np.tile(np.arange(S), len(uv) // S)
+    assert np.allclose(uv[:, 1], (1.0 - np.cos(2 * np.pi * k / S)) / 2, atol=1e-6)
+    first = uv.reshape(-1, S, 2)[:, 0, 0]
+    assert first.min() == 0.0 and first.max() == 1.0
+    mats = (pt.pt_material * 1)()
+    nori.nori_materials(h, mats, 1)
+    assert mats[0].type == pt.PT_MAT_HAIR and abs(mats[0].roughness - 0.2) < 1e-7 and abs(mats[0].intIOR - 1.55) < 1e-7
+    nori.nori_free(h)
+
+
+@pytest.mark.parametrize("case,msg", [("signature", "not a HAIR file"), ("counts", "do not add up"),
+                                      ("truncated", "truncated"), ("nopoints", "no points array")])
+def test_hair_file_errors(nori, tmp_path, case, msg):
+    s = wavy_strands(3, 4)
+    p = tmp_path / "strands.hair"
+    write_hair(p, s)
+    b = bytearray(p.read_bytes())
+    if case == "signature":
+        b[0:4] = b"HAIX"
+    elif case == "counts":  # first strand's segment count one short of its points
+        b[128:130] = (int.from_bytes(b[128:130], "little") - 1).to_bytes(2, "little")
+    elif case == "truncated":
+        b = b[:200]
+    elif case == "nopoints":
+        b[12:16] = (int.from_bytes(b[12:16], "little") & ~2).to_bytes(4, "little")
+    p.write_bytes(bytes(b))
+    (tmp_path / "scene.xml").write_text(HAIR_XML.format(sides=6, scale=1.0))
+    h, err = load(nori, tmp_path / "scene.xml")
+    assert not h and msg in err, err
+
+
+@pytest.mark.gpu
+def test_hair_xml_furnace_matches_direct_scene(nori, pt, hair_dir):
+    """The reference's hair white-furnace setup (white BCSDF colour, white
+    envmap, path_mis) on a synthetic strand file: the XML render equals the
+    same buffers rendered through libpt, and conserves energy to 3e-3."""
+    d, _, _ = hair_dir
+    h, err = load(nori, d / "scene.xml")
+    assert h, err
+    W, H = 64, 48
+    s = np.zeros((H, W, 4), np.float32)
+    c = np.zeros_like(s)
+    st = pt.pt_stats()
+    e = C.create_string_buffer(512)
+    assert nori.nori_render(h, 64, 0, s.ctypes.data, c.ctypes.data, C.byref(st), e, 512) == 0, e.value
+    mats = (pt.pt_material * 1)()
+    nori.nori_materials(h, mats, 1)
+    cam = pt.pt_camera()
+    nori.nori_camera(h, C.byref(cam))
+    pos, nrm, uv, tan, idx, env = (flat(nori, h, k) for k in range(6))
+    ew = int(nori.nori_flat(h, 6, None))
+    sc = pt.Scene(pos, idx, list(mats), normals=nrm, texcoords=uv, tangents=tan, env_rgb=env.reshape(-1, ew, 3))
+    ctx = pt.Context(0)
+    ctx.upload(sc)
+    dd, _, _ = ctx.render(pt.render_params(W, H, 64, cam, max_depth=32))
+    ctx.close()
+    assert np.array_equal(s, dd), np.abs(s - dd).max()
+    img = (s[..., :3] - c[..., :3]) / 64.0
+    hairpix = img[np.abs(img - 1.0).max(-1) > 1e-6]
+    assert len(hairpix) > 200  # the strands cover part of the frame
+    assert abs(float(img.mean()) - 1.0) < 3e-3 and abs(float(hairpix.mean()) - 1.0) < 1e-2
     nori.nori_free(h)
 
 
