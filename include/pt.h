@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define PT_ABI_VERSION 1
+#define PT_ABI_VERSION 2
 
 /* ---- status codes ---------------------------------------------------- */
 #define PT_OK 0
@@ -121,6 +121,20 @@ typedef struct pt_grid {
 } pt_grid;
 
 /*
+ * pt_texture — one material texture as LoadTexture loads it
+ * (src/gpu/DXRApp_Textures.cpp:34-176): 8-bit RGBA, row 0 = top of the
+ * image, `srgb` = 1 for colour data stored sRGB-encoded (albedo maps; decoded
+ * to linear per texel before filtering), 0 for linear data (normal,
+ * roughness, specular, subsurface, alpha maps).  The library builds the mip
+ * chain.  pt_material's *TexIndex fields index pt_scene_desc.textures.
+ */
+typedef struct pt_texture {
+    uint32_t width, height;
+    const uint8_t *rgba8; /* 4 x width x height bytes */
+    uint32_t srgb;
+} pt_texture;
+
+/*
  * pt_scene_desc — the flattened scene CreateSceneBuffers uploads
  * (src/gpu/DXRApp_Scene.cpp:172-451).  Arrays are host memory owned by the
  * caller; pt_upload_scene copies them.  `indices` are local to each mesh
@@ -146,6 +160,8 @@ typedef struct pt_scene_desc {
     const pt_volume *volumes;
     uint32_t num_grids;
     const pt_grid *grids;
+    uint32_t num_textures;
+    const pt_texture *textures;
 } pt_scene_desc;
 
 /* Camera constants of shaders/Common.hlsli:31-51, built as
@@ -325,7 +341,9 @@ typedef struct pt_hit {
  * Closest hit (TraceClosestInline, shaders/RayQueryTrace.hlsli:36-81) and
  * occlusion (TraceShadowInline, shaders/RayQueryTrace.hlsli:88-129;
  * occluded_out = 1 when an opaque surface blocks, transmission_out = the
- * product of (1 - Fr) over mirror/dielectric surfaces crossed, 3 floats). */
+ * product of (1 - Fr) over mirror/dielectric surfaces crossed, 3 floats).
+ * Alpha-mapped triangles take the stochastic alpha test with the ray's index
+ * in the batch as its seed. */
 int pt_trace_closest(pt_ctx *ctx, const float *rays, size_t n, pt_hit *out, uint32_t location);
 int pt_trace_shadow(pt_ctx *ctx, const float *rays, size_t n, uint32_t *occluded_out,
                     float *transmission_out, uint32_t location);

@@ -681,6 +681,13 @@ struct Scene {
     std::vector<uint32_t> triMesh, triPrim;
     Bvh bvh;
     std::string err;
+    // material textures: RGBA8 mip chains (level l of texture t starts at
+    // texel texOff[t][l]), sRGB byte -> linear table
+    struct Tex { uint32_t w, h, levels, srgb; std::vector<size_t> off; };
+    std::vector<Tex> tex;
+    std::vector<uint8_t> texels;  // 4 bytes per texel
+    float srgbLut[256];
+    bool hasAlpha = false;
 };
 
 static inline F3 ld3(const std::vector<float> &b, uint32_t i) { return F3(b[3 * i], b[3 * i + 1], b[3 * i + 2]); }
@@ -1000,6 +1007,170 @@ static F3 interp_tangent(const Scene &s, uint32_t mesh, uint32_t prim, float bx,
 }
 
 // ---------------------------------------------------------------------------
+// Material textures (shaders/Shaders.hlsl:232-315, shaders/GeometryUtils.hlsli:
+// 120-154, src/gpu/DXRApp_Textures.cpp:34-176): RGBA8 with a box-filtered mip
+// chain, sRGB colour maps decoded per texel, trilinear filtering with wrap
+// addressing (the hardware sampler s0), LOD from the hit's UV footprint.
+// ---------------------------------------------------------------------------
+static void build_textures(Scene &s, const pt_scene_desc *d) {
+    for (uint32_t i = 0; i < 256; i++) {  // the _SRGB decode, in double
+        double v = i / 255.0;
+        s.srgbLut[i] = (float)(v <= 0.04045 ? v / 12.92 : std::pow((v + 0.055) / 1.055, 2.4));
+    }
+    for (uint32_t t = 0; t < d->num_textures; t++) {
+        const pt_texture &src = d->textures[t];
+        Scene::Tex tx{src.width, src.height, 1, src.srgb ? 1u : 0u, {}};
+        for (uint32_t dim = std::max(src.width, src.height); dim > 1; dim >>= 1) tx.levels++;
+        tx.off.push_back(s.texels.size() / 4);
+        s.texels.insert(s.texels.end(), src.rgba8, src.rgba8 + (size_t)src.width * src.height * 4);
+        uint32_t pw = src.width, ph = src.height;
+        for (uint32_t l = 1; l < tx.levels; l++) {  // integer mean of 2 x 2, edges repeated
+            uint32_t mw = std::max(pw / 2, 1u), mh = std::max(ph / 2, 1u);
+            size_t prev = tx.off[l - 1], cur = s.texels.size() / 4;
+            tx.off.push_back(cur);
+            s.texels.resize((cur + (size_t)mw * mh) * 4);
+            for (uint32_t y = 0; y < mh; y++)
+                for (uint32_t x = 0; x < mw; x++) {
+                    uint32_t sx = std::min(x * 2, pw - 1), sy = std::min(y * 2, ph - 1);
+                    uint32_t sx1 = std::min(sx + 1, pw - 1), sy1 = std::min(sy + 1, ph - 1);
+                    for (int c = 0; c < 4; c++) {
+                        auto at = [&](uint32_t xx, uint32_t yy) { return (int)s.texels[(prev + (size_t)yy * pw + xx) * 4 + c]; };
+                        s.texels[(cur + (size_t)y * mw + x) * 4 + c] =
+                            (uint8_t)((at(sx, sy) + at(sx1, sy) + at(sx, sy1) + at(sx1, sy1)) / 4);
+                    }
+                }
+            pw = mw;
+            ph = mh;
+        }
+        s.tex.push_back(std::move(tx));
+    }
+    for (const pt_material &m : s.mats)
+        if (m.indexCount && m.alphaTexIndex != PT_NO_TEXTURE) s.hasAlpha = true;
+}
+struct F4 { float x, y, z, w; };
+static F4 lerp4(F4 a, F4 b, float t) {
+    return {a.x + (b.x - a.x) * t, a.y + (b.y - a.y) * t, a.z + (b.z - a.z) * t, a.w + (b.w - a.w) * t};
+}
+static F4 tex_texel(const Scene &s, const Scene::Tex &t, uint32_t level, int W, int x, int y) {
+    const uint8_t *c = &s.texels[(t.off[level] + (size_t)y * W + x) * 4];
+    if (t.srgb) return {s.srgbLut[c[0]], s.srgbLut[c[1]], s.srgbLut[c[2]], (float)c[3] / 255.0f};
+    return {(float)c[0] / 255.0f, (float)c[1] / 255.0f, (float)c[2] / 255.0f, (float)c[3] / 255.0f};
+}
+static F4 tex_bilinear(const Scene &s, const Scene::Tex &t, uint32_t level, float u, float v) {
+    const int W = (int)std::max(t.w >> level, 1u), H = (int)std::max(t.h >> level, 1u);
+    u -= std::floor(u);
+    v -= std::floor(v);
+    float x = u * (float)W - 0.5f, y = v * (float)H - 0.5f;
+    float fx0 = std::floor(x), fy0 = std::floor(y);
+    float fx = x - fx0, fy = y - fy0;
+    int x0 = std::isfinite(fx0) ? (int)fx0 : 0, y0 = std::isfinite(fy0) ? (int)fy0 : 0;
+    int xa = ((x0 % W) + W) % W, xb = (((x0 + 1) % W) + W) % W;
+    int ya = ((y0 % H) + H) % H, yb = (((y0 + 1) % H) + H) % H;
+    F4 top = lerp4(tex_texel(s, t, level, W, xa, ya), tex_texel(s, t, level, W, xb, ya), fx);
+    F4 bot = lerp4(tex_texel(s, t, level, W, xa, yb), tex_texel(s, t, level, W, xb, yb), fx);
+    return lerp4(top, bot, fy);
+}
+static F4 tex_sample(const Scene &s, uint32_t index, float u, float v, float lod) {
+    const Scene::Tex &t = s.tex[index];
+    lod = std::min(std::max(lod, 0.0f), (float)(t.levels - 1));
+    uint32_t l0 = (uint32_t)std::floor(lod);
+    float f = lod - (float)l0;
+    F4 a = tex_bilinear(s, t, l0, u, v);
+    if (f > 0.0f && l0 + 1 < t.levels) a = lerp4(a, tex_bilinear(s, t, l0 + 1, u, v), f);
+    return a;
+}
+static float uv_footprint(const Scene &s, uint32_t mesh, uint32_t prim, float hitT, uint32_t W, uint32_t H) {  // :120-145
+    uint32_t i0, i1, i2;
+    tri_idx(s, mesh, prim, i0, i1, i2);
+    F3 p0 = ld3(s.pos, i0), p1 = ld3(s.pos, i1), p2 = ld3(s.pos, i2);
+    float u0 = s.uv[2 * i0], v0 = s.uv[2 * i0 + 1], u1 = s.uv[2 * i1], v1 = s.uv[2 * i1 + 1];
+    float u2 = s.uv[2 * i2], v2 = s.uv[2 * i2 + 1];
+    float worldArea = 0.5f * length(cross(p1 - p0, p2 - p0));
+    float uvArea = 0.5f * std::fabs((u1 - u0) * (v2 - v0) - (u2 - u0) * (v1 - v0));
+    if (worldArea < 1e-12f || uvArea < 1e-12f) return 0.0f;
+    float pixelAngle = 1.0f / (float)std::max(W, H);
+    return hitT * pixelAngle * std::sqrt(uvArea / worldArea);
+}
+static float tex_lod(const Scene &s, uint32_t index, float footprint) {  // :148-154
+    const Scene::Tex &t = s.tex[index];
+    float tpp = footprint * (float)std::max(t.w, t.h);
+    return std::max(std::log2(std::max(tpp, 1.0f)), 0.0f);
+}
+// Shaders.hlsl:232-315 on a copy of the hit's material; bends N.
+static void apply_textures(const Scene &s, pt_material &m, uint32_t mesh, uint32_t prim, float hitT, float bx, float by,
+                           F3 &N, uint32_t W, uint32_t H) {
+    float foot = uv_footprint(s, mesh, prim, hitT, W, H);
+    float u, v;
+    interp_uv(s, mesh, prim, bx, by, u, v);
+    F3 alb(m.albedo[0], m.albedo[1], m.albedo[2]);
+    if (m.albedoTexIndex != PT_NO_TEXTURE) {
+        F4 c = tex_sample(s, m.albedoTexIndex, u, v, tex_lod(s, m.albedoTexIndex, foot));
+        alb = F3(c.x, c.y, c.z);
+    }
+    if (m.normalTexIndex != PT_NO_TEXTURE) {
+        uint32_t i0, i1, i2;
+        tri_idx(s, mesh, prim, i0, i1, i2);
+        F3 p0 = ld3(s.pos, i0), p1 = ld3(s.pos, i1), p2 = ld3(s.pos, i2);
+        F3 e1 = p1 - p0, e2 = p2 - p0;
+        float u0 = s.uv[2 * i0], v0 = s.uv[2 * i0 + 1];
+        float du1 = s.uv[2 * i1] - u0, dv1 = s.uv[2 * i1 + 1] - v0;
+        float du2 = s.uv[2 * i2] - u0, dv2 = s.uv[2 * i2 + 1] - v0;
+        float det = du1 * dv2 - du2 * dv1;
+        F3 T, B;
+        if (std::fabs(det) > 1e-8f) {
+            float invDet = 1.0f / det;
+            T = normalize((dv2 * e1 - dv1 * e2) * invDet);
+            T = normalize(T - N * dot(N, T));
+            B = cross(N, T);
+        } else {
+            build_onb(N, T, B);
+        }
+        F4 c = tex_sample(s, m.normalTexIndex, u, v, tex_lod(s, m.normalTexIndex, foot));
+        F3 tn = F3(c.x, c.y, c.z) * 2.0f - F3(1.0f);
+        N = normalize(T * tn.x + B * tn.y + N * tn.z);
+    }
+    m.albedo[0] = alb.x; m.albedo[1] = alb.y; m.albedo[2] = alb.z;
+    if (m.type != PT_MAT_HAIR && m.roughnessTexIndex != PT_NO_TEXTURE) {
+        float r = tex_sample(s, m.roughnessTexIndex, u, v, tex_lod(s, m.roughnessTexIndex, foot)).x;
+        m.alpha = r;
+        m.roughness = r;
+    }
+    if (m.specularTexIndex != PT_NO_TEXTURE)
+        m.specular = tex_sample(s, m.specularTexIndex, u, v, tex_lod(s, m.specularTexIndex, foot)).x * 0.5f;
+    if (m.subsurfaceTexIndex != PT_NO_TEXTURE)
+        m.subsurface = tex_sample(s, m.subsurfaceTexIndex, u, v, tex_lod(s, m.subsurfaceTexIndex, foot)).x;
+}
+static bool has_shading_textures(const pt_material &m) {
+    return m.albedoTexIndex != PT_NO_TEXTURE || m.normalTexIndex != PT_NO_TEXTURE ||
+           m.roughnessTexIndex != PT_NO_TEXTURE || m.specularTexIndex != PT_NO_TEXTURE ||
+           m.subsurfaceTexIndex != PT_NO_TEXTURE;
+}
+// Stochastic alpha of an alpha-mapped candidate (shaders/RayQueryTrace.hlsli:
+// 50-62, 100-112): alpha at level 0 (.r; shadow rays: .a when below 1),
+// ignored below 0.01, kept with probability alpha^2.  The uniform is a hash
+// of (path seed, ray key, triangle) instead of the reference's PCG stream
+// threaded through candidates in hardware order, so the outcome of each
+// candidate does not depend on the traversal order.
+static bool alpha_pass(const Scene &s, uint32_t g, float bx, float by, uint32_t seed, uint32_t key, bool shadow) {
+    const pt_material &m = s.mats[s.triMesh[g]];
+    float u, v;
+    interp_uv(s, s.triMesh[g], s.triPrim[g], bx, by, u, v);
+    F4 c = tex_sample(s, m.alphaTexIndex, u, v, 0.0f);
+    float a = shadow ? (c.w < 1.0f ? c.w : c.x) : c.x;
+    if (a < 0.01f) return false;
+    uint32_t x = pcg_hash(seed ^ pcg_hash(key * 0x9e3779b9u ^ g));
+    float xi = std::min(float(x) * 2.3283064365386963e-10f, 0.99999994f);
+    return !(a * a < xi);
+}
+static inline uint32_t alpha_seed(uint32_t pixelSeed, uint32_t sample) {
+    return pcg_hash(pixelSeed * 0x85ebca6bu ^ pcg_hash(sample + 0x27d4eb2fu));
+}
+static inline uint32_t alpha_key(uint32_t bounce, uint32_t kind) { return bounce * 4u + kind; }
+static inline bool alpha_mapped(const Scene &s, uint32_t g) {
+    return s.mats[s.triMesh[g]].alphaTexIndex != PT_NO_TEXTURE;
+}
+
+// ---------------------------------------------------------------------------
 // BVH: binned SAH (16 bins, largest axis) as in src/cpu/accel.cpp:55-324,
 // single-threaded; triangle test = Moller-Trumbore of src/cpu/mesh.cpp:51-89.
 // ---------------------------------------------------------------------------
@@ -1114,7 +1285,7 @@ static bool tri_hit(const F3 &p0, const F3 &p1, const F3 &p2, const F3 &o, const
 }
 static thread_local uint64_t g_ext_rays = 0, g_shadow_rays = 0;
 struct Hit { bool hit; float t, u, v; uint32_t mesh, prim, gid; };
-static Hit trace_closest(const Scene &s, F3 o, F3 d, float tmin, float tmax) {
+static Hit trace_closest(const Scene &s, F3 o, F3 d, float tmin, float tmax, uint32_t seed = 0, uint32_t key = 0) {
     Hit h{false, tmax, 0, 0, 0, 0, 0};
     g_ext_rays++;
     if (s.bvh.nodes.empty()) return h;
@@ -1134,6 +1305,7 @@ static Hit trace_closest(const Scene &s, F3 o, F3 d, float tmin, float tmax) {
                 if (tri_hit(p0, p1, p2, o, d, tmin, h.t, u, v, t)) {
                     // equal-t ties resolve to the lower global triangle id
                     if (!h.hit || t < h.t || (t == h.t && g < h.gid)) {
+                        if (s.hasAlpha && alpha_mapped(s, g) && !alpha_pass(s, g, u, v, seed, key, false)) continue;
                         h.hit = true; h.t = t; h.u = u; h.v = v; h.gid = g;
                     }
                 }
@@ -1149,7 +1321,8 @@ static Hit trace_closest(const Scene &s, F3 o, F3 d, float tmin, float tmax) {
 // TraceShadowInline (shaders/RayQueryTrace.hlsli:88-129) for scenes without
 // alpha textures: an opaque hit occludes; mirror/dielectric surfaces in
 // [tmin, tmax] attenuate by (1 - Fr) with |cos| against the geometric normal.
-static bool trace_shadow(const Scene &s, F3 o, F3 d, float tmin, float tmax, F3 &trans) {
+static bool trace_shadow(const Scene &s, F3 o, F3 d, float tmin, float tmax, F3 &trans, uint32_t seed = 0,
+                         uint32_t key = 0) {
     trans = F3(1.0f);
     g_shadow_rays++;
     if (s.bvh.nodes.empty()) return false;
@@ -1169,6 +1342,10 @@ static bool trace_shadow(const Scene &s, F3 o, F3 d, float tmin, float tmax, F3 
                 tri_verts(s, g, p0, p1, p2);
                 float u, v, t;
                 if (!tri_hit(p0, p1, p2, o, d, tmin, tmax, u, v, t)) continue;
+                if (s.hasAlpha && alpha_mapped(s, g)) {  // occludes when the stochastic test keeps it
+                    if (alpha_pass(s, g, u, v, seed, key, true)) return true;
+                    continue;
+                }
                 const pt_material &m = s.mats[s.triMesh[g]];
                 if (m.type == PT_MAT_MIRROR || m.type == PT_MAT_DIELECTRIC) glass.push_back({g, t});
                 else return true;
@@ -1446,7 +1623,8 @@ static inline float env_pdf(const Ctx &c, F3 d) {
     return c.envMode == PT_ENV_ALIAS ? env_pdf_alias(*c.s, d) : env_pdf_cdf(*c.s, d);
 }
 
-static F3 mis_direct(const Ctx &c, F3 hp, F3 N, F3 Ng, F3 T, F3 B, F3 wil, const Mat<float> &m, float h, Rng &rng) {  // Emitter.hlsli:105-153
+static F3 mis_direct(const Ctx &c, F3 hp, F3 N, F3 Ng, F3 T, F3 B, F3 wil, const Mat<float> &m, float h, Rng &rng,
+                     uint32_t aseed, uint32_t bounce) {  // Emitter.hlsli:105-153
     const Scene &s = *c.s;
     EmitterSample es = sample_emitter(s, rng);
     if (!es.valid) return F3(0.0f);
@@ -1460,7 +1638,7 @@ static F3 mis_direct(const Ctx &c, F3 hp, F3 N, F3 Ng, F3 T, F3 B, F3 wil, const
     F3 sng = hair ? (dot(ww, Ng) >= 0.0f ? Ng : -Ng) : Ng;
     F3 so = offset_ray_origin(hp, sng, sng);
     F3 trans;
-    if (trace_shadow(s, so, ww, 0.0f, dist - 0.001f, trans)) return F3(0.0f);
+    if (trace_shadow(s, so, ww, 0.0f, dist - 0.001f, trans, aseed, alpha_key(bounce, 1u))) return F3(0.0f);
     F3 wol = to_local(ww, T, B, N);
     F3 f = material_eval(wil, wol, m, h);
     float pb = material_pdf(wil, wol, m, h);
@@ -1469,7 +1647,8 @@ static F3 mis_direct(const Ctx &c, F3 hp, F3 N, F3 Ng, F3 T, F3 B, F3 wil, const
     F3 vt = multi_volume_tr(s, so, ww, dist, rng);
     return es.rad * f * act / std::max(pe, 1e-20f) * w * vt * trans;
 }
-static F3 env_direct(const Ctx &c, F3 hp, F3 N, F3 Ng, F3 T, F3 B, F3 wil, const Mat<float> &m, float h, Rng &rng) {  // Emitter.hlsli:275-326
+static F3 env_direct(const Ctx &c, F3 hp, F3 N, F3 Ng, F3 T, F3 B, F3 wil, const Mat<float> &m, float h, Rng &rng,
+                     uint32_t aseed, uint32_t bounce) {  // Emitter.hlsli:275-326
     const Scene &s = *c.s;
     float u1 = next_float(rng), u2 = next_float(rng);
     F3 ww, Le;
@@ -1483,7 +1662,7 @@ static F3 env_direct(const Ctx &c, F3 hp, F3 N, F3 Ng, F3 T, F3 B, F3 wil, const
     F3 sng = hair ? (dot(ww, Ng) >= 0.0f ? Ng : -Ng) : Ng;
     F3 so = offset_ray_origin(hp, sng, sng);
     F3 trans;
-    if (trace_shadow(s, so, ww, 0.0f, 1e20f, trans)) return F3(0.0f);
+    if (trace_shadow(s, so, ww, 0.0f, 1e20f, trans, aseed, alpha_key(bounce, 2u))) return F3(0.0f);
     F3 wol = to_local(ww, T, B, N);
     F3 f = material_eval(wil, wol, m, h);
     float pb = material_pdf(wil, wol, m, h);
@@ -1499,7 +1678,7 @@ static bool vol_nee_skip(const pt_volume &v, F3 p) {
     float md = std::min(std::min(dmn.x, dmn.y), std::min(dmn.z, std::min(dmx.x, std::min(dmx.y, dmx.z))));
     return md * smin > 8.0f;
 }
-static F3 vol_nee_area(const Ctx &c, F3 sp, F3 wo, uint32_t vi, Rng &rng) {  // Emitter.hlsli:334-390
+static F3 vol_nee_area(const Ctx &c, F3 sp, F3 wo, uint32_t vi, Rng &rng, uint32_t aseed, uint32_t bounce) {  // Emitter.hlsli:334-390
     const Scene &s = *c.s;
     const pt_volume &v = s.vols[vi];
     if (vol_nee_skip(v, sp)) return F3(0.0f);
@@ -1511,14 +1690,14 @@ static F3 vol_nee_area(const Ctx &c, F3 sp, F3 wo, uint32_t vi, Rng &rng) {  // 
     float cl = dot(es.nrm, -wi);
     if (cl <= 0.0f) return F3(0.0f);
     F3 trans;
-    if (trace_shadow(s, sp, wi, 0.001f, dist - 0.001f, trans)) return F3(0.0f);
+    if (trace_shadow(s, sp, wi, 0.001f, dist - 0.001f, trans, aseed, alpha_key(bounce, 1u))) return F3(0.0f);
     float fp = hg(dot(wo, wi), v.phase_g);
     float pe = es.pdfArea * dist * dist / cl;
     float w = balance_heuristic(pe, fp);
     F3 vt = multi_volume_tr(s, sp, wi, dist, rng);
     return es.rad * fp / std::max(pe, 1e-20f) * w * vt * trans;
 }
-static F3 vol_nee_env(const Ctx &c, F3 sp, F3 wo, uint32_t vi, Rng &rng) {  // Emitter.hlsli:392-434
+static F3 vol_nee_env(const Ctx &c, F3 sp, F3 wo, uint32_t vi, Rng &rng, uint32_t aseed, uint32_t bounce) {  // Emitter.hlsli:392-434
     const Scene &s = *c.s;
     const pt_volume &v = s.vols[vi];
     if (vol_nee_skip(v, sp)) return F3(0.0f);
@@ -1528,7 +1707,7 @@ static F3 vol_nee_env(const Ctx &c, F3 sp, F3 wo, uint32_t vi, Rng &rng) {  // E
     env_sample(c, u1, u2, wi, Le, pe);
     if (pe <= 0.0f) return F3(0.0f);
     F3 trans;
-    if (trace_shadow(s, sp, wi, 0.001f, 1e20f, trans)) return F3(0.0f);
+    if (trace_shadow(s, sp, wi, 0.001f, 1e20f, trans, aseed, alpha_key(bounce, 2u))) return F3(0.0f);
     float fp = hg(dot(wo, wi), v.phase_g);
     float w = balance_heuristic(pe, fp);
     F3 vt = multi_volume_tr(s, sp, wi, 1e20f, rng);
@@ -1571,8 +1750,9 @@ static F3 trace_path(const Ctx &c, const pt_render_params &P, uint32_t px, uint3
     }
     F3 Lo(0.0f), thr(1.0f);
     float lastPdf = 0.0f, eta = 1.0f;
+    const uint32_t aseed = s.hasAlpha ? alpha_seed(rng.pixelSeed, rng.sampleIndex) : 0u;
     for (int bounce = 0; bounce < (int)P.max_depth; bounce++) {
-        Hit hit = trace_closest(s, ro, rd, tmin, tmax);
+        Hit hit = trace_closest(s, ro, rd, tmin, tmax, aseed, alpha_key((uint32_t)bounce, 0u));
         if (st) st->ext++;
         bool volScat = false;
         if (!s.vols.empty()) {  // Shaders.hlsl:133-179
@@ -1588,8 +1768,8 @@ static F3 trace_path(const Ctx &c, const pt_render_params &P, uint32_t px, uint3
                 F3 sst = vol_sigma_t(v);
                 F3 spos = ro + tsc * rd;
                 thr *= F3(v.sigma_s[0], v.sigma_s[1], v.sigma_s[2]) / vmax(sst, F3(1e-20f));
-                Lo += thr * vol_nee_area(c, spos, rd, svi, rng);
-                Lo += thr * vol_nee_env(c, spos, rd, svi, rng);
+                Lo += thr * vol_nee_area(c, spos, rd, svi, rng, aseed, (uint32_t)bounce);
+                Lo += thr * vol_nee_env(c, spos, rd, svi, rng, aseed, (uint32_t)bounce);
                 float x1 = next_float(rng), x2 = next_float(rng);
                 float pp;
                 F3 nd = sample_hg(rd, v.phase_g, x1, x2, pp);
@@ -1611,13 +1791,14 @@ static F3 trace_path(const Ctx &c, const pt_render_params &P, uint32_t px, uint3
             F3 hp = ro + rd * hit.t;
             F3 N = normalize(interp_normal(s, hit.mesh, hit.prim, hit.u, hit.v));
             F3 Ng = normalize(geometric_normal(s, hit.mesh, hit.prim));
-            const pt_material &pm = s.mats[hit.mesh];
-            Mat<float> m = Mat<float>::from(pm);
+            pt_material pm = s.mats[hit.mesh];
             float hu, hv;
             interp_uv(s, hit.mesh, hit.prim, hit.u, hit.v, hu, hv);
             bool back = dot(Ng, rd) > 0.0f;
             if (back) Ng = -Ng;
             if (dot(N, Ng) < 0.0f) N = -N;
+            if (has_shading_textures(pm)) apply_textures(s, pm, hit.mesh, hit.prim, hit.t, hit.u, hit.v, N, P.width, P.height);
+            Mat<float> m = Mat<float>::from(pm);
             if (pm.isEmitter) {  // Shaders.hlsl:317-335
                 F3 rad(pm.radiance[0], pm.radiance[1], pm.radiance[2]);
                 if (lastPdf == 0.0f) Lo += thr * rad;
@@ -1692,9 +1873,9 @@ static F3 trace_path(const Ctx &c, const pt_render_params &P, uint32_t px, uint3
                 if (refr) eta *= etaI / etaT;
             } else if (pm.type == PT_MAT_DIFFUSE || pm.type == PT_MAT_MICROFACET || pm.type == PT_MAT_DISNEY ||
                        pm.type == PT_MAT_HAIR) {  // Shaders.hlsl:473-511
-                Lo += thr * mis_direct(c, hp, N, Ng, T, B, wil, m, h, rng);
+                Lo += thr * mis_direct(c, hp, N, Ng, T, B, wil, m, h, rng, aseed, (uint32_t)bounce);
                 if (st && s.emitterCount) st->shadow++;
-                Lo += thr * env_direct(c, hp, N, Ng, T, B, wil, m, h, rng);
+                Lo += thr * env_direct(c, hp, N, Ng, T, B, wil, m, h, rng, aseed, (uint32_t)bounce);
                 if (st) st->shadow++;
                 float u[4];
                 int k = (pm.type == PT_MAT_DIFFUSE || pm.type == PT_MAT_MICROFACET) ? 2 : (pm.type == PT_MAT_DISNEY ? 3 : 4);
@@ -1764,6 +1945,7 @@ void *or_scene_create(const pt_scene_desc *d) {
         s->grids.push_back(std::move(gr));
     }
     build_majorants(*s);
+    build_textures(*s, d);
     build_bvh(*s);
     return s;
 }
@@ -1952,7 +2134,7 @@ void or_trace_closest(void *sp, const float *rays, size_t n, pt_hit *out) {
     Scene *s = static_cast<Scene *>(sp);
     for (size_t i = 0; i < n; i++) {
         const float *r = &rays[8 * i];
-        Hit h = trace_closest(*s, F3(r[0], r[1], r[2]), F3(r[4], r[5], r[6]), r[3], r[7]);
+        Hit h = trace_closest(*s, F3(r[0], r[1], r[2]), F3(r[4], r[5], r[6]), r[3], r[7], (uint32_t)i, 0u);
         out[i] = pt_hit{h.hit ? h.t : 0.0f, h.mesh, h.prim, h.u, h.v, h.hit ? 1u : 0u};
     }
 }
@@ -1961,7 +2143,7 @@ void or_trace_shadow(void *sp, const float *rays, size_t n, uint32_t *occ, float
     for (size_t i = 0; i < n; i++) {
         const float *r = &rays[8 * i];
         F3 t;
-        occ[i] = trace_shadow(*s, F3(r[0], r[1], r[2]), F3(r[4], r[5], r[6]), r[3], r[7], t) ? 1u : 0u;
+        occ[i] = trace_shadow(*s, F3(r[0], r[1], r[2]), F3(r[4], r[5], r[6]), r[3], r[7], t, (uint32_t)i, 0u) ? 1u : 0u;
         trans[3 * i] = t.x; trans[3 * i + 1] = t.y; trans[3 * i + 2] = t.z;
     }
 }

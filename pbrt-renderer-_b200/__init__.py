@@ -60,6 +60,10 @@ class pt_grid(C.Structure):
     _fields_ = [("w", C.c_uint32), ("h", C.c_uint32), ("d", C.c_uint32), ("data", C.POINTER(C.c_float))]
 
 
+class pt_texture(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("rgba8", C.POINTER(C.c_uint8)), ("srgb", C.c_uint32)]
+
+
 class pt_scene_desc(C.Structure):
     _fields_ = [
         ("num_vertices", C.c_uint32), ("positions", C.POINTER(C.c_float)), ("normals", C.POINTER(C.c_float)),
@@ -70,6 +74,7 @@ class pt_scene_desc(C.Structure):
         ("env_scale", C.c_float), ("ev_compensation", C.c_float),
         ("num_volumes", C.c_uint32), ("volumes", C.POINTER(pt_volume)),
         ("num_grids", C.c_uint32), ("grids", C.POINTER(pt_grid)),
+        ("num_textures", C.c_uint32), ("textures", C.POINTER(pt_texture)),
     ]
 
 
@@ -118,7 +123,9 @@ class Scene:
     """Flattened scene arrays (the buffers CreateSceneBuffers uploads) + pt_scene_desc."""
 
     def __init__(self, positions, indices, materials, normals=None, texcoords=None, tangents=None,
-                 env_rgb=None, env_scale=1.0, ev_compensation=0.0, volumes=(), grids=()):
+                 env_rgb=None, env_scale=1.0, ev_compensation=0.0, volumes=(), grids=(), textures=()):
+        """textures: (H, W, 4) uint8 RGBA arrays, or (array, srgb) pairs (srgb
+        defaults to False); materials refer to them by index."""
         self.positions = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
         self.indices = np.ascontiguousarray(indices, np.uint32).reshape(-1)
         nv = len(self.positions)
@@ -136,6 +143,16 @@ class Scene:
         self.grid_arrays = [np.ascontiguousarray(g, np.float32) for g in grids]
         gl = [pt_grid(g.shape[2], g.shape[1], g.shape[0], fptr(g)) for g in self.grid_arrays]
         self.grids = (pt_grid * max(1, len(gl)))(*gl)
+        self.tex_arrays, self.tex_srgb, tl = [], [], []
+        for t in textures:
+            img, srgb = (t if isinstance(t, tuple) else (t, False))
+            self.tex_srgb.append(bool(srgb))
+            img = np.ascontiguousarray(img, np.uint8)
+            if img.ndim != 3 or img.shape[2] != 4:
+                raise ValueError("textures are (H, W, 4) uint8 RGBA arrays")
+            self.tex_arrays.append(img)
+            tl.append(pt_texture(img.shape[1], img.shape[0], img.ctypes.data_as(C.POINTER(C.c_uint8)), int(srgb)))
+        self.textures = (pt_texture * max(1, len(tl)))(*tl)
 
     @property
     def num_triangles(self):
@@ -160,6 +177,8 @@ class Scene:
         d.volumes = C.cast(self.volumes, C.POINTER(pt_volume))
         d.num_grids = len(self.grid_arrays)
         d.grids = C.cast(self.grids, C.POINTER(pt_grid))
+        d.num_textures = len(self.tex_arrays)
+        d.textures = C.cast(self.textures, C.POINTER(pt_texture))
         self._desc = d
         return d
 

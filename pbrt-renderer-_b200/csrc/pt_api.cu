@@ -208,7 +208,9 @@ __global__ void k_trace_closest(DevScene S, const float *rays, size_t n, pt_hit 
     size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float *r = rays + 8 * i;
-    Hit h = trace_closest(S, make_float3(r[0], r[1], r[2]), make_float3(r[4], r[5], r[6]), r[3], r[7], err);
+    // alpha tests: path seed = ray index, key 0
+    Hit h = trace_closest(S, make_float3(r[0], r[1], r[2]), make_float3(r[4], r[5], r[6]), r[3], r[7], err,
+                          (uint32_t)i, 0u);
     pt_hit o;
     if (h.gid != 0xFFFFFFFFu) {
         uint32_t m = S.triMesh[h.gid];
@@ -223,7 +225,8 @@ __global__ void k_trace_shadow(DevScene S, const float *rays, size_t n, uint32_t
     if (i >= n) return;
     const float *r = rays + 8 * i;
     float3 t;
-    occ[i] = trace_shadow(S, make_float3(r[0], r[1], r[2]), make_float3(r[4], r[5], r[6]), r[3], r[7], t, err) ? 1u : 0u;
+    occ[i] = trace_shadow(S, make_float3(r[0], r[1], r[2]), make_float3(r[4], r[5], r[6]), r[3], r[7], t, err,
+                          (uint32_t)i, 0u) ? 1u : 0u;
     tr[3 * i] = t.x; tr[3 * i + 1] = t.y; tr[3 * i + 2] = t.z;
 }
 
@@ -357,6 +360,74 @@ int pt_set_stream(pt_ctx *ctx, void *stream) {
 
 const char *pt_last_error(const pt_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
+// LoadTexture's mip chain (src/gpu/DXRApp_Textures.cpp:49-95): levels halve
+// (integer division, at least 1) down to 1 x 1, each texel the truncated
+// integer mean of the 2 x 2 texels below it, edge texels repeated.
+static void build_mips(const pt_texture &t, std::vector<uchar4> &texels, DevTexture &dt) {
+    uint32_t levels = 1;
+    for (uint32_t dim = std::max(t.width, t.height); dim > 1; dim >>= 1) levels++;
+    dt.w = t.width;
+    dt.h = t.height;
+    dt.levels = levels;
+    dt.srgb = t.srgb ? 1u : 0u;
+    size_t base = texels.size();
+    dt.off[0] = (uint32_t)base;
+    texels.resize(base + (size_t)t.width * t.height);
+    std::memcpy(&texels[base], t.rgba8, (size_t)t.width * t.height * 4);
+    uint32_t pw = t.width, ph = t.height;
+    for (uint32_t m = 1; m < levels; m++) {
+        uint32_t mw = std::max(pw / 2, 1u), mh = std::max(ph / 2, 1u);
+        size_t src = dt.off[m - 1], dst = texels.size();
+        dt.off[m] = (uint32_t)dst;
+        texels.resize(dst + (size_t)mw * mh);
+        for (uint32_t y = 0; y < mh; y++)
+            for (uint32_t x = 0; x < mw; x++) {
+                uint32_t sx = std::min(x * 2, pw - 1), sy = std::min(y * 2, ph - 1);
+                uint32_t sx1 = std::min(sx + 1, pw - 1), sy1 = std::min(sy + 1, ph - 1);
+                const uchar4 a = texels[src + (size_t)sy * pw + sx], b = texels[src + (size_t)sy * pw + sx1];
+                const uchar4 c = texels[src + (size_t)sy1 * pw + sx], e = texels[src + (size_t)sy1 * pw + sx1];
+                texels[dst + (size_t)y * mw + x] =
+                    make_uchar4((unsigned char)((a.x + b.x + c.x + e.x) / 4), (unsigned char)((a.y + b.y + c.y + e.y) / 4),
+                                (unsigned char)((a.z + b.z + c.z + e.z) / 4), (unsigned char)((a.w + b.w + c.w + e.w) / 4));
+            }
+        pw = mw;
+        ph = mh;
+    }
+}
+
+// sRGB-encoded byte -> linear (the _SRGB format decode: v / 12.92 up to
+// 0.04045, ((v + 0.055) / 1.055)^2.4 above), evaluated in double.
+static float srgb_to_linear(uint32_t byte) {
+    double v = byte / 255.0;
+    return (float)(v <= 0.04045 ? v / 12.92 : std::pow((v + 0.055) / 1.055, 2.4));
+}
+
+static int upload_textures(pt_ctx *ctx, const pt_scene_desc *d) {
+    DevScene &S = ctx->S;
+    std::vector<DevTexture> dts(std::max(1u, d->num_textures));
+    std::vector<uchar4> texels;
+    for (uint32_t t = 0; t < d->num_textures; t++) build_mips(d->textures[t], texels, dts[t]);
+    if (texels.empty()) texels.push_back(make_uchar4(0, 0, 0, 0));
+    float lut[256];
+    for (uint32_t i = 0; i < 256; i++) lut[i] = srgb_to_linear(i);
+    DevTexture *dtex;
+    uchar4 *dtexels;
+    float *dlut;
+    PT_CUDA(ctx->alloc_scene(&dtex, dts.size()));
+    PT_CUDA(ctx->alloc_scene(&dtexels, texels.size()));
+    PT_CUDA(ctx->alloc_scene(&dlut, 256));
+    PT_CUDA(cudaMemcpyAsync(dtex, dts.data(), dts.size() * sizeof(DevTexture), cudaMemcpyHostToDevice, ctx->stream));
+    PT_CUDA(cudaMemcpyAsync(dtexels, texels.data(), texels.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+    PT_CUDA(cudaMemcpyAsync(dlut, lut, sizeof(lut), cudaMemcpyHostToDevice, ctx->stream));
+    // the host arrays above are freed on return: finish the copies first
+    PT_CUDA(cudaStreamSynchronize(ctx->stream));
+    S.tex = dtex;
+    S.texels = dtexels;
+    S.srgbLut = dlut;
+    S.numTex = d->num_textures;
+    return PT_OK;
+}
+
 int pt_upload_scene(pt_ctx *ctx, const pt_scene_desc *d) {
     if (!ctx) return PT_E_INVALID;
     if (!d) return ctx->fail(PT_E_INVALID, "null scene");
@@ -371,15 +442,17 @@ int pt_upload_scene(pt_ctx *ctx, const pt_scene_desc *d) {
     std::vector<pt_material> mats(d->materials, d->materials + d->num_meshes);
     std::vector<uint32_t> meshFirstTri(std::max(1u, d->num_meshes), 0);
     uint32_t numTris = 0;
-    bool hasGlass = false;
+    bool hasGlass = false, hasAlpha = false;
     uint32_t clsMask = 1u << CLS_MISS;  // shading classes the scene can produce
+    std::vector<uint32_t> meshClass(std::max(1u, d->num_meshes), 0u);
     for (uint32_t m = 0; m < d->num_meshes; m++) {
         const pt_material &pm = mats[m];
         if (pm.type > PT_MAT_SUBSURFACE) return ctx->fail(PT_E_INVALID, "unknown material type");
         if (pm.type == PT_MAT_SUBSURFACE) return ctx->fail(PT_E_UNSUPPORTED, "subsurface materials are not built");
-        const uint32_t *tex = &pm.albedoTexIndex;
+        const uint32_t *tex = &pm.albedoTexIndex;  // albedo .. alpha: 7 consecutive indices
         for (int t = 0; t < 7; t++)
-            if (tex[t] != PT_NO_TEXTURE) return ctx->fail(PT_E_UNSUPPORTED, "textured materials are not built");
+            if (tex[t] != PT_NO_TEXTURE && tex[t] >= d->num_textures)
+                return ctx->fail(PT_E_INVALID, "material texture index out of range");
         if (pm.indexCount % 3) return ctx->fail(PT_E_INVALID, "indexCount is not a multiple of 3");
         if ((uint64_t)pm.indexOffset + pm.indexCount > d->num_indices) return ctx->fail(PT_E_INVALID, "index range");
         if ((uint64_t)pm.vertexOffset + pm.vertexCount > d->num_vertices) return ctx->fail(PT_E_INVALID, "vertex range");
@@ -388,7 +461,15 @@ int pt_upload_scene(pt_ctx *ctx, const pt_scene_desc *d) {
         meshFirstTri[m] = numTris;
         numTris += pm.indexCount / 3;
         hasGlass |= pm.type == PT_MAT_MIRROR || pm.type == PT_MAT_DIELECTRIC;
-        if (pm.indexCount) clsMask |= 1u << shade_class(true, pm.isEmitter != 0, pm.type);
+        meshClass[m] = (uint32_t)shade_class(true, pm.isEmitter != 0, pm.type, has_shading_textures(pm));
+        if (pm.indexCount) clsMask |= 1u << meshClass[m];
+        if (pm.indexCount && pm.alphaTexIndex != PT_NO_TEXTURE) hasAlpha = true;
+    }
+    if (d->num_textures && !d->textures) return ctx->fail(PT_E_INVALID, "textures is null");
+    for (uint32_t t = 0; t < d->num_textures; t++) {
+        const pt_texture &tx = d->textures[t];
+        if (!tx.rgba8 || !tx.width || !tx.height) return ctx->fail(PT_E_INVALID, "empty texture");
+        if (tx.width > 32768u || tx.height > 32768u) return ctx->fail(PT_E_INVALID, "texture larger than 32768");
     }
     for (uint32_t v = 0; v < d->num_volumes; v++) {
         const pt_volume &vol = d->volumes[v];
@@ -472,6 +553,8 @@ int pt_upload_scene(pt_ctx *ctx, const pt_scene_desc *d) {
     PT_CUDA(ctx->alloc_scene(&dmft, meshFirstTri.size()));
     PT_CUDA(ctx->alloc_scene(&dcdf, all.size() + 1));
     PT_CUDA(ctx->alloc_scene(&demit, (size_t)ne + 1));
+    uint32_t *dmcls;
+    PT_CUDA(ctx->alloc_scene(&dmcls, meshClass.size()));
     auto h2d = [&](void *dst, const void *src, size_t bytes) -> int {
         if (!bytes) return PT_OK;
         cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
@@ -490,8 +573,11 @@ int pt_upload_scene(pt_ctx *ctx, const pt_scene_desc *d) {
     if ((rc = h2d(dmft, meshFirstTri.data(), meshFirstTri.size() * 4))) return rc;
     if ((rc = h2d(dcdf, all.data(), all.size() * 4))) return rc;
     if ((rc = h2d(demit, emitters.data(), emitters.size() * 4))) return rc;
+    if ((rc = h2d(dmcls, meshClass.data(), meshClass.size() * 4))) return rc;
+    if ((rc = upload_textures(ctx, d))) return rc;
+    S.hasAlpha = hasAlpha ? 1u : 0u;
     S.pos = dpos; S.nrm = dnrm; S.uv = duv; S.tan = dtan; S.idx = didx;
-    S.mats = dmats; S.numMeshes = d->num_meshes; S.meshFirstTri = dmft;
+    S.mats = dmats; S.meshClass = dmcls; S.numMeshes = d->num_meshes; S.meshFirstTri = dmft;
     S.emitterCdf = dcdf; S.emitterList = demit; S.emitterCount = ne;
     S.hasGlass = hasGlass ? 1u : 0u;
     // --- BVH ----------------------------------------------------------------------

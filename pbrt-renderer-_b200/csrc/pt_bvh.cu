@@ -304,7 +304,7 @@ __global__ void k_collapse(CollapseIn C, const int2 *__restrict__ qin, uint32_t 
                 float3 e1 = p1 - p0, e2 = p2 - p0;
                 float4 *t = C.tri + 3u * (triBase + toff + k);
                 t[0] = make_float4(p0.x, p0.y, p0.z, __uint_as_float(g));
-                t[1] = make_float4(e1.x, e1.y, e1.z, 0.0f);
+                t[1] = make_float4(e1.x, e1.y, e1.z, __uint_as_float(m.alphaTexIndex != PT_NO_TEXTURE ? 1u : 0u));
                 t[2] = make_float4(e2.x, e2.y, e2.z, 0.0f);
             }
             toff += count;

@@ -35,13 +35,15 @@ struct BVH8Node { uint4 n[5]; };
 
 struct DevScene {
     // geometry in BVH8 leaf order: 3 x float4 per triangle
-    // (v0.xyz, gid bits), (e1 = v1 - v0, 0), (e2 = v2 - v0, 0)
+    // (v0.xyz, gid bits), (e1 = v1 - v0, alpha flag bits), (e2 = v2 - v0, 0);
+    // alpha flag = 1 when the triangle's material has an alpha map
     const float4 *tri;
     const BVH8Node *nodes;
     uint32_t numTris, numNodes;
     const uint32_t *triMesh;      // global triangle id -> mesh
     const uint32_t *meshFirstTri; // mesh -> first global triangle id
     const pt_material *mats;
+    const uint32_t *meshClass;    // mesh -> shading class of its hits
     uint32_t numMeshes;
     uint32_t hasGlass;            // any mirror/dielectric mesh (non-opaque for shadow rays)
     const float *pos, *nrm, *uv, *tan;
@@ -63,6 +65,20 @@ struct DevScene {
     uint32_t numVols;
     // sampler tables
     const uint32_t *sobol1;     // 4 x 256 GF(2) product table of Sobol dimension 1
+    // material textures: RGBA8 mip chains, sRGB decode table
+    const struct DevTexture *tex;
+    const uchar4 *texels;
+    const float *srgbLut;       // 256 entries: sRGB-encoded byte -> linear
+    uint32_t numTex;
+    uint32_t hasAlpha;          // any alpha-mapped mesh (alpha-tested triangles)
+};
+
+// One texture's mip chain in DevScene::texels (level l: max(w >> l, 1) x
+// max(h >> l, 1) texels starting at off[l]).
+constexpr int kMaxTexLevels = 16;
+struct DevTexture {
+    uint32_t w, h, levels, srgb;
+    uint32_t off[kMaxTexLevels];
 };
 
 // ---------------------------------------------------------------------------
@@ -471,6 +487,106 @@ __device__ inline float3 multi_volume_tr(const DevScene &S, float3 o, float3 d, 
 }
 
 // ---------------------------------------------------------------------------
+// material textures: trilinear, wrap in u and v (sampler s0 of
+// src/gpu/DXRApp_Pipeline.cpp:49-53), texel centres at i + 0.5; sRGB texels
+// are decoded to linear before filtering, as an _SRGB format is
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float4 tex_texel(const DevScene &S, const DevTexture &t, uint32_t level, int W, int x,
+                                            int y) {
+    uchar4 c = __ldg(&S.texels[t.off[level] + (uint32_t)y * (uint32_t)W + (uint32_t)x]);
+    if (t.srgb)
+        return make_float4(__ldg(S.srgbLut + c.x), __ldg(S.srgbLut + c.y), __ldg(S.srgbLut + c.z),
+                           (float)c.w / 255.0f);
+    return make_float4((float)c.x / 255.0f, (float)c.y / 255.0f, (float)c.z / 255.0f, (float)c.w / 255.0f);
+}
+__device__ __forceinline__ float4 lerp4(float4 a, float4 b, float t) {
+    return make_float4(a.x + (b.x - a.x) * t, a.y + (b.y - a.y) * t, a.z + (b.z - a.z) * t, a.w + (b.w - a.w) * t);
+}
+__device__ __forceinline__ float4 tex_bilinear(const DevScene &S, const DevTexture &t, uint32_t level, float u,
+                                               float v) {
+    const int W = (int)max(t.w >> level, 1u), H = (int)max(t.h >> level, 1u);
+    u -= floorf(u);
+    v -= floorf(v);
+    float x = u * (float)W - 0.5f, y = v * (float)H - 0.5f;
+    float fx0 = floorf(x), fy0 = floorf(y);
+    float fx = x - fx0, fy = y - fy0;
+    int x0 = (int)fx0, y0 = (int)fy0;
+    int xa = ((x0 % W) + W) % W, xb = (((x0 + 1) % W) + W) % W;
+    int ya = ((y0 % H) + H) % H, yb = (((y0 + 1) % H) + H) % H;
+    float4 top = lerp4(tex_texel(S, t, level, W, xa, ya), tex_texel(S, t, level, W, xb, ya), fx);
+    float4 bot = lerp4(tex_texel(S, t, level, W, xa, yb), tex_texel(S, t, level, W, xb, yb), fx);
+    return lerp4(top, bot, fy);
+}
+// SampleLevel(g_sampler, uv, lod): linear between the two nearest mip levels.
+__device__ __forceinline__ float4 tex_sample(const DevScene &S, uint32_t index, float u, float v, float lod) {
+    const DevTexture &t = S.tex[index];
+    lod = fminf(fmaxf(lod, 0.0f), (float)(t.levels - 1));
+    uint32_t l0 = (uint32_t)floorf(lod);
+    float f = lod - (float)l0;
+    float4 a = tex_bilinear(S, t, l0, u, v);
+    if (f > 0.0f && l0 + 1 < t.levels) a = lerp4(a, tex_bilinear(S, t, l0 + 1, u, v), f);
+    return a;
+}
+// ComputeUVFootprint (shaders/GeometryUtils.hlsli:120-145): world-space pixel
+// footprint at distance hitT mapped to UV space by the triangle's UV/world
+// area ratio.
+__device__ __forceinline__ float uv_footprint(const DevScene &S, uint32_t mesh, uint32_t prim, float hitT,
+                                              uint32_t width, uint32_t height) {
+    uint32_t i0, i1, i2;
+    tri_vidx(S, mesh, prim, i0, i1, i2);
+    float3 p0 = ld3(S.pos, i0), p1 = ld3(S.pos, i1), p2 = ld3(S.pos, i2);
+    float u0 = __ldg(S.uv + 2 * i0), v0 = __ldg(S.uv + 2 * i0 + 1);
+    float u1 = __ldg(S.uv + 2 * i1), v1 = __ldg(S.uv + 2 * i1 + 1);
+    float u2 = __ldg(S.uv + 2 * i2), v2 = __ldg(S.uv + 2 * i2 + 1);
+    float worldArea = 0.5f * len(cross(p1 - p0, p2 - p0));
+    float uvArea = 0.5f * fabsf((u1 - u0) * (v2 - v0) - (u2 - u0) * (v1 - v0));
+    if (worldArea < 1e-12f || uvArea < 1e-12f) return 0.0f;
+    float pixelAngle = 1.0f / (float)max(width, height);
+    return hitT * pixelAngle * sqrtf(uvArea / worldArea);
+}
+// ComputeTexLOD (shaders/GeometryUtils.hlsli:148-154).
+__device__ __forceinline__ float tex_lod(const DevScene &S, uint32_t index, float footprint) {
+    const DevTexture &t = S.tex[index];
+    float texelsPerPixel = footprint * (float)max(t.w, t.h);
+    return fmaxf(log2f(fmaxf(texelsPerPixel, 1.0f)), 0.0f);
+}
+__device__ __forceinline__ float2 interp_uv(const DevScene &S, uint32_t i0, uint32_t i1, uint32_t i2, float b1,
+                                            float b2) {
+    float w0 = 1.0f - b1 - b2;
+    return make_float2(__ldg(S.uv + 2 * i0) * w0 + __ldg(S.uv + 2 * i1) * b1 + __ldg(S.uv + 2 * i2) * b2,
+                       __ldg(S.uv + 2 * i0 + 1) * w0 + __ldg(S.uv + 2 * i1 + 1) * b1 + __ldg(S.uv + 2 * i2 + 1) * b2);
+}
+
+// Stochastic alpha test of an alpha-mapped candidate hit (PrimaryAnyHit /
+// ShadowAnyHit of shaders/RayQueryTrace.hlsli:50-62,100-112): alpha from
+// mip level 0 (closest hit: .r; shadow: .a when below 1, else .r), ignored
+// below 0.01, kept with probability alpha^2.  The reference draws the
+// uniform from a PCG stream threaded through the candidates in hardware
+// traversal order; here it is a hash of (path seed, ray key, triangle), so
+// the decision for a candidate does not depend on the order in which a
+// traversal meets the candidates.
+__device__ __forceinline__ bool alpha_pass(const DevScene &S, uint32_t gid, float b1, float b2, uint32_t seed,
+                                           uint32_t key, bool shadow) {
+    uint32_t mesh = __ldg(S.triMesh + gid);
+    uint32_t prim = gid - __ldg(S.meshFirstTri + mesh);
+    uint32_t i0, i1, i2;
+    tri_vidx(S, mesh, prim, i0, i1, i2);
+    float2 uv = interp_uv(S, i0, i1, i2, b1, b2);
+    float4 c = tex_sample(S, __ldg(&S.mats[mesh].alphaTexIndex), uv.x, uv.y, 0.0f);
+    float a = shadow ? (c.w < 1.0f ? c.w : c.x) : c.x;
+    if (a < 0.01f) return false;
+    float xi = u32_to_unit(pcg_hash(seed ^ pcg_hash(key * 0x9e3779b9u ^ gid)));
+    return !(a * a < xi);
+}
+// Per-path seed of the alpha tests, fixed for the path: the sampler's pixel
+// seed and sample index.
+__device__ __forceinline__ uint32_t alpha_seed(uint32_t pixelSeed, uint32_t sample) {
+    return pcg_hash(pixelSeed * 0x85ebca6bu ^ pcg_hash(sample + 0x27d4eb2fu));
+}
+// Ray keys: extension ray of bounce b, area / envmap NEE shadow ray of bounce b.
+__device__ __forceinline__ uint32_t alpha_key(uint32_t bounce, uint32_t kind) { return bounce * 4u + kind; }
+
+// ---------------------------------------------------------------------------
 // BVH8 traversal
 // ---------------------------------------------------------------------------
 constexpr int kTraversalStack = 32;
@@ -592,6 +708,7 @@ __device__ __forceinline__ void intersect_node(const DevScene &S, uint32_t ni, c
 struct Trav {
     RayPre r;
     float tmin, tmax;
+    uint32_t seed, key;  // alpha tests: path seed and ray key
     uint32_t gBase, gImask, gHits, tBase, tHits;
     uint32_t visits;
     int sp;
@@ -599,10 +716,13 @@ struct Trav {
 struct TravStack {
     uint32_t base[kTraversalStack], mask[kTraversalStack];
 };
-__device__ __forceinline__ void trav_init(Trav &T, const DevScene &S, float3 o, float3 d, float tmin, float tmax) {
+__device__ __forceinline__ void trav_init(Trav &T, const DevScene &S, float3 o, float3 d, float tmin, float tmax,
+                                          uint32_t seed = 0u, uint32_t key = 0u) {
     T.r = ray_pre(o, d);
     T.tmin = tmin;
     T.tmax = tmax;
+    T.seed = seed;
+    T.key = key;
     T.sp = 0;
     T.visits = 1;
     T.gHits = T.tHits = 0;
@@ -650,7 +770,11 @@ __device__ __forceinline__ bool trav_step_closest(Trav &T, TravStack &K, const D
         float t, u, v;
         if (tri_test(T.r.o, T.r.d, a, b, c, T.tmin, h.t, t, u, v)) {
             uint32_t g = __float_as_uint(a.w);
-            if (t < h.t || (t == h.t && g < h.gid)) { h.t = t; h.u = u; h.v = v; h.gid = g; }
+            if (t < h.t || (t == h.t && g < h.gid)) {
+                // b.w != 0: the triangle's material has an alpha map
+                if (__float_as_uint(b.w) && !alpha_pass(S, g, u, v, T.seed, T.key, false)) continue;
+                h.t = t; h.u = u; h.v = v; h.gid = g;
+            }
         }
     }
     return !trav_next_node(T, K, S, h.t, err);
@@ -667,6 +791,10 @@ __device__ __forceinline__ bool trav_step_shadow(Trav &T, TravStack &K, const De
         float t, u, v;
         if (tri_test(T.r.o, T.r.d, a, b, c, T.tmin, T.tmax, t, u, v)) {
             uint32_t g = __float_as_uint(a.w);
+            if (__float_as_uint(b.w)) {  // alpha-mapped: occludes when the stochastic test keeps it
+                if (alpha_pass(S, g, u, v, T.seed, T.key, true)) { occluded = true; return true; }
+                continue;
+            }
             if (!S.hasGlass) { occluded = true; return true; }
             uint32_t mesh = __ldg(S.triMesh + g);
             const pt_material &m = S.mats[mesh];
@@ -682,13 +810,13 @@ __device__ __forceinline__ bool trav_step_shadow(Trav &T, TravStack &K, const De
 // Closest hit (TraceClosestInline semantics for opaque geometry).  Sets *err
 // on stack overflow or a runaway visit count.
 __device__ __forceinline__ Hit trace_closest(const DevScene &S, float3 o, float3 d, float tmin, float tmax,
-                                             uint32_t *err) {
+                                             uint32_t *err, uint32_t seed = 0u, uint32_t key = 0u) {
     Hit h;
     h.t = tmax; h.u = 0.0f; h.v = 0.0f; h.gid = 0xFFFFFFFFu;
     if (S.numNodes == 0) return h;
     Trav T;
     TravStack K;
-    trav_init(T, S, o, d, tmin, tmax);
+    trav_init(T, S, o, d, tmin, tmax, seed, key);
     while (!trav_step_closest(T, K, S, h, err)) {
     }
     return h;
@@ -698,12 +826,12 @@ __device__ __forceinline__ Hit trace_closest(const DevScene &S, float3 o, float3
 // scenes without alpha textures): the first opaque hit in [tmin, tmax]
 // occludes; mirror/dielectric surfaces multiply `trans` by (1 - Fr).
 __device__ __forceinline__ bool trace_shadow(const DevScene &S, float3 o, float3 d, float tmin, float tmax,
-                                             float3 &trans, uint32_t *err) {
+                                             float3 &trans, uint32_t *err, uint32_t seed = 0u, uint32_t key = 0u) {
     trans = v3(1.0f);
     if (S.numNodes == 0) return false;
     Trav T;
     TravStack K;
-    trav_init(T, S, o, d, tmin, tmax);
+    trav_init(T, S, o, d, tmin, tmax, seed, key);
     bool occ = false;
     while (!trav_step_shadow(T, K, S, trans, occ, err)) {
     }

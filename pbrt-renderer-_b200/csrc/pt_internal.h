@@ -33,19 +33,33 @@ enum ShadeClass : int {
     CLS_MICRO = 4,
     CLS_DISNEY = 5,
     CLS_HAIR = 6,
-    CLS_N = 7
+    CLS_TEX = 7,  // + CLS_TEX: the same class for materials with shading textures
+    CLS_N = 14
 };
-__host__ __device__ inline int shade_class(bool hit, bool emitter, uint32_t type) {
-    if (!hit) return CLS_MISS;
-    if (emitter) return CLS_EMIT;
-    switch (type) {
-        case PT_MAT_MIRROR: case PT_MAT_DIELECTRIC: return CLS_DELTA;
-        case PT_MAT_DIFFUSE: return CLS_DIFFUSE;
-        case PT_MAT_MICROFACET: return CLS_MICRO;
-        case PT_MAT_DISNEY: return CLS_DISNEY;
-        default: return CLS_HAIR;  // upload admits no other type
-    }
+// The reference's hasAnyTex (shaders/Shaders.hlsl:232-236): texture maps the
+// shading reads (alpha maps act in the traversal, metallic maps nowhere).
+__host__ __device__ inline bool has_shading_textures(const pt_material &m) {
+    return m.albedoTexIndex != PT_NO_TEXTURE || m.normalTexIndex != PT_NO_TEXTURE ||
+           m.roughnessTexIndex != PT_NO_TEXTURE || m.specularTexIndex != PT_NO_TEXTURE ||
+           m.subsurfaceTexIndex != PT_NO_TEXTURE;
 }
+__host__ __device__ inline int shade_class(bool hit, bool emitter, uint32_t type, bool textured = false) {
+    if (!hit) return CLS_MISS;
+    int c;
+    if (emitter) c = CLS_EMIT;
+    else switch (type) {
+        case PT_MAT_MIRROR: case PT_MAT_DIELECTRIC: c = CLS_DELTA; break;
+        case PT_MAT_DIFFUSE: c = CLS_DIFFUSE; break;
+        case PT_MAT_MICROFACET: c = CLS_MICRO; break;
+        case PT_MAT_DISNEY: c = CLS_DISNEY; break;
+        default: c = CLS_HAIR;  // upload admits no other type
+    }
+    return textured ? c + CLS_TEX : c;
+}
+
+// Words of the per-wave counter block (WaveBuffers::counters).
+constexpr int kCounterWords = 32;
+static_assert(8 + CLS_N <= kCounterWords, "class queue counts must fit the counter block");
 
 // Per-wave buffers of the wavefront integrator (structure of arrays).
 struct WaveBuffers {
@@ -66,7 +80,8 @@ struct WaveBuffers {
     uint32_t *sslot = nullptr;           // slot | kind << 31
     float4 *so = nullptr, *sd = nullptr, *sX = nullptr, *sthr = nullptr;
     // counters: [0] ray count q0, [1] ray count q1, [2] shadow count,
-    // [4..7] total extension / shadow rays (two uint64), [8..14] class queue counts
+    // [4..7] total extension / shadow rays (two uint64), [8 .. 8+CLS_N) class
+    // queue counts; kCounterWords words in all
     uint32_t *counters = nullptr;
 };
 

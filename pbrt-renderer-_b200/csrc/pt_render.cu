@@ -156,15 +156,8 @@ template <bool CLASSIFY>
 __device__ __forceinline__ void finish_extend(const WaveArgs &A, uint32_t i, const Hit &h) {
     A.qhit[i] = make_float4(h.t, __uint_as_float(h.gid), h.u, h.v);
     if (CLASSIFY) {
-        bool hit = h.gid != 0xFFFFFFFFu;
-        bool emitter = false;
-        uint32_t type = 0;
-        if (hit) {
-            const pt_material *m = A.S.mats + __ldg(A.S.triMesh + h.gid);
-            type = __ldg(&m->type);
-            emitter = __ldg(&m->isEmitter) != 0u;
-        }
-        class_append(A, shade_class(hit, emitter, type), i);
+        int c = h.gid == 0xFFFFFFFFu ? (int)CLS_MISS : (int)__ldg(A.S.meshClass + __ldg(A.S.triMesh + h.gid));
+        class_append(A, c, i);
     }
 }
 template <bool CLASSIFY>
@@ -176,7 +169,15 @@ __global__ void __launch_bounds__(kBlock) k_extend(WaveArgs A) {
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&A.rayTotals[0], (unsigned long long)n);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float4 o = A.qoIn[i], d = A.qdIn[i];
-        Hit h = trace_closest(A.S, make_float3(o.x, o.y, o.z), make_float3(d.x, d.y, d.z), o.w, d.w, A.err);
+        uint32_t aseed = 0, akey = 0;
+        if (A.S.hasAlpha) {  // alpha tests: the path's seed, key of this bounce's extension ray
+            uint32_t slot = A.qslotIn[i];
+            Rng r = load_rng(A, slot, A.rng[slot]);
+            aseed = alpha_seed(r.pixelSeed, r.sampleIndex);
+            akey = alpha_key(A.rng[slot].z, 0u);
+        }
+        Hit h = trace_closest(A.S, make_float3(o.x, o.y, o.z), make_float3(d.x, d.y, d.z), o.w, d.w, A.err, aseed,
+                              akey);
         finish_extend<CLASSIFY>(A, i, h);
     }
 }
@@ -188,7 +189,15 @@ __global__ void __launch_bounds__(kBlock) k_shadow(WaveArgs A) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         float4 o = A.so[i], d = A.sd[i];
         float3 tr;
-        bool occ = trace_shadow(A.S, make_float3(o.x, o.y, o.z), make_float3(d.x, d.y, d.z), o.w, d.w, tr, A.err);
+        uint32_t aseed = 0, akey = 0;
+        if (A.S.hasAlpha) {  // the shading kernel already advanced the path's bounce counter
+            uint32_t s = A.sslot[i], slot = s & 0x7FFFFFFFu;
+            Rng r = load_rng(A, slot, A.rng[slot]);
+            aseed = alpha_seed(r.pixelSeed, r.sampleIndex);
+            akey = alpha_key(A.rng[slot].z - 1u, (s >> 31) ? 2u : 1u);
+        }
+        bool occ = trace_shadow(A.S, make_float3(o.x, o.y, o.z), make_float3(d.x, d.y, d.z), o.w, d.w, tr, A.err,
+                                aseed, akey);
         float4 X = A.sX[i], Th = A.sthr[i];
         uint32_t s = A.sslot[i];
         float3 thr = make_float3(Th.x, Th.y, Th.z);
@@ -212,7 +221,7 @@ struct NeeOut {
 template <bool INLINE>
 __device__ __forceinline__ float3 nee_area(const WaveArgs &A, float3 hp, float3 N, float3 Ng, float3 T, float3 B,
                                            float3 wil, uint32_t type, const pt_material &m, float h, Rng &rng,
-                                           NeeOut &out) {
+                                           NeeOut &out, uint32_t aseed, uint32_t bounce) {
     const DevScene &S = A.S;
     out.ray = false;
     EmitterSample es = sample_emitter(S, rng);
@@ -228,7 +237,7 @@ __device__ __forceinline__ float3 nee_area(const WaveArgs &A, float3 hp, float3 
     float3 so = offset_origin(hp, sng, sng);
     float3 trans = v3(1.0f);
     if (INLINE) {
-        if (trace_shadow(S, so, ww, 0.0f, dist - 0.001f, trans, A.err)) return v3(0.0f);
+        if (trace_shadow(S, so, ww, 0.0f, dist - 0.001f, trans, A.err, aseed, alpha_key(bounce, 1u))) return v3(0.0f);
     }
     float3 f;
     float pb;
@@ -246,7 +255,7 @@ __device__ __forceinline__ float3 nee_area(const WaveArgs &A, float3 hp, float3 
 template <bool INLINE>
 __device__ __forceinline__ float3 nee_env(const WaveArgs &A, float3 hp, float3 N, float3 Ng, float3 T, float3 B,
                                           float3 wil, uint32_t type, const pt_material &m, float h, Rng &rng,
-                                          NeeOut &out) {
+                                          NeeOut &out, uint32_t aseed, uint32_t bounce) {
     const DevScene &S = A.S;
     out.ray = false;
     float u1 = next_float(rng, S.sobol1), u2 = next_float(rng, S.sobol1);
@@ -262,7 +271,7 @@ __device__ __forceinline__ float3 nee_env(const WaveArgs &A, float3 hp, float3 N
     float3 so = offset_origin(hp, sng, sng);
     float3 trans = v3(1.0f);
     if (INLINE) {
-        if (trace_shadow(S, so, ww, 0.0f, 1e20f, trans, A.err)) return v3(0.0f);
+        if (trace_shadow(S, so, ww, 0.0f, 1e20f, trans, A.err, aseed, alpha_key(bounce, 2u))) return v3(0.0f);
     }
     float3 f;
     float pb;
@@ -284,7 +293,8 @@ __device__ bool vol_nee_skip(const pt_volume &v, float3 p) {
     float md = mn(mn(dmn.x, dmn.y), mn(dmn.z, mn(dmx.x, mn(dmx.y, dmx.z))));
     return md * smin > 8.0f;
 }
-__device__ float3 vol_nee_area(const WaveArgs &A, float3 sp, float3 wo, uint32_t vi, Rng &rng) {
+__device__ float3 vol_nee_area(const WaveArgs &A, float3 sp, float3 wo, uint32_t vi, Rng &rng, uint32_t aseed,
+                               uint32_t bounce) {
     const DevScene &S = A.S;
     const pt_volume &v = S.vols[vi];
     if (vol_nee_skip(v, sp)) return v3(0.0f);
@@ -296,14 +306,15 @@ __device__ float3 vol_nee_area(const WaveArgs &A, float3 sp, float3 wo, uint32_t
     float cl = dot(es.nrm, -wi);
     if (cl <= 0.0f) return v3(0.0f);
     float3 trans;
-    if (trace_shadow(S, sp, wi, 0.001f, dist - 0.001f, trans, A.err)) return v3(0.0f);
+    if (trace_shadow(S, sp, wi, 0.001f, dist - 0.001f, trans, A.err, aseed, alpha_key(bounce, 1u))) return v3(0.0f);
     float fp = hg(dot(wo, wi), v.phase_g);
     float pe = es.pdfArea * dist * dist / cl;
     float w = balance(pe, fp);
     float3 vt = multi_volume_tr(S, sp, wi, dist, rng);
     return es.rad * fp / v3(mx(pe, 1e-20f)) * w * vt * trans;
 }
-__device__ float3 vol_nee_env(const WaveArgs &A, float3 sp, float3 wo, uint32_t vi, Rng &rng) {
+__device__ float3 vol_nee_env(const WaveArgs &A, float3 sp, float3 wo, uint32_t vi, Rng &rng, uint32_t aseed,
+                              uint32_t bounce) {
     const DevScene &S = A.S;
     const pt_volume &v = S.vols[vi];
     if (vol_nee_skip(v, sp)) return v3(0.0f);
@@ -313,7 +324,7 @@ __device__ float3 vol_nee_env(const WaveArgs &A, float3 sp, float3 wo, uint32_t 
     env_sample(S, A.envMode, u1, u2, wi, Le, pe);
     if (pe <= 0.0f) return v3(0.0f);
     float3 trans;
-    if (trace_shadow(S, sp, wi, 0.001f, 1e20f, trans, A.err)) return v3(0.0f);
+    if (trace_shadow(S, sp, wi, 0.001f, 1e20f, trans, A.err, aseed, alpha_key(bounce, 2u))) return v3(0.0f);
     float fp = hg(dot(wo, wi), v.phase_g);
     float w = balance(pe, fp);
     float3 vt = multi_volume_tr(S, sp, wi, 1e20f, rng);
@@ -348,12 +359,64 @@ __host__ __device__ constexpr uint32_t class_type(int c) {
 // their register use gives anyway (a bound makes the compiler spend up to it).
 template <int CLS>
 struct ShadeBlocks {
-    static constexpr int value = CLS == CLS_MISS ? 5 : (CLS == CLS_EMIT || CLS == CLS_DELTA) ? 4
-                                                     : CLS == CLS_DISNEY ? 3 : 2;
+    static constexpr int base = CLS < 0 ? CLS : CLS % CLS_TEX;
+    static constexpr int value = base == CLS_MISS ? 5 : (base == CLS_EMIT || base == CLS_DELTA) ? 4
+                                                      : base == CLS_DISNEY ? 3 : 2;
 };
 
+// Texture maps at a surface hit (Shaders.hlsl:232-315): albedo (sRGB),
+// normal map in the frame of the triangle's UV derivatives, roughness (not
+// for hair, whose `roughness` is beta_m), specular (x 0.5), subsurface; each
+// at the mip level of the hit's UV footprint.  Overrides m's fields, bends N.
+__device__ __forceinline__ void apply_textures(const DevScene &S, pt_material &m, uint32_t mesh, uint32_t prim,
+                                               float hitT, uint32_t i0, uint32_t i1, uint32_t i2, float b1, float b2,
+                                               float3 &N, uint32_t width, uint32_t height) {
+    const float foot = uv_footprint(S, mesh, prim, hitT, width, height);
+    const float2 uv = interp_uv(S, i0, i1, i2, b1, b2);
+    float3 alb = make_float3(m.albedo[0], m.albedo[1], m.albedo[2]);
+    if (m.albedoTexIndex != PT_NO_TEXTURE) {
+        float4 c = tex_sample(S, m.albedoTexIndex, uv.x, uv.y, tex_lod(S, m.albedoTexIndex, foot));
+        alb = make_float3(c.x, c.y, c.z);
+    }
+    if (m.normalTexIndex != PT_NO_TEXTURE) {
+        float3 p0 = ld3(S.pos, i0), p1 = ld3(S.pos, i1), p2 = ld3(S.pos, i2);
+        float3 e1 = p1 - p0, e2 = p2 - p0;
+        float u0 = __ldg(S.uv + 2 * i0), v0 = __ldg(S.uv + 2 * i0 + 1);
+        float du1 = __ldg(S.uv + 2 * i1) - u0, dv1 = __ldg(S.uv + 2 * i1 + 1) - v0;
+        float du2 = __ldg(S.uv + 2 * i2) - u0, dv2 = __ldg(S.uv + 2 * i2 + 1) - v0;
+        float det = du1 * dv2 - du2 * dv1;
+        float3 T, B;
+        if (fabsf(det) > 1e-8f) {
+            float invDet = 1.0f / det;
+            T = normalize((dv2 * e1 - dv1 * e2) * invDet);
+            T = normalize(T - N * dot(N, T));
+            B = cross(N, T);
+        } else {
+            build_onb(N, T, B);
+        }
+        float4 c = tex_sample(S, m.normalTexIndex, uv.x, uv.y, tex_lod(S, m.normalTexIndex, foot));
+        float3 tn = make_float3(c.x, c.y, c.z) * 2.0f - v3(1.0f);
+        N = normalize(T * tn.x + B * tn.y + N * tn.z);
+    }
+    m.albedo[0] = alb.x;
+    m.albedo[1] = alb.y;
+    m.albedo[2] = alb.z;
+    if (m.type != PT_MAT_HAIR && m.roughnessTexIndex != PT_NO_TEXTURE) {
+        float r = tex_sample(S, m.roughnessTexIndex, uv.x, uv.y, tex_lod(S, m.roughnessTexIndex, foot)).x;
+        m.alpha = r;
+        m.roughness = r;
+    }
+    if (m.specularTexIndex != PT_NO_TEXTURE)
+        m.specular = tex_sample(S, m.specularTexIndex, uv.x, uv.y, tex_lod(S, m.specularTexIndex, foot)).x * 0.5f;
+    if (m.subsurfaceTexIndex != PT_NO_TEXTURE)
+        m.subsurface = tex_sample(S, m.subsurfaceTexIndex, uv.x, uv.y, tex_lod(S, m.subsurfaceTexIndex, foot)).x;
+}
+
+// CLS + CLS_TEX: the kernel of class CLS for materials with shading textures.
 template <bool INLINE, int CLS>
 __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveArgs A) {
+    constexpr int C = ShadeBlocks<CLS>::base;    // the event / material class
+    constexpr bool TEX = CLS >= (int)CLS_TEX;    // shading textures present
     const DevScene &S = A.S;
     uint32_t n = CLS == CLS_ANY ? *(volatile uint32_t *)A.cntIn : *(volatile uint32_t *)(A.cntCls + CLS);
     uint32_t iters = (n + gridDim.x * blockDim.x - 1) / (gridDim.x * blockDim.x);
@@ -388,6 +451,7 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
                 st.w &= ~kFlagPending;
             }
             rng = load_rng(A, slot, st);
+            const uint32_t aseed = S.hasAlpha ? alpha_seed(rng.pixelSeed, rng.sampleIndex) : 0u;
             float4 o4 = A.qoIn[i], d4 = A.qdIn[i], h4 = A.qhit[i];
             float3 ro = make_float3(o4.x, o4.y, o4.z), rd = make_float3(d4.x, d4.y, d4.z);
             uint32_t gid = __float_as_uint(h4.y);
@@ -405,8 +469,8 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
                     const pt_volume &v = S.vols[svi];
                     float3 spos = xpos(ro, rd, tsc);
                     thr *= make_float3(v.sigma_s[0], v.sigma_s[1], v.sigma_s[2]) / vmax(vsigma_t(v), v3(1e-20f));
-                    Lo += thr * vol_nee_area(A, spos, rd, svi, rng);
-                    Lo += thr * vol_nee_env(A, spos, rd, svi, rng);
+                    Lo += thr * vol_nee_area(A, spos, rd, svi, rng, aseed, st.z);
+                    Lo += thr * vol_nee_env(A, spos, rd, svi, rng, aseed, st.z);
                     float x1 = next_float(rng, S.sobol1), x2 = next_float(rng, S.sobol1);
                     float pp;
                     nd = sample_hg(rd, v.phase_g, x1, x2, pp);
@@ -417,15 +481,15 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
                 }
             }
             if (volScat) {
-            } else if (CLS == CLS_MISS || (CLS == CLS_ANY && !hit)) {  // Shaders.hlsl:188-212
+            } else if (C == CLS_MISS || (C == CLS_ANY && !hit)) {  // Shaders.hlsl:188-212
                 float3 env = eval_env(S, rd);
                 if (lastPdf == 0.0f) Lo += thr * env;
                 else Lo += thr * env * balance(lastPdf, env_pdf(S, A.envMode, rd));
-            } else if (CLS != CLS_MISS) {
+            } else if (C != CLS_MISS) {
                 uint32_t mesh = __ldg(S.triMesh + gid);
                 uint32_t prim = gid - __ldg(S.meshFirstTri + mesh);
-                const pt_material m = S.mats[mesh];
-                const uint32_t type = CLS >= CLS_DIFFUSE ? class_type(CLS) : m.type;
+                pt_material m = S.mats[mesh];
+                const uint32_t type = C >= CLS_DIFFUSE ? class_type(C) : m.type;
                 uint32_t i0, i1, i2;
                 tri_vidx(S, mesh, prim, i0, i1, i2);
                 float bx = h4.z, by = h4.w, w0 = 1.0f - bx - by;
@@ -438,11 +502,13 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
                 bool back = dot(Ng, rd) > 0.0f;
                 if (back) Ng = -Ng;
                 if (dot(N, Ng) < 0.0f) N = -N;
-                if (CLS == CLS_EMIT || (CLS == CLS_ANY && m.isEmitter)) {  // Shaders.hlsl:317-335
+                if (TEX || (C == CLS_ANY && has_shading_textures(m)))
+                    apply_textures(S, m, mesh, prim, h4.x, i0, i1, i2, bx, by, N, A.width, A.height);
+                if (C == CLS_EMIT || (C == CLS_ANY && m.isEmitter)) {  // Shaders.hlsl:317-335
                     float3 rad = make_float3(m.radiance[0], m.radiance[1], m.radiance[2]);
                     if (lastPdf == 0.0f) Lo += thr * rad;
                     else Lo += thr * rad * balance(lastPdf, emitter_pdf_sa(S, m, hp, ro, N));
-                } else if (CLS != CLS_EMIT) {
+                } else if (C != CLS_EMIT) {
                     float3 T, B;
                     float h = 0.0f;
                     if (type == PT_MAT_HAIR) {  // Shaders.hlsl:340-387
@@ -497,11 +563,11 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
                         lastPdf = 0.0f;
                         if (refr) eta *= etaI / etaT;
                         cont = true;
-                    } else if (CLS != CLS_DELTA &&
+                    } else if (C != CLS_DELTA &&
                                (type == PT_MAT_DIFFUSE || type == PT_MAT_MICROFACET || type == PT_MAT_DISNEY ||
                                 type == PT_MAT_HAIR)) {  // Shaders.hlsl:473-511
-                        float3 ra = nee_area<INLINE>(A, hp, N, Ng, T, B, wil, type, m, h, rng, neeA);
-                        float3 re = nee_env<INLINE>(A, hp, N, Ng, T, B, wil, type, m, h, rng, neeE);
+                        float3 ra = nee_area<INLINE>(A, hp, N, Ng, T, B, wil, type, m, h, rng, neeA, aseed, st.z);
+                        float3 re = nee_env<INLINE>(A, hp, N, Ng, T, B, wil, type, m, h, rng, neeE, aseed, st.z);
                         if (INLINE) {
                             Lo += thr * ra;
                             Lo += thr * re;
@@ -619,7 +685,7 @@ constexpr size_t kWaveBytesPerPath = 5 * 16 + 2 * (4 + 16 + 16) + 16 + 4 * CLS_N
 // several waves, whose tails are small at this size, instead of regrowing the
 // buffers (a free + malloc of tens of GB that would stall the render).
 constexpr size_t kMaxWavePaths = (size_t)1 << 26;
-static_assert(kWaveBytesPerPath == 332, "wave state layout");
+static_assert(kWaveBytesPerPath == 360, "wave state layout");
 
 static int wave_alloc(pt_ctx *ctx, size_t cap) {
     if (ctx->W.cap >= cap) return PT_OK;
@@ -635,7 +701,7 @@ static int wave_alloc(pt_ctx *ctx, size_t cap) {
     A((void **)&W.cls, cap * 4 * CLS_N);
     A((void **)&W.sslot, sc * 4); A((void **)&W.so, sc * 16); A((void **)&W.sd, sc * 16);
     A((void **)&W.sX, sc * 16); A((void **)&W.sthr, sc * 16);
-    A((void **)&W.counters, 64);
+    A((void **)&W.counters, kCounterWords * sizeof(uint32_t));
     if (e != cudaSuccess) {
         pt_wave_free(ctx);
         return ctx->fail(PT_E_NOMEM, "wave buffers", cudaGetErrorString(e));
@@ -647,9 +713,13 @@ static int wave_alloc(pt_ctx *ctx, size_t cap) {
 
 namespace {
 using Kernel = void (*)(WaveArgs);
-const Kernel kShadeCls[CLS_N] = {k_shade<false, CLS_MISS>,  k_shade<false, CLS_EMIT>,    k_shade<false, CLS_DELTA>,
-                                 k_shade<false, CLS_DIFFUSE>, k_shade<false, CLS_MICRO>, k_shade<false, CLS_DISNEY>,
-                                 k_shade<false, CLS_HAIR>};
+// per class; entry CLS_TEX + CLS_MISS (a textured miss) never receives paths
+const Kernel kShadeCls[CLS_N] = {
+    k_shade<false, CLS_MISS>,           k_shade<false, CLS_EMIT>,           k_shade<false, CLS_DELTA>,
+    k_shade<false, CLS_DIFFUSE>,        k_shade<false, CLS_MICRO>,          k_shade<false, CLS_DISNEY>,
+    k_shade<false, CLS_HAIR>,           k_shade<false, CLS_MISS>,           k_shade<false, CLS_TEX + CLS_EMIT>,
+    k_shade<false, CLS_TEX + CLS_DELTA>, k_shade<false, CLS_TEX + CLS_DIFFUSE>, k_shade<false, CLS_TEX + CLS_MICRO>,
+    k_shade<false, CLS_TEX + CLS_DISNEY>, k_shade<false, CLS_TEX + CLS_HAIR>};
 int gExt = 0, gExtC = 0, gShadeI = 0, gShadow = 0, gCls[CLS_N];
 
 enum { STG_RAYGEN, STG_EXTEND, STG_SHADE, STG_SHADOW, STG_FILM, STG_N };
@@ -676,13 +746,18 @@ struct Enqueue {
     }
 };
 
-void enqueue_render(const pt_ctx *ctx, Enqueue &E, WaveArgs A, const pt_render_params *P, size_t cap, uint64_t total,
-                    uint64_t npix, float *d_sum, float *d_comp) {
+// Returns the first failing call's status (cudaSuccess if none).
+cudaError_t enqueue_render(const pt_ctx *ctx, Enqueue &E, WaveArgs A, const pt_render_params *P, size_t cap,
+                           uint64_t total, uint64_t npix, float *d_sum, float *d_comp) {
     const WaveBuffers &B = ctx->W;
     const bool inl = ctx->S.numVols > 0;
     cudaStream_t st = E.st;
-    cudaMemsetAsync(B.counters, 0, 64, st);
-    cudaMemsetAsync(ctx->d_err, 0, 4, st);
+    cudaError_t err = cudaSuccess;
+    auto chk = [&](cudaError_t e) {
+        if (err == cudaSuccess && e != cudaSuccess) err = e;
+    };
+    chk(cudaMemsetAsync(B.counters, 0, kCounterWords * sizeof(uint32_t), st));
+    chk(cudaMemsetAsync(ctx->d_err, 0, 4, st));
     for (uint64_t ws = 0; ws < total; ws += cap) {
         A.waveStart = ws;
         A.waveCount = (uint32_t)std::min<uint64_t>(cap, total - ws);
@@ -695,8 +770,8 @@ void enqueue_render(const pt_ctx *ctx, Enqueue &E, WaveArgs A, const pt_render_p
             A.qslotIn = B.qslot[cur]; A.qoIn = B.qo[cur]; A.qdIn = B.qd[cur]; A.cntIn = B.counters + cur;
             A.qslotOut = B.qslot[1 - cur]; A.qoOut = B.qo[1 - cur]; A.qdOut = B.qd[1 - cur];
             A.cntOut = B.counters + (1 - cur);
-            cudaMemsetAsync(A.cntOut, 0, 4, st);
-            cudaMemsetAsync(A.cntShadow, 0, 4, st);
+            chk(cudaMemsetAsync(A.cntOut, 0, 4, st));
+            chk(cudaMemsetAsync(A.cntShadow, 0, 4, st));
             if (inl) {
                 E.begin(STG_EXTEND);
                 k_extend<false><<<gExt, kBlock, 0, st>>>(A);
@@ -705,7 +780,7 @@ void enqueue_render(const pt_ctx *ctx, Enqueue &E, WaveArgs A, const pt_render_p
                 k_shade<true, CLS_ANY><<<gShadeI, kBlock, 0, st>>>(A);
                 E.end();
             } else {
-                cudaMemsetAsync(A.cntCls, 0, CLS_N * sizeof(uint32_t), st);
+                chk(cudaMemsetAsync(A.cntCls, 0, CLS_N * sizeof(uint32_t), st));
                 E.begin(STG_EXTEND);
                 k_extend<true><<<gExtC, kBlock, 0, st>>>(A);
                 E.end();
@@ -725,7 +800,9 @@ void enqueue_render(const pt_ctx *ctx, Enqueue &E, WaveArgs A, const pt_render_p
         E.begin(STG_FILM);
         k_film<<<(cover + kBlock - 1) / kBlock, kBlock, 0, st>>>(A, (float4 *)d_sum, (float4 *)d_comp);
         E.end();
+        chk(cudaGetLastError());  // launch-configuration errors of this wave
     }
+    return err;
 }
 
 __global__ void k_set_u32(uint32_t *p, uint32_t v) { *p = v; }
@@ -751,7 +828,7 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
     // Default wave: the whole render, up to kMaxWavePaths and half of the
     // free device memory.  Each bounce of a wave ends with a latency-bound
     // tail (a few slow traversals), so fewer, larger waves amortise it; the
-    // 59 M paths of a 1280 x 720 x 64 frame take ~20 GB.
+    // 59 M paths of a 1280 x 720 x 64 frame take ~21 GB.
     // The free-memory query runs only when the buffers would have to grow: it
     // is a driver call that can block on other clients of the driver.
     size_t cap = P->wave_paths;
@@ -809,8 +886,8 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
         cudaGraphExec_t exec = nullptr;
         bool ok = cudaStreamBeginCapture(ctx->ownStream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
         if (ok) {
-            enqueue_render(ctx, E, A, P, cap, total, npix, d_sum, d_comp);
-            ok = cudaStreamEndCapture(ctx->ownStream, &g) == cudaSuccess && g;
+            cudaError_t qe = enqueue_render(ctx, E, A, P, cap, total, npix, d_sum, d_comp);
+            ok = cudaStreamEndCapture(ctx->ownStream, &g) == cudaSuccess && g && qe == cudaSuccess;
         }
         ok = ok && cudaGraphInstantiate(&exec, g, 0) == cudaSuccess;
         if (g) cudaGraphDestroy(g);
@@ -836,12 +913,17 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
         PT_CUDA(cudaGraphLaunch(ctx->graph.exec, st));
         launches += ctx->graph.launches;
     } else {
-        enqueue_render(ctx, E, A, P, cap, total, npix, d_sum, d_comp);
+        cudaError_t qe = enqueue_render(ctx, E, A, P, cap, total, npix, d_sum, d_comp);
         launches += E.launches;
+        if (qe != cudaSuccess) {
+            cudaStreamSynchronize(st);
+            for (Mark &m : E.marks) { cudaEventDestroy(m.a); cudaEventDestroy(m.b); }
+            return ctx->fail(PT_E_CUDA, "render launch", cudaGetErrorString(qe));
+        }
     }
     cudaEventRecord(ev[1], st);
-    uint32_t hostCnt[16];
-    PT_CUDA(cudaMemcpyAsync(hostCnt, B.counters, 64, cudaMemcpyDeviceToHost, st));
+    uint32_t hostCnt[kCounterWords];
+    PT_CUDA(cudaMemcpyAsync(hostCnt, B.counters, sizeof(hostCnt), cudaMemcpyDeviceToHost, st));
     uint32_t derr = 0;
     PT_CUDA(cudaMemcpyAsync(&derr, ctx->d_err, 4, cudaMemcpyDeviceToHost, st));
     cudaError_t se = cudaStreamSynchronize(st);

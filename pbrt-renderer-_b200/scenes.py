@@ -181,6 +181,62 @@ def cornell(width=256, height=256, subdiv=3):
 
 
 # ---------------------------------------------------------------------------
+# textured materials: every map the shading reads, plus an alpha cut-out
+# ---------------------------------------------------------------------------
+def texture_maps(seed=0):
+    """Seeded procedural RGBA8 maps: (albedo checker [sRGB], bump normal map,
+    roughness ramp, specular noise, floor albedo [sRGB], soft circular alpha)."""
+    rng = np.random.default_rng(seed)
+    n = 64
+    y, x = np.mgrid[0:n, 0:n]
+    check = ((x // 8 + y // 8) % 2)[..., None]
+    albedo = np.where(check, [200, 60, 40, 255], [40, 90, 200, 255]).astype(np.uint8)
+    hx, hy = np.sin(x / n * 8 * math.pi), np.cos(y / n * 6 * math.pi)
+    nv = np.stack([-0.4 * hx, -0.4 * hy, np.ones_like(hx)], -1)
+    nv /= np.linalg.norm(nv, axis=-1, keepdims=True)
+    normal = np.concatenate([np.clip(np.rint((nv * 0.5 + 0.5) * 255), 0, 255), np.full((n, n, 1), 255)], -1)
+    rough = np.zeros((16, 16, 4), np.uint8)
+    rough[..., 0] = np.linspace(25, 230, 16, dtype=np.uint8)[None, :]
+    rough[..., 3] = 255
+    spec = rng.integers(0, 256, (8, 8, 4)).astype(np.uint8)
+    spec[..., 3] = 255
+    floor = rng.integers(60, 220, (128, 128, 4)).astype(np.uint8)
+    floor[..., 3] = 255
+    r = np.hypot(x - n / 2 + 0.5, y - n / 2 + 0.5) / (n / 2)
+    a = np.clip((1.0 - r) * 3.0, 0, 1)
+    alpha = np.stack([a * 255, a * 180, a * 120, a * 255], -1)
+    return [(albedo, True), normal.astype(np.uint8), rough, spec, (floor, True),
+            np.clip(np.rint(alpha), 0, 255).astype(np.uint8)]
+
+
+def textured_scene(width=96, height=72, seed=0, slices=48, rings=25, maps=None):
+    """A Disney sphere with albedo / normal / roughness / specular maps, a
+    floor with a tiled albedo map (UVs up to 4, wrap addressing), an
+    alpha-cut quad between them and a small area light under a dim sky."""
+    b = _Builder()
+    maps = texture_maps(seed) if maps is None else maps
+    v, f = uv_sphere(slices, rings)
+    uv = np.stack([np.arctan2(v[:, 2], v[:, 0]) / (2 * math.pi) + 0.5, np.arccos(np.clip(v[:, 1], -1, 1)) / math.pi], 1)
+    sph = make_material(PT_MAT_DISNEY, (0.8, 0.8, 0.8), roughness=0.5, metallic=0.1, clearcoat=0.3)
+    sph.albedoTexIndex, sph.normalTexIndex, sph.roughnessTexIndex, sph.specularTexIndex = 0, 1, 2, 3
+    b.add(v * 0.8 + np.array([0.0, 0.0, 0.0]), f, sph, normals=v, uvs=uv)
+    fl = make_material(PT_MAT_DIFFUSE, (0.7, 0.7, 0.7))
+    fl.albedoTexIndex = 4
+    fp, ff = _quad((-3, -0.8, -3), (-3, -0.8, 3), (3, -0.8, 3), (3, -0.8, -3))
+    b.add(fp, ff, fl, normals=_flat_normals(fp, ff), uvs=[(0, 0), (0, 4), (4, 4), (4, 0)])
+    cut = make_material(PT_MAT_DIFFUSE, (0.3, 0.8, 0.3))
+    cut.alphaTexIndex = 5
+    cp, cf = _quad((-0.6, -0.6, 1.2), (0.6, -0.6, 1.2), (0.6, 0.6, 1.2), (-0.6, 0.6, 1.2))
+    b.add(cp, cf, cut, normals=_flat_normals(cp, cf), uvs=[(0, 1), (1, 1), (1, 0), (0, 0)])
+    light = make_material(PT_MAT_DIFFUSE, (0.0, 0.0, 0.0), radiance=(12.0, 12.0, 12.0))
+    lp, lf = _quad((-0.5, 2.5, 1.5), (0.5, 2.5, 1.5), (0.5, 2.5, 2.5), (-0.5, 2.5, 2.5))
+    b.add(lp, lf, light, normals=_flat_normals(lp, lf))
+    scene = b.scene(env_rgb=sky_envmap(64, 32, sun_peak=30.0), env_scale=0.3, textures=maps)
+    cam = look_at_camera((0.4, 0.6, 3.2), (0.0, -0.1, 0.0), (0, 1, 0), 45.0, width / height)
+    return scene, cam
+
+
+# ---------------------------------------------------------------------------
 # configuration 2: Disney sphere grid under a procedural sky
 # ---------------------------------------------------------------------------
 def sky_envmap(width=2048, height=1024, sun_peak=5.0e4, sun_elev_deg=35.0, sun_azim_deg=60.0, sun_sigma_deg=0.6):
