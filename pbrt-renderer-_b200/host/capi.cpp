@@ -58,42 +58,66 @@ int nori_camera(void *scene, pt_camera *out) {
 
 // Flattened materials in mesh order (no GPU needed); returns the count.
 uint32_t nori_materials(void *scene, pt_material *out, uint32_t maxCount) {
-    const Scene *s = static_cast<const Scene *>(scene);
-    std::vector<float> pos, nrm, uv, tan, env;
-    std::vector<uint32_t> idx;
-    std::vector<pt_material> mats;
-    std::vector<pt_volume> vols;
-    std::vector<std::vector<float>> grids;
-    std::vector<pt_grid> gd;
-    uint32_t w, h;
-    flattenScene(s, pos, nrm, uv, tan, idx, mats, env, w, h, vols, grids, gd);
-    for (uint32_t i = 0; i < mats.size() && i < maxCount; i++) out[i] = mats[i];
-    return (uint32_t)mats.size();
+    FlatScene f;
+    flattenScene(static_cast<const Scene *>(scene), f);
+    for (uint32_t i = 0; i < f.mats.size() && i < maxCount; i++) out[i] = f.mats[i];
+    return (uint32_t)f.mats.size();
 }
 
 // One flattened scene array (no GPU needed): which = 0 positions, 1 normals,
 // 2 texcoords, 3 tangents (floats), 4 indices (u32), 5 envmap RGB (floats),
-// 6 envmap width.  Copies into out when it is not NULL; returns the element
-// count (the width for 6).
+// 6 envmap width, 7 texture count.  Copies into out when it is not NULL;
+// returns the element count (the width for 6, the count for 7).
 uint64_t nori_flat(void *scene, int which, void *out) {
-    const Scene *s = static_cast<const Scene *>(scene);
-    std::vector<float> pos, nrm, uv, tan, env;
-    std::vector<uint32_t> idx;
-    std::vector<pt_material> mats;
-    std::vector<pt_volume> vols;
-    std::vector<std::vector<float>> grids;
-    std::vector<pt_grid> gd;
-    uint32_t w, h;
-    flattenScene(s, pos, nrm, uv, tan, idx, mats, env, w, h, vols, grids, gd);
-    const std::vector<float> *f[] = {&pos, &nrm, &uv, &tan, nullptr, &env};
-    if (which == 6) return w;
+    FlatScene f;
+    flattenScene(static_cast<const Scene *>(scene), f);
+    const std::vector<float> *v[] = {&f.pos, &f.nrm, &f.uv, &f.tan, nullptr, &f.env};
+    if (which == 6) return f.envW;
+    if (which == 7) return f.textures.size();
     if (which == 4) {
-        if (out) std::memcpy(out, idx.data(), idx.size() * 4);
-        return idx.size();
+        if (out) std::memcpy(out, f.idx.data(), f.idx.size() * 4);
+        return f.idx.size();
     }
     if (which < 0 || which > 5) return 0;
-    if (out) std::memcpy(out, f[which]->data(), f[which]->size() * 4);
-    return f[which]->size();
+    if (out) std::memcpy(out, v[which]->data(), v[which]->size() * 4);
+    return v[which]->size();
+}
+
+// Texture `index` of the flattened scene (no GPU needed): wh_srgb receives
+// width, height, sRGB flag; the RGBA8 texels are copied into rgba when it is
+// not NULL.  Returns the byte count, or 0 for an index out of range.
+uint64_t nori_texture(void *scene, uint32_t index, uint32_t *wh_srgb, uint8_t *rgba) {
+    FlatScene f;
+    flattenScene(static_cast<const Scene *>(scene), f);
+    if (index >= f.textures.size()) return 0;
+    const pt_texture &t = f.textures[index];
+    if (wh_srgb) {
+        wh_srgb[0] = t.width;
+        wh_srgb[1] = t.height;
+        wh_srgb[2] = t.srgb;
+    }
+    if (rgba) std::memcpy(rgba, f.texData[index].data(), f.texData[index].size());
+    return f.texData[index].size();
+}
+
+// Decode one image file to RGBA8 (no scene needed): wh receives width and
+// height; the texels are copied into rgba when it is not NULL and cap bytes
+// hold them.  Returns the byte count, or 0 with err set.
+uint64_t nori_load_image(const char *path, uint32_t *wh, uint8_t *rgba, uint64_t cap, char *err, size_t errlen) {
+    try {
+        std::vector<uint8_t> px;
+        uint32_t w = 0, h = 0;
+        loadImageRGBA8(path ? path : "", w, h, px);
+        if (wh) {
+            wh[0] = w;
+            wh[1] = h;
+        }
+        if (rgba && cap >= px.size()) std::memcpy(rgba, px.data(), px.size());
+        return px.size();
+    } catch (const std::exception &e) {
+        seterr(err, errlen, e.what());
+        return 0;
+    }
 }
 
 // Write W x H x 3 floats (top row first) as an uncompressed OpenEXR file.

@@ -5,6 +5,7 @@
 // src/gpu/DXRApp_Textures.cpp, src/gpu/DXRApp_Camera.cpp).
 #include <cstdio>
 #include <cstring>
+#include <unordered_map>
 
 #include "nori/nori.h"
 
@@ -19,26 +20,48 @@ std::vector<float> RenderResult::mean() const {
     return m;
 }
 
-// CreateSceneBuffers (src/gpu/DXRApp_Scene.cpp:172-451), LoadEnvmap
+// CreateSceneBuffers (src/gpu/DXRApp_Scene.cpp:172-451), CreateTextures
+// (src/gpu/DXRApp_Textures.cpp:448-537), LoadEnvmap
 // (src/gpu/DXRApp_Textures.cpp:181-275), SetupVolumes + LoadVolume
-// (src/gpu/DXRApp_Scene.cpp:453-548).  Emitter CDFs, surface areas, the
-// envmap tables and majorant grids are built by pt_upload_scene.
-void flattenScene(const Scene *scene, std::vector<float> &pos, std::vector<float> &nrm, std::vector<float> &uv,
-                  std::vector<float> &tan, std::vector<uint32_t> &idx, std::vector<pt_material> &mats,
-                  std::vector<float> &envRGB, uint32_t &envW, uint32_t &envH, std::vector<pt_volume> &vols,
-                  std::vector<std::vector<float>> &grids, std::vector<pt_grid> &gridDesc) {
-    pos.clear(); nrm.clear(); uv.clear(); tan.clear(); idx.clear(); mats.clear();
-    vols.clear(); grids.clear(); gridDesc.clear();
+// (src/gpu/DXRApp_Scene.cpp:453-548).  Emitter CDFs, surface areas, mip
+// chains, the envmap tables and majorant grids are built by pt_upload_scene.
+void flattenScene(const Scene *scene, FlatScene &out) {
+    out = FlatScene{};
     uint32_t nv = 0, ni = 0;
-    bool warnedTex = false;
+    // Textures are keyed by resolved path: a file named by several materials
+    // (or maps) loads once, with the colour space of its first use; a file
+    // that cannot be read leaves the map unset (the constant parameter is used).
+    std::unordered_map<std::string, uint32_t> texCache;
+    auto texture = [&](const std::string &rel, bool srgb) -> uint32_t {
+        if (rel.empty()) return PT_NO_TEXTURE;
+        std::string path = resolvePath(rel);
+        auto it = texCache.find(path);
+        if (it != texCache.end()) return it->second;
+        std::vector<uint8_t> rgba;
+        uint32_t w = 0, h = 0;
+        try {
+            loadImageRGBA8(path, w, h, rgba);
+        } catch (const std::exception &e) {
+            std::fprintf(stderr, "[texture] Failed to load: %s (%s)\n", path.c_str(), e.what());
+            return PT_NO_TEXTURE;
+        }
+        uint32_t index = (uint32_t)out.texData.size();
+        out.texData.push_back(std::move(rgba));
+        out.textures.push_back(pt_texture{w, h, nullptr, srgb ? 1u : 0u});
+        out.texPaths.push_back(path);
+        texCache[path] = index;
+        return index;
+    };
     for (const Mesh *mesh : scene->getMeshes()) {
         BSDFGPUData gd = mesh->getBSDF()->getGPUData();
-        if (!warnedTex && (!gd.albedoTexture.empty() || !gd.normalTexture.empty() || !gd.roughnessTexture.empty() ||
-                           !gd.specularTexture.empty() || !gd.subsurfaceTexture.empty() || !gd.alphaTexture.empty())) {
-            std::fprintf(stderr, "[scene] textures are not rendered by this build; constant parameters are used\n");
-            warnedTex = true;
-        }
         pt_material m = toGPUMaterial(gd);
+        // metallic maps are loaded by the reference but read by no shader: not loaded here
+        m.albedoTexIndex = texture(gd.albedoTexture, true);
+        m.normalTexIndex = texture(gd.normalTexture, false);
+        m.roughnessTexIndex = texture(gd.roughnessTexture, false);
+        m.specularTexIndex = texture(gd.specularTexture, false);
+        m.subsurfaceTexIndex = texture(gd.subsurfaceTexture, false);
+        m.alphaTexIndex = texture(gd.alphaTexture, false);
         if (mesh->isEmitter()) {
             Color3f Le = mesh->getEmitter()->getRadiance();
             m.isEmitter = 1;
@@ -49,38 +72,41 @@ void flattenScene(const Scene *scene, std::vector<float> &pos, std::vector<float
         m.indexOffset = ni;
         m.vertexCount = vc;
         m.indexCount = ic;
-        mats.push_back(m);
+        out.mats.push_back(m);
         const auto &V = mesh->getVertexPositions();
-        pos.insert(pos.end(), V.begin(), V.end());
+        out.pos.insert(out.pos.end(), V.begin(), V.end());
         const auto &N = mesh->getVertexNormals();
-        if (N.size() == (size_t)vc * 3) nrm.insert(nrm.end(), N.begin(), N.end());
-        else nrm.insert(nrm.end(), (size_t)vc * 3, 0.0f);
+        if (N.size() == (size_t)vc * 3) out.nrm.insert(out.nrm.end(), N.begin(), N.end());
+        else out.nrm.insert(out.nrm.end(), (size_t)vc * 3, 0.0f);
         const auto &F = mesh->getIndices();
-        idx.insert(idx.end(), F.begin(), F.end());
+        out.idx.insert(out.idx.end(), F.begin(), F.end());
         const auto &UV = mesh->getVertexTexCoords();
         bool hair = mesh->hasTangents();
         for (uint32_t v = 0; v < vc; v++) {
             if (UV.size() == (size_t)vc * 2) {
-                uv.push_back(UV[2 * v]);
-                uv.push_back(hair ? UV[2 * v + 1] : 1.0f - UV[2 * v + 1]);  // V flip for OBJ meshes
+                out.uv.push_back(UV[2 * v]);
+                out.uv.push_back(hair ? UV[2 * v + 1] : 1.0f - UV[2 * v + 1]);  // V flip for OBJ meshes
             } else {
-                uv.push_back(0.0f);
-                uv.push_back(0.0f);
+                out.uv.push_back(0.0f);
+                out.uv.push_back(0.0f);
             }
         }
         const auto &T = mesh->getVertexTangents();
-        if (T.size() == (size_t)vc * 3) tan.insert(tan.end(), T.begin(), T.end());
-        else tan.insert(tan.end(), (size_t)vc * 3, 0.0f);
+        if (T.size() == (size_t)vc * 3) out.tan.insert(out.tan.end(), T.begin(), T.end());
+        else out.tan.insert(out.tan.end(), (size_t)vc * 3, 0.0f);
         nv += vc;
         ni += ic;
     }
+    for (size_t t = 0; t < out.textures.size(); t++) out.textures[t].rgba8 = out.texData[t].data();
     // envmap: the reference falls back to a 1x1 0.5 grey texel when the HDR cannot be read
     std::string hdr = resolvePath(scene->getEnvmap());
-    if (!loadHDR(hdr, envRGB, envW, envH)) {
+    if (!loadHDR(hdr, out.env, out.envW, out.envH)) {
         std::fprintf(stderr, "[envmap] No HDR at '%s' - falling back to flat gray.\n", hdr.c_str());
-        envW = envH = 1;
-        envRGB.assign(3, 0.5f);
+        out.envW = out.envH = 1;
+        out.env.assign(3, 0.5f);
     }
+    out.envScale = scene->getEnvmapScale();
+    out.evCompensation = scene->getEvCompensation();
     if (const Medium *med = scene->getMedium()) {
         BoundingBox3f b = med->hasExplicitBounds() ? med->getExplicitBounds() : scene->getBoundingBox();
         Color3f sa = med->getSigmaARGB(), ss = med->getSigmaSRGB();
@@ -97,16 +123,42 @@ void flattenScene(const Scene *scene, std::vector<float> &pos, std::vector<float
             uint32_t w, h, d;
             std::string p = resolvePath(med->getVolumePath());
             if (loadVol(p, data, w, h, d)) {
-                v.density_grid = (uint32_t)grids.size();
-                grids.push_back(std::move(data));
-                gridDesc.push_back(pt_grid{w, h, d, nullptr});
+                v.density_grid = (uint32_t)out.gridData.size();
+                out.gridData.push_back(std::move(data));
+                out.grids.push_back(pt_grid{w, h, d, nullptr});
             } else {
                 std::fprintf(stderr, "[volume] WARNING: could not open '%s'\n", p.c_str());
             }
         }
-        vols.push_back(v);
+        out.vols.push_back(v);
     }
-    for (size_t g = 0; g < grids.size(); g++) gridDesc[g].data = grids[g].data();
+    for (size_t g = 0; g < out.gridData.size(); g++) out.grids[g].data = out.gridData[g].data();
+}
+
+pt_scene_desc FlatScene::desc() const {
+    pt_scene_desc d;
+    std::memset(&d, 0, sizeof(d));
+    d.num_vertices = (uint32_t)(pos.size() / 3);
+    d.positions = pos.data();
+    d.normals = nrm.data();
+    d.texcoords = uv.data();
+    d.tangents = tan.data();
+    d.num_indices = (uint32_t)idx.size();
+    d.indices = idx.data();
+    d.num_meshes = (uint32_t)mats.size();
+    d.materials = mats.data();
+    d.env_width = envW;
+    d.env_height = envH;
+    d.env_rgb = env.data();
+    d.env_scale = envScale;
+    d.ev_compensation = evCompensation;
+    d.num_volumes = (uint32_t)vols.size();
+    d.volumes = vols.data();
+    d.num_grids = (uint32_t)grids.size();
+    d.grids = grids.data();
+    d.num_textures = (uint32_t)textures.size();
+    d.textures = textures.data();
+    return d;
 }
 
 // SetupCamera + RecomputeCameraPlane (src/gpu/DXRApp_Camera.cpp:23-112):
@@ -161,27 +213,8 @@ GPUIntegrator::~GPUIntegrator() {
 }
 void GPUIntegrator::preprocess(const Scene *scene) {
     m_scene = scene;
-    uint32_t ew = 0, eh = 0;
-    flattenScene(scene, m_pos, m_nrm, m_uv, m_tan, m_idx, m_mats, m_env, ew, eh, m_vols, m_gridData, m_grids);
-    std::memset(&m_desc, 0, sizeof(m_desc));
-    m_desc.num_vertices = (uint32_t)(m_pos.size() / 3);
-    m_desc.positions = m_pos.data();
-    m_desc.normals = m_nrm.data();
-    m_desc.texcoords = m_uv.data();
-    m_desc.tangents = m_tan.data();
-    m_desc.num_indices = (uint32_t)m_idx.size();
-    m_desc.indices = m_idx.data();
-    m_desc.num_meshes = (uint32_t)m_mats.size();
-    m_desc.materials = m_mats.data();
-    m_desc.env_width = ew;
-    m_desc.env_height = eh;
-    m_desc.env_rgb = m_env.data();
-    m_desc.env_scale = scene->getEnvmapScale();
-    m_desc.ev_compensation = scene->getEvCompensation();
-    m_desc.num_volumes = (uint32_t)m_vols.size();
-    m_desc.volumes = m_vols.data();
-    m_desc.num_grids = (uint32_t)m_grids.size();
-    m_desc.grids = m_grids.data();
+    flattenScene(scene, m_flat);
+    m_desc = m_flat.desc();
     const Camera *cam = scene->getCamera();
     m_width = cam->getOutputSize()[0];
     m_height = cam->getOutputSize()[1];

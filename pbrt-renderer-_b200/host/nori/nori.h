@@ -413,6 +413,23 @@ public:
     EClassType getClassType() const override { return EIntegrator; }
 };
 
+// A scene flattened into the arrays pt_upload_scene takes.  desc() points
+// into the vectors, so the FlatScene outlives every upload made from it.
+struct FlatScene {
+    std::vector<float> pos, nrm, uv, tan, env;
+    std::vector<uint32_t> idx;
+    std::vector<pt_material> mats;
+    uint32_t envW = 0, envH = 0;
+    std::vector<pt_volume> vols;
+    std::vector<std::vector<float>> gridData;
+    std::vector<pt_grid> grids;
+    std::vector<std::vector<uint8_t>> texData;  // RGBA8, level 0
+    std::vector<pt_texture> textures;
+    std::vector<std::string> texPaths;  // resolved file of each texture
+    float envScale = 1.0f, evCompensation = 0.0f;
+    pt_scene_desc desc() const;
+};
+
 // The GPU integrators ("path_mis", "direct"): preprocess() flattens the scene
 // and uploads it through pt_upload_scene; render() runs pt_render.
 class GPUIntegrator : public Integrator {
@@ -437,13 +454,8 @@ protected:
     const Scene *m_scene = nullptr;
     pt_camera m_cam{};
     int m_width = 0, m_height = 0;
-    // flattened scene (CreateSceneBuffers); kept alive while uploaded
-    std::vector<float> m_pos, m_nrm, m_uv, m_tan, m_env;
-    std::vector<uint32_t> m_idx;
-    std::vector<pt_material> m_mats;
-    std::vector<pt_volume> m_vols;
-    std::vector<std::vector<float>> m_gridData;
-    std::vector<pt_grid> m_grids;
+    // flattened scene (CreateSceneBuffers, CreateTextures); kept alive while uploaded
+    FlatScene m_flat;
     pt_scene_desc m_desc{};
 };
 
@@ -453,11 +465,12 @@ NoriObject *loadFromXML(const std::string &filename);
 void writeEXR(const std::string &path, int width, int height, const float *rgb);
 
 // Flatten a scene the way src/gpu/DXRApp_Scene.cpp:172-493 and
-// src/gpu/DXRApp_Textures.cpp:181-275 do (shared with GPUIntegrator).
-void flattenScene(const Scene *scene, std::vector<float> &pos, std::vector<float> &nrm, std::vector<float> &uv,
-                  std::vector<float> &tan, std::vector<uint32_t> &idx, std::vector<pt_material> &mats,
-                  std::vector<float> &envRGB, uint32_t &envW, uint32_t &envH, std::vector<pt_volume> &vols,
-                  std::vector<std::vector<float>> &grids, std::vector<pt_grid> &gridDesc);
+// src/gpu/DXRApp_Textures.cpp:181-275,448-537 do (shared with GPUIntegrator).
+void flattenScene(const Scene *scene, FlatScene &out);
+// A PNG / TGA / BMP / PPM / PGM image as 8-bit RGBA, top row first (the
+// 4-channel load of src/gpu/DXRApp_Textures.cpp:34-40).  Throws
+// NoriException for unreadable, malformed or unsupported files.
+void loadImageRGBA8(const std::string &path, uint32_t &width, uint32_t &height, std::vector<uint8_t> &rgba);
 // Camera constants of src/gpu/DXRApp_Camera.cpp:23-112 from a Nori camera.
 pt_camera cameraConstants(const Camera *cam, int width, int height);
 
