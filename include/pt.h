@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define PT_ABI_VERSION 2
+#define PT_ABI_VERSION 3
 
 /* ---- status codes ---------------------------------------------------- */
 #define PT_OK 0
@@ -197,6 +197,7 @@ typedef struct pt_render_params {
 
 /* pt_render_params.flags */
 #define PT_RENDER_STAGE_TIMING 0x1u /* fill pt_stats.ms_* per stage (CUDA events per launch) */
+#define PT_RENDER_RADIANCE_CACHE 0x2u /* terminate paths into the radiance cache (pt_cache_init) */
 
 /* Film: per pixel Σ(L, 1) as RGBA float32 (shaders/Shaders.hlsl:632-634)
  * plus the Kahan compensation of the same shape.  location 0 = host
@@ -347,6 +348,66 @@ typedef struct pt_hit {
 int pt_trace_closest(pt_ctx *ctx, const float *rays, size_t n, pt_hit *out, uint32_t location);
 int pt_trace_shadow(pt_ctx *ctx, const float *rays, size_t n, uint32_t *occluded_out,
                     float *transmission_out, uint32_t location);
+
+/* ---- radiance cache ---------------------------------------------------------
+ * No counterpart in the reference (its paths run to Russian roulette).  A
+ * neural radiance cache after Müller et al. 2021: a fully fused MLP of 64
+ * encoded inputs, 5 hidden layers of 64 (ReLU) and 3 outputs (RGB), BF16
+ * operands on the tensor cores with FP32 accumulation, trained online.
+ * With PT_RENDER_RADIANCE_CACHE a render ends each path at the first surface
+ * vertex reached after a rough bounce (diffuse, hair, microfacet / Disney at
+ * or above rough_threshold) and adds throughput x cache(vertex).  A subset of
+ * paths (about train_records per call) continues past that vertex; its
+ * suffix, itself ended in the cache at its next rough bounce (self-training),
+ * gives the radiance estimate the network is trained on after the render
+ * (one Adam step per call on relative L2 loss).  One training path in
+ * unbiased_every continues without the cache instead.
+ *
+ * Records (pt_cache_encode_batch): 16 floats per query — position,
+ * roughness; direction toward the previous vertex, 0; shading normal, 0;
+ * albedo, 0.  Features: 64 floats per query (the network's input).
+ * Parameters: PT_CACHE_PARAMS floats, layer by layer, each [out][in]
+ * row-major (64x64 x 5, then 16x64 of which rows 0..2 are used). */
+#define PT_CACHE_PARAMS 21504u
+#define PT_CACHE_FEATURES 64u
+#define PT_CACHE_RECORD_FLOATS 16u
+#define PT_CACHE_MAX_RECORDS 262144u
+#define PT_CACHE_NO_TRAIN 0x1u /* render with the cache, take no training paths and no steps */
+typedef struct pt_cache_params {
+    uint32_t train_records;  /* training paths per render call (0 = 65536; <= PT_CACHE_MAX_RECORDS) */
+    uint32_t unbiased_every; /* one training path in this many runs without the cache (0 = none) */
+    float rough_threshold;   /* microfacet alpha / Disney roughness counted as rough (0 = 0.3) */
+    float learning_rate;     /* Adam step size (0 = 5e-3); beta1 0.9, beta2 0.99, eps 1e-8 */
+    float ema;               /* decay of the weight average used for inference (0 = none) */
+    uint32_t seed;           /* weight initialisation */
+    uint32_t flags;          /* PT_CACHE_* */
+    float bbox_min[3];       /* position normalisation; bbox_max <= bbox_min: the scene's bounds */
+    float bbox_max[3];
+} pt_cache_params;
+typedef struct pt_cache_stats {
+    uint64_t steps;        /* Adam steps taken */
+    uint32_t last_records; /* records in the last step */
+    float last_loss;       /* mean relative L2 loss of the last step */
+    uint64_t queries;      /* cache queries of the last render */
+} pt_cache_stats;
+/* (Re)initialise the cache of ctx: weights from params->seed, zero moments. */
+int pt_cache_init(pt_ctx *ctx, const pt_cache_params *params);
+int pt_cache_release(pt_ctx *ctx);
+/* Copy the FP32 parameters out (get != NULL) and/or replace them (set != NULL;
+ * moments reset, the inference average restarts from the new weights). */
+int pt_cache_weights(pt_ctx *ctx, float *get, const float *set);
+/* Batched network entry points (parity): records -> features, features ->
+ * outputs (3 per query, the inference weights), and features + targets (3
+ * per query) -> the summed parameter gradient of the relative L2 loss
+ * sum_c (y_c - t_c)^2 / (y_c^2 + 0.01) (denominator held constant) and the
+ * loss sum, or one Adam step on it. */
+int pt_cache_encode_batch(pt_ctx *ctx, const float *records, size_t n, float *features, uint32_t location);
+int pt_cache_infer_batch(pt_ctx *ctx, const float *features, size_t n, float *out, uint32_t location);
+int pt_cache_gradient_batch(pt_ctx *ctx, const float *features, const float *targets, size_t n,
+                            float *grad_out, float *loss_out, uint32_t location);
+int pt_cache_train_batch(pt_ctx *ctx, const float *features, const float *targets, size_t n, float *loss_out,
+                         uint32_t location);
+int pt_cache_get_stats(pt_ctx *ctx, pt_cache_stats *out);
 
 #ifdef __cplusplus
 }

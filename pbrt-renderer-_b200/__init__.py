@@ -29,6 +29,12 @@ PT_ENV_CDF, PT_ENV_ALIAS = 0, 1
 PT_MEM_HOST, PT_MEM_DEVICE = 0, 1
 PT_SAMPLE_DIMS = 4
 PT_RENDER_STAGE_TIMING = 1
+PT_RENDER_RADIANCE_CACHE = 2
+PT_CACHE_PARAMS = 21504
+PT_CACHE_FEATURES = 64
+PT_CACHE_RECORD_FLOATS = 16
+PT_CACHE_MAX_RECORDS = 262144
+PT_CACHE_NO_TRAIN = 1
 
 
 class pt_material(C.Structure):
@@ -105,6 +111,28 @@ class pt_stats(C.Structure):
 class pt_hit(C.Structure):
     _fields_ = [("t", C.c_float), ("mesh", C.c_uint32), ("prim", C.c_uint32), ("u", C.c_float),
                 ("v", C.c_float), ("hit", C.c_uint32)]
+
+
+class pt_cache_params(C.Structure):
+    _fields_ = [("train_records", C.c_uint32), ("unbiased_every", C.c_uint32), ("rough_threshold", C.c_float),
+                ("learning_rate", C.c_float), ("ema", C.c_float), ("seed", C.c_uint32), ("flags", C.c_uint32),
+                ("bbox_min", C.c_float * 3), ("bbox_max", C.c_float * 3)]
+
+
+class pt_cache_stats(C.Structure):
+    _fields_ = [("steps", C.c_uint64), ("last_records", C.c_uint32), ("last_loss", C.c_float),
+                ("queries", C.c_uint64)]
+
+
+def cache_params(train_records=0, unbiased_every=0, rough_threshold=0.0, learning_rate=0.0, ema=0.0, seed=0,
+                 flags=0, bbox=None) -> pt_cache_params:
+    p = pt_cache_params()
+    p.train_records, p.unbiased_every, p.rough_threshold = train_records, unbiased_every, rough_threshold
+    p.learning_rate, p.ema, p.seed, p.flags = learning_rate, ema, seed, flags
+    if bbox is not None:
+        p.bbox_min[:] = bbox[0]
+        p.bbox_max[:] = bbox[1]
+    return p
 
 
 def fptr(a):
@@ -247,6 +275,14 @@ def lib():
         L.pt_bvh_read.argtypes = [P, U, U, C.POINTER(C.c_int32)]
         L.pt_trace_closest.argtypes = [P, F, S, C.POINTER(pt_hit), C.c_uint32]
         L.pt_trace_shadow.argtypes = [P, F, S, U, F, C.c_uint32]
+        L.pt_cache_init.argtypes = [P, C.POINTER(pt_cache_params)]
+        L.pt_cache_release.argtypes = [P]
+        L.pt_cache_weights.argtypes = [P, F, F]
+        L.pt_cache_encode_batch.argtypes = [P, F, S, F, C.c_uint32]
+        L.pt_cache_infer_batch.argtypes = [P, F, S, F, C.c_uint32]
+        L.pt_cache_gradient_batch.argtypes = [P, F, F, S, F, F, C.c_uint32]
+        L.pt_cache_train_batch.argtypes = [P, F, F, S, F, C.c_uint32]
+        L.pt_cache_get_stats.argtypes = [P, C.POINTER(pt_cache_stats)]
         _lib = L
     return _lib
 
@@ -382,3 +418,53 @@ class Context:
         tr = np.zeros((n, 3), np.float32)
         self._check(self.L.pt_trace_shadow(self.h, fptr(rays), n, uptr(occ), fptr(tr), PT_MEM_HOST))
         return occ, tr
+
+    # ---- radiance cache ------------------------------------------------------------
+    def cache_init(self, params: pt_cache_params | None = None):
+        self._check(self.L.pt_cache_init(self.h, C.byref(params if params is not None else cache_params())))
+
+    def cache_release(self):
+        self._check(self.L.pt_cache_release(self.h))
+
+    def cache_weights(self, set_to=None):
+        """The FP32 parameters (PT_CACHE_PARAMS); with set_to, replace them first."""
+        if set_to is not None:
+            w = np.ascontiguousarray(set_to, np.float32)
+            assert w.size == PT_CACHE_PARAMS
+            self._check(self.L.pt_cache_weights(self.h, None, fptr(w)))
+        out = np.zeros(PT_CACHE_PARAMS, np.float32)
+        self._check(self.L.pt_cache_weights(self.h, fptr(out), None))
+        return out
+
+    def cache_encode(self, records):
+        r = np.ascontiguousarray(records, np.float32).reshape(-1, PT_CACHE_RECORD_FLOATS)
+        out = np.zeros((len(r), PT_CACHE_FEATURES), np.float32)
+        self._check(self.L.pt_cache_encode_batch(self.h, fptr(r), len(r), fptr(out), PT_MEM_HOST))
+        return out
+
+    def cache_infer(self, features):
+        f = np.ascontiguousarray(features, np.float32).reshape(-1, PT_CACHE_FEATURES)
+        out = np.zeros((len(f), 3), np.float32)
+        self._check(self.L.pt_cache_infer_batch(self.h, fptr(f), len(f), fptr(out), PT_MEM_HOST))
+        return out
+
+    def cache_gradient(self, features, targets):
+        f = np.ascontiguousarray(features, np.float32).reshape(-1, PT_CACHE_FEATURES)
+        t = np.ascontiguousarray(targets, np.float32).reshape(-1, 3)
+        g = np.zeros(PT_CACHE_PARAMS, np.float32)
+        loss = np.zeros(1, np.float32)
+        self._check(self.L.pt_cache_gradient_batch(self.h, fptr(f), fptr(t), len(f), fptr(g), fptr(loss),
+                                                   PT_MEM_HOST))
+        return g, float(loss[0])
+
+    def cache_train(self, features, targets):
+        f = np.ascontiguousarray(features, np.float32).reshape(-1, PT_CACHE_FEATURES)
+        t = np.ascontiguousarray(targets, np.float32).reshape(-1, 3)
+        loss = np.zeros(1, np.float32)
+        self._check(self.L.pt_cache_train_batch(self.h, fptr(f), fptr(t), len(f), fptr(loss), PT_MEM_HOST))
+        return float(loss[0])
+
+    def cache_stats(self) -> pt_cache_stats:
+        st = pt_cache_stats()
+        self._check(self.L.pt_cache_get_stats(self.h, C.byref(st)))
+        return st

@@ -237,67 +237,6 @@ __global__ void k_trace_shadow(DevScene S, const float *rays, size_t n, uint32_t
 // ===========================================================================
 static inline unsigned blocks_for(size_t n, unsigned b = 256) { return (unsigned)((n + b - 1) / b); }
 
-// Device scratch for host-memory batch calls: grows, never shrinks.
-static int scratch(pt_ctx *ctx, size_t bytes, char **out) {
-    if (ctx->scratchBytes < bytes) {
-        if (ctx->scratch) cudaFree(ctx->scratch);
-        ctx->scratch = nullptr;
-        ctx->scratchBytes = 0;
-        cudaError_t e = cudaMalloc(&ctx->scratch, bytes);
-        if (e != cudaSuccess) return ctx->fail(PT_E_NOMEM, "scratch", cudaGetErrorString(e));
-        ctx->scratchBytes = bytes;
-    }
-    *out = (char *)ctx->scratch;
-    return PT_OK;
-}
-static size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
-
-// Stage host arrays into device scratch (location == PT_MEM_HOST) or pass
-// device pointers through.  `ins` are copied in; `outs` copied back by finish().
-struct Staging {
-    pt_ctx *ctx;
-    uint32_t loc;
-    struct Buf { const void *host; size_t bytes; void *dev; bool out; };
-    std::vector<Buf> bufs;
-    int setup() {
-        if (loc == PT_MEM_DEVICE) {
-            for (auto &b : bufs) b.dev = const_cast<void *>(b.host);
-            return PT_OK;
-        }
-        size_t tot = 0;
-        for (auto &b : bufs) tot += al256(b.bytes);
-        char *base;
-        int rc = scratch(ctx, tot + 256, &base);
-        if (rc) return rc;
-        for (auto &b : bufs) {
-            if (!b.host) { b.dev = nullptr; continue; }
-            b.dev = base;
-            base += al256(b.bytes);
-            if (!b.out) {
-                cudaError_t e = cudaMemcpyAsync(b.dev, b.host, b.bytes, cudaMemcpyHostToDevice, ctx->stream);
-                if (e != cudaSuccess) return ctx->fail(PT_E_CUDA, "staging copy", cudaGetErrorString(e));
-            }
-        }
-        return PT_OK;
-    }
-    int finish() {
-        if (loc == PT_MEM_HOST)
-            for (auto &b : bufs)
-                if (b.out && b.host) {
-                    cudaError_t e = cudaMemcpyAsync(const_cast<void *>(b.host), b.dev, b.bytes, cudaMemcpyDeviceToHost,
-                                                    ctx->stream);
-                    if (e != cudaSuccess) return ctx->fail(PT_E_CUDA, "staging copy back", cudaGetErrorString(e));
-                }
-        cudaError_t e = cudaStreamSynchronize(ctx->stream);
-        if (e != cudaSuccess) return ctx->fail(PT_E_CUDA, "batch kernel", cudaGetErrorString(e));
-        return PT_OK;
-    }
-    void *add(const void *p, size_t bytes, bool out) {
-        bufs.push_back({p, bytes, nullptr, out});
-        return nullptr;
-    }
-    void *dev(size_t i) { return bufs[i].dev; }
-};
 
 // ===========================================================================
 // C ABI

@@ -1,0 +1,710 @@
+// pt_cache.cu — the radiance cache of libpt: a fully fused BF16 MLP on the
+// sm_100a tensor cores (tcgen05.mma, operands in shared memory, FP32
+// accumulators in tensor memory), its training step and Adam update, and the
+// host entry points.  No counterpart in the reference.
+//
+// Kernel structure (one CTA = 128 threads = one 128-row tile per pass):
+// * the BF16 weight image (43 KB) is placed in shared memory by one bulk
+//   copy per CTA and stays there for all of the CTA's tiles;
+// * each thread encodes one row (query) into the BF16 activation tile;
+// * per layer one thread issues 4 MMAs (K = 64 in steps of 16) into TMEM
+//   and commits them to an mbarrier; the 4 warps read their 32 TMEM lanes
+//   back (tcgen05.ld), apply ReLU and write the next activation tile;
+// * training keeps all six activation tiles, runs the backward pass with the
+//   same MMAs on transposed views of the same shared-memory images
+//   (K-major for dZ.W, MN-major for dZ^T.A), and accumulates the weight
+//   gradients in TMEM across the CTA's tiles before one atomic flush.
+// Every mbarrier wait is bounded; a timeout raises an error flag and the CTA
+// frees its tensor memory and returns.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <random>
+
+#include "pt_cache.cuh"
+#include "pt_internal.h"
+
+namespace pt {
+
+constexpr int kRcThreads = 128;
+constexpr uint32_t kTileBytes = kRcTile * kRcIn * 2;  // 16 KB: one 128 x 64 BF16 tile
+constexpr uint32_t kGradBytes = 2 * kTileBytes;       // dZ tiles carry a zero upper half (M = 128 views)
+constexpr uint32_t kInferSmem = kRcImageBytes + kTileBytes + 64;
+constexpr uint32_t kTrainSmem = kRcImageBytes + 6 * kTileBytes + 2 * kGradBytes + 64;
+static_assert(kTrainSmem <= 227 * 1024, "training kernel shared memory");
+constexpr uint32_t kDevErrCache = 8u;  // device error bit: a cache kernel's wait timed out
+
+struct RcNet {
+    const uint8_t *img;  // BF16 weight image
+    float bmin[3], binv[3];
+    uint32_t *err;
+};
+
+// Input of one row: a record (encoded here) or a ready feature vector.
+template <int SRC>
+struct RcRows;
+template <>
+struct RcRows<0> {  // features n x 64, targets n x 3 (training)
+    const float *feat, *targ;
+    uint32_t n;
+    __device__ uint32_t count() const { return n; }
+    __device__ void load(const RcNet &, uint32_t row, float f[kRcIn]) const {
+        const float4 *p = reinterpret_cast<const float4 *>(feat + (size_t)row * kRcIn);
+#pragma unroll
+        for (int k = 0; k < kRcIn / 4; k++) {
+            float4 v = p[k];
+            f[4 * k] = v.x; f[4 * k + 1] = v.y; f[4 * k + 2] = v.z; f[4 * k + 3] = v.w;
+        }
+    }
+    __device__ float3 target(uint32_t row) const {
+        return make_float3(targ[3 * row], targ[3 * row + 1], targ[3 * row + 2]);
+    }
+};
+template <>
+struct RcRows<1> {  // records (render queries or training records)
+    const float4 *r0, *r1, *r2, *r3, *tgt;
+    const uint32_t *cnt;
+    uint32_t cap;
+    __device__ uint32_t count() const { return min(*(volatile const uint32_t *)cnt, cap); }
+    __device__ void load(const RcNet &N, uint32_t row, float f[kRcIn]) const {
+        rc_encode(r0[row], r1[row], r2[row], r3[row], N.bmin, N.binv, f);
+    }
+    __device__ float3 target(uint32_t row) const {
+        float4 t = tgt[row];
+        return make_float3(t.x, t.y, t.z);
+    }
+};
+
+// ---- weight staging and TMEM set-up shared by the kernels -------------------
+struct CtaCtl {
+    uint32_t mbW, mbM, tbase, tl;
+    uint32_t phase;
+    bool ok;
+};
+__device__ __forceinline__ void rc_setup(CtaCtl &c, uint8_t *W, uint64_t *bars, uint32_t *tslot, const uint8_t *img,
+                                         uint32_t cols) {
+    const uint32_t t = threadIdx.x, warp = t >> 5;
+    c.mbW = smem_u32(bars);
+    c.mbM = smem_u32(bars + 1);
+    if (t == 0) {
+        mbar_init(c.mbW, 1);
+        mbar_init(c.mbM, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (t == 0) {
+        mbar_expect_tx(c.mbW, kRcImageBytes);
+        bulk_g2s(smem_u32(W), img, kRcImageBytes, c.mbW);
+    }
+    __syncwarp();
+    if (warp == 0) tmem_alloc(smem_u32(tslot), cols);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    c.tbase = *tslot;
+    c.tl = c.tbase + ((warp * 32u) << 16);
+    c.phase = 0;
+    c.ok = __syncthreads_and(mbar_wait(c.mbW, 0)) != 0;
+}
+// Wait for the MMAs committed to mbM; uniform across the CTA.
+__device__ __forceinline__ bool rc_wait_mma(CtaCtl &c) {
+    bool done = mbar_wait(c.mbM, c.phase);
+    bool all = __syncthreads_and(done) != 0;
+    if (all) c.phase ^= 1u;
+    tc_fence_after();
+    return all;
+}
+__device__ __forceinline__ void rc_teardown(CtaCtl &c, uint32_t cols, uint32_t *err) {
+    if (!c.ok) {
+        if (threadIdx.x == 0) atomicOr(err, kDevErrCache);
+        mbar_wait(c.mbW, 0, 1u << 20);        // the weight copy, if it is still in flight
+        mbar_wait(c.mbM, c.phase, 1u << 20);  // MMAs of the wait that gave up
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if ((threadIdx.x >> 5) == 0) tmem_free(c.tbase, cols);
+}
+// Forward MMAs of layer l: D[0:N) = A (128 x 64) . W_l^T.
+__device__ __forceinline__ void rc_issue_forward(const CtaCtl &c, const uint8_t *A, const uint8_t *W, int l) {
+    const uint32_t N = rc_rows(l);
+    tc_fence_after();
+    const uint32_t idesc = umma_idesc(128, N, 0, 0);
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+        uint64_t ad = umma_desc(smem_u32(A) + s * 2 * (kRcTile * 16), kRcTile * 16, 128);
+        uint64_t bd = umma_desc(smem_u32(W) + rc_image_base(l) + s * 2 * (N * 16), N * 16, 128);
+        umma_bf16(c.tbase, ad, bd, idesc, s > 0 ? 1u : 0u);
+    }
+    umma_commit(c.mbM);
+}
+
+// ---- inference: features / render queries -> radiance ------------------------
+// MODE 0: rows from a feature array, outputs to out[n x 3].
+// MODE 1: rows from render queries; lo_eta[slot] += weight * max(y, 0).
+struct RcInferArgs {
+    RcNet net;
+    RcRows<0> feat;
+    RcRows<1> qry;
+    const float4 *qw;  // per query: throughput weight
+    float *out;
+    float4 *lo_eta;
+};
+template <int MODE>
+__global__ void __launch_bounds__(kRcThreads) k_rc_infer(RcInferArgs a) {
+    extern __shared__ __align__(1024) uint8_t sm[];
+    uint8_t *W = sm, *T = sm + kRcImageBytes;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sm + kRcImageBytes + kTileBytes);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2);
+    const uint32_t t = threadIdx.x;
+    const uint32_t n = MODE == 0 ? a.feat.count() : a.qry.count();
+    const uint32_t ntiles = (n + kRcTile - 1) / kRcTile;
+    if (blockIdx.x >= ntiles) return;  // uniform: before any set-up
+    CtaCtl c;
+    rc_setup(c, W, bars, tslot, a.net.img, 64);
+    for (uint32_t tile = blockIdx.x; tile < ntiles && c.ok; tile += gridDim.x) {
+        const uint32_t row = tile * kRcTile + t;
+        const bool valid = row < n;
+        float f[kRcIn];
+        if (valid) {
+            if (MODE == 0) a.feat.load(a.net, row, f);
+            else a.qry.load(a.net, row, f);
+        } else {
+#pragma unroll
+            for (int k = 0; k < kRcIn; k++) f[k] = 0.0f;
+        }
+        store_row_bf16(T, t, f);
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        for (int l = 0; l < kRcLayers && c.ok; l++) {
+            if (t == 0) rc_issue_forward(c, T, W, l);
+            if (!(c.ok = rc_wait_mma(c))) break;
+            if (l < kRcLayers - 1) {
+                float v[64];
+                tmem_ld64(c.tl, v);
+                tmem_wait_ld();
+#pragma unroll
+                for (int k = 0; k < 64; k++) v[k] = fmaxf(v[k], 0.0f);
+                store_row_bf16(T, t, v);
+                fence_async_smem();
+            } else {
+                float v[16];
+                tmem_ld16(c.tl, v);
+                tmem_wait_ld();
+                if (valid) {
+                    if (MODE == 0) {
+                        a.out[3 * (size_t)row] = v[0];
+                        a.out[3 * (size_t)row + 1] = v[1];
+                        a.out[3 * (size_t)row + 2] = v[2];
+                    } else {
+                        uint32_t slot = __float_as_uint(a.qry.r1[row].w);
+                        float4 w = a.qw[row], le = a.lo_eta[slot];
+                        le.x += w.x * fmaxf(v[0], 0.0f);
+                        le.y += w.y * fmaxf(v[1], 0.0f);
+                        le.z += w.z * fmaxf(v[2], 0.0f);
+                        a.lo_eta[slot] = le;
+                    }
+                }
+            }
+            tc_fence_before();
+            __syncthreads();
+        }
+    }
+    rc_teardown(c, 64, a.net.err);
+}
+
+// ---- training: forward, relative L2 loss, backward, weight gradients ---------
+struct RcTrainArgs {
+    RcNet net;
+    RcRows<0> feat;
+    RcRows<1> rec;
+    float *grad;     // kRcParams FP32, added to
+    float *lossSum;  // added to
+};
+// TMEM columns: [0, 64) layer output / input gradient, [64 + 64 l, 128 + 64 l)
+// the weight gradient of layer l.
+template <int MODE>
+__global__ void __launch_bounds__(kRcThreads, 1) k_rc_train(RcTrainArgs a) {
+    extern __shared__ __align__(1024) uint8_t sm[];
+    uint8_t *W = sm;
+    uint8_t *Act = sm + kRcImageBytes;                     // 6 tiles: A_0 (input) .. A_5
+    uint8_t *dZo = Act + 6 * kTileBytes;                   // output-layer gradient (16 columns used)
+    uint8_t *dZ = dZo + kGradBytes;                        // hidden-layer gradient
+    uint64_t *bars = reinterpret_cast<uint64_t *>(dZ + kGradBytes);
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2);
+    const uint32_t t = threadIdx.x;
+    const uint32_t n = MODE == 0 ? a.feat.count() : a.rec.count();
+    const uint32_t ntiles = (n + kRcTile - 1) / kRcTile;
+    if (blockIdx.x >= ntiles) return;
+    // the dZ images are read as M = 128 operands: their upper halves (and the
+    // unused columns of dZo) must hold zeros
+    for (uint32_t i = t; i < 2 * kGradBytes / 16; i += kRcThreads)
+        reinterpret_cast<uint4 *>(dZo)[i] = make_uint4(0, 0, 0, 0);
+    fence_async_smem();
+    CtaCtl c;
+    rc_setup(c, W, bars, tslot, a.net.img, 512);
+    float loss = 0.0f;
+    bool first = true;
+    for (uint32_t tile = blockIdx.x; tile < ntiles && c.ok; tile += gridDim.x) {
+        const uint32_t row = tile * kRcTile + t;
+        const bool valid = row < n;
+        float f[kRcIn];
+        float3 tg = make_float3(0.0f, 0.0f, 0.0f);
+        if (valid) {
+            if (MODE == 0) { a.feat.load(a.net, row, f); tg = a.feat.target(row); }
+            else { a.rec.load(a.net, row, f); tg = a.rec.target(row); }
+        } else {
+#pragma unroll
+            for (int k = 0; k < kRcIn; k++) f[k] = 0.0f;
+        }
+        store_row_bf16(Act, t, f);
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        // forward
+        for (int l = 0; l < kRcLayers && c.ok; l++) {
+            if (t == 0) rc_issue_forward(c, Act + l * kTileBytes, W, l);
+            if (!(c.ok = rc_wait_mma(c))) break;
+            if (l < kRcLayers - 1) {
+                float v[64];
+                tmem_ld64(c.tl, v);
+                tmem_wait_ld();
+#pragma unroll
+                for (int k = 0; k < 64; k++) v[k] = fmaxf(v[k], 0.0f);
+                store_row_bf16(Act + (l + 1) * kTileBytes, t, v);
+            } else {
+                float v[16];
+                tmem_ld16(c.tl, v);
+                tmem_wait_ld();
+                const float y[3] = {v[0], v[1], v[2]}, tt[3] = {tg.x, tg.y, tg.z};
+                float g[16];
+#pragma unroll
+                for (int k = 0; k < 16; k++) g[k] = 0.0f;
+                if (valid) {
+#pragma unroll
+                    for (int k = 0; k < 3; k++) {
+                        float d = y[k] - tt[k], den = y[k] * y[k] + 0.01f;
+                        loss += d * d / den;
+                        g[k] = 2.0f * d / den;
+                    }
+                }
+                uint4 w0 = make_uint4(pack_bf16(g[0], g[1]), pack_bf16(g[2], g[3]), pack_bf16(g[4], g[5]),
+                                      pack_bf16(g[6], g[7]));
+                uint4 w1 = make_uint4(pack_bf16(g[8], g[9]), pack_bf16(g[10], g[11]), pack_bf16(g[12], g[13]),
+                                      pack_bf16(g[14], g[15]));
+                *reinterpret_cast<uint4 *>(dZo + rc_core_offset(t, 0, kRcTile)) = w0;
+                *reinterpret_cast<uint4 *>(dZo + rc_core_offset(t, 8, kRcTile)) = w1;
+            }
+            fence_async_smem();
+            tc_fence_before();
+            __syncthreads();
+        }
+        // backward: layer l consumes dZ_l (dZo for the output layer)
+        for (int l = kRcLayers - 1; l >= 0 && c.ok; l--) {
+            const uint8_t *G = l == kRcLayers - 1 ? dZo : dZ;
+            const uint32_t Kout = rc_rows(l);
+            if (t == 0) {
+                tc_fence_after();
+                // dW_l += dZ_l^T . A_l : M = 128 (rows = out, zero above Kout), N = 64, K = 128 (batch)
+                const uint32_t idw = umma_idesc(128, 64, 1, 1);
+#pragma unroll
+                for (int s = 0; s < 8; s++) {
+                    uint64_t ad = umma_desc(smem_u32(G) + s * 256, 128, kRcTile * 16);
+                    uint64_t bd = umma_desc(smem_u32(Act + l * kTileBytes) + s * 256, 128, kRcTile * 16);
+                    umma_bf16(c.tbase + 64 + 64 * l, ad, bd, idw, (first && s == 0) ? 0u : 1u);
+                }
+                if (l > 0) {
+                    // dA_l = dZ_l . W_l : M = 128 (batch), N = 64 (in), K = Kout
+                    const uint32_t ida = umma_idesc(128, 64, 0, 1);
+                    for (uint32_t s = 0; s < Kout / 16; s++) {
+                        uint64_t ad = umma_desc(smem_u32(G) + s * 2 * (kRcTile * 16), kRcTile * 16, 128);
+                        uint64_t bd = umma_desc(smem_u32(W) + rc_image_base(l) + s * 256, 128, Kout * 16);
+                        umma_bf16(c.tbase, ad, bd, ida, s > 0 ? 1u : 0u);
+                    }
+                }
+                umma_commit(c.mbM);
+            }
+            if (!(c.ok = rc_wait_mma(c))) break;
+            if (l > 0) {  // dZ_{l-1} = dA_l (x) [A_l > 0]
+                float v[64], act[64];
+                tmem_ld64(c.tl, v);
+                tmem_wait_ld();
+                load_row_bf16(Act + l * kTileBytes, t, act);
+#pragma unroll
+                for (int k = 0; k < 64; k++) v[k] = act[k] > 0.0f ? v[k] : 0.0f;
+                store_row_bf16(dZ, t, v);
+                fence_async_smem();
+            }
+            tc_fence_before();
+            __syncthreads();
+        }
+        first = false;
+    }
+    // flush the weight gradients: thread t holds row t (an output unit)
+    if (c.ok && !first) {
+        tc_fence_after();
+        for (int l = 0; l < kRcLayers; l++) {
+            float v[64];
+            tmem_ld64(c.tl + 64 + 64 * l, v);
+            tmem_wait_ld();
+            if (t < (uint32_t)rc_rows(l)) {
+                float *g = a.grad + rc_param_base(l) + t * kRcIn;
+#pragma unroll
+                for (int k = 0; k < 64; k++) atomicAdd(g + k, v[k]);
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xFFFFFFFFu, loss, o);
+    if ((t & 31) == 0 && c.ok) atomicAdd(a.lossSum, loss);
+    rc_teardown(c, 512, a.net.err);
+}
+
+// ---- Adam (one CTA): FP32 master weights -> BF16 images ------------------------
+struct RcAdamArgs {
+    float *w, *m, *v, *ema, *grad;
+    uint8_t *imgTrain, *imgInfer;
+    uint32_t *ctr;           // [0] steps (read, incremented), [4] records of the step (written)
+    const uint32_t *nrec;    // records the gradient sums over
+    uint32_t nrecCap;
+    float lr, emaDecay;
+    float *lossSum;          // mean loss of the step -> ctr[3] as float bits; reset
+};
+__device__ __forceinline__ void put_bf16(uint8_t *img, int i, float x) {
+    int l = i < rc_param_base(5) ? i / (kRcWidth * kRcIn) : 5;
+    int j = i - rc_param_base(l);
+    int o = j / kRcIn, in = j % kRcIn;
+    *reinterpret_cast<__nv_bfloat16 *>(img + rc_image_base(l) + rc_core_offset(o, in, rc_rows(l))) =
+        __float2bfloat16_rn(x);
+}
+__global__ void __launch_bounds__(1024) k_rc_adam(RcAdamArgs a) {
+    __shared__ uint32_t sStep, sN;
+    if (threadIdx.x == 0) {
+        sStep = a.ctr[0] + 1u;
+        sN = min(*a.nrec, a.nrecCap);
+    }
+    __syncthreads();
+    const uint32_t n = sN, step = sStep;
+    if (n == 0) return;
+    const float b1 = 0.9f, b2 = 0.99f, eps = 1e-8f;
+    const float gs = 1.0f / (3.0f * (float)n);
+    const float bc1 = 1.0f - powf(b1, (float)step), bc2 = 1.0f - powf(b2, (float)step);
+    for (int i = threadIdx.x; i < kRcParams; i += blockDim.x) {
+        float g = a.grad[i] * gs;
+        a.grad[i] = 0.0f;
+        if (!isfinite(g)) g = 0.0f;
+        float m = b1 * a.m[i] + (1.0f - b1) * g;
+        float v = b2 * a.v[i] + (1.0f - b2) * g * g;
+        a.m[i] = m;
+        a.v[i] = v;
+        float w = a.w[i] - a.lr * (m / bc1) / (sqrtf(v / bc2) + eps);
+        a.w[i] = w;
+        float e = (step == 1u || a.emaDecay == 0.0f) ? w : a.emaDecay * a.ema[i] + (1.0f - a.emaDecay) * w;
+        a.ema[i] = e;
+        put_bf16(a.imgTrain, i, w);
+        put_bf16(a.imgInfer, i, e);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        a.ctr[0] = step;
+        a.ctr[4] = n;
+        a.ctr[3] = __float_as_uint(*a.lossSum / (3.0f * (float)n));
+        *a.lossSum = 0.0f;
+    }
+}
+
+// Images from the FP32 weights (initialisation, pt_cache_weights).
+__global__ void k_rc_images(const float *w, uint8_t *imgTrain, uint8_t *imgInfer, float *ema) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kRcParams; i += gridDim.x * blockDim.x) {
+        ema[i] = w[i];
+        put_bf16(imgTrain, i, w[i]);
+        put_bf16(imgInfer, i, w[i]);
+    }
+}
+
+__global__ void k_rc_encode(const float4 *rec, uint32_t n, float bx, float by, float bz, float ix, float iy, float iz,
+                            float *feat) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float bmin[3] = {bx, by, bz}, binv[3] = {ix, iy, iz};
+    float f[kRcIn];
+    rc_encode(rec[4 * i], rec[4 * i + 1], rec[4 * i + 2], rec[4 * i + 3], bmin, binv, f);
+    for (int k = 0; k < kRcIn; k++) feat[(size_t)i * kRcIn + k] = f[k];
+}
+
+}  // namespace pt
+
+using namespace pt;
+
+// ---- host side ------------------------------------------------------------------
+namespace {
+bool gRcAttr = false;
+int rc_attrs(pt_ctx *ctx) {
+    if (gRcAttr) return PT_OK;
+    const void *fns[] = {(const void *)k_rc_infer<0>, (const void *)k_rc_infer<1>};
+    for (const void *f : fns)
+        if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kInferSmem) != cudaSuccess)
+            return ctx->fail(PT_E_CUDA, "cache kernel attributes");
+    const void *tf[] = {(const void *)k_rc_train<0>, (const void *)k_rc_train<1>};
+    for (const void *f : tf)
+        if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrainSmem) != cudaSuccess)
+            return ctx->fail(PT_E_CUDA, "cache kernel attributes");
+    gRcAttr = true;
+    return PT_OK;
+}
+RcNet rc_net(const pt_ctx *ctx, const uint8_t *img) {
+    RcNet n;
+    n.img = img;
+    for (int k = 0; k < 3; k++) {
+        n.bmin[k] = ctx->cache.bmin[k];
+        n.binv[k] = ctx->cache.binv[k];
+    }
+    n.err = ctx->d_err;
+    return n;
+}
+// Cache bounds: the parameters' box, else the scene's vertex bounds.
+void rc_bounds(pt_ctx *ctx) {
+    RadianceCache &C = ctx->cache;
+    const pt_cache_params &P = C.params;
+    bool own = P.bbox_max[0] > P.bbox_min[0] && P.bbox_max[1] > P.bbox_min[1] && P.bbox_max[2] > P.bbox_min[2];
+    const float *lo = own ? P.bbox_min : ctx->sceneMin, *hi = own ? P.bbox_max : ctx->sceneMax;
+    for (int k = 0; k < 3; k++) {
+        float e = hi[k] - lo[k];
+        C.bmin[k] = lo[k];
+        C.binv[k] = e > 0.0f ? 1.0f / e : 1.0f;
+    }
+}
+int rc_check(pt_ctx *ctx) {
+    if (!ctx) return PT_E_INVALID;
+    if (!ctx->cache.ready) return ctx->fail(PT_E_INVALID, "radiance cache not initialised (pt_cache_init)");
+    cudaSetDevice(ctx->device);
+    return rc_attrs(ctx);
+}
+int rc_device_error(pt_ctx *ctx) {
+    uint32_t derr = 0;
+    if (cudaMemcpy(&derr, ctx->d_err, 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return ctx->fail(PT_E_CUDA, "cache error flag");
+    if (derr & kDevErrCache) {
+        cudaMemset(ctx->d_err, 0, 4);
+        return ctx->fail(PT_E_DEVICE, "radiance cache kernel: a tensor-core wait timed out");
+    }
+    return PT_OK;
+}
+unsigned rc_grid(const pt_ctx *ctx, uint32_t n, unsigned perSM) {
+    unsigned tiles = (n + kRcTile - 1) / kRcTile;
+    return std::max(1u, std::min(tiles, (unsigned)ctx->numSMs * perSM));
+}
+}  // namespace
+
+void pt_cache_free(pt_ctx *ctx) {
+    RadianceCache &C = ctx->cache;
+    void *ps[] = {C.w, C.m, C.v, C.ema, C.grad, C.imgTrain, C.imgInfer, C.ctr};
+    for (void *p : ps)
+        if (p) cudaFree(p);
+    for (float4 *p : C.q)
+        if (p) cudaFree(p);
+    for (float4 *p : C.rec)
+        if (p) cudaFree(p);
+    uint64_t gen = C.gen + 1;
+    C = RadianceCache{};
+    C.gen = gen;
+}
+
+int pt_cache_prepare(pt_ctx *ctx, size_t queryCap) {
+    RadianceCache &C = ctx->cache;
+    if (C.queryCap >= queryCap) return PT_OK;
+    for (float4 *&p : C.q) {
+        if (p) cudaFree(p);
+        p = nullptr;
+    }
+    C.queryCap = 0;
+    C.gen++;
+    for (float4 *&p : C.q)
+        if (cudaMalloc(&p, queryCap * sizeof(float4)) != cudaSuccess)
+            return ctx->fail(PT_E_NOMEM, "cache query buffers");
+    C.queryCap = queryCap;
+    return PT_OK;
+}
+
+extern "C" {
+
+int pt_cache_init(pt_ctx *ctx, const pt_cache_params *params) {
+    if (!ctx || !params) return PT_E_INVALID;
+    if (params->train_records > PT_CACHE_MAX_RECORDS) return ctx->fail(PT_E_INVALID, "train_records above the maximum");
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    pt_cache_free(ctx);
+    RadianceCache &C = ctx->cache;
+    C.params = *params;
+    if (!C.params.train_records) C.params.train_records = 65536u;
+    if (C.params.rough_threshold <= 0.0f) C.params.rough_threshold = 0.3f;
+    if (C.params.learning_rate <= 0.0f) C.params.learning_rate = 5e-3f;
+    rc_bounds(ctx);
+    cudaError_t e = cudaSuccess;
+    auto A = [&](void **p, size_t b) { if (e == cudaSuccess) e = cudaMalloc(p, b); };
+    for (float **p : {&C.w, &C.m, &C.v, &C.ema, &C.grad}) A((void **)p, kRcParams * sizeof(float));
+    A((void **)&C.imgTrain, kRcImageBytes);
+    A((void **)&C.imgInfer, kRcImageBytes);
+    A((void **)&C.ctr, 16 * sizeof(uint32_t));
+    C.recCap = C.params.train_records;
+    for (float4 *&p : C.rec) A((void **)&p, C.recCap * sizeof(float4));
+    if (e != cudaSuccess) {
+        pt_cache_free(ctx);
+        return ctx->fail(PT_E_NOMEM, "radiance cache", cudaGetErrorString(e));
+    }
+    // He-uniform initialisation of the hidden layers; the output layer starts
+    // small so the untrained cache returns about zero
+    std::vector<float> w(kRcParams, 0.0f);
+    std::mt19937 rng(params->seed);
+    for (int l = 0; l < kRcLayers; l++) {
+        float lim = l < kRcLayers - 1 ? std::sqrt(6.0f / kRcIn) : 0.01f;
+        std::uniform_real_distribution<float> U(-lim, lim);
+        for (int o = 0; o < rc_rows(l); o++)
+            for (int i = 0; i < kRcIn; i++)
+                w[rc_param_base(l) + o * kRcIn + i] = (l == kRcLayers - 1 && o >= 3) ? 0.0f : U(rng);
+    }
+    cudaMemcpy(C.w, w.data(), w.size() * 4, cudaMemcpyHostToDevice);
+    for (float *p : {C.m, C.v, C.grad}) cudaMemset(p, 0, kRcParams * sizeof(float));
+    cudaMemset(C.imgTrain, 0, kRcImageBytes);
+    cudaMemset(C.imgInfer, 0, kRcImageBytes);
+    cudaMemset(C.ctr, 0, 16 * sizeof(uint32_t));
+    k_rc_images<<<21, 1024>>>(C.w, C.imgTrain, C.imgInfer, C.ema);
+    e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return ctx->fail(PT_E_CUDA, "cache initialisation", cudaGetErrorString(e));
+    C.ready = true;
+    return PT_OK;
+}
+
+int pt_cache_release(pt_ctx *ctx) {
+    if (!ctx) return PT_E_INVALID;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    pt_cache_free(ctx);
+    return PT_OK;
+}
+
+int pt_cache_weights(pt_ctx *ctx, float *get, const float *set) {
+    int rc = rc_check(ctx);
+    if (rc) return rc;
+    RadianceCache &C = ctx->cache;
+    cudaStreamSynchronize(ctx->stream);
+    if (get && cudaMemcpy(get, C.w, kRcParams * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return ctx->fail(PT_E_CUDA, "cache weights");
+    if (set) {
+        if (cudaMemcpy(C.w, set, kRcParams * 4, cudaMemcpyHostToDevice) != cudaSuccess)
+            return ctx->fail(PT_E_CUDA, "cache weights");
+        for (float *p : {C.m, C.v, C.grad}) cudaMemset(p, 0, kRcParams * sizeof(float));
+        cudaMemset(C.ctr, 0, 16 * sizeof(uint32_t));
+        k_rc_images<<<21, 1024>>>(C.w, C.imgTrain, C.imgInfer, C.ema);
+        cudaError_t e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) return ctx->fail(PT_E_CUDA, "cache weights", cudaGetErrorString(e));
+    }
+    return PT_OK;
+}
+
+int pt_cache_encode_batch(pt_ctx *ctx, const float *records, size_t n, float *features, uint32_t loc) {
+    int rc = rc_check(ctx);
+    if (rc) return rc;
+    if (!records || !features) return ctx->fail(PT_E_INVALID, "null argument");
+    if (!n) return PT_OK;
+    if (n > 0xFFFFFFFFull) return ctx->fail(PT_E_INVALID, "too many records");
+    Staging s{ctx, loc, {}};
+    s.add(records, n * kRcRecFloats * 4, false);
+    s.add(features, n * kRcIn * 4, true);
+    if ((rc = s.setup())) return rc;
+    const RadianceCache &C = ctx->cache;
+    k_rc_encode<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(
+        (const float4 *)s.dev(0), (uint32_t)n, C.bmin[0], C.bmin[1], C.bmin[2], C.binv[0], C.binv[1], C.binv[2],
+        (float *)s.dev(1));
+    return s.finish();
+}
+
+int pt_cache_infer_batch(pt_ctx *ctx, const float *features, size_t n, float *out, uint32_t loc) {
+    int rc = rc_check(ctx);
+    if (rc) return rc;
+    if (!features || !out) return ctx->fail(PT_E_INVALID, "null argument");
+    if (!n) return PT_OK;
+    if (n > 0x7FFFFFFFull) return ctx->fail(PT_E_INVALID, "too many queries");
+    Staging s{ctx, loc, {}};
+    s.add(features, n * kRcIn * 4, false);
+    s.add(out, n * 12, true);
+    if ((rc = s.setup())) return rc;
+    RcInferArgs a{};
+    a.net = rc_net(ctx, ctx->cache.imgInfer);
+    a.feat.feat = (const float *)s.dev(0);
+    a.feat.n = (uint32_t)n;
+    a.out = (float *)s.dev(1);
+    k_rc_infer<0><<<rc_grid(ctx, (uint32_t)n, 3), kRcThreads, kInferSmem, ctx->stream>>>(a);
+    if ((rc = s.finish())) return rc;
+    return rc_device_error(ctx);
+}
+
+static int rc_train_impl(pt_ctx *ctx, const float *features, const float *targets, size_t n, float *grad,
+                         float *loss, uint32_t loc, bool step) {
+    int rc = rc_check(ctx);
+    if (rc) return rc;
+    if (!features || !targets) return ctx->fail(PT_E_INVALID, "null argument");
+    if (n > PT_CACHE_MAX_RECORDS) return ctx->fail(PT_E_INVALID, "too many records");
+    RadianceCache &C = ctx->cache;
+    Staging s{ctx, loc, {}};
+    s.add(features, n * kRcIn * 4, false);
+    s.add(targets, n * 12, false);
+    if ((rc = s.setup())) return rc;
+    float *lossDev = reinterpret_cast<float *>(C.ctr + 8);
+    uint32_t *nDev = C.ctr + 9;
+    uint32_t n32 = (uint32_t)n;
+    cudaMemsetAsync(lossDev, 0, 4, ctx->stream);
+    cudaMemcpyAsync(nDev, &n32, 4, cudaMemcpyHostToDevice, ctx->stream);
+    if (n) {
+        RcTrainArgs a{};
+        a.net = rc_net(ctx, C.imgTrain);
+        a.feat.feat = (const float *)s.dev(0);
+        a.feat.targ = (const float *)s.dev(1);
+        a.feat.n = n32;
+        a.grad = C.grad;
+        a.lossSum = lossDev;
+        k_rc_train<0><<<rc_grid(ctx, n32, 1), kRcThreads, kTrainSmem, ctx->stream>>>(a);
+    }
+    float lossHost = 0.0f;
+    cudaMemcpyAsync(&lossHost, lossDev, 4, cudaMemcpyDeviceToHost, ctx->stream);
+    if (step) {
+        RcAdamArgs d{C.w, C.m, C.v, C.ema, C.grad, C.imgTrain, C.imgInfer, C.ctr, nDev, PT_CACHE_MAX_RECORDS,
+                     C.params.learning_rate, C.params.ema, lossDev};
+        k_rc_adam<<<1, 1024, 0, ctx->stream>>>(d);
+    } else if (grad) {
+        cudaMemcpyAsync(grad, C.grad, kRcParams * 4, cudaMemcpyDeviceToHost, ctx->stream);
+        cudaMemsetAsync(C.grad, 0, kRcParams * 4, ctx->stream);
+    }
+    if ((rc = s.finish())) return rc;
+    if (loss) *loss = lossHost;
+    return rc_device_error(ctx);
+}
+
+int pt_cache_gradient_batch(pt_ctx *ctx, const float *features, const float *targets, size_t n, float *grad,
+                            float *loss, uint32_t loc) {
+    if (ctx && !grad) return ctx->fail(PT_E_INVALID, "null argument");
+    return rc_train_impl(ctx, features, targets, n, grad, loss, loc, false);
+}
+
+int pt_cache_train_batch(pt_ctx *ctx, const float *features, const float *targets, size_t n, float *loss,
+                         uint32_t loc) {
+    return rc_train_impl(ctx, features, targets, n, nullptr, loss, loc, true);
+}
+
+int pt_cache_get_stats(pt_ctx *ctx, pt_cache_stats *out) {
+    int rc = rc_check(ctx);
+    if (rc) return rc;
+    if (!out) return ctx->fail(PT_E_INVALID, "null argument");
+    uint32_t c[16];
+    cudaStreamSynchronize(ctx->stream);
+    if (cudaMemcpy(c, ctx->cache.ctr, sizeof(c), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return ctx->fail(PT_E_CUDA, "cache counters");
+    out->steps = c[0];
+    out->last_records = c[4];
+    memcpy(&out->last_loss, &c[3], 4);
+    out->queries = c[5];
+    return PT_OK;
+}
+
+}  // extern "C"

@@ -98,6 +98,27 @@ struct RenderGraph {
     uint64_t launches = 0;
 };
 
+// Radiance cache state (pt_cache.cu): FP32 master weights, Adam moments,
+// the inference average, the BF16 images the kernels copy into shared
+// memory, and the per-render query / training-record buffers.
+struct RadianceCache {
+    bool ready = false;
+    pt_cache_params params{};
+    float bmin[3] = {0, 0, 0}, binv[3] = {1, 1, 1};
+    bool boundsFromScene = true;
+    float *w = nullptr, *m = nullptr, *v = nullptr, *ema = nullptr, *grad = nullptr;
+    uint8_t *imgTrain = nullptr, *imgInfer = nullptr;
+    // counters: [0] Adam steps, [1] queries of the wave, [2] records of the
+    // call, [3] loss sum (float bits), [4] records of the last step, [5]
+    // queries of the call, [6] first record not yet given a target
+    uint32_t *ctr = nullptr;
+    size_t queryCap = 0;
+    float4 *q[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // record float4 x 4, weight
+    size_t recCap = 0;
+    float4 *rec[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // x 4, beta+slot, Lo, target
+    uint64_t gen = 1;  // bumped when buffers move
+};
+
 struct pt_ctx {
     int device = 0;
     int numSMs = 148;
@@ -118,6 +139,8 @@ struct pt_ctx {
     WaveBuffers W;
     RenderGraph graph;
     uint64_t sceneGen = 1, waveGen = 1;  // bumped when scene / wave buffers are replaced
+    float sceneMin[3] = {0, 0, 0}, sceneMax[3] = {1, 1, 1};  // vertex bounds of the uploaded scene
+    RadianceCache cache;
     // scratch of the batch entry points
     void *scratch = nullptr;
     size_t scratchBytes = 0;
@@ -144,10 +167,75 @@ struct pt_ctx {
     }
 };
 
+// Device scratch for host-memory batch calls: grows, never shrinks.
+inline int scratch(pt_ctx *ctx, size_t bytes, char **out) {
+    if (ctx->scratchBytes < bytes) {
+        if (ctx->scratch) cudaFree(ctx->scratch);
+        ctx->scratch = nullptr;
+        ctx->scratchBytes = 0;
+        cudaError_t e = cudaMalloc(&ctx->scratch, bytes);
+        if (e != cudaSuccess) return ctx->fail(PT_E_NOMEM, "scratch", cudaGetErrorString(e));
+        ctx->scratchBytes = bytes;
+    }
+    *out = (char *)ctx->scratch;
+    return PT_OK;
+}
+inline size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// Stage host arrays into device scratch (location == PT_MEM_HOST) or pass
+// device pointers through.  `ins` are copied in; `outs` copied back by finish().
+struct Staging {
+    pt_ctx *ctx;
+    uint32_t loc;
+    struct Buf { const void *host; size_t bytes; void *dev; bool out; };
+    std::vector<Buf> bufs;
+    int setup() {
+        if (loc == PT_MEM_DEVICE) {
+            for (auto &b : bufs) b.dev = const_cast<void *>(b.host);
+            return PT_OK;
+        }
+        size_t tot = 0;
+        for (auto &b : bufs) tot += al256(b.bytes);
+        char *base;
+        int rc = scratch(ctx, tot + 256, &base);
+        if (rc) return rc;
+        for (auto &b : bufs) {
+            if (!b.host) { b.dev = nullptr; continue; }
+            b.dev = base;
+            base += al256(b.bytes);
+            if (!b.out) {
+                cudaError_t e = cudaMemcpyAsync(b.dev, b.host, b.bytes, cudaMemcpyHostToDevice, ctx->stream);
+                if (e != cudaSuccess) return ctx->fail(PT_E_CUDA, "staging copy", cudaGetErrorString(e));
+            }
+        }
+        return PT_OK;
+    }
+    int finish() {
+        if (loc == PT_MEM_HOST)
+            for (auto &b : bufs)
+                if (b.out && b.host) {
+                    cudaError_t e = cudaMemcpyAsync(const_cast<void *>(b.host), b.dev, b.bytes, cudaMemcpyDeviceToHost,
+                                                    ctx->stream);
+                    if (e != cudaSuccess) return ctx->fail(PT_E_CUDA, "staging copy back", cudaGetErrorString(e));
+                }
+        cudaError_t e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) return ctx->fail(PT_E_CUDA, "batch kernel", cudaGetErrorString(e));
+        return PT_OK;
+    }
+    void *add(const void *p, size_t bytes, bool out) {
+        bufs.push_back({p, bytes, nullptr, out});
+        return nullptr;
+    }
+    void *dev(size_t i) { return bufs[i].dev; }
+};
+
 // pt_bvh.cu: builds S.tri / S.nodes / S.triMesh / S.meshFirstTri and the
 // parity exports on the device from the uploaded geometry.
 int pt_build_bvh_device(pt_ctx *ctx, const uint32_t *d_meshFirstTri, uint32_t numTris);
 // pt_render.cu
 int pt_render_impl(pt_ctx *ctx, const pt_render_params *p, float *d_sum, float *d_comp, pt_stats *stats);
 int pt_wave_free(pt_ctx *ctx);
+// pt_cache.cu
+void pt_cache_free(pt_ctx *ctx);
+int pt_cache_prepare(pt_ctx *ctx, size_t queryCap);  // query buffers for a cached render
 void pt_graph_free(pt_ctx *ctx);

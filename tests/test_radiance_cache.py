@@ -1,0 +1,202 @@
+"""Radiance cache network (csrc/pt_cache.cu) against its numpy restatement
+(oracle/radiance_cache.py).
+
+CPU: the restatement's backward pass against finite differences (without
+BF16 rounding), the BF16 rounding helper, the constant-output weights, and
+the ABI record sizes.
+GPU: encoding, inference, the summed gradient and one Adam step against the
+restatement; training reduces the loss on a smooth target; the constant-output
+weights give the constant exactly.  Tolerances: the kernels accumulate in
+FP32 in the tensor cores' order and the restatement sums exactly, so a
+BF16-rounded activation can land one BF16 step (2^-8 relative) apart.
+"""
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle import radiance_cache as rc
+
+
+def random_weights(seed):
+    rng = np.random.default_rng(seed)
+    w = np.zeros(rc.PARAMS, np.float32)
+    o = 0
+    for l in range(rc.LAYERS):
+        n = rc.rows(l) * rc.IN
+        lim = np.sqrt(6.0 / rc.IN) if l < 5 else 0.3
+        w[o:o + n] = rng.uniform(-lim, lim, n)
+        o += n
+    return w
+
+
+def random_features(n, seed):
+    rng = np.random.default_rng(seed)
+    f = rng.uniform(-1.0, 1.0, (n, rc.IN)).astype(np.float32)
+    f[:, 49] = 1.0
+    f[:, 50:] = 0.0
+    return f
+
+
+def random_records(n, seed):
+    rng = np.random.default_rng(seed)
+    r = np.zeros((n, 16), np.float32)
+    r[:, 0:3] = rng.uniform(-3, 5, (n, 3))
+    r[:, 3] = rng.uniform(0, 1, n)
+    d = rng.normal(size=(n, 3))
+    r[:, 4:7] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    nn = rng.normal(size=(n, 3))
+    r[:, 8:11] = nn / np.linalg.norm(nn, axis=1, keepdims=True)
+    r[:, 12:15] = rng.uniform(0, 1, (n, 3))
+    return r
+
+
+# ---------------------------------------------------------------------------- CPU
+def test_bf16_rounding():
+    x = np.array([1.0, 1.0 + 2 ** -8, 1.0 + 2 ** -7 + 2 ** -9, -3.5, 1e-30, np.inf], np.float32)
+    y = rc.bf16(x)
+    assert y[0] == 1.0 and y[1] == 1.0  # tie -> even
+    assert y[2] == 1.0 + 2 ** -7  # below half way
+    assert y[3] == -3.5 and np.isinf(y[5])
+
+
+def test_restated_backward_matches_finite_differences(monkeypatch):
+    """Without BF16 rounding, the restated gradient is the derivative of the
+    loss with its denominator held constant."""
+    monkeypatch.setattr(rc, "bf16", lambda x: np.asarray(x, np.float64))
+    monkeypatch.setattr(rc, "fp32", lambda x: np.asarray(x, np.float64))
+    w = random_weights(1).astype(np.float64)
+    f = random_features(7, 2)
+    t = np.random.default_rng(3).uniform(0, 2, (7, 3))
+    g, _ = rc.gradient(w, f, t)
+    _, y0 = rc.forward(w, f)
+    den = y0[:, :3] ** 2 + 0.01
+
+    def loss(wv):
+        _, y = rc.forward(wv, f)
+        return float(np.sum((y[:, :3] - t) ** 2 / den))
+
+    rng = np.random.default_rng(4)
+    for i in rng.choice(rc.PARAMS, 40, replace=False):
+        e = np.zeros_like(w)
+        e[i] = 1e-6
+        fd = (loss(w + e) - loss(w - e)) / 2e-6
+        assert abs(fd - g[i]) <= 1e-4 * max(1.0, abs(fd)), (i, fd, g[i])
+
+
+def test_constant_weights_in_restatement():
+    w = rc.constant_weights([0.5, 0.25, 0.125])
+    y = rc.infer(w, random_features(50, 5))
+    assert np.array_equal(y, np.tile([0.5, 0.25, 0.125], (50, 1)))
+
+
+def test_cache_abi_sizes(pt):
+    assert C.sizeof(pt.pt_cache_params) == 52
+    assert C.sizeof(pt.pt_cache_stats) == 24
+    assert pt.PT_CACHE_PARAMS == rc.PARAMS
+
+
+# ---------------------------------------------------------------------------- GPU
+@pytest.fixture()
+def cctx(pt, ctx):
+    ctx.cache_init(pt.cache_params(seed=1, bbox=((-3, -3, -3), (5, 5, 5))))
+    yield ctx
+    ctx.cache_release()
+
+
+@pytest.mark.gpu
+def test_encode_parity(pt, cctx):
+    r = random_records(5000, 6)
+    g = cctx.cache_encode(r)
+    o = rc.encode(r, (-3, -3, -3), (5, 5, 5))
+    assert np.abs(g - o).max() < 2e-5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 127, 128, 1000, 70000])
+def test_infer_parity(pt, cctx, n):
+    w = random_weights(10 + n % 7)
+    cctx.cache_weights(w)
+    f = random_features(n, n)
+    g = cctx.cache_infer(f)
+    o = rc.infer(w, f)
+    err = np.abs(g - o)
+    scale = np.abs(o).mean() + 1e-3
+    assert np.isfinite(g).all()
+    assert err.max() <= 5e-2 * scale + 2e-2 * np.abs(o).max(), (err.max(), scale)
+    assert np.quantile(err / (np.abs(o) + scale), 0.99) < 1e-2
+
+
+@pytest.mark.gpu
+def test_constant_weights_exact_gpu(pt, cctx):
+    cctx.cache_weights(rc.constant_weights([0.5, 0.25, 0.125]))
+    y = cctx.cache_infer(random_features(3000, 8))
+    assert np.array_equal(y, np.tile(np.float32([0.5, 0.25, 0.125]), (3000, 1)))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [100, 128, 5000, 65536])
+def test_gradient_parity(pt, cctx, n):
+    w = random_weights(20)
+    cctx.cache_weights(w)
+    f = random_features(n, 30 + n)
+    t = np.random.default_rng(n).uniform(0.0, 2.0, (n, 3)).astype(np.float32)
+    g, loss = cctx.cache_gradient(f, t)
+    go, lo = rc.gradient(w, f, t)
+    assert abs(loss - lo) <= 1e-2 * abs(lo)
+    o = 0
+    for l in range(rc.LAYERS):
+        k = rc.rows(l) * rc.IN
+        a, b = g[o:o + k], go[o:o + k]
+        if l == rc.LAYERS - 1:  # rows 3..15 receive no gradient
+            a, b = a.reshape(16, 64)[:3], b.reshape(16, 64)[:3]
+            assert not g[o + 3 * 64:o + k].any()
+        rel = np.linalg.norm(a - b) / (np.linalg.norm(b) + 1e-12)
+        assert rel < 2e-2, (l, rel)
+        o += k
+
+
+@pytest.mark.gpu
+def test_adam_step_parity(pt, cctx):
+    w = random_weights(40)
+    cctx.cache_weights(w)
+    n = 4096
+    f = random_features(n, 41)
+    t = np.random.default_rng(42).uniform(0.0, 2.0, (n, 3)).astype(np.float32)
+    # the step's gradient, as the kernels compute it, then the step itself
+    g, _ = cctx.cache_gradient(f, t)
+    cctx.cache_weights(w)
+    cctx.cache_train(f, t)
+    w1 = cctx.cache_weights()
+    lr = 5e-3
+    wo, _, _ = rc.adam(w, np.zeros_like(w), np.zeros_like(w), g, n, 1, lr)
+    assert np.abs(w1 - wo).max() <= 1e-6 + 1e-5 * np.abs(wo).max()
+    st = cctx.cache_stats()
+    assert st.steps == 1 and st.last_records == n
+
+
+@pytest.mark.gpu
+def test_training_reduces_loss(pt, ctx):
+    """A smooth radiance-like function of position and normal, learned in
+    300 steps of 8192 records: the relative L2 loss falls by 10x."""
+    ctx.cache_init(pt.cache_params(seed=2, learning_rate=1e-2, bbox=((-3, -3, -3), (5, 5, 5))))
+    try:
+        rng = np.random.default_rng(9)
+
+        def batch(n):
+            r = random_records(n, int(rng.integers(1 << 30)))
+            p = (r[:, 0:3] + 3) / 8
+            t = np.stack([1 + np.sin(3 * p[:, 0]) * r[:, 9], 0.5 + p[:, 1] * r[:, 12], 0.2 + p[:, 2] ** 2], 1)
+            return ctx.cache_encode(r), np.maximum(t, 0).astype(np.float32)
+
+        fv, tv = batch(8192)
+        first = ctx.cache_train(fv, tv) / (3 * 8192)
+        for _ in range(300):
+            ctx.cache_train(*batch(8192))
+        ctx.cache_weights(ctx.cache_weights())  # inference copy = current weights
+        y = ctx.cache_infer(fv)
+        last = float(np.mean((y - tv) ** 2 / (y ** 2 + 0.01)))
+        assert last < first / 10, (first, last)
+    finally:
+        ctx.cache_release()
