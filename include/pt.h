@@ -225,6 +225,7 @@ typedef struct pt_stats {
     float ms_shade;    /* surface / medium / light events */
     float ms_shadow;   /* any-hit traversal */
     float ms_film;     /* film accumulation */
+    float ms_cache;    /* radiance-cache inference, training targets, training step */
 } pt_stats;
 
 typedef struct pt_ctx pt_ctx;

@@ -77,6 +77,8 @@ class Oracle:
         L.or_trace_shadow.argtypes = [P, F, S, U, F]
         L.or_render.argtypes = [P, C.POINTER(pt.pt_render_params), F, F, C.c_int, C.POINTER(C.c_uint64)]
         L.or_render.restype = C.c_int
+        L.or_render_cached.argtypes = [P, C.POINTER(pt.pt_render_params), F, F, C.c_int, F, C.c_float]
+        L.or_render_cached.restype = C.c_int
         self.L = L
         self.h = None
         self.scene = None
@@ -179,6 +181,17 @@ class Oracle:
         if rc != 0:
             raise RuntimeError("oracle: unsupported scene")
         return s, pp, (cnt[0], cnt[1])
+
+    def render_cached(self, params, value, rough_threshold=0.3, per_path=False, threads=0):
+        """Render with paths ended into a constant radiance cache."""
+        W, H = params.width, params.height
+        s = np.zeros((H, W, 4), np.float32)
+        pp = np.zeros((params.spp, H, W, 3), np.float32) if per_path else None
+        v = np.asarray(value, np.float32)
+        rc = self.L.or_render_cached(self.h, C.byref(params), _f(s), _f(pp), threads, _f(v), rough_threshold)
+        if rc != 0:
+            raise RuntimeError("oracle: unsupported scene")
+        return s, pp
 
 
 class Reference:

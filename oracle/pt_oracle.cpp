@@ -1721,7 +1721,13 @@ static inline void draw(Rng &rng, float *u, int k) { for (int i = 0; i < k; i++)
 // The path (shaders/Shaders.hlsl:25-651, RayGen), one camera sample.
 // ---------------------------------------------------------------------------
 struct PathStats { uint64_t ext = 0, shadow = 0; };
-static F3 trace_path(const Ctx &c, const pt_render_params &P, uint32_t px, uint32_t py, uint32_t frame, PathStats *st) {
+// Radiance-cache termination with a cache that returns the constant `value`
+// (the library's rule: a path ends at the first non-emitting surface vertex
+// reached by a rough bounce and adds throughput x cache there).  Used to
+// check the library's termination logic independently of its network.
+struct CacheConst { float value[3]; float roughThr; };
+static F3 trace_path(const Ctx &c, const pt_render_params &P, uint32_t px, uint32_t py, uint32_t frame, PathStats *st,
+                     const CacheConst *cc = nullptr) {
     const Scene &s = *c.s;
     const pt_camera &cam = P.camera;
     Rng rng = init_rng(px, py, P.width, P.height, frame, P.rng_kind);
@@ -1750,6 +1756,7 @@ static F3 trace_path(const Ctx &c, const pt_render_params &P, uint32_t px, uint3
     }
     F3 Lo(0.0f), thr(1.0f);
     float lastPdf = 0.0f, eta = 1.0f;
+    bool rough = false;  // the last bounce was rough (radiance-cache termination)
     const uint32_t aseed = s.hasAlpha ? alpha_seed(rng.pixelSeed, rng.sampleIndex) : 0u;
     for (int bounce = 0; bounce < (int)P.max_depth; bounce++) {
         Hit hit = trace_closest(s, ro, rd, tmin, tmax, aseed, alpha_key((uint32_t)bounce, 0u));
@@ -1775,6 +1782,7 @@ static F3 trace_path(const Ctx &c, const pt_render_params &P, uint32_t px, uint3
                 F3 nd = sample_hg(rd, v.phase_g, x1, x2, pp);
                 ro = spos; rd = nd; tmin = 0.0f; tmax = 1e20f;
                 lastPdf = std::max(pp, 1e-20f);
+                rough = true;
             }
         }
         if (volScat) {
@@ -1806,6 +1814,10 @@ static F3 trace_path(const Ctx &c, const pt_render_params &P, uint32_t px, uint3
                     float pe = emitter_pdf_sa(s, pm, hp, ro, N);
                     Lo += thr * rad * balance_heuristic(lastPdf, pe);
                 }
+                break;
+            }
+            if (cc && rough) {
+                Lo += thr * F3(cc->value[0], cc->value[1], cc->value[2]);
                 break;
             }
             F3 T, B;
@@ -1851,6 +1863,7 @@ static F3 trace_path(const Ctx &c, const pt_render_params &P, uint32_t px, uint3
                 F3 rf = reflect(rd, N);
                 ro = hp + Ng * 0.001f; rd = rf; tmin = 0.0f; tmax = 1e20f;
                 lastPdf = 0.0f;
+                rough = false;
             } else if (pm.type == PT_MAT_DIELECTRIC) {  // Shaders.hlsl:429-472
                 F3 I = rd, Nf = N;
                 float etaI, etaT;
@@ -1871,6 +1884,7 @@ static F3 trace_path(const Ctx &c, const pt_render_params &P, uint32_t px, uint3
                 ro = hp + on * 0.001f; rd = nd; tmin = 0.0f; tmax = 1e20f;
                 lastPdf = 0.0f;
                 if (refr) eta *= etaI / etaT;
+                rough = false;
             } else if (pm.type == PT_MAT_DIFFUSE || pm.type == PT_MAT_MICROFACET || pm.type == PT_MAT_DISNEY ||
                        pm.type == PT_MAT_HAIR) {  // Shaders.hlsl:473-511
                 Lo += thr * mis_direct(c, hp, N, Ng, T, B, wil, m, h, rng, aseed, (uint32_t)bounce);
@@ -1892,6 +1906,10 @@ static F3 trace_path(const Ctx &c, const pt_render_params &P, uint32_t px, uint3
                 ro = offset_ray_origin(hp, on, on); rd = ww; tmin = 0.0f; tmax = 1e20f;
                 thr *= wt;
                 lastPdf = std::max(bp, 1e-20f);
+                if (cc)
+                    rough = pm.type == PT_MAT_DIFFUSE || pm.type == PT_MAT_HAIR ||
+                            (pm.type == PT_MAT_MICROFACET && pm.alpha >= cc->roughThr) ||
+                            (pm.type == PT_MAT_DISNEY && pm.roughness >= cc->roughThr);
             } else {
                 break;  // subsurface (type 6) is not part of this path
             }
@@ -2152,7 +2170,20 @@ void or_trace_shadow(void *sp, const float *rays, size_t n, uint32_t *occ, float
 // reference's accumulation order (per pixel, frame by frame, float32).
 // per_path (optional): W*H*spp*3 floats, Lo of every path (frame-major).
 // threads <= 0: all hardware threads.  Returns 0 or -1 (unsupported scene).
+static int render_impl(void *sp, const pt_render_params *P, float *sum, float *per_path, int threads,
+                       uint64_t *counters, const CacheConst *cc);
 int or_render(void *sp, const pt_render_params *P, float *sum, float *per_path, int threads, uint64_t *counters) {
+    return render_impl(sp, P, sum, per_path, threads, counters, nullptr);
+}
+// or_render with radiance-cache termination into a constant cache (value: 3
+// floats, rough_threshold as the library's pt_cache_params field).
+int or_render_cached(void *sp, const pt_render_params *P, float *sum, float *per_path, int threads,
+                     const float *value, float rough_threshold) {
+    CacheConst cc{{value[0], value[1], value[2]}, rough_threshold};
+    return render_impl(sp, P, sum, per_path, threads, nullptr, &cc);
+}
+static int render_impl(void *sp, const pt_render_params *P, float *sum, float *per_path, int threads,
+                       uint64_t *counters, const CacheConst *cc) {
     Scene *s = static_cast<Scene *>(sp);
     for (auto &m : s->mats)
         if (m.type == PT_MAT_SUBSURFACE) { s->err = "subsurface"; return -1; }
@@ -2173,7 +2204,7 @@ int or_render(void *sp, const pt_render_params *P, float *sum, float *per_path, 
                 for (uint32_t x = x0; x < std::min(W, x0 + TS); x++) {
                     float *acc = &sum[4 * ((size_t)y * W + x)];
                     for (uint32_t k = 0; k < P->spp; k++) {
-                        F3 L = trace_path(c, *P, x, y, P->sample_offset + k, counters ? &ps : nullptr);
+                        F3 L = trace_path(c, *P, x, y, P->sample_offset + k, counters ? &ps : nullptr, cc);
                         acc[0] = acc[0] + L.x; acc[1] = acc[1] + L.y; acc[2] = acc[2] + L.z; acc[3] = acc[3] + 1.0f;
                         if (per_path) {
                             float *pp = &per_path[3 * ((size_t)k * W * H + (size_t)y * W + x)];

@@ -479,6 +479,21 @@ int pt_upload_scene(pt_ctx *ctx, const pt_scene_desc *d) {
     DevScene &S = ctx->S;
     S.sobol1 = ctx->d_sobol1;
     const size_t nv = d->num_vertices;
+    {  // vertex bounds (the radiance cache's default position box)
+        float lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
+        if (nv) {
+            for (int k = 0; k < 3; k++) lo[k] = hi[k] = d->positions[k];
+            for (size_t v = 1; v < nv; v++)
+                for (int k = 0; k < 3; k++) {
+                    lo[k] = std::min(lo[k], d->positions[3 * v + k]);
+                    hi[k] = std::max(hi[k], d->positions[3 * v + k]);
+                }
+        }
+        for (int k = 0; k < 3; k++) {
+            ctx->sceneMin[k] = lo[k];
+            ctx->sceneMax[k] = hi[k];
+        }
+    }
     float *dpos, *dnrm, *duv, *dtan, *dcdf;
     uint32_t *didx, *dmft, *demit;
     pt_material *dmats;

@@ -32,7 +32,7 @@ constexpr uint32_t kGradBytes = 2 * kTileBytes;       // dZ tiles carry a zero u
 constexpr uint32_t kInferSmem = kRcImageBytes + kTileBytes + 64;
 constexpr uint32_t kTrainSmem = kRcImageBytes + 6 * kTileBytes + 2 * kGradBytes + 64;
 static_assert(kTrainSmem <= 227 * 1024, "training kernel shared memory");
-constexpr uint32_t kDevErrCache = 8u;  // device error bit: a cache kernel's wait timed out
+constexpr uint32_t kDevErrCache = PT_DEVERR_CACHE;
 
 struct RcNet {
     const uint8_t *img;  // BF16 weight image
@@ -200,9 +200,10 @@ __global__ void __launch_bounds__(kRcThreads) k_rc_infer(RcInferArgs a) {
                     } else {
                         uint32_t slot = __float_as_uint(a.qry.r1[row].w);
                         float4 w = a.qw[row], le = a.lo_eta[slot];
-                        le.x += w.x * fmaxf(v[0], 0.0f);
-                        le.y += w.y * fmaxf(v[1], 0.0f);
-                        le.z += w.z * fmaxf(v[2], 0.0f);
+                        // Lo += throughput * cache, rounded as two operations (no FMA)
+                        le.x = __fadd_rn(le.x, __fmul_rn(w.x, fmaxf(v[0], 0.0f)));
+                        le.y = __fadd_rn(le.y, __fmul_rn(w.y, fmaxf(v[1], 0.0f)));
+                        le.z = __fadd_rn(le.z, __fmul_rn(w.z, fmaxf(v[2], 0.0f)));
                         a.lo_eta[slot] = le;
                     }
                 }
@@ -423,6 +424,43 @@ __global__ void k_rc_images(const float *w, uint8_t *imgTrain, uint8_t *imgInfer
     }
 }
 
+// Training targets of the records written in this wave: the radiance the
+// path gathered after its record vertex, divided by the throughput there.
+// One CTA; records [ctr[6], count) belong to the wave that just ended.
+__global__ void __launch_bounds__(1024) k_rc_targets(RcRows<1> rec, float4 *beta, float4 *lo0, float4 *tgt,
+                                                    uint32_t *ctr, const float4 *lo_eta, const uint4 *rng,
+                                                    const float4 *pendA, const float4 *pendE) {
+    __shared__ uint32_t s0, s1;
+    if (threadIdx.x == 0) {
+        s0 = ctr[6];
+        s1 = rec.count();
+    }
+    __syncthreads();
+    for (uint32_t r = s0 + threadIdx.x; r < s1; r += blockDim.x) {
+        uint32_t slot = __float_as_uint(rec.r1[r].w);
+        float4 le = lo_eta[slot];
+        float L[3] = {le.x, le.y, le.z};
+        if (rng[slot].w & 1u) {  // NEE of the last bounce, folded in as the film does
+            float4 pa = pendA[slot], pe = pendE[slot];
+            L[0] += pa.x; L[1] += pa.y; L[2] += pa.z;
+            L[0] += pe.x; L[1] += pe.y; L[2] += pe.z;
+        }
+        float4 b = beta[r], l0 = lo0[r];
+        const float bb[3] = {b.x, b.y, b.z}, ll[3] = {l0.x, l0.y, l0.z};
+        float o[3];
+        for (int k = 0; k < 3; k++) {
+            float x = bb[k] > 1e-8f ? (L[k] - ll[k]) / bb[k] : 0.0f;
+            o[k] = isfinite(x) ? fmaxf(x, 0.0f) : 0.0f;
+        }
+        tgt[r] = make_float4(o[0], o[1], o[2], 0.0f);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ctr[6] = s1;
+        ctr[5] += ctr[1];
+    }
+}
+
 __global__ void k_rc_encode(const float4 *rec, uint32_t n, float bx, float by, float bz, float ix, float iy, float iz,
                             float *feat) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -496,6 +534,49 @@ unsigned rc_grid(const pt_ctx *ctx, uint32_t n, unsigned perSM) {
     return std::max(1u, std::min(tiles, (unsigned)ctx->numSMs * perSM));
 }
 }  // namespace
+
+// ---- launches of a cached render (stream-ordered, capturable) ------------------
+cudaError_t rc_enqueue_resolve(pt_ctx *ctx, cudaStream_t st, float4 *lo_eta) {
+    const RadianceCache &C = ctx->cache;
+    RcInferArgs a{};
+    a.net = rc_net(ctx, C.imgInfer);
+    a.qry.r0 = C.q[0]; a.qry.r1 = C.q[1]; a.qry.r2 = C.q[2]; a.qry.r3 = C.q[3];
+    a.qry.cnt = C.ctr + 1;
+    a.qry.cap = (uint32_t)C.queryCap;
+    a.qw = C.q[4];
+    a.lo_eta = lo_eta;
+    k_rc_infer<1><<<ctx->numSMs * 3, kRcThreads, kInferSmem, st>>>(a);
+    return cudaGetLastError();
+}
+cudaError_t rc_enqueue_targets(pt_ctx *ctx, cudaStream_t st, const float4 *lo_eta, const uint4 *rng,
+                               const float4 *pendA, const float4 *pendE) {
+    const RadianceCache &C = ctx->cache;
+    RcRows<1> rec{C.rec[0], C.rec[1], C.rec[2], C.rec[3], C.rec[6], C.ctr + 2, (uint32_t)C.recCap};
+    k_rc_targets<<<1, 1024, 0, st>>>(rec, C.rec[4], C.rec[5], C.rec[6], C.ctr, lo_eta, rng, pendA, pendE);
+    return cudaGetLastError();
+}
+cudaError_t rc_enqueue_train(pt_ctx *ctx, cudaStream_t st) {
+    RadianceCache &C = ctx->cache;
+    float *lossDev = reinterpret_cast<float *>(C.ctr + 8);
+    cudaError_t e = cudaMemsetAsync(lossDev, 0, 4, st);
+    if (e != cudaSuccess) return e;
+    RcTrainArgs a{};
+    a.net = rc_net(ctx, C.imgTrain);
+    a.rec = RcRows<1>{C.rec[0], C.rec[1], C.rec[2], C.rec[3], C.rec[6], C.ctr + 2, (uint32_t)C.recCap};
+    a.grad = C.grad;
+    a.lossSum = lossDev;
+    k_rc_train<1><<<ctx->numSMs, kRcThreads, kTrainSmem, st>>>(a);
+    RcAdamArgs d{C.w, C.m, C.v, C.ema, C.grad, C.imgTrain, C.imgInfer, C.ctr, C.ctr + 2, (uint32_t)C.recCap,
+                 C.params.learning_rate, C.params.ema, lossDev};
+    k_rc_adam<<<1, 1024, 0, st>>>(d);
+    return cudaGetLastError();
+}
+int rc_render_setup(pt_ctx *ctx, size_t waveCap) {
+    int rc = rc_check(ctx);
+    if (rc) return rc;
+    rc_bounds(ctx);
+    return pt_cache_prepare(ctx, waveCap);
+}
 
 void pt_cache_free(pt_ctx *ctx) {
     RadianceCache &C = ctx->cache;

@@ -19,6 +19,7 @@ enum : uint32_t {
     PT_DEVERR_STACK = 1u,     // traversal stack overflow
     PT_DEVERR_QUEUE = 2u,     // queue overflow
     PT_DEVERR_BVH = 4u,       // traversal visited more nodes than exist
+    PT_DEVERR_CACHE = 8u,     // a radiance-cache kernel's bounded wait gave up
 };
 
 // Shading classes: the closest-hit kernel sorts each path into one of these
@@ -95,6 +96,8 @@ struct RenderGraph {
     size_t cap = 0;
     const void *sum = nullptr, *comp = nullptr;
     uint64_t sceneGen = 0, waveGen = 0;
+    uint32_t cached = 0, trainStride = 0;  // radiance-cache configuration baked into the launches
+    uint64_t cacheGen = 0;
     uint64_t launches = 0;
 };
 
@@ -238,4 +241,9 @@ int pt_wave_free(pt_ctx *ctx);
 // pt_cache.cu
 void pt_cache_free(pt_ctx *ctx);
 int pt_cache_prepare(pt_ctx *ctx, size_t queryCap);  // query buffers for a cached render
+int rc_render_setup(pt_ctx *ctx, size_t waveCap);     // checks, bounds, query buffers
+cudaError_t rc_enqueue_resolve(pt_ctx *ctx, cudaStream_t st, float4 *lo_eta);
+cudaError_t rc_enqueue_targets(pt_ctx *ctx, cudaStream_t st, const float4 *lo_eta, const uint4 *rng,
+                               const float4 *pendA, const float4 *pendE);
+cudaError_t rc_enqueue_train(pt_ctx *ctx, cudaStream_t st);
 void pt_graph_free(pt_ctx *ctx);

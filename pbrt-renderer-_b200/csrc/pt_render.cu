@@ -30,6 +30,11 @@
 namespace pt {
 
 constexpr uint32_t kFlagPending = 1u;
+// radiance-cache path flags (rng.w); the record index of a training path sits above bit 8
+constexpr uint32_t kFlagRough = 2u;     // the last bounce scattered off a rough surface or a medium
+constexpr uint32_t kFlagTrain = 4u;     // training path
+constexpr uint32_t kFlagUnbiased = 8u;  // training path whose suffix does not use the cache
+constexpr uint32_t kFlagHasRec = 16u;   // its training record has been written
 constexpr int kBlock = 256;
 
 struct WaveArgs {
@@ -53,6 +58,13 @@ struct WaveArgs {
     unsigned long long *rayTotals;  // [0] extension, [1] shadow
     uint32_t *err;
     uint32_t shadowCap;
+    // radiance cache (cacheOn == 0: plain path tracing)
+    uint32_t cacheOn, trainStride, unbiasedEvery, recCap;
+    float roughThr;
+    float4 *cq[5];      // queries: 4 record float4 + throughput weight
+    uint32_t *cqCount;
+    float4 *cr[7];      // training records: 4 record float4, throughput, Lo so far, target
+    uint32_t *crCount;
 };
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
@@ -136,7 +148,15 @@ __global__ void k_raygen(WaveArgs A) {
     A.qdOut[slot] = make_float4(rd.x, rd.y, rd.z, 1e20f);
     A.thr_pdf[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
     A.lo_eta[slot] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
-    A.rng[slot] = make_uint4(r.dim, r.white, 0u, 0u);
+    uint32_t flags = 0u;
+    if (A.cacheOn && A.trainStride) {  // about one path in trainStride trains the cache
+        uint64_t k = A.waveStart + slot + pcg_hash(__ldg(A.sampleOffset)) % A.trainStride;
+        if (k % A.trainStride == 0) {
+            flags |= kFlagTrain;
+            if (A.unbiasedEvery && (k / A.trainStride) % A.unbiasedEvery == 0) flags |= kFlagUnbiased;
+        }
+    }
+    A.rng[slot] = make_uint4(r.dim, r.white, 0u, flags);
     if (slot == 0) *A.cntOut = A.waveCount;
 }
 
@@ -412,6 +432,23 @@ __device__ __forceinline__ void apply_textures(const DevScene &S, pt_material &m
         m.subsurface = tex_sample(S, m.subsurfaceTexIndex, uv.x, uv.y, tex_lod(S, m.subsurfaceTexIndex, foot)).x;
 }
 
+// Radiance-cache record of a surface vertex: position + roughness input,
+// direction toward the previous vertex + path slot, shading normal, albedo.
+__device__ __forceinline__ void cache_record(float4 *const *buf, uint32_t i, float3 p, float3 wo, float3 n,
+                                             const pt_material &m, uint32_t type, uint32_t slot) {
+    float rough = type == PT_MAT_MICROFACET ? m.alpha : type == PT_MAT_DISNEY ? m.roughness
+                  : (type == PT_MAT_MIRROR || type == PT_MAT_DIELECTRIC) ? 0.0f : 1.0f;
+    buf[0][i] = make_float4(p.x, p.y, p.z, rough);
+    buf[1][i] = make_float4(wo.x, wo.y, wo.z, __uint_as_float(slot));
+    buf[2][i] = make_float4(n.x, n.y, n.z, 0.0f);
+    buf[3][i] = make_float4(m.albedo[0], m.albedo[1], m.albedo[2], 0.0f);
+}
+// A BSDF-sampled bounce that ends the path into the cache at its next vertex.
+__device__ __forceinline__ bool rough_bounce(const WaveArgs &A, uint32_t type, const pt_material &m) {
+    return type == PT_MAT_DIFFUSE || type == PT_MAT_HAIR || (type == PT_MAT_MICROFACET && m.alpha >= A.roughThr) ||
+           (type == PT_MAT_DISNEY && m.roughness >= A.roughThr);
+}
+
 // CLS + CLS_TEX: the kernel of class CLS for materials with shading textures.
 template <bool INLINE, int CLS>
 __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveArgs A) {
@@ -478,6 +515,7 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
                     ntmin = 0.0f;
                     lastPdf = mx(pp, 1e-20f);
                     cont = true;
+                    st.w |= kFlagRough;
                 }
             }
             if (volScat) {
@@ -504,11 +542,36 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
                 if (dot(N, Ng) < 0.0f) N = -N;
                 if (TEX || (C == CLS_ANY && has_shading_textures(m)))
                     apply_textures(S, m, mesh, prim, h4.x, i0, i1, i2, bx, by, N, A.width, A.height);
+                // Radiance cache: the first surface vertex after a rough bounce ends
+                // the path (a query, resolved after the wave) or, on a training
+                // path, records its state and the path goes on.
+                bool cacheStop = false;
+                if (A.cacheOn && (st.w & kFlagRough) && !(C == CLS_EMIT || (C == CLS_ANY && m.isEmitter))) {
+                    const bool train = (st.w & kFlagTrain) != 0;
+                    if (train && !(st.w & kFlagHasRec)) {
+                        uint32_t r = warp_append(A.crCount, true);
+                        if (r < A.recCap) {
+                            cache_record(A.cr, r, hp, -rd, N, m, type, slot);
+                            A.cr[4][r] = make_float4(thr.x, thr.y, thr.z, 0.0f);
+                            A.cr[5][r] = make_float4(Lo.x, Lo.y, Lo.z, 0.0f);
+                            st.w |= kFlagHasRec | (r << 8);
+                        }
+                    } else if (!(train && (st.w & kFlagUnbiased))) {
+                        uint32_t q = warp_append(A.cqCount, true);
+                        if (q < A.clsStride) {
+                            cache_record(A.cq, q, hp, -rd, N, m, type, slot);
+                            A.cq[4][q] = make_float4(thr.x, thr.y, thr.z, 0.0f);
+                        } else {
+                            atomicOr(A.err, (uint32_t)PT_DEVERR_QUEUE);
+                        }
+                        cacheStop = true;
+                    }
+                }
                 if (C == CLS_EMIT || (C == CLS_ANY && m.isEmitter)) {  // Shaders.hlsl:317-335
                     float3 rad = make_float3(m.radiance[0], m.radiance[1], m.radiance[2]);
                     if (lastPdf == 0.0f) Lo += thr * rad;
                     else Lo += thr * rad * balance(lastPdf, emitter_pdf_sa(S, m, hp, ro, N));
-                } else if (C != CLS_EMIT) {
+                } else if (C != CLS_EMIT && !cacheStop) {
                     float3 T, B;
                     float h = 0.0f;
                     if (type == PT_MAT_HAIR) {  // Shaders.hlsl:340-387
@@ -549,6 +612,7 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
                         no = hp + Ng * 0.001f;
                         lastPdf = 0.0f;
                         cont = true;
+                        st.w &= ~kFlagRough;
                     } else if (type == PT_MAT_DIELECTRIC) {  // Shaders.hlsl:429-472
                         float etaI = back ? m.intIOR : m.extIOR, etaT = back ? m.extIOR : m.intIOR;
                         float Fr = fresnel(dot(-rd, N), etaI, etaT);
@@ -563,6 +627,7 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
                         lastPdf = 0.0f;
                         if (refr) eta *= etaI / etaT;
                         cont = true;
+                        st.w &= ~kFlagRough;
                     } else if (C != CLS_DELTA &&
                                (type == PT_MAT_DIFFUSE || type == PT_MAT_MICROFACET || type == PT_MAT_DISNEY ||
                                 type == PT_MAT_HAIR)) {  // Shaders.hlsl:473-511
@@ -591,6 +656,7 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
                             thr *= wt;
                             lastPdf = mx(bp, 1e-20f);
                             cont = true;
+                            if (A.cacheOn) st.w = rough_bounce(A, type, m) ? (st.w | kFlagRough) : (st.w & ~kFlagRough);
                         }
                     }
                 }
@@ -722,7 +788,7 @@ const Kernel kShadeCls[CLS_N] = {
     k_shade<false, CLS_TEX + CLS_DISNEY>, k_shade<false, CLS_TEX + CLS_HAIR>};
 int gExt = 0, gExtC = 0, gShadeI = 0, gShadow = 0, gCls[CLS_N];
 
-enum { STG_RAYGEN, STG_EXTEND, STG_SHADE, STG_SHADOW, STG_FILM, STG_N };
+enum { STG_RAYGEN, STG_EXTEND, STG_SHADE, STG_SHADOW, STG_FILM, STG_CACHE, STG_N };
 struct Mark { int stage; cudaEvent_t a, b; };
 
 // Issues one render's work on a stream: directly (optionally with an event
@@ -756,11 +822,17 @@ cudaError_t enqueue_render(const pt_ctx *ctx, Enqueue &E, WaveArgs A, const pt_r
     auto chk = [&](cudaError_t e) {
         if (err == cudaSuccess && e != cudaSuccess) err = e;
     };
+    const bool cached = A.cacheOn != 0;
     chk(cudaMemsetAsync(B.counters, 0, kCounterWords * sizeof(uint32_t), st));
     chk(cudaMemsetAsync(ctx->d_err, 0, 4, st));
+    if (cached) {  // per-call cache counters: records [2], queries of the call [5], records with targets [6]
+        chk(cudaMemsetAsync(A.crCount, 0, 4, st));
+        chk(cudaMemsetAsync(ctx->cache.ctr + 5, 0, 8, st));
+    }
     for (uint64_t ws = 0; ws < total; ws += cap) {
         A.waveStart = ws;
         A.waveCount = (uint32_t)std::min<uint64_t>(cap, total - ws);
+        if (cached) chk(cudaMemsetAsync(A.cqCount, 0, 4, st));
         A.qslotOut = B.qslot[0]; A.qoOut = B.qo[0]; A.qdOut = B.qd[0]; A.cntOut = B.counters + 0;
         E.begin(STG_RAYGEN);
         k_raygen<<<(A.waveCount + kBlock - 1) / kBlock, kBlock, 0, st>>>(A);
@@ -796,22 +868,39 @@ cudaError_t enqueue_render(const pt_ctx *ctx, Enqueue &E, WaveArgs A, const pt_r
             }
             cur = 1 - cur;
         }
+        if (cached) {  // cache queries of this wave: lo_eta[slot] += throughput x cache
+            E.begin(STG_CACHE);
+            chk(rc_enqueue_resolve(const_cast<pt_ctx *>(ctx), st, A.lo_eta));
+            E.end();
+        }
         uint32_t cover = (uint32_t)std::min<uint64_t>(A.waveCount, npix);
         E.begin(STG_FILM);
         k_film<<<(cover + kBlock - 1) / kBlock, kBlock, 0, st>>>(A, (float4 *)d_sum, (float4 *)d_comp);
         E.end();
+        if (cached) {  // training targets of the wave's records (also counts the wave's queries)
+            E.begin(STG_CACHE);
+            chk(rc_enqueue_targets(const_cast<pt_ctx *>(ctx), st, A.lo_eta, A.rng, A.pendA, A.pendE));
+            E.end();
+        }
         chk(cudaGetLastError());  // launch-configuration errors of this wave
+    }
+    if (cached && A.trainStride) {  // one training step on the call's records
+        E.begin(STG_CACHE);
+        chk(rc_enqueue_train(const_cast<pt_ctx *>(ctx), st));
+        E.end();
     }
     return err;
 }
 
 __global__ void k_set_u32(uint32_t *p, uint32_t v) { *p = v; }
 
-bool graph_matches(const pt_ctx *ctx, const pt_render_params *P, size_t cap, const float *sum, const float *comp) {
+bool graph_matches(const pt_ctx *ctx, const pt_render_params *P, size_t cap, const float *sum, const float *comp,
+                   const WaveArgs &A) {
     const RenderGraph &G = ctx->graph;
     return G.exec && G.width == P->width && G.height == P->height && G.spp == P->spp && G.maxDepth == P->max_depth &&
            G.rngKind == P->rng_kind && G.envSampling == P->env_sampling && G.cap == cap && G.sum == sum &&
            G.comp == comp && G.sceneGen == ctx->sceneGen && G.waveGen == ctx->waveGen &&
+           G.cached == A.cacheOn && G.trainStride == A.trainStride && (!A.cacheOn || G.cacheGen == ctx->cache.gen) &&
            memcmp(&G.cam, &P->camera, sizeof(pt_camera)) == 0;
 }
 }  // namespace
@@ -873,13 +962,32 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
     A.rayTotals = (unsigned long long *)(B.counters + 4);
     A.err = ctx->d_err;
     A.shadowCap = (uint32_t)(2 * B.cap);
+    A.cacheOn = (P->flags & PT_RENDER_RADIANCE_CACHE) ? 1u : 0u;
+    A.trainStride = A.unbiasedEvery = A.recCap = 0;
+    A.roughThr = 0.0f;
+    for (float4 *&q : A.cq) q = nullptr;
+    for (float4 *&r : A.cr) r = nullptr;
+    A.cqCount = A.crCount = nullptr;
+    if (A.cacheOn) {
+        if ((rc = rc_render_setup(ctx, B.cap))) return rc;
+        const RadianceCache &C = ctx->cache;
+        A.roughThr = C.params.rough_threshold;
+        A.unbiasedEvery = C.params.unbiased_every;
+        A.recCap = (uint32_t)C.recCap;
+        if (!(C.params.flags & PT_CACHE_NO_TRAIN))
+            A.trainStride = (uint32_t)std::max<uint64_t>(1, total / std::max<size_t>(C.recCap, 1));
+        for (int k = 0; k < 5; k++) A.cq[k] = C.q[k];
+        for (int k = 0; k < 7; k++) A.cr[k] = C.rec[k];
+        A.cqCount = C.ctr + 1;
+        A.crCount = C.ctr + 2;
+    }
     const uint64_t waves = (total + cap - 1) / cap;
     // Without per-launch timing the render replays a CUDA graph of its launch
     // sequence, captured on the first call with this configuration: no host
     // gaps between the ~100 launches of a render.
     const bool timing = (P->flags & PT_RENDER_STAGE_TIMING) != 0;
     bool useGraph = !timing;
-    if (useGraph && !graph_matches(ctx, P, cap, d_sum, d_comp)) {
+    if (useGraph && !graph_matches(ctx, P, cap, d_sum, d_comp, A)) {
         pt_graph_free(ctx);
         Enqueue E{ctx->ownStream, false, {}, 0};
         cudaGraph_t g = nullptr;
@@ -898,6 +1006,7 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
             G.rngKind = P->rng_kind; G.envSampling = P->env_sampling; G.cam = P->camera;
             G.cap = cap; G.sum = d_sum; G.comp = d_comp;
             G.sceneGen = ctx->sceneGen; G.waveGen = ctx->waveGen;
+            G.cached = A.cacheOn; G.trainStride = A.trainStride; G.cacheGen = ctx->cache.gen;
             G.launches = E.launches;
         } else {  // capture unavailable: issue the launches directly
             cudaGetLastError();
@@ -929,7 +1038,7 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
     cudaError_t se = cudaStreamSynchronize(st);
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, ev[0], ev[1]);
-    float stage[STG_N] = {0, 0, 0, 0, 0};
+    float stage[STG_N] = {0, 0, 0, 0, 0, 0};
     for (Mark &m : E.marks) {
         float t = 0.0f;
         if (se == cudaSuccess) cudaEventElapsedTime(&t, m.a, m.b);
@@ -941,7 +1050,8 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
     if (derr)
         return ctx->fail(PT_E_DEVICE, (derr & PT_DEVERR_STACK) ? "traversal stack overflow"
                                       : (derr & PT_DEVERR_BVH) ? "traversal visited more nodes than the BVH has"
-                                                               : "queue overflow");
+                                      : (derr & PT_DEVERR_CACHE) ? "radiance cache kernel: a tensor-core wait timed out"
+                                                                 : "queue overflow");
     if (stats) {
         unsigned long long tot[2];
         memcpy(tot, hostCnt + 4, sizeof(tot));
@@ -957,6 +1067,7 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
         stats->ms_shade = stage[STG_SHADE];
         stats->ms_shadow = stage[STG_SHADOW];
         stats->ms_film = stage[STG_FILM];
+        stats->ms_cache = stage[STG_CACHE];
     }
     return PT_OK;
 }

@@ -200,3 +200,73 @@ def test_training_reduces_loss(pt, ctx):
         assert last < first / 10, (first, last)
     finally:
         ctx.cache_release()
+
+
+# ---------------------------------------------------------------------------- cached renders
+def mean_img(s):
+    return s[..., :3] / np.maximum(s[..., 3:4], 1.0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("scene", ["cornell", "disney", "textured"])
+def test_cached_render_constant_cache_matches_oracle(pt, scenes, ctx, oracle, scene):
+    """Paths end at the first surface vertex after a rough bounce and add
+    throughput x cache: with a cache that returns a constant, the image equals
+    the oracle's render with the same termination rule, path by path."""
+    if scene == "cornell":
+        sc, cam = scenes.cornell(64, 64)
+        W, H = 64, 64
+    elif scene == "disney":
+        sc, cam = scenes.disney_spheres(96, 64, grid=3, slices=32, rings=17, env_w=256, env_h=128)
+        W, H = 96, 64
+    else:
+        sc, cam = scenes.textured_scene(64, 48)
+        W, H = 64, 48
+    ctx.upload(sc)
+    oracle.load(sc)
+    value = np.float32([0.5, 0.25, 0.125])
+    ctx.cache_init(pt.cache_params(flags=pt.PT_CACHE_NO_TRAIN, rough_threshold=0.3))
+    try:
+        ctx.cache_weights(rc.constant_weights(value))
+        P = pt.render_params(W, H, 2, cam, max_depth=8, flags=pt.PT_RENDER_RADIANCE_CACHE)
+        g, _, st = ctx.render(P)
+        o, per = oracle.render_cached(P, value, 0.3, per_path=True)
+        close = np.abs(mean_img(g) - mean_img(o)) <= 1e-3 * np.maximum(np.abs(mean_img(o)), 1e-2)
+        assert close.all(-1).mean() > 0.97, close.all(-1).mean()
+        assert ctx.cache_stats().queries > 0
+        # a plain render of the same scene differs (the cache term replaced the tails)
+        Pp = pt.render_params(W, H, 2, cam, max_depth=8)
+        p, _, _ = ctx.render(Pp)
+        assert not np.allclose(p, g)
+    finally:
+        ctx.cache_release()
+
+
+@pytest.mark.gpu
+def test_cached_render_trains(pt, scenes, ctx):
+    """Training paths record their first rough vertex and continue; each call
+    takes one Adam step on those records, and the cached image approaches the
+    plain converged image."""
+    sc, cam = scenes.cornell(64, 64)
+    ctx.upload(sc)
+    ctx.cache_init(pt.cache_params(seed=3, train_records=1024, learning_rate=1e-2, unbiased_every=16))
+    try:
+        P = pt.render_params(64, 64, 1, cam, max_depth=8, flags=pt.PT_RENDER_RADIANCE_CACHE)
+        losses = []
+        for k in range(200):
+            P.sample_offset = k
+            ctx.render(P)
+            st = ctx.cache_stats()
+            losses.append(st.last_loss)
+        assert st.steps == 200 and 700 <= st.last_records <= 1024, st.last_records
+        assert np.mean(losses[-20:]) < np.mean(losses[:5])
+        acc = np.zeros((64, 64, 4), np.float32)
+        Pc = pt.render_params(64, 64, 64, cam, max_depth=8, sample_offset=1000, flags=pt.PT_RENDER_RADIANCE_CACHE)
+        cached, _, _ = ctx.render(Pc, film_sum=acc)
+        ref, _, _ = ctx.render(pt.render_params(64, 64, 1024, cam, max_depth=8, sample_offset=5000))
+        a, b = mean_img(cached), mean_img(ref)
+        rel = float(np.mean((a - b) ** 2 / (b ** 2 + 1e-2)))
+        print("cached vs plain relMSE", rel, "loss", losses[:3], losses[-3:])
+        assert rel < 2e-2, rel
+    finally:
+        ctx.cache_release()
