@@ -152,23 +152,74 @@ def relmse(x, ref):
     return float(((x - ref) ** 2 / (ref ** 2 + 1e-2)).mean())
 
 
-def time_to_relmse(pt, ctx, stream, W, H, cam, depth, env_mode, chunk):
-    """Device time for plain path tracing to reach relMSE <= 1e-2 against a
-    4096-spp render of the same scene: progressive accumulation (the
-    reference's frame-by-frame accumulation) at 1, 2, 4, ... spp, timed with
-    CUDA events per render call; the first point at or below the bar gives
-    the time.  The radiance-cache form is not built (cached: null)."""
-    import torch
-
+def reference_image(pt, ctx, W, H, cam, depth, env_mode, chunk):
+    """The 4096-spp plain render (samples [0, 4096)) both forms are scored against."""
     D = importlib.import_module("pbrt_b200.distributed")
     ref = D.new_film(H, W, device="cuda")
     for k in range(REF_SPP // chunk):
         P = pt.render_params(W, H, chunk, cam, max_depth=depth, sample_offset=k * chunk, env_sampling=env_mode)
         ctx.render(P, ref[0].data_ptr(), ref[1].data_ptr(), pt.PT_MEM_DEVICE)
-    ref_img = D.resolve(ref)
+    return D.resolve(ref)
+
+
+def progressive(pt, ctx, stream, W, H, ref_img, make_params, spf, warm=0):
+    """Progressive accumulation (the reference's frame-by-frame accumulation):
+    render calls of `spf` samples, the first `warm` of them into a discarded
+    film (cache training only), every call timed with CUDA events on the
+    stream.  relMSE against ref_img at 1, 2, 4, ... accumulated spp (outside
+    the timing); the first point at or below the bar gives the time."""
+    import torch
+
+    D = importlib.import_module("pbrt_b200.distributed")
     film = D.new_film(H, W, device="cuda")
-    done, total_ms, curve, reached = 0, 0.0, [], None
-    add = 1
+    scratch = D.new_film(H, W, device="cuda") if warm else None
+    calls, acc, total_ms, curve, reached, check = 0, 0, 0.0, [], None, spf
+    while acc < REF_SPP // 4:
+        P = make_params(TTQ_OFFSET + calls * spf)
+        tgt = scratch if calls < warm else film
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        ctx.render(P, tgt[0].data_ptr(), tgt[1].data_ptr(), pt.PT_MEM_DEVICE)
+        b.record(stream)
+        torch.cuda.synchronize()
+        total_ms += a.elapsed_time(b)
+        calls += 1
+        if calls <= warm:
+            continue
+        acc += spf
+        if acc >= check:
+            e = relmse(D.resolve(film), ref_img)
+            curve.append([acc, round(e, 6), round(total_ms / 1e3, 5)])
+            if e <= TTQ_TARGET:
+                reached = (acc, total_ms / 1e3)
+                break
+            check *= 2
+    return {"seconds": None if reached is None else round(reached[1], 5),
+            "spp": None if reached is None else reached[0], "curve": curve}
+
+
+# Radiance-cache settings of the cached form: 2-spp calls (4 training steps
+# each), the first CACHE_WARM calls training only, up to 65,536 records per
+# call from at most 10 % of the paths that reach a cache vertex, bounces with
+# Disney roughness >= 0.1 end into the cache, no unbiased suffixes.
+CACHE_SPF, CACHE_WARM, CACHE_RECORDS, CACHE_LR = 2, 16, 65536, 1e-2
+CACHE_FRACTION, CACHE_ROUGH = 0.1, 0.1
+
+
+def time_to_relmse(pt, ctx, stream, W, H, cam, depth, env_mode, chunk):
+    """Device time for plain and radiance-cached path tracing to reach relMSE
+    <= 1e-2 against a 4096-spp plain render of the same scene.  Plain:
+    progressive renders of 1, 2, 4, ... spp (doubling calls).  Cached:
+    CACHE_SPF-spp calls with training steps in each, from an untrained cache
+    (training time and the warm-up calls are inside the timed total)."""
+    ref_img = reference_image(pt, ctx, W, H, cam, depth, env_mode, chunk)
+
+    # plain: doubling render calls
+    D = importlib.import_module("pbrt_b200.distributed")
+    import torch
+    film = D.new_film(H, W, device="cuda")
+    done, total_ms, curve, reached, add = 0, 0.0, [], None, 1
     while done < REF_SPP // 4:
         P = pt.render_params(W, H, add, cam, max_depth=depth, sample_offset=TTQ_OFFSET + done, env_sampling=env_mode)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -184,10 +235,39 @@ def time_to_relmse(pt, ctx, stream, W, H, cam, depth, env_mode, chunk):
         if e <= TTQ_TARGET:
             reached = (done, total_ms / 1e3)
             break
-        add = done  # double the sample count
-    return {"target": TTQ_TARGET, "reference_spp": REF_SPP, "plain": {
-        "seconds": None if reached is None else round(reached[1], 5),
-        "spp": None if reached is None else reached[0], "curve": curve}, "cached": None}
+        add = done
+    plain = {"seconds": None if reached is None else round(reached[1], 5),
+             "spp": None if reached is None else reached[0], "curve": curve}
+
+    def cache_params():
+        return pt.cache_params(seed=0, train_records=CACHE_RECORDS, learning_rate=CACHE_LR,
+                               max_train_fraction=CACHE_FRACTION, rough_threshold=CACHE_ROUGH)
+
+    def cached_params(off):
+        return pt.render_params(W, H, CACHE_SPF, cam, max_depth=depth, sample_offset=off, env_sampling=env_mode,
+                                flags=pt.PT_RENDER_RADIANCE_CACHE)
+
+    # one untimed cached call first: the cache kernels' first launch in the
+    # process (module loading, graph instantiation) is set-up, not rendering
+    ctx.cache_init(cache_params())
+    warm = D.new_film(H, W, device="cuda")
+    ctx.render(cached_params(0), warm[0].data_ptr(), warm[1].data_ptr(), pt.PT_MEM_DEVICE)
+    ctx.cache_release()
+    torch.cuda.synchronize()
+    ctx.cache_init(cache_params())
+    try:
+        cached = progressive(pt, ctx, stream, W, H, ref_img, cached_params, CACHE_SPF, warm=CACHE_WARM)
+        st = ctx.cache_stats()
+        cached["settings"] = {"spp_per_call": CACHE_SPF, "warmup_calls": CACHE_WARM,
+                              "train_records_per_call": CACHE_RECORDS, "max_train_fraction": CACHE_FRACTION,
+                              "rough_threshold": CACHE_ROUGH, "learning_rate": CACHE_LR, "adam_steps": int(st.steps),
+                              "network": "64 in, 5 x 64 ReLU, 3 out; BF16 tcgen05, FP32 accumulation"}
+    finally:
+        ctx.cache_release()
+    out = {"target": TTQ_TARGET, "reference_spp": REF_SPP, "plain": plain, "cached": cached}
+    if plain["seconds"] and cached["seconds"]:
+        out["cached_speedup"] = round(plain["seconds"] / cached["seconds"], 3)
+    return out
 
 
 def cpu_reference_run(pt, sc, cam, W, H, depth, seconds=15.0, prefer_reference=True):

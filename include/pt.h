@@ -358,7 +358,8 @@ int pt_trace_shadow(pt_ctx *ctx, const float *rays, size_t n, uint32_t *occluded
  * With PT_RENDER_RADIANCE_CACHE a render ends each path at the first surface
  * vertex reached after a rough bounce (diffuse, hair, microfacet / Disney at
  * or above rough_threshold) and adds throughput x cache(vertex).  A subset of
- * paths (about train_records per call) continues past that vertex; its
+ * the paths reaching that vertex (about train_records per call, at most
+ * max_train_fraction of them) continues past it; its
  * suffix, itself ended in the cache at its next rough bounce (self-training),
  * gives the radiance estimate the network is trained on after the render
  * (one Adam step per call on relative L2 loss).  One training path in
@@ -384,6 +385,7 @@ typedef struct pt_cache_params {
     uint32_t flags;          /* PT_CACHE_* */
     float bbox_min[3];       /* position normalisation; bbox_max <= bbox_min: the scene's bounds */
     float bbox_max[3];
+    float max_train_fraction; /* at most this share of cache vertices trains (0 = 0.25) */
 } pt_cache_params;
 typedef struct pt_cache_stats {
     uint64_t steps;        /* Adam steps taken */

@@ -116,7 +116,7 @@ class pt_hit(C.Structure):
 class pt_cache_params(C.Structure):
     _fields_ = [("train_records", C.c_uint32), ("unbiased_every", C.c_uint32), ("rough_threshold", C.c_float),
                 ("learning_rate", C.c_float), ("ema", C.c_float), ("seed", C.c_uint32), ("flags", C.c_uint32),
-                ("bbox_min", C.c_float * 3), ("bbox_max", C.c_float * 3)]
+                ("bbox_min", C.c_float * 3), ("bbox_max", C.c_float * 3), ("max_train_fraction", C.c_float)]
 
 
 class pt_cache_stats(C.Structure):
@@ -125,8 +125,9 @@ class pt_cache_stats(C.Structure):
 
 
 def cache_params(train_records=0, unbiased_every=0, rough_threshold=0.0, learning_rate=0.0, ema=0.0, seed=0,
-                 flags=0, bbox=None) -> pt_cache_params:
+                 flags=0, bbox=None, max_train_fraction=0.0) -> pt_cache_params:
     p = pt_cache_params()
+    p.max_train_fraction = max_train_fraction
     p.train_records, p.unbiased_every, p.rough_threshold = train_records, unbiased_every, rough_threshold
     p.learning_rate, p.ema, p.seed, p.flags = learning_rate, ema, seed, flags
     if bbox is not None:

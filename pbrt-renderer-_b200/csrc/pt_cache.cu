@@ -61,16 +61,22 @@ struct RcRows<0> {  // features n x 64, targets n x 3 (training)
     }
 };
 template <>
-struct RcRows<1> {  // records (render queries or training records)
+struct RcRows<1> {  // records (render queries or training records): rows phase, phase + stride, ...
     const float4 *r0, *r1, *r2, *r3, *tgt;
     const uint32_t *cnt;
     uint32_t cap;
-    __device__ uint32_t count() const { return min(*(volatile const uint32_t *)cnt, cap); }
+    uint32_t stride = 1, phase = 0;
+    __device__ uint32_t total() const { return min(*(volatile const uint32_t *)cnt, cap); }
+    __device__ uint32_t count() const {
+        uint32_t n = total();
+        return n > phase ? (n - phase + stride - 1) / stride : 0u;
+    }
     __device__ void load(const RcNet &N, uint32_t row, float f[kRcIn]) const {
-        rc_encode(r0[row], r1[row], r2[row], r3[row], N.bmin, N.binv, f);
+        const uint32_t i = row * stride + phase;
+        rc_encode(r0[i], r1[i], r2[i], r3[i], N.bmin, N.binv, f);
     }
     __device__ float3 target(uint32_t row) const {
-        float4 t = tgt[row];
+        float4 t = tgt[row * stride + phase];
         return make_float3(t.x, t.y, t.z);
     }
 };
@@ -367,10 +373,12 @@ struct RcAdamArgs {
     float *w, *m, *v, *ema, *grad;
     uint8_t *imgTrain, *imgInfer;
     uint32_t *ctr;           // [0] steps (read, incremented), [4] records of the step (written)
-    const uint32_t *nrec;    // records the gradient sums over
-    uint32_t nrecCap;
+    const uint32_t *nrec;    // records of the call; this step's gradient sums over rows phase + k stride
+    uint32_t nrecCap, stride, phase;
     float lr, emaDecay;
     float *lossSum;          // mean loss of the step -> ctr[3] as float bits; reset
+    uint32_t updateProb;     // last step of a render call: set ctr[7] for the next call
+    float maxFrac;           // upper bound of ctr[7]
 };
 __device__ __forceinline__ void put_bf16(uint8_t *img, int i, float x) {
     int l = i < rc_param_base(5) ? i / (kRcWidth * kRcIn) : 5;
@@ -383,7 +391,14 @@ __global__ void __launch_bounds__(1024) k_rc_adam(RcAdamArgs a) {
     __shared__ uint32_t sStep, sN;
     if (threadIdx.x == 0) {
         sStep = a.ctr[0] + 1u;
-        sN = min(*a.nrec, a.nrecCap);
+        uint32_t tot = min(*a.nrec, a.nrecCap);
+        sN = tot > a.phase ? (tot - a.phase + a.stride - 1) / a.stride : 0u;
+        if (a.updateProb) {
+            // training chance of the next call: about nrecCap records out of
+            // this call's cache vertices (queries + records)
+            float verts = (float)a.ctr[5] + (float)tot;
+            reinterpret_cast<float *>(a.ctr)[7] = verts > 0.0f ? fminf(a.maxFrac, (float)a.nrecCap / verts) : a.maxFrac;
+        }
     }
     __syncthreads();
     const uint32_t n = sN, step = sStep;
@@ -433,7 +448,7 @@ __global__ void __launch_bounds__(1024) k_rc_targets(RcRows<1> rec, float4 *beta
     __shared__ uint32_t s0, s1;
     if (threadIdx.x == 0) {
         s0 = ctr[6];
-        s1 = rec.count();
+        s1 = rec.total();
     }
     __syncthreads();
     for (uint32_t r = s0 + threadIdx.x; r < s1; r += blockDim.x) {
@@ -551,24 +566,31 @@ cudaError_t rc_enqueue_resolve(pt_ctx *ctx, cudaStream_t st, float4 *lo_eta) {
 cudaError_t rc_enqueue_targets(pt_ctx *ctx, cudaStream_t st, const float4 *lo_eta, const uint4 *rng,
                                const float4 *pendA, const float4 *pendE) {
     const RadianceCache &C = ctx->cache;
-    RcRows<1> rec{C.rec[0], C.rec[1], C.rec[2], C.rec[3], C.rec[6], C.ctr + 2, (uint32_t)C.recCap};
+    RcRows<1> rec{C.rec[0], C.rec[1], C.rec[2], C.rec[3], C.rec[6], C.ctr + 2, (uint32_t)C.recCap, 1u, 0u};
     k_rc_targets<<<1, 1024, 0, st>>>(rec, C.rec[4], C.rec[5], C.rec[6], C.ctr, lo_eta, rng, pendA, pendE);
     return cudaGetLastError();
 }
+// kRcStepsPerCall Adam steps per render call, step s on records s, s + steps,
+// ... (interleaved, so each batch spans the whole frame).
+constexpr uint32_t kRcStepsPerCall = 4;
 cudaError_t rc_enqueue_train(pt_ctx *ctx, cudaStream_t st) {
     RadianceCache &C = ctx->cache;
     float *lossDev = reinterpret_cast<float *>(C.ctr + 8);
-    cudaError_t e = cudaMemsetAsync(lossDev, 0, 4, st);
-    if (e != cudaSuccess) return e;
-    RcTrainArgs a{};
-    a.net = rc_net(ctx, C.imgTrain);
-    a.rec = RcRows<1>{C.rec[0], C.rec[1], C.rec[2], C.rec[3], C.rec[6], C.ctr + 2, (uint32_t)C.recCap};
-    a.grad = C.grad;
-    a.lossSum = lossDev;
-    k_rc_train<1><<<ctx->numSMs, kRcThreads, kTrainSmem, st>>>(a);
-    RcAdamArgs d{C.w, C.m, C.v, C.ema, C.grad, C.imgTrain, C.imgInfer, C.ctr, C.ctr + 2, (uint32_t)C.recCap,
-                 C.params.learning_rate, C.params.ema, lossDev};
-    k_rc_adam<<<1, 1024, 0, st>>>(d);
+    for (uint32_t s = 0; s < kRcStepsPerCall; s++) {
+        cudaError_t e = cudaMemsetAsync(lossDev, 0, 4, st);
+        if (e != cudaSuccess) return e;
+        RcTrainArgs a{};
+        a.net = rc_net(ctx, C.imgTrain);
+        a.rec = RcRows<1>{C.rec[0], C.rec[1], C.rec[2], C.rec[3], C.rec[6], C.ctr + 2, (uint32_t)C.recCap,
+                          kRcStepsPerCall, s};
+        a.grad = C.grad;
+        a.lossSum = lossDev;
+        k_rc_train<1><<<ctx->numSMs, kRcThreads, kTrainSmem, st>>>(a);
+        RcAdamArgs d{C.w, C.m, C.v, C.ema, C.grad, C.imgTrain, C.imgInfer, C.ctr, C.ctr + 2, (uint32_t)C.recCap,
+                     kRcStepsPerCall, s, C.params.learning_rate, C.params.ema, lossDev,
+                     s + 1 == kRcStepsPerCall ? 1u : 0u, C.params.max_train_fraction};
+        k_rc_adam<<<1, 1024, 0, st>>>(d);
+    }
     return cudaGetLastError();
 }
 int rc_render_setup(pt_ctx *ctx, size_t waveCap) {
@@ -621,6 +643,7 @@ int pt_cache_init(pt_ctx *ctx, const pt_cache_params *params) {
     if (!C.params.train_records) C.params.train_records = 65536u;
     if (C.params.rough_threshold <= 0.0f) C.params.rough_threshold = 0.3f;
     if (C.params.learning_rate <= 0.0f) C.params.learning_rate = 5e-3f;
+    if (C.params.max_train_fraction <= 0.0f || C.params.max_train_fraction > 1.0f) C.params.max_train_fraction = 0.25f;
     rc_bounds(ctx);
     cudaError_t e = cudaSuccess;
     auto A = [&](void **p, size_t b) { if (e == cudaSuccess) e = cudaMalloc(p, b); };
@@ -650,6 +673,8 @@ int pt_cache_init(pt_ctx *ctx, const pt_cache_params *params) {
     cudaMemset(C.imgTrain, 0, kRcImageBytes);
     cudaMemset(C.imgInfer, 0, kRcImageBytes);
     cudaMemset(C.ctr, 0, 16 * sizeof(uint32_t));
+    // the first call trains on the first records it finds, up to the cap
+    cudaMemcpy(C.ctr + 7, &C.params.max_train_fraction, 4, cudaMemcpyHostToDevice);
     k_rc_images<<<21, 1024>>>(C.w, C.imgTrain, C.imgInfer, C.ema);
     e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return ctx->fail(PT_E_CUDA, "cache initialisation", cudaGetErrorString(e));
@@ -677,6 +702,7 @@ int pt_cache_weights(pt_ctx *ctx, float *get, const float *set) {
             return ctx->fail(PT_E_CUDA, "cache weights");
         for (float *p : {C.m, C.v, C.grad}) cudaMemset(p, 0, kRcParams * sizeof(float));
         cudaMemset(C.ctr, 0, 16 * sizeof(uint32_t));
+        cudaMemcpy(C.ctr + 7, &C.params.max_train_fraction, 4, cudaMemcpyHostToDevice);
         k_rc_images<<<21, 1024>>>(C.w, C.imgTrain, C.imgInfer, C.ema);
         cudaError_t e = cudaDeviceSynchronize();
         if (e != cudaSuccess) return ctx->fail(PT_E_CUDA, "cache weights", cudaGetErrorString(e));
@@ -751,7 +777,7 @@ static int rc_train_impl(pt_ctx *ctx, const float *features, const float *target
     cudaMemcpyAsync(&lossHost, lossDev, 4, cudaMemcpyDeviceToHost, ctx->stream);
     if (step) {
         RcAdamArgs d{C.w, C.m, C.v, C.ema, C.grad, C.imgTrain, C.imgInfer, C.ctr, nDev, PT_CACHE_MAX_RECORDS,
-                     C.params.learning_rate, C.params.ema, lossDev};
+                     1u, 0u, C.params.learning_rate, C.params.ema, lossDev, 0u, 1.0f};
         k_rc_adam<<<1, 1024, 0, ctx->stream>>>(d);
     } else if (grad) {
         cudaMemcpyAsync(grad, C.grad, kRcParams * 4, cudaMemcpyDeviceToHost, ctx->stream);

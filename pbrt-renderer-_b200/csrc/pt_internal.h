@@ -96,7 +96,7 @@ struct RenderGraph {
     size_t cap = 0;
     const void *sum = nullptr, *comp = nullptr;
     uint64_t sceneGen = 0, waveGen = 0;
-    uint32_t cached = 0, trainStride = 0;  // radiance-cache configuration baked into the launches
+    uint32_t cached = 0, trainOn = 0;  // radiance-cache configuration baked into the launches
     uint64_t cacheGen = 0;
     uint64_t launches = 0;
 };
@@ -113,7 +113,8 @@ struct RadianceCache {
     uint8_t *imgTrain = nullptr, *imgInfer = nullptr;
     // counters: [0] Adam steps, [1] queries of the wave, [2] records of the
     // call, [3] loss sum (float bits), [4] records of the last step, [5]
-    // queries of the call, [6] first record not yet given a target
+    // queries of the call, [6] first record not yet given a target, [7] the
+    // chance (float) that a path at a cache vertex trains, set after each call
     uint32_t *ctr = nullptr;
     size_t queryCap = 0;
     float4 *q[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // record float4 x 4, weight

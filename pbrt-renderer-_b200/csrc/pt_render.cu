@@ -59,8 +59,9 @@ struct WaveArgs {
     uint32_t *err;
     uint32_t shadowCap;
     // radiance cache (cacheOn == 0: plain path tracing)
-    uint32_t cacheOn, trainStride, unbiasedEvery, recCap;
+    uint32_t cacheOn, trainOn, unbiasedEvery, recCap;
     float roughThr;
+    const float *trainProb;  // chance that a path reaching a cache vertex trains (device, per call)
     float4 *cq[5];      // queries: 4 record float4 + throughput weight
     uint32_t *cqCount;
     float4 *cr[7];      // training records: 4 record float4, throughput, Lo so far, target
@@ -148,15 +149,7 @@ __global__ void k_raygen(WaveArgs A) {
     A.qdOut[slot] = make_float4(rd.x, rd.y, rd.z, 1e20f);
     A.thr_pdf[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
     A.lo_eta[slot] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
-    uint32_t flags = 0u;
-    if (A.cacheOn && A.trainStride) {  // about one path in trainStride trains the cache
-        uint64_t k = A.waveStart + slot + pcg_hash(__ldg(A.sampleOffset)) % A.trainStride;
-        if (k % A.trainStride == 0) {
-            flags |= kFlagTrain;
-            if (A.unbiasedEvery && (k / A.trainStride) % A.unbiasedEvery == 0) flags |= kFlagUnbiased;
-        }
-    }
-    A.rng[slot] = make_uint4(r.dim, r.white, 0u, flags);
+    A.rng[slot] = make_uint4(r.dim, r.white, 0u, 0u);
     if (slot == 0) *A.cntOut = A.waveCount;
 }
 
@@ -543,18 +536,36 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
                 if (TEX || (C == CLS_ANY && has_shading_textures(m)))
                     apply_textures(S, m, mesh, prim, h4.x, i0, i1, i2, bx, by, N, A.width, A.height);
                 // Radiance cache: the first surface vertex after a rough bounce ends
-                // the path (a query, resolved after the wave) or, on a training
-                // path, records its state and the path goes on.
+                // the path (a query, resolved after the wave), or, with probability
+                // *trainProb, records its state there and the path goes on as a
+                // training path (its suffix ends at its own next cache vertex, or
+                // for one in unbiasedEvery, runs without the cache).
                 bool cacheStop = false;
                 if (A.cacheOn && (st.w & kFlagRough) && !(C == CLS_EMIT || (C == CLS_ANY && m.isEmitter))) {
-                    const bool train = (st.w & kFlagTrain) != 0;
-                    if (train && !(st.w & kFlagHasRec)) {
-                        uint32_t r = warp_append(A.crCount, true);
-                        if (r < A.recCap) {
-                            cache_record(A.cr, r, hp, -rd, N, m, type, slot);
-                            A.cr[4][r] = make_float4(thr.x, thr.y, thr.z, 0.0f);
-                            A.cr[5][r] = make_float4(Lo.x, Lo.y, Lo.z, 0.0f);
-                            st.w |= kFlagHasRec | (r << 8);
+                    bool train = (st.w & kFlagTrain) != 0;
+                    if (!train && A.trainOn) {
+                        const uint32_t hsh = pcg_hash(pcg_hash(rng.pixelSeed ^ (rng.sampleIndex * 0x9E3779B9u)) ^ st.z);
+                        if ((float)(hsh >> 8) * (1.0f / 16777216.0f) < __ldg(A.trainProb)) {
+                            uint32_t r = warp_append(A.crCount, true);
+                            if (r < A.recCap) {
+                                cache_record(A.cr, r, hp, -rd, N, m, type, slot);
+                                A.cr[4][r] = make_float4(thr.x, thr.y, thr.z, 0.0f);
+                                A.cr[5][r] = make_float4(Lo.x, Lo.y, Lo.z, 0.0f);
+                                st.w |= kFlagTrain | kFlagHasRec | (r << 8);
+                                if (A.unbiasedEvery && pcg_hash(hsh) % A.unbiasedEvery == 0) st.w |= kFlagUnbiased;
+                                train = true;
+                            }
+                        }
+                        if (train) {
+                        } else {
+                            uint32_t q = warp_append(A.cqCount, true);
+                            if (q < A.clsStride) {
+                                cache_record(A.cq, q, hp, -rd, N, m, type, slot);
+                                A.cq[4][q] = make_float4(thr.x, thr.y, thr.z, 0.0f);
+                            } else {
+                                atomicOr(A.err, (uint32_t)PT_DEVERR_QUEUE);
+                            }
+                            cacheStop = true;
                         }
                     } else if (!(train && (st.w & kFlagUnbiased))) {
                         uint32_t q = warp_append(A.cqCount, true);
@@ -884,7 +895,7 @@ cudaError_t enqueue_render(const pt_ctx *ctx, Enqueue &E, WaveArgs A, const pt_r
         }
         chk(cudaGetLastError());  // launch-configuration errors of this wave
     }
-    if (cached && A.trainStride) {  // one training step on the call's records
+    if (cached && A.trainOn) {  // training steps on the call's records
         E.begin(STG_CACHE);
         chk(rc_enqueue_train(const_cast<pt_ctx *>(ctx), st));
         E.end();
@@ -900,7 +911,7 @@ bool graph_matches(const pt_ctx *ctx, const pt_render_params *P, size_t cap, con
     return G.exec && G.width == P->width && G.height == P->height && G.spp == P->spp && G.maxDepth == P->max_depth &&
            G.rngKind == P->rng_kind && G.envSampling == P->env_sampling && G.cap == cap && G.sum == sum &&
            G.comp == comp && G.sceneGen == ctx->sceneGen && G.waveGen == ctx->waveGen &&
-           G.cached == A.cacheOn && G.trainStride == A.trainStride && (!A.cacheOn || G.cacheGen == ctx->cache.gen) &&
+           G.cached == A.cacheOn && G.trainOn == A.trainOn && (!A.cacheOn || G.cacheGen == ctx->cache.gen) &&
            memcmp(&G.cam, &P->camera, sizeof(pt_camera)) == 0;
 }
 }  // namespace
@@ -963,8 +974,9 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
     A.err = ctx->d_err;
     A.shadowCap = (uint32_t)(2 * B.cap);
     A.cacheOn = (P->flags & PT_RENDER_RADIANCE_CACHE) ? 1u : 0u;
-    A.trainStride = A.unbiasedEvery = A.recCap = 0;
+    A.trainOn = A.unbiasedEvery = A.recCap = 0;
     A.roughThr = 0.0f;
+    A.trainProb = nullptr;
     for (float4 *&q : A.cq) q = nullptr;
     for (float4 *&r : A.cr) r = nullptr;
     A.cqCount = A.crCount = nullptr;
@@ -974,8 +986,8 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
         A.roughThr = C.params.rough_threshold;
         A.unbiasedEvery = C.params.unbiased_every;
         A.recCap = (uint32_t)C.recCap;
-        if (!(C.params.flags & PT_CACHE_NO_TRAIN))
-            A.trainStride = (uint32_t)std::max<uint64_t>(1, total / std::max<size_t>(C.recCap, 1));
+        A.trainOn = (C.params.flags & PT_CACHE_NO_TRAIN) ? 0u : 1u;
+        A.trainProb = reinterpret_cast<const float *>(C.ctr + 7);
         for (int k = 0; k < 5; k++) A.cq[k] = C.q[k];
         for (int k = 0; k < 7; k++) A.cr[k] = C.rec[k];
         A.cqCount = C.ctr + 1;
@@ -1006,7 +1018,7 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
             G.rngKind = P->rng_kind; G.envSampling = P->env_sampling; G.cam = P->camera;
             G.cap = cap; G.sum = d_sum; G.comp = d_comp;
             G.sceneGen = ctx->sceneGen; G.waveGen = ctx->waveGen;
-            G.cached = A.cacheOn; G.trainStride = A.trainStride; G.cacheGen = ctx->cache.gen;
+            G.cached = A.cacheOn; G.trainOn = A.trainOn; G.cacheGen = ctx->cache.gen;
             G.launches = E.launches;
         } else {  // capture unavailable: issue the launches directly
             cudaGetLastError();
