@@ -22,6 +22,7 @@ else the oracle restatement) on the host cores.
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import importlib
 import importlib.util
 import json
@@ -270,6 +271,58 @@ def time_to_relmse(pt, ctx, stream, W, H, cam, depth, env_mode, chunk):
     return out
 
 
+# Radiance-cache network FLOPs (the MMA shapes: 64 inputs, 5 x 64 hidden,
+# output padded to 16): forward per query; training per record adds the
+# weight gradients of all 6 layers and the input gradients of layers 5..1.
+CACHE_FLOPS_INFER = 2 * (5 * 64 * 64 + 16 * 64)
+CACHE_FLOPS_TRAIN = CACHE_FLOPS_INFER + 2 * (5 * 64 * 64 + 16 * 64) + 2 * (16 * 64 + 4 * 64 * 64)
+
+
+def cache_kernel_roofline(pt, ctx):
+    """Tensor-core roofline of the two network kernels on large batches in
+    device memory: k_rc_infer over 2^21 queries, k_rc_train over 2^18
+    records; device time from the library's CUDA events around the kernel,
+    median of 10 calls after 3 warm-up calls; peak = measured dense BF16."""
+    import torch
+
+    pk = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    peak = float(pk.get("bf16_tflops", 1590.0))
+    L, h = ctx.L, ctx.h
+    ctx.cache_init(pt.cache_params(seed=0, bbox=((0, 0, 0), (1, 1, 1))))
+    g = torch.Generator(device="cuda").manual_seed(0)
+    out = {}
+    try:
+        for kind, n, flops in (("infer", 1 << 21, CACHE_FLOPS_INFER), ("train", 1 << 18, CACHE_FLOPS_TRAIN)):
+            f = torch.rand((n, 64), device="cuda", generator=g) * 2 - 1
+            f[:, 49] = 1.0
+            f[:, 50:] = 0.0
+            fp = C.cast(f.data_ptr(), C.POINTER(C.c_float))
+            if kind == "infer":
+                y = torch.empty((n, 3), device="cuda")
+                yp = C.cast(y.data_ptr(), C.POINTER(C.c_float))
+                call = lambda: L.pt_cache_infer_batch(h, fp, n, yp, pt.PT_MEM_DEVICE)  # noqa: E731
+            else:
+                t = torch.rand((n, 3), device="cuda", generator=g) * 2
+                tp = C.cast(t.data_ptr(), C.POINTER(C.c_float))
+                gr = np.zeros(pt.PT_CACHE_PARAMS, np.float32)
+                loss = np.zeros(1, np.float32)
+                call = lambda: L.pt_cache_gradient_batch(h, fp, tp, n, pt.fptr(gr), pt.fptr(loss),  # noqa: E731
+                                                         pt.PT_MEM_DEVICE)
+            ms = []
+            for k in range(13):
+                ctx._check(call())
+                if k >= 3:
+                    ms.append(ctx.cache_stats().last_kernel_ms)
+            m = float(np.median(ms))
+            tf = n * flops / (m / 1e3) / 1e12
+            out[kind] = {"rows": n, "flops_per_row": flops, "ms": round(m, 4), "achieved": round(tf, 2),
+                         "peak": peak, "unit": "TFLOP/s", "frac": round(tf / peak, 4)}
+    finally:
+        ctx.cache_release()
+    return out
+
+
 def cpu_reference_run(pt, sc, cam, W, H, depth, seconds=15.0, prefer_reference=True):
     """Time the CPU implementation on a bounded sample of the workload:
     whole frames at 1 spp (the reference's one-sample dispatch), repeated
@@ -334,9 +387,17 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--wave-paths", type=int, default=0, help="paths in flight per wave (0 = library default)")
     ap.add_argument("--no-ttq", action="store_true", help="skip the time-to-relMSE measurement")
+    ap.add_argument("--cache-kernels-only", action="store_true",
+                    help="only the radiance-cache network kernels' roofline (profiling of those kernels)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.cache_kernels_only:
+        pt = load_pkg()
+        ctx = pt.Context(0)
+        print(json.dumps({"cache_roofline": cache_kernel_roofline(pt, ctx)}), flush=True)
+        ctx.close()
+        return 0
 
     import torch
     import torch.distributed as dist
@@ -412,6 +473,13 @@ def main():
         hsum = torch.zeros((H, W, 4), dtype=torch.float32, pin_memory=True)
         hcomp = torch.zeros_like(hsum, pin_memory=True)
         film_np, comp_np = hsum.numpy(), hcomp.numpy()
+        # untimed warm-up through the same call: the library captures its
+        # launch graph for the host-film staging buffers on the first call
+        for k in range(args.warmup):
+            P = pt.render_params(W, H, spp, cam, max_depth=depth, sample_offset=D.sample_offset(k, rank, world, spp),
+                                 env_sampling=env_mode, wave_paths=args.wave_paths)
+            ctx.render(P, film_np, comp_np, pt.PT_MEM_HOST)
+        torch.cuda.synchronize()
         e2e_ms = 0.0
         for k in range(args.steps):
             P = pt.render_params(W, H, spp, cam, max_depth=depth,
@@ -476,6 +544,7 @@ def main():
     }
     if world == 1 and not args.no_ttq:
         line["time_to_relmse"] = time_to_relmse(pt, ctx, stream, W, H, cam, depth, env_mode, max(spp, 64))
+        line["cache_roofline"] = cache_kernel_roofline(pt, ctx)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, kind, cores, sample = cpu_reference_run(pt, sc, cam, W, H, depth, seconds=args.cpu_seconds)
         line["cpu_baseline"] = {"value": round(v, 4), "unit": "Mpaths/s", "cores": cores, "kind": kind,

@@ -392,6 +392,7 @@ typedef struct pt_cache_stats {
     uint32_t last_records; /* records in the last step */
     float last_loss;       /* mean relative L2 loss of the last step */
     uint64_t queries;      /* cache queries of the last render */
+    float last_kernel_ms;  /* device time of the last batch call's network kernel (infer / train) */
 } pt_cache_stats;
 /* (Re)initialise the cache of ctx: weights from params->seed, zero moments. */
 int pt_cache_init(pt_ctx *ctx, const pt_cache_params *params);

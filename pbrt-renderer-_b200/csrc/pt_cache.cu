@@ -742,8 +742,11 @@ int pt_cache_infer_batch(pt_ctx *ctx, const float *features, size_t n, float *ou
     a.feat.feat = (const float *)s.dev(0);
     a.feat.n = (uint32_t)n;
     a.out = (float *)s.dev(1);
+    cudaEventRecord(ctx->ev[0], ctx->stream);
     k_rc_infer<0><<<rc_grid(ctx, (uint32_t)n, 3), kRcThreads, kInferSmem, ctx->stream>>>(a);
+    cudaEventRecord(ctx->ev[1], ctx->stream);
     if ((rc = s.finish())) return rc;
+    cudaEventElapsedTime(&ctx->cache.lastKernelMs, ctx->ev[0], ctx->ev[1]);
     return rc_device_error(ctx);
 }
 
@@ -771,7 +774,9 @@ static int rc_train_impl(pt_ctx *ctx, const float *features, const float *target
         a.feat.n = n32;
         a.grad = C.grad;
         a.lossSum = lossDev;
+        cudaEventRecord(ctx->ev[0], ctx->stream);
         k_rc_train<0><<<rc_grid(ctx, n32, 1), kRcThreads, kTrainSmem, ctx->stream>>>(a);
+        cudaEventRecord(ctx->ev[1], ctx->stream);
     }
     float lossHost = 0.0f;
     cudaMemcpyAsync(&lossHost, lossDev, 4, cudaMemcpyDeviceToHost, ctx->stream);
@@ -784,6 +789,7 @@ static int rc_train_impl(pt_ctx *ctx, const float *features, const float *target
         cudaMemsetAsync(C.grad, 0, kRcParams * 4, ctx->stream);
     }
     if ((rc = s.finish())) return rc;
+    if (n) cudaEventElapsedTime(&C.lastKernelMs, ctx->ev[0], ctx->ev[1]);
     if (loss) *loss = lossHost;
     return rc_device_error(ctx);
 }
@@ -811,6 +817,7 @@ int pt_cache_get_stats(pt_ctx *ctx, pt_cache_stats *out) {
     out->last_records = c[4];
     memcpy(&out->last_loss, &c[3], 4);
     out->queries = c[5];
+    out->last_kernel_ms = ctx->cache.lastKernelMs;
     return PT_OK;
 }
 

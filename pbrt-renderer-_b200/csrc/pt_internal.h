@@ -121,6 +121,7 @@ struct RadianceCache {
     size_t recCap = 0;
     float4 *rec[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // x 4, beta+slot, Lo, target
     uint64_t gen = 1;  // bumped when buffers move
+    float lastKernelMs = 0.0f;  // network kernel of the last batch call (CUDA events)
 };
 
 struct pt_ctx {
