@@ -257,6 +257,38 @@ int pt_upload_scene(pt_ctx *ctx, const pt_scene_desc *scene);
  * them into film.  stats may be NULL. */
 int pt_render(pt_ctx *ctx, const pt_render_params *params, pt_film *film, pt_stats *stats);
 
+/* ---- batched render requests ---------------------------------------------
+ * No counterpart in the reference (one DispatchRays per frame).  Renders n
+ * requests of one scene — each its own image size, spp, sample offset, max
+ * depth, camera and film — as one wavefront: the requests' paths are laid
+ * out shortest request first and processed in waves that span requests; the
+ * launch sequence is captured as a CUDA graph per batch shape and replayed.
+ * rng_kind, env_sampling and flags must agree across the batch;
+ * wave_paths of requests[0] (0 = the tuned or default size) sets the wave.
+ * request_ms (n floats, may be NULL): device time from the batch's start to
+ * the end of the wave that finished each request.  Each request's image
+ * equals the same request rendered alone by pt_render. */
+#define PT_BATCH_MAX_REQUESTS 256u
+#define PT_BATCH_MAX_PIXELS (1u << 24) /* per request */
+typedef struct pt_request {
+    pt_render_params params;
+    pt_film film;
+} pt_request;
+int pt_render_batch(pt_ctx *ctx, const pt_request *requests, uint32_t n, float *request_ms, pt_stats *stats);
+/* Autotuner of the batch launch shape: times the batch (films untouched:
+ * it renders into scratch films) for each candidate wave size and traversal
+ * grid, keeps the fastest for later pt_render_batch calls on this scene. */
+typedef struct pt_batch_tuning {
+    uint32_t wave_paths;    /* chosen paths per wave */
+    float traversal_grid;   /* chosen traversal / shading grid, share of full occupancy */
+    float ms;               /* its batch time */
+    uint32_t candidates;    /* configurations timed */
+    float candidate_ms[16]; /* their times, in trial order */
+    uint32_t candidate_wave[16];
+    float candidate_grid[16];
+} pt_batch_tuning;
+int pt_batch_autotune(pt_ctx *ctx, const pt_request *requests, uint32_t n, pt_batch_tuning *out);
+
 /* ---- parity entry points (batched, device or host arrays) ----------------
  * wi, wo: local-frame directions, 3 floats each; h: hair offset per query
  * (may be NULL = 0).  Replace MaterialEval / MaterialPdf / MaterialSample

@@ -113,6 +113,16 @@ class pt_hit(C.Structure):
                 ("v", C.c_float), ("hit", C.c_uint32)]
 
 
+class pt_request(C.Structure):
+    _fields_ = [("params", pt_render_params), ("film", pt_film)]
+
+
+class pt_batch_tuning(C.Structure):
+    _fields_ = [("wave_paths", C.c_uint32), ("traversal_grid", C.c_float), ("ms", C.c_float),
+                ("candidates", C.c_uint32), ("candidate_ms", C.c_float * 16), ("candidate_wave", C.c_uint32 * 16),
+                ("candidate_grid", C.c_float * 16)]
+
+
 class pt_cache_params(C.Structure):
     _fields_ = [("train_records", C.c_uint32), ("unbiased_every", C.c_uint32), ("rough_threshold", C.c_float),
                 ("learning_rate", C.c_float), ("ema", C.c_float), ("seed", C.c_uint32), ("flags", C.c_uint32),
@@ -276,6 +286,8 @@ def lib():
         L.pt_bvh_read.argtypes = [P, U, U, C.POINTER(C.c_int32)]
         L.pt_trace_closest.argtypes = [P, F, S, C.POINTER(pt_hit), C.c_uint32]
         L.pt_trace_shadow.argtypes = [P, F, S, U, F, C.c_uint32]
+        L.pt_render_batch.argtypes = [P, C.POINTER(pt_request), C.c_uint32, F, C.POINTER(pt_stats)]
+        L.pt_batch_autotune.argtypes = [P, C.POINTER(pt_request), C.c_uint32, C.POINTER(pt_batch_tuning)]
         L.pt_cache_init.argtypes = [P, C.POINTER(pt_cache_params)]
         L.pt_cache_release.argtypes = [P]
         L.pt_cache_weights.argtypes = [P, F, F]
@@ -419,6 +431,41 @@ class Context:
         tr = np.zeros((n, 3), np.float32)
         self._check(self.L.pt_trace_shadow(self.h, fptr(rays), n, uptr(occ), fptr(tr), PT_MEM_HOST))
         return occ, tr
+
+    # ---- batched requests ------------------------------------------------------------
+    @staticmethod
+    def _requests(params_list, films, location):
+        n = len(params_list)
+        reqs = (pt_request * n)()
+        for i, (p, f) in enumerate(zip(params_list, films)):
+            reqs[i].params = p
+            if location == PT_MEM_HOST:
+                reqs[i].film = pt_film(p.width, p.height, f[0].ctypes.data, f[1].ctypes.data, PT_MEM_HOST)
+            else:
+                reqs[i].film = pt_film(p.width, p.height, f[0], f[1], PT_MEM_DEVICE)
+        return reqs
+
+    def render_batch(self, params_list, films=None, location=PT_MEM_HOST):
+        """Render several requests in one batch.  films: per request (sum, comp)
+        host arrays (H, W, 4) or device pointers; None = fresh host films.
+        Returns (films, per-request ms, stats)."""
+        if films is None:
+            films = [(np.zeros((p.height, p.width, 4), np.float32), np.zeros((p.height, p.width, 4), np.float32))
+                     for p in params_list]
+        reqs = self._requests(params_list, films, location)
+        ms = np.zeros(len(params_list), np.float32)
+        st = pt_stats()
+        self._check(self.L.pt_render_batch(self.h, reqs, len(params_list), fptr(ms), C.byref(st)))
+        return films, ms, st
+
+    def batch_autotune(self, params_list, films=None, location=PT_MEM_HOST) -> pt_batch_tuning:
+        if films is None:
+            films = [(np.zeros((p.height, p.width, 4), np.float32), np.zeros((p.height, p.width, 4), np.float32))
+                     for p in params_list]
+        reqs = self._requests(params_list, films, location)
+        out = pt_batch_tuning()
+        self._check(self.L.pt_batch_autotune(self.h, reqs, len(params_list), C.byref(out)))
+        return out
 
     # ---- radiance cache ------------------------------------------------------------
     def cache_init(self, params: pt_cache_params | None = None):

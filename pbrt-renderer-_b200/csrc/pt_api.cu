@@ -277,6 +277,7 @@ int pt_destroy(pt_ctx *ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     pt_graph_free(ctx);
+    pt_batch_free(ctx);
     ctx->free_scene();
     pt_wave_free(ctx);
     if (ctx->scratch) cudaFree(ctx->scratch);

@@ -124,6 +124,24 @@ struct RadianceCache {
     float lastKernelMs = 0.0f;  // network kernel of the last batch call (CUDA events)
 };
 
+// Batched renders (pt_render_batch): the device request table, per-slot
+// request / pixel / sample, per-wave completion events, the launch graph of
+// the last batch shape, staging of host films, and the autotuned launch shape.
+struct BatchState {
+    void *reqs = nullptr;  // PT_BATCH_MAX_REQUESTS device records
+    uint2 *slotInfo = nullptr;
+    size_t slotCap = 0;
+    std::vector<cudaEvent_t> ev;  // one per wave
+    cudaGraphExec_t exec = nullptr;
+    std::vector<uint64_t> key;
+    uint64_t launches = 0;
+    void *films = nullptr;  // device copies of host films
+    size_t filmBytes = 0;
+    uint32_t tunedWave = 0;  // 0: not tuned
+    float tunedGrid = 1.0f;
+    uint64_t tunedSceneGen = 0;
+};
+
 struct pt_ctx {
     int device = 0;
     int numSMs = 148;
@@ -146,6 +164,7 @@ struct pt_ctx {
     uint64_t sceneGen = 1, waveGen = 1;  // bumped when scene / wave buffers are replaced
     float sceneMin[3] = {0, 0, 0}, sceneMax[3] = {1, 1, 1};  // vertex bounds of the uploaded scene
     RadianceCache cache;
+    BatchState batch;
     // scratch of the batch entry points
     void *scratch = nullptr;
     size_t scratchBytes = 0;
@@ -249,3 +268,4 @@ cudaError_t rc_enqueue_targets(pt_ctx *ctx, cudaStream_t st, const float4 *lo_et
                                const float4 *pendA, const float4 *pendE);
 cudaError_t rc_enqueue_train(pt_ctx *ctx, cudaStream_t st);
 void pt_graph_free(pt_ctx *ctx);
+void pt_batch_free(pt_ctx *ctx);

@@ -25,6 +25,8 @@
 // reference traces NEE shadow rays before deciding whether to draw ratio
 // tracking samples (Emitter.hlsli:138-148); there shade traces its shadow
 // rays inline to keep that order.
+#include <algorithm>
+
 #include "pt_internal.h"
 
 namespace pt {
@@ -36,6 +38,14 @@ constexpr uint32_t kFlagTrain = 4u;     // training path
 constexpr uint32_t kFlagUnbiased = 8u;  // training path whose suffix does not use the cache
 constexpr uint32_t kFlagHasRec = 16u;   // its training record has been written
 constexpr int kBlock = 256;
+
+// One request of a batched render (pt_render_batch), in the device table.
+struct ReqDev {
+    uint64_t pathStart;  // first path id of the request in the batch's path order
+    uint32_t width, height, npix, spp, sampleOffset, maxDepth;
+    pt_camera cam;
+    float4 *sum, *comp;  // film (device memory)
+};
 
 struct WaveArgs {
     DevScene S;
@@ -66,6 +76,10 @@ struct WaveArgs {
     uint32_t *cqCount;
     float4 *cr[7];      // training records: 4 record float4, throughput, Lo so far, target
     uint32_t *crCount;
+    // batched render (batch != 0): requests and, per path slot, (pixel | request << 24, sample index)
+    uint32_t batch, numReqs;
+    const ReqDev *reqs;
+    uint2 *slotInfo;
 };
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
@@ -86,8 +100,8 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t *counter, bool pred) {
 // tiles (one warp's paths cover one tile: compact bundles of camera rays),
 // tiles row by row; pixels right of the last full tile column or below the
 // last full tile row follow in row-major order.  A bijection on [0, W*H).
-__device__ __forceinline__ uint32_t tile_pixel(const WaveArgs &A, uint32_t p) {
-    const uint32_t W = A.width, Wt = A.width / 8u, Ht = A.height / 4u;
+__device__ __forceinline__ uint32_t tile_pixel_wh(uint32_t W, uint32_t H, uint32_t p) {
+    const uint32_t Wt = W / 8u, Ht = H / 4u;
     const uint32_t full = 32u * Wt * Ht;
     if (p < full) {
         uint32_t t = p >> 5, w = p & 31u;
@@ -98,10 +112,38 @@ __device__ __forceinline__ uint32_t tile_pixel(const WaveArgs &A, uint32_t p) {
     q -= 4u * Ht * rw;
     return (4u * Ht + q / W) * W + q % W;
 }
+__device__ __forceinline__ uint32_t tile_pixel(const WaveArgs &A, uint32_t p) {
+    return tile_pixel_wh(A.width, A.height, p);
+}
+// Request of batch path id pid: the last request whose first path id <= pid.
+__device__ __forceinline__ uint32_t find_request(const WaveArgs &A, uint64_t pid) {
+    uint32_t lo = 0, hi = A.numReqs;
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (A.reqs[mid].pathStart <= pid) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
 __device__ __forceinline__ void path_coords(const WaveArgs &A, uint32_t slot, uint32_t &pix, uint32_t &frame) {
+    if (A.batch) {
+        uint2 si = A.slotInfo[slot];
+        pix = si.x & 0xFFFFFFu;
+        frame = si.y;
+        return;
+    }
     uint64_t pid = A.waveStart + slot;
     pix = tile_pixel(A, (uint32_t)(pid % A.npix));
     frame = __ldg(A.sampleOffset) + (uint32_t)(pid / A.npix);
+}
+// Per-request image size and depth of a path (the render's own without a batch).
+__device__ __forceinline__ uint32_t path_depth(const WaveArgs &A, uint32_t slot) {
+    return A.batch ? A.reqs[A.slotInfo[slot].x >> 24].maxDepth : A.maxDepth;
+}
+__device__ __forceinline__ uint2 path_image(const WaveArgs &A, uint32_t slot) {
+    if (!A.batch) return make_uint2(A.width, A.height);
+    const ReqDev &q = A.reqs[A.slotInfo[slot].x >> 24];
+    return make_uint2(q.width, q.height);
 }
 __device__ __forceinline__ Rng load_rng(const WaveArgs &A, uint32_t slot, uint4 st) {
     uint32_t pix, frame;
@@ -119,14 +161,27 @@ __device__ __forceinline__ Rng load_rng(const WaveArgs &A, uint32_t slot, uint4 
 __global__ void k_raygen(WaveArgs A) {
     uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= A.waveCount) return;
-    uint32_t pix, frame;
-    path_coords(A, slot, pix, frame);
-    uint32_t px = pix % A.width, py = pix / A.width;
-    Rng r = rng_init(pix, A.npix, frame, A.rngKind);
+    uint32_t pix, frame, W = A.width, H = A.height, npix = A.npix;
+    const pt_camera *cp = &A.cam;
+    if (A.batch) {  // the path's request, pixel and sample; kept per slot for the later kernels
+        uint64_t pid = A.waveStart + slot;
+        uint32_t q = find_request(A, pid);
+        const ReqDev &R = A.reqs[q];
+        W = R.width; H = R.height; npix = R.npix;
+        uint64_t local = pid - R.pathStart;
+        pix = tile_pixel_wh(W, H, (uint32_t)(local % npix));
+        frame = R.sampleOffset + (uint32_t)(local / npix);
+        A.slotInfo[slot] = make_uint2(pix | (q << 24), frame);
+        cp = &R.cam;
+    } else {
+        path_coords(A, slot, pix, frame);
+    }
+    uint32_t px = pix % W, py = pix / W;
+    Rng r = rng_init(pix, npix, frame, A.rngKind);
     float jx = next_float(r, A.S.sobol1), jy = next_float(r, A.S.sobol1);
-    float ux = ((float)px + jx) / (float)A.width;
-    float uy = 1.0f - ((float)py + jy) / (float)A.height;
-    const pt_camera &c = A.cam;
+    float ux = ((float)px + jx) / (float)W;
+    float uy = 1.0f - ((float)py + jy) / (float)H;
+    const pt_camera &c = *cp;
     float3 cpos = make_float3(c.pos[0], c.pos[1], c.pos[2]);
     float3 llc = make_float3(c.llc[0], c.llc[1], c.llc[2]);
     float3 hor = make_float3(c.horizontal[0], c.horizontal[1], c.horizontal[2]);
@@ -534,7 +589,10 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
                 if (back) Ng = -Ng;
                 if (dot(N, Ng) < 0.0f) N = -N;
                 if (TEX || (C == CLS_ANY && has_shading_textures(m)))
-                    apply_textures(S, m, mesh, prim, h4.x, i0, i1, i2, bx, by, N, A.width, A.height);
+                {
+                    const uint2 wh = path_image(A, slot);
+                    apply_textures(S, m, mesh, prim, h4.x, i0, i1, i2, bx, by, N, wh.x, wh.y);
+                }
                 // Radiance cache: the first surface vertex after a rough bounce ends
                 // the path (a query, resolved after the wave), or, with probability
                 // *trainProb, records its state there and the path goes on as a
@@ -679,7 +737,7 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
                 else thr = thr / v3(q);
             }
             st.z += 1u;
-            if (st.z >= A.maxDepth) cont = false;
+            if (st.z >= path_depth(A, slot)) cont = false;
             st.x = rng.dim;
             st.y = rng.white;
             A.thr_pdf[slot] = make_float4(thr.x, thr.y, thr.z, lastPdf);
@@ -731,6 +789,37 @@ __global__ void k_film(WaveArgs A, float4 *sum, float4 *comp) {
     }
     sum[pix] = s;
     comp[pix] = c;
+}
+
+// Film of request q for the paths of this wave (k_film's order: per pixel,
+// the wave's samples of the request in sample order).
+__global__ void k_film_req(WaveArgs A, uint32_t q) {
+    const ReqDev &R = A.reqs[q];
+    const uint64_t ps = R.pathStart, pe = R.pathStart + (uint64_t)R.npix * R.spp;
+    const uint64_t ws = A.waveStart, we = A.waveStart + A.waveCount;
+    const uint64_t lo = (ws > ps ? ws : ps) - ps, hi = (we < pe ? we : pe) - ps;
+    if (hi <= lo) return;
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= min(hi - lo, (uint64_t)R.npix)) return;
+    uint32_t pix = tile_pixel_wh(R.width, R.height, (uint32_t)((lo + t) % R.npix));
+    float4 s = R.sum[pix], c = R.comp[pix];
+    for (uint64_t l = lo + t; l < hi; l += R.npix) {
+        uint32_t slot = (uint32_t)(ps + l - ws);
+        float4 le = A.lo_eta[slot];
+        float3 L = make_float3(le.x, le.y, le.z);
+        if (A.rng[slot].w & kFlagPending) {
+            float4 pa = A.pendA[slot], pe4 = A.pendE[slot];
+            L += make_float3(pa.x, pa.y, pa.z);
+            L += make_float3(pe4.x, pe4.y, pe4.z);
+        }
+        if (isnan(L.x) || isnan(L.y) || isnan(L.z) || isinf(L.x) || isinf(L.y) || isinf(L.z)) L = v3(0.0f);
+        kahan(s.x, c.x, L.x);
+        kahan(s.y, c.y, L.y);
+        kahan(s.z, c.z, L.z);
+        kahan(s.w, c.w, 1.0f);
+    }
+    R.sum[pix] = s;
+    R.comp[pix] = c;
 }
 
 }  // namespace pt
@@ -823,9 +912,15 @@ struct Enqueue {
     }
 };
 
+// Grid sizes of the traversal and shading kernels (grid-stride loops).
+struct Grids {
+    int ext, extC, shadeI, shadow;
+    const int *cls;
+};
+
+// Raygen and `depth` bounces of one wave (A.waveStart / A.waveCount set).
 // Returns the first failing call's status (cudaSuccess if none).
-cudaError_t enqueue_render(const pt_ctx *ctx, Enqueue &E, WaveArgs A, const pt_render_params *P, size_t cap,
-                           uint64_t total, uint64_t npix, float *d_sum, float *d_comp) {
+cudaError_t enqueue_paths(const pt_ctx *ctx, Enqueue &E, WaveArgs &A, uint32_t depth, const Grids &G) {
     const WaveBuffers &B = ctx->W;
     const bool inl = ctx->S.numVols > 0;
     cudaStream_t st = E.st;
@@ -833,7 +928,55 @@ cudaError_t enqueue_render(const pt_ctx *ctx, Enqueue &E, WaveArgs A, const pt_r
     auto chk = [&](cudaError_t e) {
         if (err == cudaSuccess && e != cudaSuccess) err = e;
     };
+    A.qslotOut = B.qslot[0]; A.qoOut = B.qo[0]; A.qdOut = B.qd[0]; A.cntOut = B.counters + 0;
+    E.begin(STG_RAYGEN);
+    k_raygen<<<(A.waveCount + kBlock - 1) / kBlock, kBlock, 0, st>>>(A);
+    E.end();
+    int cur = 0;
+    for (uint32_t b = 0; b < depth; b++) {
+        A.qslotIn = B.qslot[cur]; A.qoIn = B.qo[cur]; A.qdIn = B.qd[cur]; A.cntIn = B.counters + cur;
+        A.qslotOut = B.qslot[1 - cur]; A.qoOut = B.qo[1 - cur]; A.qdOut = B.qd[1 - cur];
+        A.cntOut = B.counters + (1 - cur);
+        chk(cudaMemsetAsync(A.cntOut, 0, 4, st));
+        chk(cudaMemsetAsync(A.cntShadow, 0, 4, st));
+        if (inl) {
+            E.begin(STG_EXTEND);
+            k_extend<false><<<G.ext, kBlock, 0, st>>>(A);
+            E.end();
+            E.begin(STG_SHADE);
+            k_shade<true, CLS_ANY><<<G.shadeI, kBlock, 0, st>>>(A);
+            E.end();
+        } else {
+            chk(cudaMemsetAsync(A.cntCls, 0, CLS_N * sizeof(uint32_t), st));
+            E.begin(STG_EXTEND);
+            k_extend<true><<<G.extC, kBlock, 0, st>>>(A);
+            E.end();
+            for (int c = 0; c < CLS_N; c++) {
+                if (!((ctx->clsMask >> c) & 1u)) continue;
+                E.begin(STG_SHADE);
+                kShadeCls[c]<<<G.cls[c], kBlock, 0, st>>>(A);
+                E.end();
+            }
+            E.begin(STG_SHADOW);
+            k_shadow<<<G.shadow, kBlock, 0, st>>>(A);
+            E.end();
+        }
+        cur = 1 - cur;
+    }
+    return err;
+}
+
+// Returns the first failing call's status (cudaSuccess if none).
+cudaError_t enqueue_render(const pt_ctx *ctx, Enqueue &E, WaveArgs A, const pt_render_params *P, size_t cap,
+                           uint64_t total, uint64_t npix, float *d_sum, float *d_comp) {
+    const WaveBuffers &B = ctx->W;
+    cudaStream_t st = E.st;
+    cudaError_t err = cudaSuccess;
+    auto chk = [&](cudaError_t e) {
+        if (err == cudaSuccess && e != cudaSuccess) err = e;
+    };
     const bool cached = A.cacheOn != 0;
+    const Grids G{gExt, gExtC, gShadeI, gShadow, gCls};
     chk(cudaMemsetAsync(B.counters, 0, kCounterWords * sizeof(uint32_t), st));
     chk(cudaMemsetAsync(ctx->d_err, 0, 4, st));
     if (cached) {  // per-call cache counters: records [2], queries of the call [5], records with targets [6]
@@ -844,41 +987,7 @@ cudaError_t enqueue_render(const pt_ctx *ctx, Enqueue &E, WaveArgs A, const pt_r
         A.waveStart = ws;
         A.waveCount = (uint32_t)std::min<uint64_t>(cap, total - ws);
         if (cached) chk(cudaMemsetAsync(A.cqCount, 0, 4, st));
-        A.qslotOut = B.qslot[0]; A.qoOut = B.qo[0]; A.qdOut = B.qd[0]; A.cntOut = B.counters + 0;
-        E.begin(STG_RAYGEN);
-        k_raygen<<<(A.waveCount + kBlock - 1) / kBlock, kBlock, 0, st>>>(A);
-        E.end();
-        int cur = 0;
-        for (uint32_t b = 0; b < P->max_depth; b++) {
-            A.qslotIn = B.qslot[cur]; A.qoIn = B.qo[cur]; A.qdIn = B.qd[cur]; A.cntIn = B.counters + cur;
-            A.qslotOut = B.qslot[1 - cur]; A.qoOut = B.qo[1 - cur]; A.qdOut = B.qd[1 - cur];
-            A.cntOut = B.counters + (1 - cur);
-            chk(cudaMemsetAsync(A.cntOut, 0, 4, st));
-            chk(cudaMemsetAsync(A.cntShadow, 0, 4, st));
-            if (inl) {
-                E.begin(STG_EXTEND);
-                k_extend<false><<<gExt, kBlock, 0, st>>>(A);
-                E.end();
-                E.begin(STG_SHADE);
-                k_shade<true, CLS_ANY><<<gShadeI, kBlock, 0, st>>>(A);
-                E.end();
-            } else {
-                chk(cudaMemsetAsync(A.cntCls, 0, CLS_N * sizeof(uint32_t), st));
-                E.begin(STG_EXTEND);
-                k_extend<true><<<gExtC, kBlock, 0, st>>>(A);
-                E.end();
-                for (int c = 0; c < CLS_N; c++) {
-                    if (!((ctx->clsMask >> c) & 1u)) continue;
-                    E.begin(STG_SHADE);
-                    kShadeCls[c]<<<gCls[c], kBlock, 0, st>>>(A);
-                    E.end();
-                }
-                E.begin(STG_SHADOW);
-                k_shadow<<<gShadow, kBlock, 0, st>>>(A);
-                E.end();
-            }
-            cur = 1 - cur;
-        }
+        chk(enqueue_paths(ctx, E, A, P->max_depth, G));
         if (cached) {  // cache queries of this wave: lo_eta[slot] += throughput x cache
             E.begin(STG_CACHE);
             chk(rc_enqueue_resolve(const_cast<pt_ctx *>(ctx), st, A.lo_eta));
@@ -973,6 +1082,7 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
     A.rayTotals = (unsigned long long *)(B.counters + 4);
     A.err = ctx->d_err;
     A.shadowCap = (uint32_t)(2 * B.cap);
+    A.batch = 0; A.numReqs = 0; A.reqs = nullptr; A.slotInfo = nullptr;
     A.cacheOn = (P->flags & PT_RENDER_RADIANCE_CACHE) ? 1u : 0u;
     A.trainOn = A.unbiasedEvery = A.recCap = 0;
     A.roughThr = 0.0f;
@@ -1081,5 +1191,369 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
         stats->ms_film = stage[STG_FILM];
         stats->ms_cache = stage[STG_CACHE];
     }
+    return PT_OK;
+}
+
+// ===========================================================================
+// Batched requests
+// ===========================================================================
+void pt_batch_free(pt_ctx *ctx) {
+    BatchState &Bt = ctx->batch;
+    if (Bt.exec) cudaGraphExecDestroy(Bt.exec);
+    for (cudaEvent_t e : Bt.ev) cudaEventDestroy(e);
+    if (Bt.reqs) cudaFree(Bt.reqs);
+    if (Bt.slotInfo) cudaFree(Bt.slotInfo);
+    if (Bt.films) cudaFree(Bt.films);
+    ctx->batch = BatchState{};
+}
+
+namespace {
+struct BatchPlan {
+    std::vector<uint32_t> order;        // request index by path order (shortest first)
+    std::vector<uint64_t> start;        // first path id, path order
+    uint64_t total = 0;
+    size_t cap = 0;
+    std::vector<uint64_t> waveStart;
+    std::vector<uint32_t> waveDepth;
+    std::vector<std::vector<uint32_t>> waveReqs;  // requests (path order) with paths in the wave
+    std::vector<uint32_t> lastWave;     // per request (path order)
+};
+
+int batch_check(pt_ctx *ctx, const pt_request *R, uint32_t n) {
+    if (!n || n > PT_BATCH_MAX_REQUESTS) return ctx->fail(PT_E_INVALID, "batch size outside 1..PT_BATCH_MAX_REQUESTS");
+    for (uint32_t i = 0; i < n; i++) {
+        const pt_render_params &P = R[i].params;
+        const pt_film &F = R[i].film;
+        if (!P.width || !P.height || !P.spp || !P.max_depth) return ctx->fail(PT_E_INVALID, "empty request");
+        if ((uint64_t)P.width * P.height >= PT_BATCH_MAX_PIXELS)
+            return ctx->fail(PT_E_INVALID, "request above PT_BATCH_MAX_PIXELS pixels");
+        if (F.width != P.width || F.height != P.height || !F.sum || !F.comp)
+            return ctx->fail(PT_E_INVALID, "request film does not match");
+        if (P.rng_kind != R[0].params.rng_kind || P.env_sampling != R[0].params.env_sampling ||
+            P.flags != R[0].params.flags)
+            return ctx->fail(PT_E_INVALID, "rng_kind, env_sampling and flags must agree across a batch");
+        if (P.rng_kind > PT_RNG_PCG_HASH || P.env_sampling > PT_ENV_ALIAS) return ctx->fail(PT_E_INVALID, "bad enum");
+        if (P.flags & PT_RENDER_RADIANCE_CACHE) return ctx->fail(PT_E_UNSUPPORTED, "radiance cache in a batch");
+    }
+    return PT_OK;
+}
+
+BatchPlan batch_plan(const pt_request *R, uint32_t n, size_t cap) {
+    BatchPlan pl;
+    pl.order.resize(n);
+    for (uint32_t i = 0; i < n; i++) pl.order[i] = i;
+    auto paths = [&](uint32_t i) { return (uint64_t)R[i].params.width * R[i].params.height * R[i].params.spp; };
+    std::stable_sort(pl.order.begin(), pl.order.end(), [&](uint32_t a, uint32_t b) { return paths(a) < paths(b); });
+    for (uint32_t k = 0; k < n; k++) {
+        pl.start.push_back(pl.total);
+        pl.total += paths(pl.order[k]);
+    }
+    pl.cap = (size_t)std::min<uint64_t>(cap, pl.total);
+    pl.lastWave.assign(n, 0);
+    uint32_t k = 0;
+    for (uint64_t ws = 0; ws < pl.total; ws += pl.cap) {
+        const uint64_t we = std::min<uint64_t>(ws + pl.cap, pl.total);
+        std::vector<uint32_t> rq;
+        uint32_t depth = 0;
+        while (k < n && pl.start[k] + paths(pl.order[k]) <= ws) k++;
+        for (uint32_t j = k; j < n && pl.start[j] < we; j++) {
+            rq.push_back(j);
+            depth = std::max(depth, R[pl.order[j]].params.max_depth);
+            pl.lastWave[j] = (uint32_t)pl.waveStart.size();
+        }
+        pl.waveStart.push_back(ws);
+        pl.waveDepth.push_back(depth);
+        pl.waveReqs.push_back(rq);
+    }
+    return pl;
+}
+
+cudaError_t enqueue_batch(const pt_ctx *ctx, Enqueue &E, WaveArgs A, const BatchPlan &pl, const Grids &G,
+                          const ReqDev *hostReqs, const std::vector<cudaEvent_t> &ev, const char **where) {
+    const WaveBuffers &B = ctx->W;
+    cudaStream_t st = E.st;
+    cudaError_t err = cudaSuccess;
+    const char *at = "";
+    auto chk = [&](cudaError_t e, const char *w = "") {
+        if (err == cudaSuccess && e != cudaSuccess) { err = e; at = w; }
+    };
+    chk(cudaMemsetAsync(B.counters, 0, kCounterWords * sizeof(uint32_t), st), "memset counters");
+    chk(cudaMemsetAsync(ctx->d_err, 0, 4, st), "memset err");
+    for (size_t w = 0; w < pl.waveStart.size(); w++) {
+        A.waveStart = pl.waveStart[w];
+        A.waveCount = (uint32_t)std::min<uint64_t>(pl.cap, pl.total - A.waveStart);
+        chk(enqueue_paths(ctx, E, A, pl.waveDepth[w], G), "paths");
+        for (uint32_t j : pl.waveReqs[w]) {
+            const ReqDev &R = hostReqs[j];
+            const uint64_t ps = R.pathStart, pe = ps + (uint64_t)R.npix * R.spp;
+            const uint64_t lo = std::max<uint64_t>(A.waveStart, ps), hi = std::min<uint64_t>(A.waveStart + A.waveCount, pe);
+            const uint64_t cover = std::min<uint64_t>(hi - lo, R.npix);
+            E.begin(STG_FILM);
+            k_film_req<<<(unsigned)((cover + kBlock - 1) / kBlock), kBlock, 0, st>>>(A, j);
+            E.end();
+            chk(cudaGetLastError(), "film launch");
+        }
+        // an external record node: the event is recorded when the graph runs
+        // (a plain record inside a capture is only an ordering edge)
+        chk(cudaEventRecordWithFlags(ev[w], st, cudaEventRecordExternal), "event record");
+        chk(cudaGetLastError(), "wave launches");
+    }
+    if (where) *where = at;
+    return err;
+}
+
+// One batch: plan, staging of host films, graph (re)capture, launch, timings.
+// tuneFilm != nullptr: every request renders into that device scratch film
+// (autotuning), the callers' films are untouched.
+int render_batch(pt_ctx *ctx, const pt_request *R, uint32_t n, float *request_ms, pt_stats *stats, size_t capIn,
+                 float gridScale, float *tuneFilm, float *msOut) {
+    int rc = batch_check(ctx, R, n);
+    if (rc) return rc;
+    cudaSetDevice(ctx->device);
+    BatchState &Bt = ctx->batch;
+    uint64_t total = 0;
+    for (uint32_t i = 0; i < n; i++) total += (uint64_t)R[i].params.width * R[i].params.height * R[i].params.spp;
+    size_t cap = capIn ? capIn : R[0].params.wave_paths;
+    if (!cap && Bt.tunedWave && Bt.tunedSceneGen == ctx->sceneGen) cap = Bt.tunedWave;
+    if (!cap) cap = (size_t)std::min<uint64_t>(total, kMaxWavePaths);
+    cap = (size_t)std::min<uint64_t>(cap, total);
+    if (cap > ctx->W.cap) {  // grow within half the free memory, as a single render does
+        size_t freeB = 0, totalB = 0;
+        if (cudaMemGetInfo(&freeB, &totalB) != cudaSuccess) freeB = (size_t)4 << 30;
+        size_t fit = (freeB / 2 + ctx->W.cap * kWaveBytesPerPath / 2) / (kWaveBytesPerPath + 8);
+        cap = std::max<size_t>(std::min(cap, fit), std::min<size_t>(cap, (size_t)1 << 16));
+    }
+    if ((rc = wave_alloc(ctx, cap))) return rc;
+    if (Bt.slotCap < cap) {
+        if (Bt.slotInfo) cudaFree(Bt.slotInfo);
+        Bt.slotInfo = nullptr;
+        Bt.slotCap = 0;
+        if (cudaMalloc(&Bt.slotInfo, cap * sizeof(uint2)) != cudaSuccess) return ctx->fail(PT_E_NOMEM, "batch slots");
+        Bt.slotCap = cap;
+    }
+    if (!Bt.reqs && cudaMalloc(&Bt.reqs, PT_BATCH_MAX_REQUESTS * sizeof(ReqDev)) != cudaSuccess)
+        return ctx->fail(PT_E_NOMEM, "batch request table");
+    if (!gExt) {
+        gExt = grid_for(ctx, (const void *)k_extend<false>);
+        gExtC = grid_for(ctx, (const void *)k_extend<true>);
+        gShadeI = grid_for(ctx, (const void *)k_shade<true, CLS_ANY>);
+        gShadow = grid_for(ctx, (const void *)k_shadow);
+        for (int c = 0; c < CLS_N; c++) gCls[c] = grid_for(ctx, (const void *)kShadeCls[c]);
+    }
+    if (gridScale <= 0.0f) gridScale = (Bt.tunedWave && Bt.tunedSceneGen == ctx->sceneGen) ? Bt.tunedGrid : 1.0f;
+    auto sc = [&](int g) { return std::max(ctx->numSMs, (int)((float)g * gridScale)); };
+    int clsG[CLS_N];
+    for (int c = 0; c < CLS_N; c++) clsG[c] = sc(gCls[c]);
+    const Grids G{sc(gExt), sc(gExtC), sc(gShadeI), sc(gShadow), clsG};
+
+    const BatchPlan pl = batch_plan(R, n, cap);
+    // films: the callers' device films, device copies of host films, or the tuning scratch
+    size_t stage = 0;
+    for (uint32_t i = 0; i < n; i++)
+        if (!tuneFilm && R[i].film.location == PT_MEM_HOST) stage += 2 * (size_t)R[i].params.width * R[i].params.height * 16;
+    if (stage > Bt.filmBytes) {
+        if (Bt.films) cudaFree(Bt.films);
+        Bt.films = nullptr;
+        Bt.filmBytes = 0;
+        if (cudaMalloc(&Bt.films, stage) != cudaSuccess) return ctx->fail(PT_E_NOMEM, "batch film staging");
+        Bt.filmBytes = stage;
+    }
+    std::vector<ReqDev> hostReqs(n);
+    std::vector<float *> devSum(n), devComp(n);
+    size_t off = 0;
+    for (uint32_t k = 0; k < n; k++) {
+        const uint32_t i = pl.order[k];
+        const pt_render_params &P = R[i].params;
+        const size_t bytes = (size_t)P.width * P.height * 16;
+        float *ds = R[i].film.sum, *dc = R[i].film.comp;
+        if (tuneFilm) {
+            ds = tuneFilm;
+            dc = tuneFilm + 4 * (size_t)P.width * P.height;
+        } else if (R[i].film.location == PT_MEM_HOST) {
+            ds = (float *)((char *)Bt.films + off);
+            dc = (float *)((char *)Bt.films + off + bytes);
+            off += 2 * bytes;
+            PT_CUDA(cudaMemcpyAsync(ds, R[i].film.sum, bytes, cudaMemcpyHostToDevice, ctx->stream));
+            PT_CUDA(cudaMemcpyAsync(dc, R[i].film.comp, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        }
+        devSum[i] = ds;
+        devComp[i] = dc;
+        ReqDev &q = hostReqs[k];
+        q.pathStart = pl.start[k];
+        q.width = P.width; q.height = P.height; q.npix = P.width * P.height; q.spp = P.spp;
+        q.sampleOffset = P.sample_offset; q.maxDepth = P.max_depth;
+        q.cam = P.camera;
+        q.sum = (float4 *)ds;
+        q.comp = (float4 *)dc;
+    }
+    while (Bt.ev.size() < pl.waveStart.size()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return ctx->fail(PT_E_CUDA, "batch events");
+        Bt.ev.push_back(e);
+    }
+    WaveBuffers &B = ctx->W;
+    WaveArgs A;
+    memset(&A, 0, sizeof(A));
+    A.S = ctx->S;
+    A.width = hostReqs[0].width; A.height = hostReqs[0].height; A.npix = hostReqs[0].npix;
+    A.sampleOffset = ctx->d_err + 1;
+    A.rngKind = R[0].params.rng_kind; A.envMode = R[0].params.env_sampling; A.maxDepth = 0;
+    A.thr_pdf = B.thr_pdf; A.lo_eta = B.lo_eta; A.pendA = B.pendA; A.pendE = B.pendE; A.rng = B.rng;
+    A.qhit = B.qhit;
+    A.sslot = B.sslot; A.so = B.so; A.sd = B.sd; A.sX = B.sX; A.sthr = B.sthr;
+    A.cntShadow = B.counters + 2;
+    A.cntCls = B.counters + 8;
+    A.cls = B.cls;
+    A.clsStride = (uint32_t)B.cap;
+    A.rayTotals = (unsigned long long *)(B.counters + 4);
+    A.err = ctx->d_err;
+    A.shadowCap = (uint32_t)(2 * B.cap);
+    A.batch = 1; A.numReqs = n; A.reqs = (const ReqDev *)Bt.reqs; A.slotInfo = Bt.slotInfo;
+    // the launch graph depends on the batch's shape, not on cameras, offsets or films (device table)
+    std::vector<uint64_t> key = {n, pl.cap, R[0].params.rng_kind, R[0].params.env_sampling, ctx->sceneGen,
+                                 ctx->waveGen, (uint64_t)(uintptr_t)Bt.slotInfo, (uint64_t)(uint32_t)G.extC,
+                                 (uint64_t)(uint32_t)G.shadow, (uint64_t)(uint32_t)clsG[CLS_DISNEY]};
+    for (uint32_t k = 0; k < n; k++) {
+        key.push_back(hostReqs[k].width | ((uint64_t)hostReqs[k].height << 32));
+        key.push_back(hostReqs[k].spp | ((uint64_t)hostReqs[k].maxDepth << 32));
+    }
+    if (!Bt.exec || Bt.key != key) {
+        if (Bt.exec) cudaGraphExecDestroy(Bt.exec);
+        Bt.exec = nullptr;
+        Enqueue E{ctx->ownStream, false, {}, 0};
+        cudaGraph_t g = nullptr;
+        const char *step = "begin capture";
+        cudaError_t ce = cudaStreamBeginCapture(ctx->ownStream, cudaStreamCaptureModeThreadLocal);
+        if (ce == cudaSuccess) {
+            const char *at = "";
+            cudaError_t qe = enqueue_batch(ctx, E, A, pl, G, hostReqs.data(), Bt.ev, &at);
+            ce = cudaStreamEndCapture(ctx->ownStream, &g);
+            step = "end capture";
+            if (ce == cudaSuccess && qe != cudaSuccess) {
+                ce = qe;
+                step = at;
+            }
+        }
+        if (ce == cudaSuccess) {
+            ce = cudaGraphInstantiate(&Bt.exec, g, 0);
+            step = "instantiate";
+        }
+        if (g) cudaGraphDestroy(g);
+        if (ce != cudaSuccess) {
+            cudaGetLastError();
+            Bt.exec = nullptr;
+            std::string what = std::string("batch graph capture (") + step + ")";
+            return ctx->fail(PT_E_CUDA, what.c_str(), cudaGetErrorString(ce));
+        }
+        Bt.key = key;
+        Bt.launches = E.launches;
+    }
+    cudaStream_t st = ctx->stream;
+    PT_CUDA(cudaMemcpyAsync(Bt.reqs, hostReqs.data(), n * sizeof(ReqDev), cudaMemcpyHostToDevice, st));
+    cudaEventRecord(ctx->ev[0], st);
+    PT_CUDA(cudaGraphLaunch(Bt.exec, st));
+    cudaEventRecord(ctx->ev[1], st);
+    uint32_t hostCnt[kCounterWords];
+    PT_CUDA(cudaMemcpyAsync(hostCnt, B.counters, sizeof(hostCnt), cudaMemcpyDeviceToHost, st));
+    uint32_t derr = 0;
+    PT_CUDA(cudaMemcpyAsync(&derr, ctx->d_err, 4, cudaMemcpyDeviceToHost, st));
+    if (!tuneFilm)
+        for (uint32_t i = 0; i < n; i++)
+            if (R[i].film.location == PT_MEM_HOST) {
+                const size_t bytes = (size_t)R[i].params.width * R[i].params.height * 16;
+                PT_CUDA(cudaMemcpyAsync(R[i].film.sum, devSum[i], bytes, cudaMemcpyDeviceToHost, st));
+                PT_CUDA(cudaMemcpyAsync(R[i].film.comp, devComp[i], bytes, cudaMemcpyDeviceToHost, st));
+            }
+    cudaError_t se = cudaStreamSynchronize(st);
+    if (se != cudaSuccess) return ctx->fail(PT_E_CUDA, "batch render", cudaGetErrorString(se));
+    if (derr)
+        return ctx->fail(PT_E_DEVICE, (derr & PT_DEVERR_STACK) ? "traversal stack overflow"
+                                      : (derr & PT_DEVERR_BVH) ? "traversal visited more nodes than the BVH has"
+                                                               : "queue overflow");
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
+    if (msOut) *msOut = ms;
+    if (request_ms)
+        for (uint32_t k = 0; k < n; k++) {
+            float t = 0.0f;
+            if (cudaEventElapsedTime(&t, ctx->ev[0], Bt.ev[pl.lastWave[k]]) != cudaSuccess) {
+                cudaGetLastError();
+                return ctx->fail(PT_E_CUDA, "batch request timing");
+            }
+            request_ms[pl.order[k]] = t;
+        }
+    if (stats) {
+        unsigned long long tot[2];
+        memcpy(tot, hostCnt + 4, sizeof(tot));
+        memset(stats, 0, sizeof(*stats));
+        stats->paths = pl.total;
+        stats->extension_rays = tot[0];
+        stats->shadow_rays = tot[1];
+        stats->waves = pl.waveStart.size();
+        uint64_t bounces = 0;
+        for (uint32_t d : pl.waveDepth) bounces += d;
+        stats->bounces = bounces;
+        stats->launches = Bt.launches;
+        stats->ms_total = ms;
+    }
+    return PT_OK;
+}
+}  // namespace
+
+extern "C" int pt_render_batch(pt_ctx *ctx, const pt_request *requests, uint32_t n, float *request_ms,
+                               pt_stats *stats) {
+    if (!ctx) return PT_E_INVALID;
+    if (!requests) return ctx->fail(PT_E_INVALID, "null requests");
+    if (!ctx->hasScene) return ctx->fail(PT_E_NOSCENE, "no scene uploaded");
+    return render_batch(ctx, requests, n, request_ms, stats, 0, 0.0f, nullptr, nullptr);
+}
+
+extern "C" int pt_batch_autotune(pt_ctx *ctx, const pt_request *requests, uint32_t n, pt_batch_tuning *out) {
+    if (!ctx) return PT_E_INVALID;
+    if (!requests || !out) return ctx->fail(PT_E_INVALID, "null argument");
+    if (!ctx->hasScene) return ctx->fail(PT_E_NOSCENE, "no scene uploaded");
+    int rc = batch_check(ctx, requests, n);
+    if (rc) return rc;
+    cudaSetDevice(ctx->device);
+    uint64_t total = 0, maxPix = 0;
+    for (uint32_t i = 0; i < n; i++) {
+        total += (uint64_t)requests[i].params.width * requests[i].params.height * requests[i].params.spp;
+        maxPix = std::max<uint64_t>(maxPix, (uint64_t)requests[i].params.width * requests[i].params.height);
+    }
+    float *film = nullptr;
+    if (cudaMalloc(&film, maxPix * 32) != cudaSuccess) return ctx->fail(PT_E_NOMEM, "tuning film");
+    // candidates: wave sizes from the whole batch down to 2^22 paths, full and half traversal grids
+    std::vector<size_t> waves;
+    for (uint64_t w = std::min<uint64_t>(total, kMaxWavePaths);; w >>= 1) {
+        waves.push_back((size_t)w);
+        if (w <= ((uint64_t)1 << 22) || waves.size() == 4) break;
+    }
+    const float grids[2] = {1.0f, 0.5f};
+    memset(out, 0, sizeof(*out));
+    float best = 1e30f;
+    for (size_t w : waves)
+        for (float g : grids) {
+            float ms = 0.0f;
+            for (int rep = 0; rep < 2 && rc == PT_OK; rep++)  // the first run captures the graph
+                rc = render_batch(ctx, requests, n, nullptr, nullptr, w, g, film, &ms);
+            if (rc) break;
+            if (out->candidates < 16) {
+                out->candidate_ms[out->candidates] = ms;
+                out->candidate_wave[out->candidates] = (uint32_t)std::min<uint64_t>(w, total);
+                out->candidate_grid[out->candidates] = g;
+                out->candidates++;
+            }
+            if (ms < best) {
+                best = ms;
+                out->wave_paths = (uint32_t)std::min<uint64_t>(w, total);
+                out->traversal_grid = g;
+                out->ms = ms;
+            }
+        }
+    cudaFree(film);
+    if (rc) return rc;
+    ctx->batch.tunedWave = out->wave_paths;
+    ctx->batch.tunedGrid = out->traversal_grid;
+    ctx->batch.tunedSceneGen = ctx->sceneGen;
     return PT_OK;
 }

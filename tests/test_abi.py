@@ -38,9 +38,10 @@ def test_struct_layouts_match_c(pt):
 #include <stddef.h>
 #include "pt.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(pt_material), sizeof(pt_volume),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(pt_material), sizeof(pt_volume),
          sizeof(pt_grid), sizeof(pt_scene_desc), sizeof(pt_camera), sizeof(pt_render_params), sizeof(pt_film),
-         sizeof(pt_stats), sizeof(pt_hit), sizeof(pt_texture), sizeof(pt_cache_params), sizeof(pt_cache_stats));
+         sizeof(pt_stats), sizeof(pt_hit), sizeof(pt_texture), sizeof(pt_cache_params), sizeof(pt_cache_stats),
+         sizeof(pt_request), sizeof(pt_batch_tuning));
   printf("%zu %zu %zu %zu %zu\n", offsetof(pt_material, roughness), offsetof(pt_scene_desc, env_rgb),
          offsetof(pt_render_params, camera), offsetof(pt_scene_desc, textures), offsetof(pt_texture, srgb));
   return 0;
@@ -56,7 +57,7 @@ int main(void) {
     offs = [int(x) for x in out[1].split()]
     py = [C.sizeof(t) for t in (pt.pt_material, pt.pt_volume, pt.pt_grid, pt.pt_scene_desc, pt.pt_camera,
                                 pt.pt_render_params, pt.pt_film, pt.pt_stats, pt.pt_hit, pt.pt_texture,
-                                pt.pt_cache_params, pt.pt_cache_stats)]
+                                pt.pt_cache_params, pt.pt_cache_stats, pt.pt_request, pt.pt_batch_tuning)]
     assert sizes == py
     assert offs == [pt.pt_material.roughness.offset, pt.pt_scene_desc.env_rgb.offset,
                     pt.pt_render_params.camera.offset, pt.pt_scene_desc.textures.offset, pt.pt_texture.srgb.offset]
