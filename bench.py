@@ -145,6 +145,8 @@ EXTEND_DRAM_BYTES_PER_RAY = {"disney_envmap": 73.1}
 REF_SPP = 4096        # reference image: plain path tracing, samples [0, 4096)
 TTQ_TARGET = 1e-2     # relMSE bar
 TTQ_OFFSET = 1 << 20  # progressive renders draw samples from here on (independent of the reference)
+# relMSE is checked at accumulated spp ~ 2^(k/2) (both forms, same points)
+TTQ_CHECKS = sorted({int(round(2 ** (k / 2))) for k in range(0, 21)})
 
 
 def relmse(x, ref):
@@ -167,14 +169,15 @@ def progressive(pt, ctx, stream, W, H, ref_img, make_params, spf, warm=0):
     """Progressive accumulation (the reference's frame-by-frame accumulation):
     render calls of `spf` samples, the first `warm` of them into a discarded
     film (cache training only), every call timed with CUDA events on the
-    stream.  relMSE against ref_img at 1, 2, 4, ... accumulated spp (outside
-    the timing); the first point at or below the bar gives the time."""
+    stream.  relMSE against ref_img at the TTQ_CHECKS points (outside the
+    timing); the first point at or below the bar gives the time."""
     import torch
 
     D = importlib.import_module("pbrt_b200.distributed")
     film = D.new_film(H, W, device="cuda")
     scratch = D.new_film(H, W, device="cuda") if warm else None
-    calls, acc, total_ms, curve, reached, check = 0, 0, 0.0, [], None, spf
+    calls, acc, total_ms, curve, reached = 0, 0, 0.0, [], None
+    checks = [c for c in TTQ_CHECKS if c >= spf]
     while acc < REF_SPP // 4:
         P = make_params(TTQ_OFFSET + calls * spf)
         tgt = scratch if calls < warm else film
@@ -189,13 +192,14 @@ def progressive(pt, ctx, stream, W, H, ref_img, make_params, spf, warm=0):
         if calls <= warm:
             continue
         acc += spf
-        if acc >= check:
+        if checks and acc >= checks[0]:
+            while checks and acc >= checks[0]:
+                checks.pop(0)
             e = relmse(D.resolve(film), ref_img)
             curve.append([acc, round(e, 6), round(total_ms / 1e3, 5)])
             if e <= TTQ_TARGET:
                 reached = (acc, total_ms / 1e3)
                 break
-            check *= 2
     return {"seconds": None if reached is None else round(reached[1], 5),
             "spp": None if reached is None else reached[0], "curve": curve}
 
@@ -210,18 +214,20 @@ CACHE_FRACTION, CACHE_ROUGH = 0.1, 0.1
 
 def time_to_relmse(pt, ctx, stream, W, H, cam, depth, env_mode, chunk):
     """Device time for plain and radiance-cached path tracing to reach relMSE
-    <= 1e-2 against a 4096-spp plain render of the same scene.  Plain:
-    progressive renders of 1, 2, 4, ... spp (doubling calls).  Cached:
+    <= 1e-2 against a 4096-spp plain render of the same scene, checked at
+    accumulated spp 1, 2, 3, 4, 6, 8, 11, ... (~2^(k/2)) in both forms.
+    Plain: one render call per check point (calls grow with it).  Cached:
     CACHE_SPF-spp calls with training steps in each, from an untrained cache
     (training time and the warm-up calls are inside the timed total)."""
     ref_img = reference_image(pt, ctx, W, H, cam, depth, env_mode, chunk)
 
-    # plain: doubling render calls
+    # plain: render calls that bring the accumulated spp to each check point
     D = importlib.import_module("pbrt_b200.distributed")
     import torch
     film = D.new_film(H, W, device="cuda")
-    done, total_ms, curve, reached, add = 0, 0.0, [], None, 1
-    while done < REF_SPP // 4:
+    done, total_ms, curve, reached = 0, 0.0, [], None
+    for nxt in TTQ_CHECKS:
+        add = nxt - done
         P = pt.render_params(W, H, add, cam, max_depth=depth, sample_offset=TTQ_OFFSET + done, env_sampling=env_mode)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
@@ -236,7 +242,6 @@ def time_to_relmse(pt, ctx, stream, W, H, cam, depth, env_mode, chunk):
         if e <= TTQ_TARGET:
             reached = (done, total_ms / 1e3)
             break
-        add = done
     plain = {"seconds": None if reached is None else round(reached[1], 5),
              "spp": None if reached is None else reached[0], "curve": curve}
 
@@ -323,6 +328,80 @@ def cache_kernel_roofline(pt, ctx):
     return out
 
 
+BATCH_STEPS = 3
+
+
+def batched_requests_run(pt):
+    """Configuration 4: 32 requests over the Cornell box and the Disney spheres
+    (random cameras, sides log-uniform 64..1024, spp U{4..256}).  Each
+    scene's requests form one batch (pt_render_batch: one wavefront, one
+    captured graph); the two batches run concurrently, each on its own
+    context and stream (one host thread per context).  Launch shapes come
+    from pt_batch_autotune (untimed); then 1 warm-up and BATCH_STEPS timed
+    batch pairs.  Device time per step = the longer batch (both start
+    together); per-request latency = device time from its batch's start to
+    the end of the wave that finished it."""
+    import torch
+
+    scenes = importlib.import_module("pbrt_b200.scenes")
+    reqs = scenes.batch_requests(32, seed=0)
+    built = {"cornell": scenes.cornell(256, 256)[0], "disney_envmap": scenes.disney_spheres(1280, 720)[0]}
+    groups = {}
+    for q in reqs:
+        groups.setdefault(q["scene"], []).append(q)
+    runs = []
+    for name, qs in groups.items():
+        ctx = pt.Context(0)
+        ctx.upload(built[name])
+        params = [pt.render_params(q["width"], q["height"], q["spp"], q["camera"], max_depth=q["max_depth"])
+                  for q in qs]
+        films = [(torch.zeros((q["height"], q["width"], 4), device="cuda"),
+                  torch.zeros((q["height"], q["width"], 4), device="cuda")) for q in qs]
+        ptrs = [(a.data_ptr(), b.data_ptr()) for a, b in films]
+        tune = ctx.batch_autotune(params, ptrs, pt.PT_MEM_DEVICE)
+        runs.append({"name": name, "ctx": ctx, "params": params, "films": films, "ptrs": ptrs, "tune": tune})
+
+    def one(r, off, res):
+        for P in r["params"]:
+            P.sample_offset = off
+        _, ms, st = r["ctx"].render_batch(r["params"], r["ptrs"], pt.PT_MEM_DEVICE)
+        res[r["name"]] = (ms, st)
+
+    steps = []
+    for k in range(BATCH_STEPS + 1):
+        res = {}
+        th = [threading.Thread(target=one, args=(r, 1000 * k, res)) for r in runs]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        if k:
+            steps.append(res)
+    paths = sum(P.width * P.height * P.spp for r in runs for P in r["params"])
+    step_ms = [max(st.ms_total for _, st in res.values()) for res in steps]
+    lat = np.concatenate([ms for res in steps for ms, _ in res.values()])
+    out = {
+        "workload": "32 requests: cornell 256^2 scene (depth 8) + disney_envmap scene (depth 16), random cameras, "
+                    "sides log-uniform 64..1024, spp U{4..256}, seed 0",
+        "requests": {r["name"]: len(r["params"]) for r in runs},
+        "paths_per_step": int(paths),
+        "steps": BATCH_STEPS,
+        "ms_per_step": round(float(np.mean(step_ms)), 3),
+        "mpaths_per_s": round(paths / (float(np.mean(step_ms)) / 1e3) / 1e6, 2),
+        "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 3), "p99": round(float(np.percentile(lat, 99)), 3),
+                       "max": round(float(lat.max()), 3)},
+        "launches": {r["name"]: int(steps[-1][r["name"]][1].launches) for r in runs},
+        "waves": {r["name"]: int(steps[-1][r["name"]][1].waves) for r in runs},
+        "autotune": {r["name"]: {"wave_paths": r["tune"].wave_paths, "traversal_grid": r["tune"].traversal_grid,
+                                 "candidates": [[int(r["tune"].candidate_wave[i]), float(r["tune"].candidate_grid[i]),
+                                                 round(float(r["tune"].candidate_ms[i]), 3)]
+                                                for i in range(r["tune"].candidates)]} for r in runs},
+    }
+    for r in runs:
+        r["ctx"].close()
+    return out
+
+
 def cpu_reference_run(pt, sc, cam, W, H, depth, seconds=15.0, prefer_reference=True):
     """Time the CPU implementation on a bounded sample of the workload:
     whole frames at 1 spp (the reference's one-sample dispatch), repeated
@@ -387,6 +466,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--wave-paths", type=int, default=0, help="paths in flight per wave (0 = library default)")
     ap.add_argument("--no-ttq", action="store_true", help="skip the time-to-relMSE measurement")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-requests measurement")
     ap.add_argument("--cache-kernels-only", action="store_true",
                     help="only the radiance-cache network kernels' roofline (profiling of those kernels)")
     args = ap.parse_args()
@@ -545,6 +625,8 @@ def main():
     if world == 1 and not args.no_ttq:
         line["time_to_relmse"] = time_to_relmse(pt, ctx, stream, W, H, cam, depth, env_mode, max(spp, 64))
         line["cache_roofline"] = cache_kernel_roofline(pt, ctx)
+    if world == 1 and not args.no_batch:
+        line["batched"] = batched_requests_run(pt)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, kind, cores, sample = cpu_reference_run(pt, sc, cam, W, H, depth, seconds=args.cpu_seconds)
         line["cpu_baseline"] = {"value": round(v, 4), "unit": "Mpaths/s", "cores": cores, "kind": kind,

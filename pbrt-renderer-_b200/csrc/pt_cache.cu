@@ -155,6 +155,7 @@ struct RcInferArgs {
     const float4 *qw;  // per query: throughput weight
     float *out;
     float4 *lo_eta;
+    float4 *recCache;  // cache value at training-record vertices (queries tagged with bit 31)
 };
 template <int MODE>
 __global__ void __launch_bounds__(kRcThreads) k_rc_infer(RcInferArgs a) {
@@ -204,13 +205,18 @@ __global__ void __launch_bounds__(kRcThreads) k_rc_infer(RcInferArgs a) {
                         a.out[3 * (size_t)row + 1] = v[1];
                         a.out[3 * (size_t)row + 2] = v[2];
                     } else {
-                        uint32_t slot = __float_as_uint(a.qry.r1[row].w);
-                        float4 w = a.qw[row], le = a.lo_eta[slot];
-                        // Lo += throughput * cache, rounded as two operations (no FMA)
-                        le.x = __fadd_rn(le.x, __fmul_rn(w.x, fmaxf(v[0], 0.0f)));
-                        le.y = __fadd_rn(le.y, __fmul_rn(w.y, fmaxf(v[1], 0.0f)));
-                        le.z = __fadd_rn(le.z, __fmul_rn(w.z, fmaxf(v[2], 0.0f)));
-                        a.lo_eta[slot] = le;
+                        const uint32_t tag = __float_as_uint(a.qry.r1[row].w);
+                        if (tag & 0x80000000u) {  // a training record's vertex: keep the value
+                            a.recCache[tag & 0x7FFFFFFFu] =
+                                make_float4(fmaxf(v[0], 0.0f), fmaxf(v[1], 0.0f), fmaxf(v[2], 0.0f), 0.0f);
+                        } else {
+                            float4 w = a.qw[row], le = a.lo_eta[tag];
+                            // Lo += throughput * cache, rounded as two operations (no FMA)
+                            le.x = __fadd_rn(le.x, __fmul_rn(w.x, fmaxf(v[0], 0.0f)));
+                            le.y = __fadd_rn(le.y, __fmul_rn(w.y, fmaxf(v[1], 0.0f)));
+                            le.z = __fadd_rn(le.z, __fmul_rn(w.z, fmaxf(v[2], 0.0f)));
+                            a.lo_eta[tag] = le;
+                        }
                     }
                 }
             }
@@ -396,7 +402,7 @@ __global__ void __launch_bounds__(1024) k_rc_adam(RcAdamArgs a) {
         if (a.updateProb) {
             // training chance of the next call: about nrecCap records out of
             // this call's cache vertices (queries + records)
-            float verts = (float)a.ctr[5] + (float)tot;
+            float verts = (float)a.ctr[5];  // every cache vertex made a query (training ones too)
             reinterpret_cast<float *>(a.ctr)[7] = verts > 0.0f ? fminf(a.maxFrac, (float)a.nrecCap / verts) : a.maxFrac;
         }
     }
@@ -442,9 +448,11 @@ __global__ void k_rc_images(const float *w, uint8_t *imgTrain, uint8_t *imgInfer
 // Training targets of the records written in this wave: the radiance the
 // path gathered after its record vertex, divided by the throughput there.
 // One CTA; records [ctr[6], count) belong to the wave that just ended.
+// The training path then takes the value a terminated path would have there,
+// prefix + throughput x cache (lo_eta), with its pending NEE dropped.
 __global__ void __launch_bounds__(1024) k_rc_targets(RcRows<1> rec, float4 *beta, float4 *lo0, float4 *tgt,
-                                                    uint32_t *ctr, const float4 *lo_eta, const uint4 *rng,
-                                                    const float4 *pendA, const float4 *pendE) {
+                                                    const float4 *recCache, uint32_t *ctr, float4 *lo_eta,
+                                                    uint4 *rng, const float4 *pendA, const float4 *pendE) {
     __shared__ uint32_t s0, s1;
     if (threadIdx.x == 0) {
         s0 = ctr[6];
@@ -468,6 +476,12 @@ __global__ void __launch_bounds__(1024) k_rc_targets(RcRows<1> rec, float4 *beta
             o[k] = isfinite(x) ? fmaxf(x, 0.0f) : 0.0f;
         }
         tgt[r] = make_float4(o[0], o[1], o[2], 0.0f);
+        const float4 cv = recCache[r];
+        lo_eta[slot] = make_float4(__fadd_rn(l0.x, __fmul_rn(b.x, cv.x)), __fadd_rn(l0.y, __fmul_rn(b.y, cv.y)),
+                                   __fadd_rn(l0.z, __fmul_rn(b.z, cv.z)), le.w);
+        uint4 st = rng[slot];
+        st.w &= ~1u;
+        rng[slot] = st;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -560,14 +574,16 @@ cudaError_t rc_enqueue_resolve(pt_ctx *ctx, cudaStream_t st, float4 *lo_eta) {
     a.qry.cap = (uint32_t)C.queryCap;
     a.qw = C.q[4];
     a.lo_eta = lo_eta;
+    a.recCache = C.rec[7];
     k_rc_infer<1><<<ctx->numSMs * 3, kRcThreads, kInferSmem, st>>>(a);
     return cudaGetLastError();
 }
-cudaError_t rc_enqueue_targets(pt_ctx *ctx, cudaStream_t st, const float4 *lo_eta, const uint4 *rng,
-                               const float4 *pendA, const float4 *pendE) {
+cudaError_t rc_enqueue_targets(pt_ctx *ctx, cudaStream_t st, float4 *lo_eta, uint4 *rng, const float4 *pendA,
+                               const float4 *pendE) {
     const RadianceCache &C = ctx->cache;
     RcRows<1> rec{C.rec[0], C.rec[1], C.rec[2], C.rec[3], C.rec[6], C.ctr + 2, (uint32_t)C.recCap, 1u, 0u};
-    k_rc_targets<<<1, 1024, 0, st>>>(rec, C.rec[4], C.rec[5], C.rec[6], C.ctr, lo_eta, rng, pendA, pendE);
+    k_rc_targets<<<1, 1024, 0, st>>>(rec, C.rec[4], C.rec[5], C.rec[6], C.rec[7], C.ctr, lo_eta, rng, pendA,
+                                     pendE);
     return cudaGetLastError();
 }
 // kRcStepsPerCall Adam steps per render call, step s on records s, s + steps,
@@ -597,7 +613,9 @@ int rc_render_setup(pt_ctx *ctx, size_t waveCap) {
     int rc = rc_check(ctx);
     if (rc) return rc;
     rc_bounds(ctx);
-    return pt_cache_prepare(ctx, waveCap);
+    // a path makes at most two queries per wave: at its cache vertex and, as a
+    // training path, at the end of its suffix
+    return pt_cache_prepare(ctx, 2 * waveCap);
 }
 
 void pt_cache_free(pt_ctx *ctx) {

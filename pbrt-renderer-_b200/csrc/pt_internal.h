@@ -119,7 +119,8 @@ struct RadianceCache {
     size_t queryCap = 0;
     float4 *q[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // record float4 x 4, weight
     size_t recCap = 0;
-    float4 *rec[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // x 4, beta+slot, Lo, target
+    // x 4, throughput, Lo so far, target, cache value at the vertex
+    float4 *rec[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     uint64_t gen = 1;  // bumped when buffers move
     float lastKernelMs = 0.0f;  // network kernel of the last batch call (CUDA events)
 };
@@ -264,8 +265,8 @@ void pt_cache_free(pt_ctx *ctx);
 int pt_cache_prepare(pt_ctx *ctx, size_t queryCap);  // query buffers for a cached render
 int rc_render_setup(pt_ctx *ctx, size_t waveCap);     // checks, bounds, query buffers
 cudaError_t rc_enqueue_resolve(pt_ctx *ctx, cudaStream_t st, float4 *lo_eta);
-cudaError_t rc_enqueue_targets(pt_ctx *ctx, cudaStream_t st, const float4 *lo_eta, const uint4 *rng,
-                               const float4 *pendA, const float4 *pendE);
+cudaError_t rc_enqueue_targets(pt_ctx *ctx, cudaStream_t st, float4 *lo_eta, uint4 *rng, const float4 *pendA,
+                               const float4 *pendE);
 cudaError_t rc_enqueue_train(pt_ctx *ctx, cudaStream_t st);
 void pt_graph_free(pt_ctx *ctx);
 void pt_batch_free(pt_ctx *ctx);

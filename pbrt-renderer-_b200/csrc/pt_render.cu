@@ -69,7 +69,7 @@ struct WaveArgs {
     uint32_t *err;
     uint32_t shadowCap;
     // radiance cache (cacheOn == 0: plain path tracing)
-    uint32_t cacheOn, trainOn, unbiasedEvery, recCap;
+    uint32_t cacheOn, trainOn, unbiasedEvery, recCap, queryCap;
     float roughThr;
     const float *trainProb;  // chance that a path reaching a cache vertex trains (device, per call)
     float4 *cq[5];      // queries: 4 record float4 + throughput weight
@@ -612,12 +612,21 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
                                 st.w |= kFlagTrain | kFlagHasRec | (r << 8);
                                 if (A.unbiasedEvery && pcg_hash(hsh) % A.unbiasedEvery == 0) st.w |= kFlagUnbiased;
                                 train = true;
+                                // the image takes this path as it takes the others (prefix +
+                                // throughput x cache here); its suffix only feeds training
+                                uint32_t q = warp_append(A.cqCount, true);
+                                if (q < A.queryCap) {
+                                    cache_record(A.cq, q, hp, -rd, N, m, type, r | 0x80000000u);
+                                    A.cq[4][q] = make_float4(thr.x, thr.y, thr.z, 0.0f);
+                                } else {
+                                    atomicOr(A.err, (uint32_t)PT_DEVERR_QUEUE);
+                                }
                             }
                         }
                         if (train) {
                         } else {
                             uint32_t q = warp_append(A.cqCount, true);
-                            if (q < A.clsStride) {
+                            if (q < A.queryCap) {
                                 cache_record(A.cq, q, hp, -rd, N, m, type, slot);
                                 A.cq[4][q] = make_float4(thr.x, thr.y, thr.z, 0.0f);
                             } else {
@@ -627,7 +636,7 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
                         }
                     } else if (!(train && (st.w & kFlagUnbiased))) {
                         uint32_t q = warp_append(A.cqCount, true);
-                        if (q < A.clsStride) {
+                        if (q < A.queryCap) {
                             cache_record(A.cq, q, hp, -rd, N, m, type, slot);
                             A.cq[4][q] = make_float4(thr.x, thr.y, thr.z, 0.0f);
                         } else {
@@ -988,20 +997,22 @@ cudaError_t enqueue_render(const pt_ctx *ctx, Enqueue &E, WaveArgs A, const pt_r
         A.waveCount = (uint32_t)std::min<uint64_t>(cap, total - ws);
         if (cached) chk(cudaMemsetAsync(A.cqCount, 0, 4, st));
         chk(enqueue_paths(ctx, E, A, P->max_depth, G));
-        if (cached) {  // cache queries of this wave: lo_eta[slot] += throughput x cache
+        if (cached) {
+            // cache queries of this wave: lo_eta[slot] += throughput x cache, or
+            // the cache value at a training record's vertex
             E.begin(STG_CACHE);
             chk(rc_enqueue_resolve(const_cast<pt_ctx *>(ctx), st, A.lo_eta));
+            E.end();
+            // training targets from the suffixes, then the training paths' image
+            // values (prefix + throughput x cache); counts the wave's queries
+            E.begin(STG_CACHE);
+            chk(rc_enqueue_targets(const_cast<pt_ctx *>(ctx), st, A.lo_eta, A.rng, A.pendA, A.pendE));
             E.end();
         }
         uint32_t cover = (uint32_t)std::min<uint64_t>(A.waveCount, npix);
         E.begin(STG_FILM);
         k_film<<<(cover + kBlock - 1) / kBlock, kBlock, 0, st>>>(A, (float4 *)d_sum, (float4 *)d_comp);
         E.end();
-        if (cached) {  // training targets of the wave's records (also counts the wave's queries)
-            E.begin(STG_CACHE);
-            chk(rc_enqueue_targets(const_cast<pt_ctx *>(ctx), st, A.lo_eta, A.rng, A.pendA, A.pendE));
-            E.end();
-        }
         chk(cudaGetLastError());  // launch-configuration errors of this wave
     }
     if (cached && A.trainOn) {  // training steps on the call's records
@@ -1084,7 +1095,7 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
     A.shadowCap = (uint32_t)(2 * B.cap);
     A.batch = 0; A.numReqs = 0; A.reqs = nullptr; A.slotInfo = nullptr;
     A.cacheOn = (P->flags & PT_RENDER_RADIANCE_CACHE) ? 1u : 0u;
-    A.trainOn = A.unbiasedEvery = A.recCap = 0;
+    A.trainOn = A.unbiasedEvery = A.recCap = A.queryCap = 0;
     A.roughThr = 0.0f;
     A.trainProb = nullptr;
     for (float4 *&q : A.cq) q = nullptr;
@@ -1097,6 +1108,7 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
         A.unbiasedEvery = C.params.unbiased_every;
         A.recCap = (uint32_t)C.recCap;
         A.trainOn = (C.params.flags & PT_CACHE_NO_TRAIN) ? 0u : 1u;
+        A.queryCap = (uint32_t)C.queryCap;
         A.trainProb = reinterpret_cast<const float *>(C.ctr + 7);
         for (int k = 0; k < 5; k++) A.cq[k] = C.q[k];
         for (int k = 0; k < 7; k++) A.cr[k] = C.rec[k];

@@ -398,3 +398,33 @@ def sample_directions(n, seed, upper=False):
     if upper:
         d[:, 2] = np.abs(d[:, 2])
     return d.astype(np.float32)
+
+
+# ---------------------------------------------------------------------------
+# configuration 4: batched serving-style requests over the configuration 1-2 scenes
+# ---------------------------------------------------------------------------
+def batch_requests(n=32, seed=0):
+    """n render requests, each on the Cornell box (configuration 1) or the
+    Disney spheres (configuration 2) at random: a random camera, image sides
+    log-uniform in [64, 1024], spp uniform in {4..256}, the scene's depth
+    (8 / 16).  Returns dicts {scene, width, height, spp, max_depth, camera}."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        scene = "cornell" if rng.random() < 0.5 else "disney_envmap"
+        w = int(round(float(np.exp(rng.uniform(np.log(64), np.log(1024))))))
+        h = int(round(float(np.exp(rng.uniform(np.log(64), np.log(1024))))))
+        spp = int(rng.integers(4, 257))
+        if scene == "cornell":
+            eye = (rng.uniform(-0.7, 0.7), rng.uniform(0.3, 1.7), rng.uniform(0.6, 0.95))
+            tgt = (rng.uniform(-0.5, 0.5), rng.uniform(0.2, 1.2), rng.uniform(-1.0, -0.2))
+            cam = look_at_camera(eye, tgt, (0, 1, 0), float(rng.uniform(40, 70)), w / h)
+            depth = 8
+        else:
+            az, el, dist = rng.uniform(0, 2 * np.pi), np.radians(rng.uniform(15, 50)), rng.uniform(12, 30)
+            eye = (dist * np.cos(el) * np.sin(az), 1.0 + dist * np.sin(el), dist * np.cos(el) * np.cos(az))
+            tgt = (rng.uniform(-3, 3), 1.0, rng.uniform(-3, 3))
+            cam = look_at_camera(eye, tgt, (0, 1, 0), float(rng.uniform(30, 50)), w / h)
+            depth = 16
+        out.append({"scene": scene, "width": w, "height": h, "spp": spp, "max_depth": depth, "camera": cam})
+    return out
