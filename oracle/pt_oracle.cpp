@@ -210,6 +210,24 @@ template <class T> T microfacet_pdf(const V3<T> &wi, const V3<T> &wo, const Mat<
     return ks * Dc * Jh + (T(1) - ks) * wo.z * kInvPi<T>;
 }
 
+// Subsurface entry lobe (shaders/Material.hlsli:48-58, 92-100).
+template <class T> V3<T> subsurface_eval(const V3<T> &wi, const V3<T> &wo, const Mat<T> &m) {
+    if (wi.z <= T(0) || wo.z <= T(0)) return V3<T>(T(0));
+    T a = std::max(m.roughness * m.roughness, T(1e-4));
+    V3<T> wh = normalize(wi + wo);
+    T D = beckmann_d(wh, a);
+    T Fr = fresnel_dielectric(dot(wh, wi), m.extIOR, m.intIOR);
+    T G = smith_g1(wi, wh, a) * smith_g1(wo, wh, a);
+    return V3<T>(T(1)) * (D * Fr * G / std::max(T(4) * wi.z * wo.z, T(1e-10)));
+}
+template <class T> T subsurface_pdf(const V3<T> &wi, const V3<T> &wo, const Mat<T> &m) {
+    if (wi.z <= T(0) || wo.z <= T(0)) return T(0);
+    T a = std::max(m.roughness * m.roughness, T(1e-4));
+    V3<T> wh = normalize(wi + wo);
+    T Fr = fresnel_dielectric(dot(wh, wi), m.extIOR, m.intIOR);
+    return Fr * beckmann_d_cos(wh, a) / std::max(T(4) * dot(wh, wo), T(1e-10));
+}
+
 // ---------------------------------------------------------------------------
 // Disney principled (shaders/Disney.hlsli:10-275)
 // ---------------------------------------------------------------------------
@@ -546,6 +564,7 @@ template <class T> V3<T> material_eval(const V3<T> &wi, const V3<T> &wo, const M
         case PT_MAT_MICROFACET: return microfacet_eval(wi, wo, m);
         case PT_MAT_DISNEY: return disney_eval(wi, wo, m);
         case PT_MAT_HAIR: return hair_eval(wi, wo, m, h);
+        case PT_MAT_SUBSURFACE: return subsurface_eval(wi, wo, m);
         default: return V3<T>(T(0));
     }
 }
@@ -557,6 +576,7 @@ template <class T> T material_pdf(const V3<T> &wi, const V3<T> &wo, const Mat<T>
         case PT_MAT_MICROFACET: return microfacet_pdf(wi, wo, m);
         case PT_MAT_DISNEY: return disney_pdf(wi, wo, m);
         case PT_MAT_HAIR: return hair_pdf(wi, wo, m, h);
+        case PT_MAT_SUBSURFACE: return subsurface_pdf(wi, wo, m);
         default: return T(0);
     }
 }
@@ -1718,6 +1738,68 @@ static F3 vol_nee_env(const Ctx &c, F3 sp, F3 wo, uint32_t vi, Rng &rng, uint32_
 static inline void draw(Rng &rng, float *u, int k) { for (int i = 0; i < k; i++) u[i] = next_float(rng); }
 
 // ---------------------------------------------------------------------------
+// SubsurfaceWalk (shaders/Subsurface.hlsli:49-144): random walk inside the
+// closed mesh `mesh` from pos along dir; scalar extinction sigmaT, per-channel
+// albedo alpha, HG phase g, Fresnel at the boundary (reflect back or leave),
+// Russian roulette after 5 steps, at most 256 steps.  Returns true with the
+// exit point, direction, outward normal and throughput factor; a hit on other
+// geometry or an absorbed walk returns false.  Interior rays take the alpha
+// test with key kind 3.
+// ---------------------------------------------------------------------------
+static bool subsurface_walk(const Scene &s, F3 pos, F3 dir, uint32_t mesh, float sigmaT, F3 alpha, float g,
+                            float intIOR, float extIOR, Rng &rng, uint32_t aseed, uint32_t bounce, F3 &exitPos,
+                            F3 &exitDir, F3 &exitN, F3 &tmul) {
+    tmul = F3(1.0f);
+    exitPos = pos;
+    exitDir = dir;
+    exitN = dir;
+    for (int step = 0; step < 256; step++) {
+        float d = sigmaT > 0.0f ? -std::log(std::max(next_float(rng), 1e-10f)) / sigmaT : 1e30f;
+        Hit p = trace_closest(s, pos, dir, 1e-4f, d, aseed, alpha_key(bounce, 3u));
+        if (p.hit && p.t < d) {
+            if (p.mesh != mesh) {
+                tmul = F3(0.0f);
+                return false;
+            }
+            F3 bPos = pos + dir * p.t;
+            F3 Nb = normalize(interp_normal(s, p.mesh, p.prim, p.u, p.v));
+            if (dot(Nb, dir) < 0.0f) Nb = -Nb;
+            float cosI = dot(dir, Nb);
+            float Fr = fresnel_dielectric(cosI, intIOR, extIOR);
+            if (next_float(rng) < Fr) {
+                dir = normalize(reflect(dir, Nb));
+                pos = bPos - Nb * 1e-4f;
+                continue;
+            }
+            F3 outDir = refract(dir, -Nb, intIOR / extIOR);
+            if (dot(outDir, outDir) < 1e-8f) {
+                dir = normalize(reflect(dir, Nb));
+                pos = bPos - Nb * 1e-4f;
+                continue;
+            }
+            exitPos = bPos;
+            exitDir = normalize(outDir);
+            exitN = Nb;
+            return true;
+        }
+        pos = pos + dir * d;
+        tmul *= alpha;
+        float x1 = next_float(rng), x2 = next_float(rng), pp;
+        dir = sample_hg(dir, g, x1, x2, pp);
+        if (step > 4) {
+            float q = std::min(std::max(std::max(tmul.x, std::max(tmul.y, tmul.z)), 0.05f), 0.95f);
+            if (next_float(rng) >= q) {
+                tmul = F3(0.0f);
+                return false;
+            }
+            tmul = tmul / q;
+        }
+    }
+    tmul = F3(0.0f);
+    return false;
+}
+
+// ---------------------------------------------------------------------------
 // The path (shaders/Shaders.hlsl:25-651, RayGen), one camera sample.
 // ---------------------------------------------------------------------------
 struct PathStats { uint64_t ext = 0, shadow = 0; };
@@ -1910,8 +1992,76 @@ static F3 trace_path(const Ctx &c, const pt_render_params &P, uint32_t px, uint3
                     rough = pm.type == PT_MAT_DIFFUSE || pm.type == PT_MAT_HAIR ||
                             (pm.type == PT_MAT_MICROFACET && pm.alpha >= cc->roughThr) ||
                             (pm.type == PT_MAT_DISNEY && pm.roughness >= cc->roughThr);
+            } else if (pm.type == PT_MAT_SUBSURFACE) {  // Shaders.hlsl:515-611
+                F3 I = rd;
+                m.roughness = m.roughness * (1.0f + std::min(std::max(m.specular * 2.0f, 0.0f), 1.0f) * (0.65f - 1.0f));
+                const float rough = m.roughness;
+                const float aR = std::max(rough * rough, 1e-4f);
+                F3 wiL = to_local(-I, T, B, N);
+                F3 wmL(0.0f, 0.0f, 1.0f);
+                if (rough > 1e-3f) {
+                    float u0 = next_float(rng), u1 = next_float(rng);
+                    wmL = beckmann_sample(u0, u1, aR);
+                }
+                F3 wm = normalize(to_world(wmL, T, B, N));
+                float cosThetaM = dot(-I, wm);
+                if (cosThetaM <= 0.0f) {
+                    wm = N;
+                    wmL = F3(0.0f, 0.0f, 1.0f);
+                    cosThetaM = dot(-I, N);
+                }
+                float G1i = rough > 1e-3f ? smith_g1(wiL, wmL, aR) : 1.0f;
+                float Fr = fresnel_dielectric(cosThetaM, m.extIOR, m.intIOR);
+                Lo += thr * mis_direct(c, hp, N, Ng, T, B, wil, m, h, rng, aseed, (uint32_t)bounce);
+                if (st && s.emitterCount) st->shadow++;
+                Lo += thr * env_direct(c, hp, N, Ng, T, B, wil, m, h, rng, aseed, (uint32_t)bounce);
+                if (st) st->shadow++;
+                if (next_float(rng) < Fr) {
+                    F3 refl = reflect(I, wm);
+                    F3 woL = to_local(refl, T, B, N);
+                    if (woL.z <= 0.0f) break;  // reflected below the surface
+                    float weight = rough > 1e-3f
+                                       ? G1i * smith_g1(woL, wmL, aR) * cosThetaM / std::max(wiL.z * wmL.z, 1e-6f)
+                                       : 1.0f;
+                    float pdfSpec = rough > 1e-3f ? Fr * beckmann_d_cos(wmL, aR) / std::max(4.0f * cosThetaM, 1e-6f)
+                                                  : 0.0f;
+                    ro = hp + Ng * 0.001f; rd = refl; tmin = 0.0f; tmax = 1e20f;
+                    thr = thr * weight;
+                    lastPdf = pdfSpec;
+                } else {
+                    F3 refr = refract(I, wm, m.extIOR / m.intIOR);
+                    if (dot(refr, refr) < 1e-8f) {
+                        ro = hp + Ng * 0.001f; rd = reflect(I, wm); tmin = 0.0f; tmax = 1e20f;
+                        lastPdf = 0.0f;
+                    } else {
+                        F3 tint(pm.sheen, pm.sheenTint, pm.clearcoat);
+                        F3 aSharp = m.albedo, aBlur = m.albedo, detail(1.0f);
+                        if (pm.albedoTexIndex != PT_NO_TEXTURE) {  // albedo blurred 4 mip levels up
+                            float foot = uv_footprint(s, hit.mesh, hit.prim, hit.t, P.width, P.height);
+                            float tu, tv;
+                            interp_uv(s, hit.mesh, hit.prim, hit.u, hit.v, tu, tv);
+                            F4 cb = tex_sample(s, pm.albedoTexIndex, tu, tv, tex_lod(s, pm.albedoTexIndex, foot) + 4.0f);
+                            aBlur = F3(cb.x, cb.y, cb.z);
+                            F3 r = aSharp / vmax(aBlur, F3(1e-3f));
+                            detail = F3(std::min(std::max(r.x, 0.5f), 2.0f), std::min(std::max(r.y, 0.5f), 2.0f),
+                                        std::min(std::max(r.z, 0.5f), 2.0f));
+                        }
+                        F3 A = aBlur * tint, A2 = A * A, A3 = A2 * A;
+                        float sigmaT = 1.0f / std::max(m.subsurface, 1e-4f);
+                        F3 e = -5.09406f * A + 2.61188f * A2 - 4.31805f * A3;
+                        F3 alb = F3(1.0f) - F3(std::exp(e.x), std::exp(e.y), std::exp(e.z));
+                        F3 ep, ed, en, tm;
+                        bool exited = subsurface_walk(s, hp - Ng * 0.001f, normalize(refr), hit.mesh, sigmaT, alb,
+                                                      m.anisotropic, m.intIOR, m.extIOR, rng, aseed,
+                                                      (uint32_t)bounce, ep, ed, en, tm);
+                        if (!exited) break;
+                        thr *= tm * detail;
+                        ro = offset_ray_origin(ep, en, en); rd = ed; tmin = 0.0f; tmax = 1e20f;
+                        lastPdf = 0.0f;
+                    }
+                }
             } else {
-                break;  // subsurface (type 6) is not part of this path
+                break;
             }
         }
         if (bounce >= 3) {  // Shaders.hlsl:620-626
@@ -2185,8 +2335,6 @@ int or_render_cached(void *sp, const pt_render_params *P, float *sum, float *per
 static int render_impl(void *sp, const pt_render_params *P, float *sum, float *per_path, int threads,
                        uint64_t *counters, const CacheConst *cc) {
     Scene *s = static_cast<Scene *>(sp);
-    for (auto &m : s->mats)
-        if (m.type == PT_MAT_SUBSURFACE) { s->err = "subsurface"; return -1; }
     Ctx c{s, P->env_sampling};
     const uint32_t W = P->width, H = P->height;
     const uint32_t TS = 32;  // NORI_BLOCK_SIZE, include/block.h:17

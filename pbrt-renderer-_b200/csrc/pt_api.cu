@@ -382,13 +382,12 @@ int pt_upload_scene(pt_ctx *ctx, const pt_scene_desc *d) {
     std::vector<pt_material> mats(d->materials, d->materials + d->num_meshes);
     std::vector<uint32_t> meshFirstTri(std::max(1u, d->num_meshes), 0);
     uint32_t numTris = 0;
-    bool hasGlass = false, hasAlpha = false;
+    bool hasGlass = false, hasAlpha = false, hasSubsurface = false;
     uint32_t clsMask = 1u << CLS_MISS;  // shading classes the scene can produce
     std::vector<uint32_t> meshClass(std::max(1u, d->num_meshes), 0u);
     for (uint32_t m = 0; m < d->num_meshes; m++) {
         const pt_material &pm = mats[m];
         if (pm.type > PT_MAT_SUBSURFACE) return ctx->fail(PT_E_INVALID, "unknown material type");
-        if (pm.type == PT_MAT_SUBSURFACE) return ctx->fail(PT_E_UNSUPPORTED, "subsurface materials are not built");
         const uint32_t *tex = &pm.albedoTexIndex;  // albedo .. alpha: 7 consecutive indices
         for (int t = 0; t < 7; t++)
             if (tex[t] != PT_NO_TEXTURE && tex[t] >= d->num_textures)
@@ -401,6 +400,7 @@ int pt_upload_scene(pt_ctx *ctx, const pt_scene_desc *d) {
         meshFirstTri[m] = numTris;
         numTris += pm.indexCount / 3;
         hasGlass |= pm.type == PT_MAT_MIRROR || pm.type == PT_MAT_DIELECTRIC;
+        hasSubsurface |= pm.indexCount && pm.type == PT_MAT_SUBSURFACE;
         meshClass[m] = (uint32_t)shade_class(true, pm.isEmitter != 0, pm.type, has_shading_textures(pm));
         if (pm.indexCount) clsMask |= 1u << meshClass[m];
         if (pm.indexCount && pm.alphaTexIndex != PT_NO_TEXTURE) hasAlpha = true;
@@ -531,6 +531,7 @@ int pt_upload_scene(pt_ctx *ctx, const pt_scene_desc *d) {
     if ((rc = h2d(dmcls, meshClass.data(), meshClass.size() * 4))) return rc;
     if ((rc = upload_textures(ctx, d))) return rc;
     S.hasAlpha = hasAlpha ? 1u : 0u;
+    S.hasSubsurface = hasSubsurface ? 1u : 0u;
     S.pos = dpos; S.nrm = dnrm; S.uv = duv; S.tan = dtan; S.idx = didx;
     S.mats = dmats; S.meshClass = dmcls; S.numMeshes = d->num_meshes; S.meshFirstTri = dmft;
     S.emitterCdf = dcdf; S.emitterList = demit; S.emitterCount = ne;

@@ -71,6 +71,7 @@ struct DevScene {
     const float *srgbLut;       // 256 entries: sRGB-encoded byte -> linear
     uint32_t numTex;
     uint32_t hasAlpha;          // any alpha-mapped mesh (alpha-tested triangles)
+    uint32_t hasSubsurface;     // any subsurface (type 6) mesh: shading traces its walks inline
 };
 
 // One texture's mip chain in DevScene::texels (level l: max(w >> l, 1) x

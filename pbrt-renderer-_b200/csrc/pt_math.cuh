@@ -244,6 +244,33 @@ PT_HD float microfacet_pdf(float3 wi, float3 wo, const pt_material &m) {
     return ks * beckmann_d_cos(wh, m.alpha) * Jh + (1.0f - ks) * wo.z * kInvPi;
 }
 
+// Subsurface entry lobe (Material.hlsli:48-58,92-100): Beckmann reflection
+// with Fresnel at the half vector, alpha = max(roughness^2, 1e-4).  The walk
+// under the surface is a shading event (Subsurface.hlsli), not a BSDF sample.
+PT_HD float3 subsurface_eval(float3 wi, float3 wo, const pt_material &m) {
+    if (wi.z <= 0.0f || wo.z <= 0.0f) return v3(0.0f);
+    float a = mx(m.roughness * m.roughness, 1e-4f);
+    float3 wh = normalize(wi + wo);
+    float D = beckmann_d(wh, a);
+    float Fr = fresnel(dot(wh, wi), m.extIOR, m.intIOR);
+    float G = smith_g1(wi, wh, a) * smith_g1(wo, wh, a);
+    return v3(1.0f) * (D * Fr * G / mx(4.0f * wi.z * wo.z, 1e-10f));
+}
+PT_HD float subsurface_pdf(float3 wi, float3 wo, const pt_material &m) {
+    if (wi.z <= 0.0f || wo.z <= 0.0f) return 0.0f;
+    float a = mx(m.roughness * m.roughness, 1e-4f);
+    float3 wh = normalize(wi + wo);
+    float Fr = fresnel(dot(wh, wi), m.extIOR, m.intIOR);
+    return Fr * beckmann_d_cos(wh, a) / mx(4.0f * dot(wh, wo), 1e-10f);
+}
+// SubsurfaceParams (Subsurface.hlsli:24-31): scalar extinction 1 / mean free
+// path and the per-channel single-scattering albedo of colour A.
+PT_HD void subsurface_params(float3 A, float d, float &sigmaT, float3 &alpha) {
+    sigmaT = 1.0f / mx(d, 1e-4f);
+    float3 A2 = A * A, A3 = A2 * A;
+    alpha = v3(1.0f) - vexp(-5.09406f * A + 2.61188f * A2 - 4.31805f * A3);
+}
+
 // ---------------------------------------------------------------------------
 // Disney principled (shaders/Disney.hlsli:10-275, Material.hlsli:30-40,74-84)
 // ---------------------------------------------------------------------------
@@ -517,6 +544,10 @@ PT_HD void material_eval_pdf_t(uint32_t type, float3 wi, float3 wo, const pt_mat
             hair_eval_pdf(wi, wo, m, p, h, f, pdf);
             return;
         }
+        case PT_MAT_SUBSURFACE:
+            f = subsurface_eval(wi, wo, m);
+            pdf = subsurface_pdf(wi, wo, m);
+            return;
         default:
             f = v3(0.0f);
             pdf = 0.0f;

@@ -432,6 +432,74 @@ struct ShadeBlocks {
                                                       : base == CLS_DISNEY ? 3 : 2;
 };
 
+// SubsurfaceWalk (Subsurface.hlsli:49-144): random walk inside the closed
+// mesh `mesh` from pos along dir; scalar extinction sigmaT, per-channel albedo
+// alpha, HG phase g, Fresnel at the boundary (reflect back or leave), Russian
+// roulette after 5 steps, at most 256 steps.  True with the exit point,
+// direction, outward normal and throughput factor; a hit on other geometry or
+// an absorbed walk gives false.  Interior rays take the alpha test with key
+// kind 3.
+__device__ bool subsurface_walk(const WaveArgs &A, float3 pos, float3 dir, uint32_t mesh, float sigmaT, float3 alpha,
+                                float g, float intIOR, float extIOR, Rng &rng, uint32_t aseed, uint32_t bounce,
+                                float3 &exitPos, float3 &exitDir, float3 &exitN, float3 &tmul) {
+    const DevScene &S = A.S;
+    tmul = v3(1.0f);
+    exitPos = pos;
+    exitDir = dir;
+    exitN = dir;
+    for (int step = 0; step < 256; step++) {
+        float d = sigmaT > 0.0f ? -logf(mx(next_float(rng, S.sobol1), 1e-10f)) / sigmaT : 1e30f;
+        Hit p = trace_closest(S, pos, dir, 1e-4f, d, A.err, aseed, alpha_key(bounce, 3u));
+        if (p.gid != 0xFFFFFFFFu && p.t < d) {
+            const uint32_t hm = __ldg(S.triMesh + p.gid);
+            if (hm != mesh) {
+                tmul = v3(0.0f);
+                return false;
+            }
+            const uint32_t prim = p.gid - __ldg(S.meshFirstTri + hm);
+            uint32_t i0, i1, i2;
+            tri_vidx(S, hm, prim, i0, i1, i2);
+            float3 bPos = pos + dir * p.t;
+            float w0 = 1.0f - p.u - p.v;
+            float3 nn = ld3(S.nrm, i0) * w0 + ld3(S.nrm, i1) * p.u + ld3(S.nrm, i2) * p.v;
+            float l2 = dot(nn, nn);
+            float3 p0 = ld3(S.pos, i0), p1 = ld3(S.pos, i1), p2 = ld3(S.pos, i2);
+            float3 Nb = normalize(l2 < 1e-8f ? normalize(cross(p1 - p0, p2 - p0)) : nn * (1.0f / sqrtf(l2)));
+            if (dot(Nb, dir) < 0.0f) Nb = -Nb;
+            float Fr = fresnel(dot(dir, Nb), intIOR, extIOR);
+            if (next_float(rng, S.sobol1) < Fr) {
+                dir = normalize(reflect(dir, Nb));
+                pos = bPos - Nb * 1e-4f;
+                continue;
+            }
+            float3 outDir = refract(dir, -Nb, intIOR / extIOR);
+            if (dot(outDir, outDir) < 1e-8f) {
+                dir = normalize(reflect(dir, Nb));
+                pos = bPos - Nb * 1e-4f;
+                continue;
+            }
+            exitPos = bPos;
+            exitDir = normalize(outDir);
+            exitN = Nb;
+            return true;
+        }
+        pos = pos + dir * d;
+        tmul *= alpha;
+        float x1 = next_float(rng, S.sobol1), x2 = next_float(rng, S.sobol1), pp;
+        dir = sample_hg(dir, g, x1, x2, pp);
+        if (step > 4) {
+            float q = clampf(maxc(tmul), 0.05f, 0.95f);
+            if (next_float(rng, S.sobol1) >= q) {
+                tmul = v3(0.0f);
+                return false;
+            }
+            tmul = tmul / v3(q);
+        }
+    }
+    tmul = v3(0.0f);
+    return false;
+}
+
 // Texture maps at a surface hit (Shaders.hlsl:232-315): albedo (sRGB),
 // normal map in the frame of the triangle's UV derivatives, roughness (not
 // for hair, whose `roughness` is beta_m), specular (x 0.5), subsurface; each
@@ -736,6 +804,82 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
                             cont = true;
                             if (A.cacheOn) st.w = rough_bounce(A, type, m) ? (st.w | kFlagRough) : (st.w & ~kFlagRough);
                         }
+                    } else if (C == CLS_ANY && type == PT_MAT_SUBSURFACE) {  // Shaders.hlsl:515-611
+                        // rough dielectric entry (Beckmann half vector, Fresnel choice),
+                        // NEE with the entry lobe, then reflect or walk the interior
+                        const float3 I = rd;
+                        m.roughness = m.roughness * (1.0f + sat(m.specular * 2.0f) * (0.65f - 1.0f));
+                        const float rough = m.roughness;
+                        const float aR = mx(rough * rough, 1e-4f);
+                        float3 wmL = make_float3(0.0f, 0.0f, 1.0f);
+                        if (rough > 1e-3f) {
+                            float u0 = next_float(rng, S.sobol1), u1 = next_float(rng, S.sobol1);
+                            wmL = beckmann_sample(u0, u1, aR);
+                        }
+                        float3 wm = normalize(to_world(wmL, T, B, N));
+                        float cosThetaM = dot(-I, wm);
+                        if (cosThetaM <= 0.0f) {
+                            wm = N;
+                            wmL = make_float3(0.0f, 0.0f, 1.0f);
+                            cosThetaM = dot(-I, N);
+                        }
+                        const float G1i = rough > 1e-3f ? smith_g1(wil, wmL, aR) : 1.0f;
+                        const float Fr = fresnel(cosThetaM, m.extIOR, m.intIOR);
+                        Lo += thr * nee_area<INLINE>(A, hp, N, Ng, T, B, wil, type, m, h, rng, neeA, aseed, st.z);
+                        Lo += thr * nee_env<INLINE>(A, hp, N, Ng, T, B, wil, type, m, h, rng, neeE, aseed, st.z);
+                        if (next_float(rng, S.sobol1) < Fr) {
+                            float3 refl = reflect(I, wm);
+                            float3 woL = to_local(refl, T, B, N);
+                            if (woL.z > 0.0f) {  // else reflected below the surface: the path ends
+                                float weight = rough > 1e-3f ? G1i * smith_g1(woL, wmL, aR) * cosThetaM /
+                                                                   mx(wil.z * wmL.z, 1e-6f)
+                                                             : 1.0f;
+                                float pdfSpec = rough > 1e-3f
+                                                    ? Fr * beckmann_d_cos(wmL, aR) / mx(4.0f * cosThetaM, 1e-6f)
+                                                    : 0.0f;
+                                no = hp + Ng * 0.001f;
+                                nd = refl;
+                                thr = thr * weight;
+                                lastPdf = pdfSpec;
+                                cont = true;
+                            }
+                        } else {
+                            float3 refr = refract(I, wm, m.extIOR / m.intIOR);
+                            if (dot(refr, refr) < 1e-8f) {
+                                no = hp + Ng * 0.001f;
+                                nd = reflect(I, wm);
+                                lastPdf = 0.0f;
+                                cont = true;
+                            } else {
+                                const float3 tint = make_float3(m.sheen, m.sheenTint, m.clearcoat);
+                                const float3 aSharp = make_float3(m.albedo[0], m.albedo[1], m.albedo[2]);
+                                float3 aBlur = aSharp, detail = v3(1.0f);
+                                if (m.albedoTexIndex != PT_NO_TEXTURE) {  // albedo blurred 4 mip levels up
+                                    const uint2 wh = path_image(A, slot);
+                                    const float foot = uv_footprint(S, mesh, prim, h4.x, wh.x, wh.y);
+                                    const float2 tuv = interp_uv(S, i0, i1, i2, bx, by);
+                                    float4 cb = tex_sample(S, m.albedoTexIndex, tuv.x, tuv.y,
+                                                           tex_lod(S, m.albedoTexIndex, foot) + 4.0f);
+                                    aBlur = make_float3(cb.x, cb.y, cb.z);
+                                    float3 r = aSharp / vmax(aBlur, v3(1e-3f));
+                                    detail = make_float3(clampf(r.x, 0.5f, 2.0f), clampf(r.y, 0.5f, 2.0f),
+                                                         clampf(r.z, 0.5f, 2.0f));
+                                }
+                                float sigmaT;
+                                float3 alb;
+                                subsurface_params(aBlur * tint, m.subsurface, sigmaT, alb);
+                                float3 ep, ed, en, tm;
+                                if (subsurface_walk(A, hp - Ng * 0.001f, normalize(refr), mesh, sigmaT, alb,
+                                                    m.anisotropic, m.intIOR, m.extIOR, rng, aseed, st.z, ep, ed, en,
+                                                    tm)) {
+                                    thr *= tm * detail;
+                                    no = offset_origin(ep, en, en);
+                                    nd = ed;
+                                    lastPdf = 0.0f;
+                                    cont = true;
+                                }
+                            }
+                        }
                     }
                 }
             }
@@ -931,7 +1075,7 @@ struct Grids {
 // Returns the first failing call's status (cudaSuccess if none).
 cudaError_t enqueue_paths(const pt_ctx *ctx, Enqueue &E, WaveArgs &A, uint32_t depth, const Grids &G) {
     const WaveBuffers &B = ctx->W;
-    const bool inl = ctx->S.numVols > 0;
+    const bool inl = ctx->S.numVols > 0 || ctx->S.hasSubsurface;
     cudaStream_t st = E.st;
     cudaError_t err = cudaSuccess;
     auto chk = [&](cudaError_t e) {

@@ -18,12 +18,13 @@ Every array is float32 / uint32 and every draw comes from
 
 from __future__ import annotations
 
+import copy
 import math
 
 import numpy as np
 
-from . import (PT_MAT_DIFFUSE, PT_MAT_DISNEY, PT_MAT_HAIR, PT_NO_TEXTURE, PT_VOLUME_HETEROGENEOUS, Scene,
-               make_material, pt_camera, pt_volume)
+from . import (PT_MAT_DIFFUSE, PT_MAT_DISNEY, PT_MAT_HAIR, PT_MAT_SUBSURFACE, PT_NO_TEXTURE,
+               PT_VOLUME_HETEROGENEOUS, Scene, make_material, pt_camera, pt_volume)
 
 
 # ---------------------------------------------------------------------------
@@ -178,6 +179,24 @@ def cornell(width=256, height=256, subdiv=3):
     scene = b.scene()
     cam = look_at_camera((0.0, 1.0, 0.95), (0.0, 0.9, -1.0), (0, 1, 0), 62.0, width / height)
     return scene, cam
+
+
+def subsurface_scene(width=64, height=64, subdiv=3, mfp=0.08, g=0.2):
+    """The Cornell room with its sphere made of a subsurface material (type 6:
+    rough dielectric boundary over a scattering interior; mean free path
+    `mfp`, HG anisotropy `g`, tint (1, 0.9, 0.8) in sheen / sheenTint /
+    clearcoat as the reference stores it)."""
+    sc, cam = cornell(width, height, subdiv)
+    mats = [copy.copy(m) for m in sc.materials]
+    m = mats[-1]
+    m.type = PT_MAT_SUBSURFACE
+    m.albedo[:] = (0.9, 0.55, 0.45)
+    m.roughness, m.specular = 0.3, 0.5
+    m.sheen, m.sheenTint, m.clearcoat = 1.0, 0.9, 0.8
+    m.subsurface, m.anisotropic = mfp, g
+    m.intIOR, m.extIOR = 1.4, 1.0
+    return Scene(sc.positions, sc.indices, mats, normals=sc.normals, texcoords=sc.texcoords,
+                 tangents=sc.tangents), cam
 
 
 # ---------------------------------------------------------------------------

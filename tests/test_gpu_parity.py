@@ -45,6 +45,8 @@ def random_materials(pt, rng, kind, count):
         elif kind == pt.PT_MAT_HAIR:
             m.roughness, m.betaN = rng.uniform(0.2, 0.6), rng.uniform(0.2, 0.6)
             m.alpha, m.intIOR = 2.0, 1.55
+        elif kind == pt.PT_MAT_SUBSURFACE:
+            m.roughness, m.intIOR, m.extIOR = rng.uniform(0.05, 1.0), rng.uniform(1.2, 1.7), 1.0
         mats.append(m)
     return mats
 
@@ -93,7 +95,7 @@ def test_sample_stream_bit_exact(ctx, oracle):
         assert np.array_equal(a, b), kind
 
 
-@pytest.mark.parametrize("kind_name", ["DIFFUSE", "MICROFACET", "DISNEY", "HAIR"])
+@pytest.mark.parametrize("kind_name", ["DIFFUSE", "MICROFACET", "DISNEY", "HAIR", "SUBSURFACE"])
 def test_bsdf_eval_parity(kind_name, pt, scenes, ctx, oracle):
     kind = getattr(pt, "PT_MAT_" + kind_name)
     rng = np.random.default_rng(17)

@@ -15,6 +15,7 @@ def _scenes(scenes):
         "cornell": scenes.cornell(48, 40),
         "spheres": scenes.disney_spheres(40, 32, grid=2, slices=24, rings=13, env_w=128, env_h=64),
         "hair_volume": scenes.hair_volume(40, 40, strands=120, segments=6, grid_n=24),
+        "subsurface": scenes.subsurface_scene(48, 40),
     }
 
 
@@ -46,7 +47,7 @@ def test_sample_stream_identical(oracle, reference):
 def test_bsdf_eval_identical(pt, scenes, oracle, reference):
     rng = np.random.default_rng(5)
     mats = []
-    for t in (pt.PT_MAT_DIFFUSE, pt.PT_MAT_MICROFACET, pt.PT_MAT_DISNEY, pt.PT_MAT_HAIR):
+    for t in (pt.PT_MAT_DIFFUSE, pt.PT_MAT_MICROFACET, pt.PT_MAT_DISNEY, pt.PT_MAT_HAIR, pt.PT_MAT_SUBSURFACE):
         for _ in range(4):
             m = pt.make_material(t, tuple(rng.uniform(0.05, 1, 3)))
             m.roughness, m.metallic, m.specular = rng.uniform(0.05, 1), rng.uniform(), rng.uniform()
@@ -87,12 +88,12 @@ def test_envmap_sample_identical(scene_set, oracle, reference):
     assert np.array_equal(po2, pr2) and np.array_equal(ro2, rr2)
 
 
-@pytest.mark.parametrize("name,depth", [("cornell", 8), ("spheres", 16), ("hair_volume", 8)])
+@pytest.mark.parametrize("name,depth", [("cornell", 8), ("spheres", 16), ("hair_volume", 8), ("subsurface", 8)])
 def test_render_identical(name, depth, scene_set, pt, oracle, reference):
     sc, cam = scene_set[name]
     oracle.load(sc)
     reference.load(sc)
-    W = 48 if name == "cornell" else 40
+    W = 48 if name in ("cornell", "subsurface") else 40
     H = 40 if name != "spheres" else 32
     P = pt.render_params(W, H, 3, cam, max_depth=depth, sample_offset=5)
     so, _, _ = oracle.render(P, threads=4)
