@@ -198,6 +198,8 @@ typedef struct pt_render_params {
 /* pt_render_params.flags */
 #define PT_RENDER_STAGE_TIMING 0x1u /* fill pt_stats.ms_* per stage (CUDA events per launch) */
 #define PT_RENDER_RADIANCE_CACHE 0x2u /* terminate paths into the radiance cache (pt_cache_init) */
+#define PT_RENDER_RIS_NEE 0x4u /* area-light NEE by resampled importance sampling: the reference's
+                                  USE_RIS=1 build (RISDirectIllumination, shaders/Emitter.hlsli:155-271) */
 
 /* Film: per pixel Σ(L, 1) as RGBA float32 (shaders/Shaders.hlsl:632-634)
  * plus the Kahan compensation of the same shape.  location 0 = host

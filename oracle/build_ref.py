@@ -74,17 +74,20 @@ def build(src: str = DEFAULT_SRC, quiet: bool = False) -> str:
             text = f.read()
         with open(os.path.join(GEN, name), "w", encoding="utf-8") as f:
             f.write(rewrite(text))
+    # libref.so: the reference's default build; libref_ris.so: its USE_RIS=1
+    # build (resampled area-light NEE, shaders/Shaders.hlsl:481-488)
     lib = os.path.join(OUT, "libref.so")
-    cmd = [
-        "g++", "-std=c++17", "-O2", "-march=x86-64-v2", "-ffp-contract=off",
-        "-fsingle-precision-constant", "-fPIC", "-shared", "-w",
-        "-DMAX_BOUNCES=g_max_bounces",
-        "-I", GEN, "-I", SHIM,
-        os.path.join(SHIM, "ref_entry.cpp"), "-o", lib, "-lpthread",
-    ]
-    if not quiet:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+    for name, extra in (("libref.so", []), ("libref_ris.so", ["-DUSE_RIS=1"])):
+        cmd = [
+            "g++", "-std=c++17", "-O2", "-march=x86-64-v2", "-ffp-contract=off",
+            "-fsingle-precision-constant", "-fPIC", "-shared", "-w",
+            "-DMAX_BOUNCES=g_max_bounces", *extra,
+            "-I", GEN, "-I", SHIM,
+            os.path.join(SHIM, "ref_entry.cpp"), "-o", os.path.join(OUT, name), "-lpthread",
+        ]
+        if not quiet:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
     return lib
 
 

@@ -16,6 +16,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libref.so")
+REF_RIS_SO = os.path.join(HERE, "_ref", "libref_ris.so")  # the reference's USE_RIS=1 build
 REF_SRC = "/root/reference/shaders"
 
 
@@ -199,11 +200,12 @@ class Reference:
 
     One scene at a time per process (the shader's resources are globals)."""
 
-    def __init__(self, pt):
-        if not os.path.exists(REF_SO):
-            raise FileNotFoundError(REF_SO)
+    def __init__(self, pt, ris=False):
+        so = REF_RIS_SO if ris else REF_SO
+        if not os.path.exists(so):
+            raise FileNotFoundError(so)
         self.pt = pt
-        L = C.CDLL(REF_SO)
+        L = C.CDLL(so)
         F, U, S = C.POINTER(C.c_float), C.POINTER(C.c_uint32), C.c_size_t
         M = C.POINTER(pt.pt_material)
         L.ref_scene_create.argtypes = [C.POINTER(pt.pt_scene_desc)]
@@ -220,8 +222,8 @@ class Reference:
         self.scene = None
 
     @staticmethod
-    def available():
-        return os.path.exists(REF_SO)
+    def available(ris=False):
+        return os.path.exists(REF_RIS_SO if ris else REF_SO)
 
     def load(self, scene):
         self.scene = scene

@@ -1667,6 +1667,67 @@ static F3 mis_direct(const Ctx &c, F3 hp, F3 N, F3 Ng, F3 T, F3 B, F3 wil, const
     F3 vt = multi_volume_tr(s, so, ww, dist, rng);
     return es.rad * f * act / std::max(pe, 1e-20f) * w * vt * trans;
 }
+// EvalLightCandidate (Emitter.hlsli:166-199): unshadowed integrand, scalar
+// target pHat = lum(f Le cos) and the solid-angle pdf of the emitter sample.
+static bool ris_candidate(const EmitterSample &es, F3 hp, F3 N, F3 T, F3 B, F3 wil, const Mat<float> &m, float h,
+                          F3 &wiw, float &dist, F3 &integ, float &pHat, float &pSA) {
+    integ = F3(0.0f);
+    pHat = 0.0f;
+    pSA = 0.0f;
+    F3 toLight = es.pos - hp;
+    dist = length(toLight);
+    if (dist < 1e-6f) {
+        wiw = F3(0.0f, 0.0f, 1.0f);
+        return false;
+    }
+    wiw = toLight / dist;
+    float cosSurface = dot(N, wiw), cosLight = dot(es.nrm, -wiw);
+    bool hair = m.type == PT_MAT_HAIR;
+    if ((!hair && cosSurface <= 0.0f) || cosLight <= 1e-8f) return false;
+    float absCos = hair ? std::fabs(cosSurface) : cosSurface;
+    F3 f = material_eval(wil, to_local(wiw, T, B, N), m, h);
+    integ = f * es.rad * absCos;
+    pHat = dot(integ, F3(0.2126f, 0.7152f, 0.0722f));
+    pSA = es.pdfArea * dist * dist / cosLight;
+    return pHat > 0.0f && pSA > 0.0f;
+}
+// RISDirectIllumination (Emitter.hlsli:201-271), RIS_M = 8 candidates streamed
+// through a one-sample reservoir, the survivor shadow-tested and MIS-weighted
+// against the BSDF with the candidate's solid-angle pdf.
+static F3 ris_direct(const Ctx &c, F3 hp, F3 N, F3 Ng, F3 T, F3 B, F3 wil, const Mat<float> &m, float h, Rng &rng,
+                     uint32_t aseed, uint32_t bounce) {
+    const Scene &s = *c.s;
+    EmitterSample y{};
+    y.valid = false;
+    float wSum = 0.0f, pHatY = 0.0f;
+    for (int i = 0; i < 8; i++) {
+        EmitterSample cnd = sample_emitter(s, rng);
+        if (!cnd.valid) continue;
+        F3 wiwC, integC;
+        float distC, pHatC, pSAC;
+        if (!ris_candidate(cnd, hp, N, T, B, wil, m, h, wiwC, distC, integC, pHatC, pSAC)) continue;
+        float w = pHatC / pSAC;
+        wSum += w;
+        if (next_float(rng) < w / std::max(wSum, 1e-20f)) {
+            y = cnd;
+            pHatY = pHatC;
+        }
+    }
+    if (!y.valid || pHatY <= 0.0f) return F3(0.0f);
+    float W = (wSum / 8.0f) / pHatY;
+    F3 wiw, integ;
+    float dist, pHat, pSA;
+    if (!ris_candidate(y, hp, N, T, B, wil, m, h, wiw, dist, integ, pHat, pSA)) return F3(0.0f);
+    bool hair = m.type == PT_MAT_HAIR;
+    F3 sng = hair ? (dot(wiw, Ng) >= 0.0f ? Ng : -Ng) : Ng;
+    F3 so = offset_ray_origin(hp, sng, sng);
+    F3 trans;
+    if (trace_shadow(s, so, wiw, 0.0f, dist - 0.001f, trans, aseed, alpha_key(bounce, 1u))) return F3(0.0f);
+    float pdfBsdf = material_pdf(wil, to_local(wiw, T, B, N), m, h);
+    float wMis = balance_heuristic(pSA, pdfBsdf);
+    F3 vt = multi_volume_tr(s, so, wiw, dist, rng);
+    return integ * W * wMis * vt * trans;
+}
 static F3 env_direct(const Ctx &c, F3 hp, F3 N, F3 Ng, F3 T, F3 B, F3 wil, const Mat<float> &m, float h, Rng &rng,
                      uint32_t aseed, uint32_t bounce) {  // Emitter.hlsli:275-326
     const Scene &s = *c.s;
@@ -1969,7 +2030,8 @@ static F3 trace_path(const Ctx &c, const pt_render_params &P, uint32_t px, uint3
                 rough = false;
             } else if (pm.type == PT_MAT_DIFFUSE || pm.type == PT_MAT_MICROFACET || pm.type == PT_MAT_DISNEY ||
                        pm.type == PT_MAT_HAIR) {  // Shaders.hlsl:473-511
-                Lo += thr * mis_direct(c, hp, N, Ng, T, B, wil, m, h, rng, aseed, (uint32_t)bounce);
+                if (P.flags & PT_RENDER_RIS_NEE) Lo += thr * ris_direct(c, hp, N, Ng, T, B, wil, m, h, rng, aseed, (uint32_t)bounce);
+                else Lo += thr * mis_direct(c, hp, N, Ng, T, B, wil, m, h, rng, aseed, (uint32_t)bounce);
                 if (st && s.emitterCount) st->shadow++;
                 Lo += thr * env_direct(c, hp, N, Ng, T, B, wil, m, h, rng, aseed, (uint32_t)bounce);
                 if (st) st->shadow++;

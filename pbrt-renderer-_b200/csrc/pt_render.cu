@@ -76,6 +76,7 @@ struct WaveArgs {
     uint32_t *cqCount;
     float4 *cr[7];      // training records: 4 record float4, throughput, Lo so far, target
     uint32_t *crCount;
+    uint32_t risNee;  // PT_RENDER_RIS_NEE: area-light NEE by resampled importance sampling
     // batched render (batch != 0): requests and, per path slot, (pixel | request << 24, sample index)
     uint32_t batch, numReqs;
     const ReqDev *reqs;
@@ -317,6 +318,82 @@ __device__ __forceinline__ float3 nee_area(const WaveArgs &A, float3 hp, float3 
     if (INLINE) return X * trans;
     out.ray = true;
     out.o = so; out.d = ww; out.tmin = 0.0f; out.tmax = dist - 0.001f; out.X = X;
+    return v3(0.0f);
+}
+// EvalLightCandidate (Emitter.hlsli:166-199): unshadowed integrand, scalar
+// target pHat = lum(f Le cos) and the solid-angle pdf of the emitter sample.
+__device__ __forceinline__ bool ris_candidate(const EmitterSample &es, float3 hp, float3 N, float3 T, float3 B,
+                                              float3 wil, uint32_t type, const pt_material &m, float h, float3 &wiw,
+                                              float &dist, float3 &integ, float &pHat, float &pSA) {
+    integ = v3(0.0f);
+    pHat = 0.0f;
+    pSA = 0.0f;
+    float3 tl = es.pos - hp;
+    dist = len(tl);
+    if (dist < 1e-6f) {
+        wiw = make_float3(0.0f, 0.0f, 1.0f);
+        return false;
+    }
+    wiw = tl / v3(dist);
+    float cs = dot(N, wiw), cl = dot(es.nrm, -wiw);
+    bool hair = type == PT_MAT_HAIR;
+    if ((!hair && cs <= 0.0f) || cl <= 1e-8f) return false;
+    float ac = hair ? fabsf(cs) : cs;
+    float3 f;
+    float pb;
+    material_eval_pdf_t(type, wil, to_local(wiw, T, B, N), m, h, f, pb);
+    integ = f * es.rad * ac;
+    pHat = dot(integ, make_float3(0.2126f, 0.7152f, 0.0722f));
+    pSA = es.pdfArea * dist * dist / cl;
+    return pHat > 0.0f && pSA > 0.0f;
+}
+// RISDirectIllumination (Emitter.hlsli:201-271) up to the shadow trace: 8
+// candidates through a one-sample reservoir, the survivor re-evaluated and
+// MIS-weighted against the BSDF with its solid-angle pdf (the same pdf the
+// emitter-hit MIS weight uses).
+template <bool INLINE>
+__device__ __forceinline__ float3 nee_ris(const WaveArgs &A, float3 hp, float3 N, float3 Ng, float3 T, float3 B,
+                                          float3 wil, uint32_t type, const pt_material &m, float h, Rng &rng,
+                                          NeeOut &out, uint32_t aseed, uint32_t bounce) {
+    const DevScene &S = A.S;
+    out.ray = false;
+    EmitterSample y;
+    y.valid = false;
+    float wSum = 0.0f, pHatY = 0.0f;
+    for (int i = 0; i < 8; i++) {
+        EmitterSample c = sample_emitter(S, rng);
+        if (!c.valid) continue;
+        float3 wiwC, integC;
+        float distC, pHatC, pSAC;
+        if (!ris_candidate(c, hp, N, T, B, wil, type, m, h, wiwC, distC, integC, pHatC, pSAC)) continue;
+        float w = pHatC / pSAC;
+        wSum += w;
+        if (next_float(rng, S.sobol1) < w / mx(wSum, 1e-20f)) {
+            y = c;
+            pHatY = pHatC;
+        }
+    }
+    if (!y.valid || pHatY <= 0.0f) return v3(0.0f);
+    float W = (wSum / 8.0f) / pHatY;
+    float3 wiw, integ;
+    float dist, pHat, pSA;
+    if (!ris_candidate(y, hp, N, T, B, wil, type, m, h, wiw, dist, integ, pHat, pSA)) return v3(0.0f);
+    bool hair = type == PT_MAT_HAIR;
+    float3 sng = hair ? (dot(wiw, Ng) >= 0.0f ? Ng : -Ng) : Ng;
+    float3 so = offset_origin(hp, sng, sng);
+    float3 trans = v3(1.0f);
+    if (INLINE) {
+        if (trace_shadow(S, so, wiw, 0.0f, dist - 0.001f, trans, A.err, aseed, alpha_key(bounce, 1u))) return v3(0.0f);
+    }
+    float3 fu;
+    float pdfBsdf;
+    material_eval_pdf_t(type, wil, to_local(wiw, T, B, N), m, h, fu, pdfBsdf);
+    float wMis = balance(pSA, pdfBsdf);
+    float3 vt = INLINE ? multi_volume_tr(S, so, wiw, dist, rng) : v3(1.0f);
+    float3 X = integ * v3(W) * v3(wMis) * vt;
+    if (INLINE) return X * trans;
+    out.ray = true;
+    out.o = so; out.d = wiw; out.tmin = 0.0f; out.tmax = dist - 0.001f; out.X = X;
     return v3(0.0f);
 }
 // EnvmapDirectIllumination (Emitter.hlsli:275-326) up to the shadow trace.
@@ -777,7 +854,8 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
                     } else if (C != CLS_DELTA &&
                                (type == PT_MAT_DIFFUSE || type == PT_MAT_MICROFACET || type == PT_MAT_DISNEY ||
                                 type == PT_MAT_HAIR)) {  // Shaders.hlsl:473-511
-                        float3 ra = nee_area<INLINE>(A, hp, N, Ng, T, B, wil, type, m, h, rng, neeA, aseed, st.z);
+                        float3 ra = A.risNee ? nee_ris<INLINE>(A, hp, N, Ng, T, B, wil, type, m, h, rng, neeA, aseed, st.z)
+                                             : nee_area<INLINE>(A, hp, N, Ng, T, B, wil, type, m, h, rng, neeA, aseed, st.z);
                         float3 re = nee_env<INLINE>(A, hp, N, Ng, T, B, wil, type, m, h, rng, neeE, aseed, st.z);
                         if (INLINE) {
                             Lo += thr * ra;
@@ -1176,6 +1254,7 @@ bool graph_matches(const pt_ctx *ctx, const pt_render_params *P, size_t cap, con
            G.rngKind == P->rng_kind && G.envSampling == P->env_sampling && G.cap == cap && G.sum == sum &&
            G.comp == comp && G.sceneGen == ctx->sceneGen && G.waveGen == ctx->waveGen &&
            G.cached == A.cacheOn && G.trainOn == A.trainOn && (!A.cacheOn || G.cacheGen == ctx->cache.gen) &&
+           G.risNee == A.risNee &&
            memcmp(&G.cam, &P->camera, sizeof(pt_camera)) == 0;
 }
 }  // namespace
@@ -1238,6 +1317,7 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
     A.err = ctx->d_err;
     A.shadowCap = (uint32_t)(2 * B.cap);
     A.batch = 0; A.numReqs = 0; A.reqs = nullptr; A.slotInfo = nullptr;
+    A.risNee = (P->flags & PT_RENDER_RIS_NEE) ? 1u : 0u;
     A.cacheOn = (P->flags & PT_RENDER_RADIANCE_CACHE) ? 1u : 0u;
     A.trainOn = A.unbiasedEvery = A.recCap = A.queryCap = 0;
     A.roughThr = 0.0f;
@@ -1284,7 +1364,7 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
             G.rngKind = P->rng_kind; G.envSampling = P->env_sampling; G.cam = P->camera;
             G.cap = cap; G.sum = d_sum; G.comp = d_comp;
             G.sceneGen = ctx->sceneGen; G.waveGen = ctx->waveGen;
-            G.cached = A.cacheOn; G.trainOn = A.trainOn; G.cacheGen = ctx->cache.gen;
+            G.cached = A.cacheOn; G.trainOn = A.trainOn; G.cacheGen = ctx->cache.gen; G.risNee = A.risNee;
             G.launches = E.launches;
         } else {  // capture unavailable: issue the launches directly
             cudaGetLastError();
@@ -1565,8 +1645,10 @@ int render_batch(pt_ctx *ctx, const pt_request *R, uint32_t n, float *request_ms
     A.err = ctx->d_err;
     A.shadowCap = (uint32_t)(2 * B.cap);
     A.batch = 1; A.numReqs = n; A.reqs = (const ReqDev *)Bt.reqs; A.slotInfo = Bt.slotInfo;
+    A.risNee = (R[0].params.flags & PT_RENDER_RIS_NEE) ? 1u : 0u;
     // the launch graph depends on the batch's shape, not on cameras, offsets or films (device table)
-    std::vector<uint64_t> key = {n, pl.cap, R[0].params.rng_kind, R[0].params.env_sampling, ctx->sceneGen,
+    std::vector<uint64_t> key = {n, pl.cap, R[0].params.rng_kind, R[0].params.env_sampling, R[0].params.flags,
+                                 ctx->sceneGen,
                                  ctx->waveGen, (uint64_t)(uintptr_t)Bt.slotInfo, (uint64_t)(uint32_t)G.extC,
                                  (uint64_t)(uint32_t)G.shadow, (uint64_t)(uint32_t)clsG[CLS_DISNEY]};
     for (uint32_t k = 0; k < n; k++) {

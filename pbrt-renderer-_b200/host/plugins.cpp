@@ -291,8 +291,10 @@ private:
     std::string m_alphaTexture;
 };
 
-// ---- subsurface (src/cpu/subsurface.cpp): parameters only on the GPU side
-// (the random walk is not built); CPU eval is the reference's Lambertian.
+// ---- subsurface (src/cpu/subsurface.cpp): the GPU renders the random walk
+// (type 6); the CPU eval is the reference's Lambertian stand-in.  Field reuse
+// as the reference's: radius -> subsurface, g -> anisotropic, tint -> sheen /
+// sheenTint / clearcoat.
 class Subsurface : public BSDF {
 public:
     explicit Subsurface(const PropertyList &p) {
@@ -304,6 +306,10 @@ public:
         m_roughness = p.getFloat("roughness", 0.3f);
         m_tint = p.getColor("tint", Color3f(1.f, 1.f, 1.f));
         m_specular = p.getFloat("specular", 0.0f);
+        m_tex[0] = p.getString("albedoTexture", "");
+        m_tex[1] = p.getString("normalTexture", "");
+        m_tex[2] = p.getString("roughnessTexture", "");
+        m_tex[3] = p.getString("specularTexture", "");
     }
     Color3f eval(const BSDFQueryRecord &b) const override {
         if (b.measure != ESolidAngle || b.wi.z() <= 0 || b.wo.z() <= 0) return Color3f(0.0f);
@@ -327,6 +333,8 @@ public:
         d.intIOR = m_intIOR; d.extIOR = m_extIOR; d.subsurface = m_radius; d.anisotropic = m_g;
         d.roughness = m_roughness; d.sheen = m_tint.r(); d.sheenTint = m_tint.g(); d.clearcoat = m_tint.b();
         d.specular = m_specular;
+        d.albedoTexture = m_tex[0]; d.normalTexture = m_tex[1]; d.roughnessTexture = m_tex[2];
+        d.specularTexture = m_tex[3];
         return d;
     }
     std::string toString() const override { return "Subsurface[]"; }
@@ -334,6 +342,7 @@ public:
 private:
     Color3f m_albedo, m_tint;
     float m_radius, m_intIOR, m_extIOR, m_g, m_roughness, m_specular;
+    std::string m_tex[4];
 };
 
 // ---- area emitter (src/cpu/area.cpp) ----------------------------------------------

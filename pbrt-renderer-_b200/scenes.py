@@ -146,7 +146,7 @@ def _flat_normals(pos, faces):
 # ---------------------------------------------------------------------------
 # configuration 1: Cornell-style box
 # ---------------------------------------------------------------------------
-def cornell(width=256, height=256, subdiv=3):
+def cornell(width=256, height=256, subdiv=3, many_lights=False):
     """Closed 12-triangle room (white 0.73, red 0.65, green 0.12 walls), a Disney
     icosphere (roughness 0.5) and a downward quad light of radiance 17."""
     b = _Builder()
@@ -167,11 +167,19 @@ def cornell(width=256, height=256, subdiv=3):
     b.add(pl, fl, red, normals=_flat_normals(pl, fl))
     pr, fr = _quad((1, 0, -1), (1, 2, -1), (1, 2, 1), (1, 0, 1))           # right (-x), green
     b.add(pr, fr, green, normals=_flat_normals(pr, fr))
-    # light: 0.5 x 0.5 quad just under the ceiling, normal -y
+    # light: 0.5 x 0.5 quad just under the ceiling, normal -y (or four small
+    # coloured quads of uneven power, for many-light sampling)
     y = 1.98
-    pq, fq = _quad((-0.25, y, -0.25), (0.25, y, -0.25), (0.25, y, 0.25), (-0.25, y, 0.25))
-    light = make_material(PT_MAT_DIFFUSE, (0.0, 0.0, 0.0), radiance=(17.0, 17.0, 17.0))
-    b.add(pq, fq, light, normals=_flat_normals(pq, fq))
+    if not many_lights:
+        pq, fq = _quad((-0.25, y, -0.25), (0.25, y, -0.25), (0.25, y, 0.25), (-0.25, y, 0.25))
+        light = make_material(PT_MAT_DIFFUSE, (0.0, 0.0, 0.0), radiance=(17.0, 17.0, 17.0))
+        b.add(pq, fq, light, normals=_flat_normals(pq, fq))
+    else:
+        for (cx, cz, s, rad) in ((-0.6, -0.6, 0.12, (40.0, 8.0, 8.0)), (0.6, -0.5, 0.2, (6.0, 20.0, 6.0)),
+                                 (0.0, 0.5, 0.3, (4.0, 4.0, 12.0)), (0.55, 0.55, 0.08, (90.0, 90.0, 60.0))):
+            pq, fq = _quad((cx - s, y, cz - s), (cx + s, y, cz - s), (cx + s, y, cz + s), (cx - s, y, cz + s))
+            light = make_material(PT_MAT_DIFFUSE, (0.0, 0.0, 0.0), radiance=rad)
+            b.add(pq, fq, light, normals=_flat_normals(pq, fq))
     v, f = icosphere(subdiv)
     sph = make_material(PT_MAT_DISNEY, (0.8, 0.6, 0.4), roughness=0.5)
     c, r = np.array([0.0, 0.55, -0.1]), 0.55

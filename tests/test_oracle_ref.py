@@ -100,3 +100,33 @@ def test_render_identical(name, depth, scene_set, pt, oracle, reference):
     sr = reference.render(P, threads=4)
     assert np.array_equal(so, sr)
     assert so[..., 3].min() == 3.0
+
+
+@pytest.fixture(scope="module")
+def reference_ris(pt):
+    from oracle.oracle import Reference
+    if not Reference.available(ris=True):
+        pytest.skip("reference shader build with USE_RIS=1 (oracle/_ref/libref_ris.so) not present")
+    return Reference(pt, ris=True)
+
+
+@pytest.mark.parametrize("name", ["many_lights", "spheres"])
+def test_ris_render_identical(name, scenes, pt, oracle, reference_ris):
+    """PT_RENDER_RIS_NEE restates the reference's USE_RIS=1 build
+    (RISDirectIllumination, shaders/Emitter.hlsli:155-271): same image bits."""
+    if name == "many_lights":
+        sc, cam = scenes.cornell(48, 40, many_lights=True)
+        W, H, depth = 48, 40, 8
+    else:
+        sc, cam = scenes.disney_spheres(40, 32, grid=2, slices=24, rings=13, env_w=128, env_h=64)
+        W, H, depth = 40, 32, 16
+    oracle.load(sc)
+    reference_ris.load(sc)
+    P = pt.render_params(W, H, 3, cam, max_depth=depth, sample_offset=2, flags=pt.PT_RENDER_RIS_NEE)
+    so, _, _ = oracle.render(P, threads=4)
+    sr = reference_ris.render(P, threads=4)
+    assert np.array_equal(so, sr)
+    # with area lights RIS draws other samples than MIS (without any it is MIS)
+    P2 = pt.render_params(W, H, 3, cam, max_depth=depth, sample_offset=2)
+    sm, _, _ = oracle.render(P2, threads=4)
+    assert np.array_equal(so, sm) == (name == "spheres")
