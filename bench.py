@@ -69,6 +69,12 @@ def workload(name, scale=1.0):
         sc, cam = scenes.cornell(W, H)
         cfg = {"workload": "cornell", "triangles": sc.num_triangles, "width": W, "height": H, "spp": spp,
                "max_depth": depth}
+    elif name == "radiance_cache":
+        W, H, spp, depth = 1920, 1080, 16, 16
+        sc, cam = scenes.radiance_cache_scene(W, H)
+        cfg = {"workload": "radiance_cache", "triangles": sc.num_triangles, "instances": 122, "width": W, "height": H,
+               "spp": spp, "max_depth": depth, "materials": "Disney + hair (every 7th instance)",
+               "medium": "homogeneous fog box, albedo 0.9, g 0.3", "envmap": "2048x1024 rgb32f"}
     elif name == "hair_volume":
         W, H, spp, depth = 1024, 1024, 128, 16
         sc, cam = scenes.hair_volume(W, H)
@@ -208,7 +214,7 @@ def progressive(pt, ctx, stream, W, H, ref_img, make_params, spf, warm=0):
 # each), the first CACHE_WARM calls training only, up to 65,536 records per
 # call from at most 10 % of the paths that reach a cache vertex, bounces with
 # Disney roughness >= 0.1 end into the cache, no unbiased suffixes.
-CACHE_SPF, CACHE_WARM, CACHE_RECORDS, CACHE_LR = 2, 16, 65536, 1e-2
+CACHE_SPF, CACHE_WARM, CACHE_RECORDS, CACHE_LR = 2, 8, 65536, 1e-2
 CACHE_FRACTION, CACHE_ROUGH = 0.1, 0.1
 
 
@@ -458,7 +464,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="pt", choices=["pt", "reference"])
-    ap.add_argument("--workload", default="disney_envmap", choices=["disney_envmap", "cornell", "hair_volume"])
+    ap.add_argument("--workload", default="disney_envmap",
+                    choices=["disney_envmap", "cornell", "hair_volume", "radiance_cache"])
     ap.add_argument("--env-sampling", default="cdf", choices=["cdf", "alias"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -417,6 +417,94 @@ def hair_volume(width=1024, height=1024, strands=20000, segments=32, seed=0, gri
     return scene, cam
 
 
+# ---------------------------------------------------------------------------
+# configuration 5: the radiance-cache scene (~10 M triangles, mixed materials)
+# ---------------------------------------------------------------------------
+def displaced_icosphere(subdiv, seed, amp=0.12):
+    """Icosphere with a smooth radial displacement (a sum of 12 random
+    spherical waves); returns positions, faces and vertex normals."""
+    v, f = icosphere(subdiv)
+    rng = np.random.default_rng(seed)
+    k = rng.normal(size=(12, 3))
+    k /= np.linalg.norm(k, axis=1, keepdims=True)
+    freq = rng.uniform(2.0, 9.0, 12)
+    ph = rng.uniform(0, 2 * np.pi, 12)
+    w = rng.uniform(0.3, 1.0, 12) / np.arange(1, 13)
+    disp = (np.sin((v @ k.T) * freq + ph) * w).sum(1)
+    disp = amp * disp / np.abs(disp).max()
+    p = v * (1.0 + disp)[:, None]
+    tri = p[f]
+    fn = np.cross(tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0])
+    n = np.zeros_like(p)
+    for c in range(3):
+        np.add.at(n, f[:, c], fn)
+    n /= np.linalg.norm(n, axis=1, keepdims=True) + 1e-20
+    return p, f, n
+
+
+def radiance_cache_scene(width=1920, height=1080, instances=122, subdiv=6, seed=0, volume=True):
+    """Configuration 5: `instances` copies (random scale, rotation, placement)
+    of one displaced icosphere of 81,920 triangles (~10 M triangles at 122),
+    on a ground plane with a back wall; Disney materials (U[0,1] parameters,
+    roughness U[0.05, 1]) with every 7th instance a hair material (BCSDF on
+    the sphere surface, h from the UV parametrisation); a homogeneous fog
+    box over part of the scene (albedo 0.9, g 0.3) when `volume`; the sky +
+    sun envmap at 2048 x 1024."""
+    rng = np.random.default_rng(seed)
+    b = _Builder()
+    base_p, base_f, base_n = displaced_icosphere(subdiv, seed + 1)
+    # spherical UVs for hair's h and tangent frame
+    base_uv = np.stack([0.5 + np.arctan2(base_p[:, 0], base_p[:, 2]) / (2 * np.pi),
+                        0.5 + np.arcsin(np.clip(base_p[:, 1] / np.linalg.norm(base_p, axis=1), -1, 1)) / np.pi], 1)
+    side = int(np.ceil(np.sqrt(instances)))
+    for i in range(instances):
+        gx, gz = i % side, i // side
+        s = rng.uniform(0.5, 1.1)
+        q = rng.normal(size=4)
+        q /= np.linalg.norm(q)
+        a, bq, c, d = q
+        R = np.array([[a * a + bq * bq - c * c - d * d, 2 * (bq * c - a * d), 2 * (bq * d + a * c)],
+                      [2 * (bq * c + a * d), a * a - bq * bq + c * c - d * d, 2 * (c * d - a * bq)],
+                      [2 * (bq * d - a * c), 2 * (c * d + a * bq), a * a - bq * bq - c * c + d * d]])
+        t = np.array([(gx - side / 2) * 2.6 + rng.uniform(-0.4, 0.4), s * 1.05,
+                      (gz - side / 2) * 2.6 + rng.uniform(-0.4, 0.4)])
+        pos = (base_p @ R.T) * s + t
+        nrm = base_n @ R.T
+        if i % 7 == 3:
+            m = make_material(PT_MAT_HAIR, tuple(eumelanin_to_color(rng.uniform(0.3, 4.0), 0.3)))
+            m.roughness, m.betaN, m.alpha, m.intIOR = 0.3, 0.3, 2.0, 1.55
+        else:
+            m = make_material(PT_MAT_DISNEY, tuple(rng.uniform(0, 1, 3)))
+            m.roughness = float(rng.uniform(0.05, 1.0))
+            m.metallic, m.specular, m.specularTint = (float(x) for x in rng.uniform(0, 1, 3))
+            m.sheen, m.sheenTint, m.subsurface = (float(x) for x in rng.uniform(0, 1, 3))
+            m.clearcoat, m.clearcoatGloss = (float(x) for x in rng.uniform(0, 1, 2))
+        b.add(pos, base_f, m, normals=nrm, uvs=base_uv)
+    ext = side * 1.3 + 4
+    pg, fg = _quad((-ext, 0, -ext), (-ext, 0, ext), (ext, 0, ext), (ext, 0, -ext))
+    ground = make_material(PT_MAT_DISNEY, (0.6, 0.58, 0.55))
+    ground.roughness = 0.7
+    b.add(pg, fg, ground, normals=_flat_normals(pg, fg))
+    pw, fw = _quad((-ext, 0, -ext), (ext, 0, -ext), (ext, 12, -ext), (-ext, 12, -ext))
+    wall = make_material(PT_MAT_DIFFUSE, (0.7, 0.7, 0.72))
+    b.add(pw, fw, wall, normals=_flat_normals(pw, fw))
+    env = sky_envmap(2048, 1024, sun_peak=2.0e4)
+    vols = []
+    if volume:
+        v = pt_volume()
+        v.vmin[:] = (-ext * 0.2, 0.0, -ext * 0.6)
+        v.vmax[:] = (ext * 0.6, 3.0, ext * 0.3)
+        v.sigma_a[:] = (0.003, 0.003, 0.003)
+        v.sigma_s[:] = (0.027, 0.027, 0.027)   # albedo 0.9
+        v.phase_g = 0.3
+        v.flags = 0
+        v.density_grid = PT_NO_TEXTURE
+        vols.append(v)
+    scene = b.scene(env_rgb=env, env_scale=1.0, volumes=vols)
+    cam = look_at_camera((0.0, side * 1.1 + 3.0, side * 1.5 + 6.0), (0.0, 0.5, 0.0), (0, 1, 0), 42.0, width / height)
+    return scene, cam
+
+
 def sample_directions(n, seed, upper=False):
     """Uniform unit vectors (upper hemisphere if `upper`), float32."""
     rng = np.random.default_rng(seed)
