@@ -532,6 +532,13 @@ int pt_upload_scene(pt_ctx *ctx, const pt_scene_desc *d) {
     if ((rc = upload_textures(ctx, d))) return rc;
     S.hasAlpha = hasAlpha ? 1u : 0u;
     S.hasSubsurface = hasSubsurface ? 1u : 0u;
+    {  // homogeneous media only (and no subsurface walks): the wavefront form
+        bool homog = d->num_volumes > 0;
+        for (uint32_t v = 0; v < d->num_volumes; v++)
+            if (d->volumes[v].flags & PT_VOLUME_HETEROGENEOUS) homog = false;
+        S.mediaWavefront = (homog && !hasSubsurface) ? 1u : 0u;
+        if (S.mediaWavefront) clsMask |= 1u << CLS_MEDIUM;
+    }
     S.pos = dpos; S.nrm = dnrm; S.uv = duv; S.tan = dtan; S.idx = didx;
     S.mats = dmats; S.meshClass = dmcls; S.numMeshes = d->num_meshes; S.meshFirstTri = dmft;
     S.emitterCdf = dcdf; S.emitterList = demit; S.emitterCount = ne;

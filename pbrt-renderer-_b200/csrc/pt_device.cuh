@@ -72,6 +72,8 @@ struct DevScene {
     uint32_t numTex;
     uint32_t hasAlpha;          // any alpha-mapped mesh (alpha-tested triangles)
     uint32_t hasSubsurface;     // any subsurface (type 6) mesh: shading traces its walks inline
+    uint32_t mediaWavefront;    // media, all homogeneous, no subsurface: free flights in the closest-hit
+                                // kernel, medium events as their own shading class, NEE deferred
 };
 
 // One texture's mip chain in DevScene::texels (level l: max(w >> l, 1) x

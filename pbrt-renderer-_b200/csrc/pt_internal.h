@@ -35,7 +35,8 @@ enum ShadeClass : int {
     CLS_DISNEY = 5,
     CLS_HAIR = 6,
     CLS_TEX = 7,  // + CLS_TEX: the same class for materials with shading textures
-    CLS_N = 14
+    CLS_MEDIUM = 14,  // a scattering event in a (homogeneous) medium, found by the closest-hit kernel
+    CLS_N = 15
 };
 // The reference's hasAnyTex (shaders/Shaders.hlsl:232-236): texture maps the
 // shading reads (alpha maps act in the traversal, metallic maps nowhere).

@@ -229,7 +229,12 @@ __device__ __forceinline__ void finish_extend(const WaveArgs &A, uint32_t i, con
         class_append(A, c, i);
     }
 }
-template <bool CLASSIFY>
+// MEDIA: the free flight of Shaders.hlsl:133-179 follows the closest hit here
+// (draws from the path's stream in the shader's order); a scattering event
+// goes to the medium class with (t, volume | 1 << 31) in the hit record and
+// the throughput gets the flight's weight.  Homogeneous media only: their
+// shadow-ray transmittance draws nothing, so NEE can be deferred.
+template <bool CLASSIFY, bool MEDIA = false>
 __global__ void __launch_bounds__(kBlock) k_extend(WaveArgs A) {
     // grid-stride over the queue in order: the 32 rays of a warp are
     // neighbours in the queue (coherent traversal), and the class queues and
@@ -247,6 +252,31 @@ __global__ void __launch_bounds__(kBlock) k_extend(WaveArgs A) {
         }
         Hit h = trace_closest(A.S, make_float3(o.x, o.y, o.z), make_float3(d.x, d.y, d.z), o.w, d.w, A.err, aseed,
                               akey);
+        if (MEDIA) {
+            const uint32_t slot = A.qslotIn[i];
+            uint4 st = A.rng[slot];
+            Rng r = load_rng(A, slot, st);
+            float3 vw = v3(1.0f);
+            float tsc;
+            uint32_t svi;
+            bool sc = sample_free_flight(A.S, make_float3(o.x, o.y, o.z), make_float3(d.x, d.y, d.z),
+                                         h.gid != 0xFFFFFFFFu ? h.t : 1e20f, r, vw, tsc, svi);
+            if (r.dim != st.x || r.white != st.y) {
+                st.x = r.dim;
+                st.y = r.white;
+                A.rng[slot] = st;
+            }
+            if (vw.x != 1.0f || vw.y != 1.0f || vw.z != 1.0f) {
+                float4 tp = A.thr_pdf[slot];
+                float3 t3 = make_float3(tp.x, tp.y, tp.z) * vw;
+                A.thr_pdf[slot] = make_float4(t3.x, t3.y, t3.z, tp.w);
+            }
+            if (sc) {
+                A.qhit[i] = make_float4(tsc, __uint_as_float(svi | 0x80000000u), 0.0f, 0.0f);
+                class_append(A, CLS_MEDIUM, i);
+                continue;
+            }
+        }
         finish_extend<CLASSIFY>(A, i, h);
     }
 }
@@ -313,7 +343,7 @@ __device__ __forceinline__ float3 nee_area(const WaveArgs &A, float3 hp, float3 
     material_eval_pdf_t(type, wil, to_local(ww, T, B, N), m, h, f, pb);
     float pe = es.pdfArea * dist * dist / cl;
     float w = balance(pe, pb);
-    float3 vt = INLINE ? multi_volume_tr(S, so, ww, dist, rng) : v3(1.0f);
+    float3 vt = (INLINE || S.mediaWavefront) ? multi_volume_tr(S, so, ww, dist, rng) : v3(1.0f);
     float3 X = es.rad * f * act / v3(mx(pe, 1e-20f)) * w * vt;
     if (INLINE) return X * trans;
     out.ray = true;
@@ -389,7 +419,7 @@ __device__ __forceinline__ float3 nee_ris(const WaveArgs &A, float3 hp, float3 N
     float pdfBsdf;
     material_eval_pdf_t(type, wil, to_local(wiw, T, B, N), m, h, fu, pdfBsdf);
     float wMis = balance(pSA, pdfBsdf);
-    float3 vt = INLINE ? multi_volume_tr(S, so, wiw, dist, rng) : v3(1.0f);
+    float3 vt = (INLINE || S.mediaWavefront) ? multi_volume_tr(S, so, wiw, dist, rng) : v3(1.0f);
     float3 X = integ * v3(W) * v3(wMis) * vt;
     if (INLINE) return X * trans;
     out.ray = true;
@@ -422,7 +452,7 @@ __device__ __forceinline__ float3 nee_env(const WaveArgs &A, float3 hp, float3 N
     float pb;
     material_eval_pdf_t(type, wil, to_local(ww, T, B, N), m, h, f, pb);
     float w = balance(pe, pb);
-    float3 vt = INLINE ? multi_volume_tr(S, so, ww, 1e20f, rng) : v3(1.0f);
+    float3 vt = (INLINE || S.mediaWavefront) ? multi_volume_tr(S, so, ww, 1e20f, rng) : v3(1.0f);
     float3 X = Le * f * act / v3(mx(pe, 1e-20f)) * w * vt;
     if (INLINE) return X * trans;
     out.ray = true;
@@ -438,9 +468,14 @@ __device__ bool vol_nee_skip(const pt_volume &v, float3 p) {
     float md = mn(mn(dmn.x, dmn.y), mn(dmn.z, mn(dmx.x, mn(dmx.y, dmx.z))));
     return md * smin > 8.0f;
 }
+// Volume NEE (Emitter.hlsli:334-434): traced inline (INLINE), or up to the
+// shadow trace with the trace deferred (homogeneous media in the wavefront,
+// whose transmittance along the shadow ray draws nothing).
+template <bool INLINE>
 __device__ float3 vol_nee_area(const WaveArgs &A, float3 sp, float3 wo, uint32_t vi, Rng &rng, uint32_t aseed,
-                               uint32_t bounce) {
+                               uint32_t bounce, NeeOut &out) {
     const DevScene &S = A.S;
+    out.ray = false;
     const pt_volume &v = S.vols[vi];
     if (vol_nee_skip(v, sp)) return v3(0.0f);
     EmitterSample es = sample_emitter(S, rng);
@@ -450,17 +485,24 @@ __device__ float3 vol_nee_area(const WaveArgs &A, float3 sp, float3 wo, uint32_t
     float3 wi = tl / v3(dist);
     float cl = dot(es.nrm, -wi);
     if (cl <= 0.0f) return v3(0.0f);
-    float3 trans;
-    if (trace_shadow(S, sp, wi, 0.001f, dist - 0.001f, trans, A.err, aseed, alpha_key(bounce, 1u))) return v3(0.0f);
+    float3 trans = v3(1.0f);
+    if (INLINE && trace_shadow(S, sp, wi, 0.001f, dist - 0.001f, trans, A.err, aseed, alpha_key(bounce, 1u)))
+        return v3(0.0f);
     float fp = hg(dot(wo, wi), v.phase_g);
     float pe = es.pdfArea * dist * dist / cl;
     float w = balance(pe, fp);
     float3 vt = multi_volume_tr(S, sp, wi, dist, rng);
-    return es.rad * fp / v3(mx(pe, 1e-20f)) * w * vt * trans;
+    float3 X = es.rad * fp / v3(mx(pe, 1e-20f)) * w * vt;
+    if (INLINE) return X * trans;
+    out.ray = true;
+    out.o = sp; out.d = wi; out.tmin = 0.001f; out.tmax = dist - 0.001f; out.X = X;
+    return v3(0.0f);
 }
+template <bool INLINE>
 __device__ float3 vol_nee_env(const WaveArgs &A, float3 sp, float3 wo, uint32_t vi, Rng &rng, uint32_t aseed,
-                              uint32_t bounce) {
+                              uint32_t bounce, NeeOut &out) {
     const DevScene &S = A.S;
+    out.ray = false;
     const pt_volume &v = S.vols[vi];
     if (vol_nee_skip(v, sp)) return v3(0.0f);
     float u1 = next_float(rng, S.sobol1), u2 = next_float(rng, S.sobol1);
@@ -468,12 +510,17 @@ __device__ float3 vol_nee_env(const WaveArgs &A, float3 sp, float3 wo, uint32_t 
     float pe;
     env_sample(S, A.envMode, u1, u2, wi, Le, pe);
     if (pe <= 0.0f) return v3(0.0f);
-    float3 trans;
-    if (trace_shadow(S, sp, wi, 0.001f, 1e20f, trans, A.err, aseed, alpha_key(bounce, 2u))) return v3(0.0f);
+    float3 trans = v3(1.0f);
+    if (INLINE && trace_shadow(S, sp, wi, 0.001f, 1e20f, trans, A.err, aseed, alpha_key(bounce, 2u)))
+        return v3(0.0f);
     float fp = hg(dot(wo, wi), v.phase_g);
     float w = balance(pe, fp);
     float3 vt = multi_volume_tr(S, sp, wi, 1e20f, rng);
-    return Le * fp / v3(mx(pe, 1e-20f)) * w * vt * trans;
+    float3 X = Le * fp / v3(mx(pe, 1e-20f)) * w * vt;
+    if (INLINE) return X * trans;
+    out.ray = true;
+    out.o = sp; out.d = wi; out.tmin = 0.001f; out.tmax = 1e20f; out.X = X;
+    return v3(0.0f);
 }
 
 __device__ __forceinline__ void push_shadow(const WaveArgs &A, bool pred, uint32_t slot, uint32_t kind,
@@ -504,9 +551,9 @@ __host__ __device__ constexpr uint32_t class_type(int c) {
 // their register use gives anyway (a bound makes the compiler spend up to it).
 template <int CLS>
 struct ShadeBlocks {
-    static constexpr int base = CLS < 0 ? CLS : CLS % CLS_TEX;
+    static constexpr int base = CLS < 0 ? CLS : CLS == CLS_MEDIUM ? CLS : CLS % CLS_TEX;
     static constexpr int value = base == CLS_MISS ? 5 : (base == CLS_EMIT || base == CLS_DELTA) ? 4
-                                                      : base == CLS_DISNEY ? 3 : 2;
+                                                      : (base == CLS_DISNEY || base == CLS_MEDIUM) ? 3 : 2;
 };
 
 // SubsurfaceWalk (Subsurface.hlsli:49-144): random walk inside the closed
@@ -646,7 +693,7 @@ __device__ __forceinline__ bool rough_bounce(const WaveArgs &A, uint32_t type, c
 template <bool INLINE, int CLS>
 __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveArgs A) {
     constexpr int C = ShadeBlocks<CLS>::base;    // the event / material class
-    constexpr bool TEX = CLS >= (int)CLS_TEX;    // shading textures present
+    constexpr bool TEX = CLS >= (int)CLS_TEX && CLS != (int)CLS_MEDIUM;  // shading textures present
     const DevScene &S = A.S;
     uint32_t n = CLS == CLS_ANY ? *(volatile uint32_t *)A.cntIn : *(volatile uint32_t *)(A.cntCls + CLS);
     uint32_t iters = (n + gridDim.x * blockDim.x - 1) / (gridDim.x * blockDim.x);
@@ -699,8 +746,8 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
                     const pt_volume &v = S.vols[svi];
                     float3 spos = xpos(ro, rd, tsc);
                     thr *= make_float3(v.sigma_s[0], v.sigma_s[1], v.sigma_s[2]) / vmax(vsigma_t(v), v3(1e-20f));
-                    Lo += thr * vol_nee_area(A, spos, rd, svi, rng, aseed, st.z);
-                    Lo += thr * vol_nee_env(A, spos, rd, svi, rng, aseed, st.z);
+                    Lo += thr * vol_nee_area<true>(A, spos, rd, svi, rng, aseed, st.z, neeA);
+                    Lo += thr * vol_nee_env<true>(A, spos, rd, svi, rng, aseed, st.z, neeE);
                     float x1 = next_float(rng, S.sobol1), x2 = next_float(rng, S.sobol1);
                     float pp;
                     nd = sample_hg(rd, v.phase_g, x1, x2, pp);
@@ -711,7 +758,26 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
                     st.w |= kFlagRough;
                 }
             }
-            if (volScat) {
+            if (C == CLS_MEDIUM) {  // scattering in a homogeneous medium (Shaders.hlsl:149-178), NEE deferred
+                const uint32_t svi = gid & 0x7FFFFFFFu;
+                const pt_volume &v = S.vols[svi];
+                float3 spos = xpos(ro, rd, h4.x);
+                thr *= make_float3(v.sigma_s[0], v.sigma_s[1], v.sigma_s[2]) / vmax(vsigma_t(v), v3(1e-20f));
+                vol_nee_area<false>(A, spos, rd, svi, rng, aseed, st.z, neeA);
+                vol_nee_env<false>(A, spos, rd, svi, rng, aseed, st.z, neeE);
+                thrNee = thr;
+                if (!neeA.ray) A.pendA[slot] = make_float4(thr.x * 0.0f, thr.y * 0.0f, thr.z * 0.0f, 0.0f);
+                if (!neeE.ray) A.pendE[slot] = make_float4(thr.x * 0.0f, thr.y * 0.0f, thr.z * 0.0f, 0.0f);
+                st.w |= kFlagPending;
+                float x1 = next_float(rng, S.sobol1), x2 = next_float(rng, S.sobol1);
+                float pp;
+                nd = sample_hg(rd, v.phase_g, x1, x2, pp);
+                no = spos;
+                ntmin = 0.0f;
+                lastPdf = mx(pp, 1e-20f);
+                cont = true;
+                st.w |= kFlagRough;
+            } else if (volScat) {
             } else if (C == CLS_MISS || (C == CLS_ANY && !hit)) {  // Shaders.hlsl:188-212
                 float3 env = eval_env(S, rd);
                 if (lastPdf == 0.0f) Lo += thr * env;
@@ -1082,7 +1148,7 @@ constexpr size_t kWaveBytesPerPath = 5 * 16 + 2 * (4 + 16 + 16) + 16 + 4 * CLS_N
 // several waves, whose tails are small at this size, instead of regrowing the
 // buffers (a free + malloc of tens of GB that would stall the render).
 constexpr size_t kMaxWavePaths = (size_t)1 << 26;
-static_assert(kWaveBytesPerPath == 360, "wave state layout");
+static_assert(kWaveBytesPerPath == 364, "wave state layout");
 
 static int wave_alloc(pt_ctx *ctx, size_t cap) {
     if (ctx->W.cap >= cap) return PT_OK;
@@ -1116,8 +1182,8 @@ const Kernel kShadeCls[CLS_N] = {
     k_shade<false, CLS_DIFFUSE>,        k_shade<false, CLS_MICRO>,          k_shade<false, CLS_DISNEY>,
     k_shade<false, CLS_HAIR>,           k_shade<false, CLS_MISS>,           k_shade<false, CLS_TEX + CLS_EMIT>,
     k_shade<false, CLS_TEX + CLS_DELTA>, k_shade<false, CLS_TEX + CLS_DIFFUSE>, k_shade<false, CLS_TEX + CLS_MICRO>,
-    k_shade<false, CLS_TEX + CLS_DISNEY>, k_shade<false, CLS_TEX + CLS_HAIR>};
-int gExt = 0, gExtC = 0, gShadeI = 0, gShadow = 0, gCls[CLS_N];
+    k_shade<false, CLS_TEX + CLS_DISNEY>, k_shade<false, CLS_TEX + CLS_HAIR>, k_shade<false, CLS_MEDIUM>};
+int gExt = 0, gExtC = 0, gExtM = 0, gShadeI = 0, gShadow = 0, gCls[CLS_N];
 
 enum { STG_RAYGEN, STG_EXTEND, STG_SHADE, STG_SHADOW, STG_FILM, STG_CACHE, STG_N };
 struct Mark { int stage; cudaEvent_t a, b; };
@@ -1145,7 +1211,7 @@ struct Enqueue {
 
 // Grid sizes of the traversal and shading kernels (grid-stride loops).
 struct Grids {
-    int ext, extC, shadeI, shadow;
+    int ext, extC, extM, shadeI, shadow;
     const int *cls;
 };
 
@@ -1153,7 +1219,7 @@ struct Grids {
 // Returns the first failing call's status (cudaSuccess if none).
 cudaError_t enqueue_paths(const pt_ctx *ctx, Enqueue &E, WaveArgs &A, uint32_t depth, const Grids &G) {
     const WaveBuffers &B = ctx->W;
-    const bool inl = ctx->S.numVols > 0 || ctx->S.hasSubsurface;
+    const bool inl = (ctx->S.numVols > 0 && !ctx->S.mediaWavefront) || ctx->S.hasSubsurface;
     cudaStream_t st = E.st;
     cudaError_t err = cudaSuccess;
     auto chk = [&](cudaError_t e) {
@@ -1180,7 +1246,8 @@ cudaError_t enqueue_paths(const pt_ctx *ctx, Enqueue &E, WaveArgs &A, uint32_t d
         } else {
             chk(cudaMemsetAsync(A.cntCls, 0, CLS_N * sizeof(uint32_t), st));
             E.begin(STG_EXTEND);
-            k_extend<true><<<G.extC, kBlock, 0, st>>>(A);
+            if (ctx->S.mediaWavefront) k_extend<true, true><<<G.extM, kBlock, 0, st>>>(A);
+            else k_extend<true><<<G.extC, kBlock, 0, st>>>(A);
             E.end();
             for (int c = 0; c < CLS_N; c++) {
                 if (!((ctx->clsMask >> c) & 1u)) continue;
@@ -1207,7 +1274,7 @@ cudaError_t enqueue_render(const pt_ctx *ctx, Enqueue &E, WaveArgs A, const pt_r
         if (err == cudaSuccess && e != cudaSuccess) err = e;
     };
     const bool cached = A.cacheOn != 0;
-    const Grids G{gExt, gExtC, gShadeI, gShadow, gCls};
+    const Grids G{gExt, gExtC, gExtM, gShadeI, gShadow, gCls};
     chk(cudaMemsetAsync(B.counters, 0, kCounterWords * sizeof(uint32_t), st));
     chk(cudaMemsetAsync(ctx->d_err, 0, 4, st));
     if (cached) {  // per-call cache counters: records [2], queries of the call [5], records with targets [6]
@@ -1296,6 +1363,7 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
     if (!gExt) {
         gExt = grid_for(ctx, (const void *)k_extend<false>);
         gExtC = grid_for(ctx, (const void *)k_extend<true>);
+        gExtM = grid_for(ctx, (const void *)k_extend<true, true>);
         gShadeI = grid_for(ctx, (const void *)k_shade<true, CLS_ANY>);
         gShadow = grid_for(ctx, (const void *)k_shadow);
         for (int c = 0; c < CLS_N; c++) gCls[c] = grid_for(ctx, (const void *)kShadeCls[c]);
@@ -1572,6 +1640,7 @@ int render_batch(pt_ctx *ctx, const pt_request *R, uint32_t n, float *request_ms
     if (!gExt) {
         gExt = grid_for(ctx, (const void *)k_extend<false>);
         gExtC = grid_for(ctx, (const void *)k_extend<true>);
+        gExtM = grid_for(ctx, (const void *)k_extend<true, true>);
         gShadeI = grid_for(ctx, (const void *)k_shade<true, CLS_ANY>);
         gShadow = grid_for(ctx, (const void *)k_shadow);
         for (int c = 0; c < CLS_N; c++) gCls[c] = grid_for(ctx, (const void *)kShadeCls[c]);
@@ -1580,7 +1649,7 @@ int render_batch(pt_ctx *ctx, const pt_request *R, uint32_t n, float *request_ms
     auto sc = [&](int g) { return std::max(ctx->numSMs, (int)((float)g * gridScale)); };
     int clsG[CLS_N];
     for (int c = 0; c < CLS_N; c++) clsG[c] = sc(gCls[c]);
-    const Grids G{sc(gExt), sc(gExtC), sc(gShadeI), sc(gShadow), clsG};
+    const Grids G{sc(gExt), sc(gExtC), sc(gExtM), sc(gShadeI), sc(gShadow), clsG};
 
     const BatchPlan pl = batch_plan(R, n, cap);
     // films: the callers' device films, device copies of host films, or the tuning scratch
