@@ -174,8 +174,10 @@ def reference_image(pt, ctx, W, H, cam, depth, env_mode, chunk):
 def progressive(pt, ctx, stream, W, H, ref_img, make_params, spf, warm=0):
     """Progressive accumulation (the reference's frame-by-frame accumulation):
     render calls of `spf` samples, the first `warm` of them into a discarded
-    film (cache training only), every call timed with CUDA events on the
-    stream.  relMSE against ref_img at the TTQ_CHECKS points (outside the
+    film (cache training only), each call's device time from libpt's CUDA
+    events around its launches (pt_stats.ms_total: the render, its cache
+    inference and training; not the one-time capture of a launch graph for a
+    new call shape).  relMSE against ref_img at the TTQ_CHECKS points (outside the
     timing); the first point at or below the bar gives the time."""
     import torch
 
@@ -187,13 +189,8 @@ def progressive(pt, ctx, stream, W, H, ref_img, make_params, spf, warm=0):
     while acc < REF_SPP // 4:
         P = make_params(TTQ_OFFSET + calls * spf)
         tgt = scratch if calls < warm else film
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        a.record(stream)
-        ctx.render(P, tgt[0].data_ptr(), tgt[1].data_ptr(), pt.PT_MEM_DEVICE)
-        b.record(stream)
-        torch.cuda.synchronize()
-        total_ms += a.elapsed_time(b)
+        _, _, st = ctx.render(P, tgt[0].data_ptr(), tgt[1].data_ptr(), pt.PT_MEM_DEVICE)
+        total_ms += st.ms_total
         calls += 1
         if calls <= warm:
             continue
@@ -210,11 +207,13 @@ def progressive(pt, ctx, stream, W, H, ref_img, make_params, spf, warm=0):
             "spp": None if reached is None else reached[0], "curve": curve}
 
 
-# Radiance-cache settings of the cached form: 2-spp calls (4 training steps
+# Radiance-cache settings of the cached form: 4-spp calls (4 training steps
 # each), the first CACHE_WARM calls training only, up to 65,536 records per
 # call from at most 10 % of the paths that reach a cache vertex, bounces with
-# Disney roughness >= 0.1 end into the cache, no unbiased suffixes.
-CACHE_SPF, CACHE_WARM, CACHE_RECORDS, CACHE_LR = 2, 8, 65536, 1e-2
+# Disney roughness >= 0.1 end into the cache, no unbiased suffixes; inference
+# uses an exponential average of the weights (decay 0.97), which removes the
+# frame-to-frame flicker of a cache that takes 4 steps per call.
+CACHE_SPF, CACHE_WARM, CACHE_RECORDS, CACHE_LR, CACHE_EMA = 4, 8, 65536, 1e-2, 0.97
 CACHE_FRACTION, CACHE_ROUGH = 0.1, 0.1
 
 
@@ -235,13 +234,8 @@ def time_to_relmse(pt, ctx, stream, W, H, cam, depth, env_mode, chunk):
     for nxt in TTQ_CHECKS:
         add = nxt - done
         P = pt.render_params(W, H, add, cam, max_depth=depth, sample_offset=TTQ_OFFSET + done, env_sampling=env_mode)
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        a.record(stream)
-        ctx.render(P, film[0].data_ptr(), film[1].data_ptr(), pt.PT_MEM_DEVICE)
-        b.record(stream)
-        torch.cuda.synchronize()
-        total_ms += a.elapsed_time(b)
+        _, _, st = ctx.render(P, film[0].data_ptr(), film[1].data_ptr(), pt.PT_MEM_DEVICE)
+        total_ms += st.ms_total
         done += add
         e = relmse(D.resolve(film), ref_img)
         curve.append([done, round(e, 6), round(total_ms / 1e3, 5)])
@@ -252,7 +246,7 @@ def time_to_relmse(pt, ctx, stream, W, H, cam, depth, env_mode, chunk):
              "spp": None if reached is None else reached[0], "curve": curve}
 
     def cache_params():
-        return pt.cache_params(seed=0, train_records=CACHE_RECORDS, learning_rate=CACHE_LR,
+        return pt.cache_params(seed=0, train_records=CACHE_RECORDS, learning_rate=CACHE_LR, ema=CACHE_EMA,
                                max_train_fraction=CACHE_FRACTION, rough_threshold=CACHE_ROUGH)
 
     def cached_params(off):
@@ -272,7 +266,8 @@ def time_to_relmse(pt, ctx, stream, W, H, cam, depth, env_mode, chunk):
         st = ctx.cache_stats()
         cached["settings"] = {"spp_per_call": CACHE_SPF, "warmup_calls": CACHE_WARM,
                               "train_records_per_call": CACHE_RECORDS, "max_train_fraction": CACHE_FRACTION,
-                              "rough_threshold": CACHE_ROUGH, "learning_rate": CACHE_LR, "adam_steps": int(st.steps),
+                              "rough_threshold": CACHE_ROUGH, "learning_rate": CACHE_LR, "ema": CACHE_EMA,
+                              "adam_steps": int(st.steps),
                               "network": "64 in, 5 x 64 ReLU, 3 out; BF16 tcgen05, FP32 accumulation"}
     finally:
         ctx.cache_release()

@@ -317,7 +317,7 @@ struct NeeOut {
 };
 
 // MISDirectIllumination (Emitter.hlsli:105-153) up to the shadow trace.
-template <bool INLINE>
+template <bool INLINE, bool MEDIA = false>
 __device__ __forceinline__ float3 nee_area(const WaveArgs &A, float3 hp, float3 N, float3 Ng, float3 T, float3 B,
                                            float3 wil, uint32_t type, const pt_material &m, float h, Rng &rng,
                                            NeeOut &out, uint32_t aseed, uint32_t bounce) {
@@ -343,7 +343,7 @@ __device__ __forceinline__ float3 nee_area(const WaveArgs &A, float3 hp, float3 
     material_eval_pdf_t(type, wil, to_local(ww, T, B, N), m, h, f, pb);
     float pe = es.pdfArea * dist * dist / cl;
     float w = balance(pe, pb);
-    float3 vt = (INLINE || S.mediaWavefront) ? multi_volume_tr(S, so, ww, dist, rng) : v3(1.0f);
+    float3 vt = (INLINE || (MEDIA && S.mediaWavefront)) ? multi_volume_tr(S, so, ww, dist, rng) : v3(1.0f);
     float3 X = es.rad * f * act / v3(mx(pe, 1e-20f)) * w * vt;
     if (INLINE) return X * trans;
     out.ray = true;
@@ -381,7 +381,7 @@ __device__ __forceinline__ bool ris_candidate(const EmitterSample &es, float3 hp
 // candidates through a one-sample reservoir, the survivor re-evaluated and
 // MIS-weighted against the BSDF with its solid-angle pdf (the same pdf the
 // emitter-hit MIS weight uses).
-template <bool INLINE>
+template <bool INLINE, bool MEDIA = false>
 __device__ __forceinline__ float3 nee_ris(const WaveArgs &A, float3 hp, float3 N, float3 Ng, float3 T, float3 B,
                                           float3 wil, uint32_t type, const pt_material &m, float h, Rng &rng,
                                           NeeOut &out, uint32_t aseed, uint32_t bounce) {
@@ -419,7 +419,7 @@ __device__ __forceinline__ float3 nee_ris(const WaveArgs &A, float3 hp, float3 N
     float pdfBsdf;
     material_eval_pdf_t(type, wil, to_local(wiw, T, B, N), m, h, fu, pdfBsdf);
     float wMis = balance(pSA, pdfBsdf);
-    float3 vt = (INLINE || S.mediaWavefront) ? multi_volume_tr(S, so, wiw, dist, rng) : v3(1.0f);
+    float3 vt = (INLINE || (MEDIA && S.mediaWavefront)) ? multi_volume_tr(S, so, wiw, dist, rng) : v3(1.0f);
     float3 X = integ * v3(W) * v3(wMis) * vt;
     if (INLINE) return X * trans;
     out.ray = true;
@@ -427,7 +427,7 @@ __device__ __forceinline__ float3 nee_ris(const WaveArgs &A, float3 hp, float3 N
     return v3(0.0f);
 }
 // EnvmapDirectIllumination (Emitter.hlsli:275-326) up to the shadow trace.
-template <bool INLINE>
+template <bool INLINE, bool MEDIA = false>
 __device__ __forceinline__ float3 nee_env(const WaveArgs &A, float3 hp, float3 N, float3 Ng, float3 T, float3 B,
                                           float3 wil, uint32_t type, const pt_material &m, float h, Rng &rng,
                                           NeeOut &out, uint32_t aseed, uint32_t bounce) {
@@ -452,7 +452,7 @@ __device__ __forceinline__ float3 nee_env(const WaveArgs &A, float3 hp, float3 N
     float pb;
     material_eval_pdf_t(type, wil, to_local(ww, T, B, N), m, h, f, pb);
     float w = balance(pe, pb);
-    float3 vt = (INLINE || S.mediaWavefront) ? multi_volume_tr(S, so, ww, 1e20f, rng) : v3(1.0f);
+    float3 vt = (INLINE || (MEDIA && S.mediaWavefront)) ? multi_volume_tr(S, so, ww, 1e20f, rng) : v3(1.0f);
     float3 X = Le * f * act / v3(mx(pe, 1e-20f)) * w * vt;
     if (INLINE) return X * trans;
     out.ray = true;
@@ -690,7 +690,9 @@ __device__ __forceinline__ bool rough_bounce(const WaveArgs &A, uint32_t type, c
 }
 
 // CLS + CLS_TEX: the kernel of class CLS for materials with shading textures.
-template <bool INLINE, int CLS>
+// EXTRA: the instantiation for RIS NEE and homogeneous media in the wavefront;
+// the default one carries neither (their code would raise register pressure).
+template <bool INLINE, int CLS, bool EXTRA = false>
 __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveArgs A) {
     constexpr int C = ShadeBlocks<CLS>::base;    // the event / material class
     constexpr bool TEX = CLS >= (int)CLS_TEX && CLS != (int)CLS_MEDIUM;  // shading textures present
@@ -758,7 +760,7 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
                     st.w |= kFlagRough;
                 }
             }
-            if (C == CLS_MEDIUM) {  // scattering in a homogeneous medium (Shaders.hlsl:149-178), NEE deferred
+            if (EXTRA && C == CLS_MEDIUM) {  // scattering in a homogeneous medium (Shaders.hlsl:149-178), NEE deferred
                 const uint32_t svi = gid & 0x7FFFFFFFu;
                 const pt_volume &v = S.vols[svi];
                 float3 spos = xpos(ro, rd, h4.x);
@@ -920,9 +922,10 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
                     } else if (C != CLS_DELTA &&
                                (type == PT_MAT_DIFFUSE || type == PT_MAT_MICROFACET || type == PT_MAT_DISNEY ||
                                 type == PT_MAT_HAIR)) {  // Shaders.hlsl:473-511
-                        float3 ra = A.risNee ? nee_ris<INLINE>(A, hp, N, Ng, T, B, wil, type, m, h, rng, neeA, aseed, st.z)
-                                             : nee_area<INLINE>(A, hp, N, Ng, T, B, wil, type, m, h, rng, neeA, aseed, st.z);
-                        float3 re = nee_env<INLINE>(A, hp, N, Ng, T, B, wil, type, m, h, rng, neeE, aseed, st.z);
+                        float3 ra = ((INLINE || EXTRA) && A.risNee)
+                                        ? nee_ris<INLINE, EXTRA>(A, hp, N, Ng, T, B, wil, type, m, h, rng, neeA, aseed, st.z)
+                                        : nee_area<INLINE, EXTRA>(A, hp, N, Ng, T, B, wil, type, m, h, rng, neeA, aseed, st.z);
+                        float3 re = nee_env<INLINE, EXTRA>(A, hp, N, Ng, T, B, wil, type, m, h, rng, neeE, aseed, st.z);
                         if (INLINE) {
                             Lo += thr * ra;
                             Lo += thr * re;
@@ -1177,13 +1180,22 @@ static int wave_alloc(pt_ctx *ctx, size_t cap) {
 namespace {
 using Kernel = void (*)(WaveArgs);
 // per class; entry CLS_TEX + CLS_MISS (a textured miss) never receives paths
-const Kernel kShadeCls[CLS_N] = {
-    k_shade<false, CLS_MISS>,           k_shade<false, CLS_EMIT>,           k_shade<false, CLS_DELTA>,
-    k_shade<false, CLS_DIFFUSE>,        k_shade<false, CLS_MICRO>,          k_shade<false, CLS_DISNEY>,
-    k_shade<false, CLS_HAIR>,           k_shade<false, CLS_MISS>,           k_shade<false, CLS_TEX + CLS_EMIT>,
-    k_shade<false, CLS_TEX + CLS_DELTA>, k_shade<false, CLS_TEX + CLS_DIFFUSE>, k_shade<false, CLS_TEX + CLS_MICRO>,
-    k_shade<false, CLS_TEX + CLS_DISNEY>, k_shade<false, CLS_TEX + CLS_HAIR>, k_shade<false, CLS_MEDIUM>};
-int gExt = 0, gExtC = 0, gExtM = 0, gShadeI = 0, gShadow = 0, gCls[CLS_N];
+template <bool X>
+struct ShadeTable {
+    static constexpr Kernel k[CLS_N] = {
+        k_shade<false, CLS_MISS, X>,            k_shade<false, CLS_EMIT, X>,
+        k_shade<false, CLS_DELTA, X>,           k_shade<false, CLS_DIFFUSE, X>,
+        k_shade<false, CLS_MICRO, X>,           k_shade<false, CLS_DISNEY, X>,
+        k_shade<false, CLS_HAIR, X>,            k_shade<false, CLS_MISS, X>,
+        k_shade<false, CLS_TEX + CLS_EMIT, X>,  k_shade<false, CLS_TEX + CLS_DELTA, X>,
+        k_shade<false, CLS_TEX + CLS_DIFFUSE, X>, k_shade<false, CLS_TEX + CLS_MICRO, X>,
+        k_shade<false, CLS_TEX + CLS_DISNEY, X>, k_shade<false, CLS_TEX + CLS_HAIR, X>,
+        k_shade<false, CLS_MEDIUM, true>};
+};
+// per class: the default kernels, and the EXTRA ones (RIS NEE, media in the wavefront)
+const Kernel *const kShadeCls = ShadeTable<false>::k;
+const Kernel *const kShadeClsX = ShadeTable<true>::k;
+int gExt = 0, gExtC = 0, gExtM = 0, gShadeI = 0, gShadow = 0, gCls[CLS_N], gClsX[CLS_N];
 
 enum { STG_RAYGEN, STG_EXTEND, STG_SHADE, STG_SHADOW, STG_FILM, STG_CACHE, STG_N };
 struct Mark { int stage; cudaEvent_t a, b; };
@@ -1212,7 +1224,7 @@ struct Enqueue {
 // Grid sizes of the traversal and shading kernels (grid-stride loops).
 struct Grids {
     int ext, extC, extM, shadeI, shadow;
-    const int *cls;
+    const int *cls, *clsX;
 };
 
 // Raygen and `depth` bounces of one wave (A.waveStart / A.waveCount set).
@@ -1249,10 +1261,12 @@ cudaError_t enqueue_paths(const pt_ctx *ctx, Enqueue &E, WaveArgs &A, uint32_t d
             if (ctx->S.mediaWavefront) k_extend<true, true><<<G.extM, kBlock, 0, st>>>(A);
             else k_extend<true><<<G.extC, kBlock, 0, st>>>(A);
             E.end();
+            const bool extra = A.risNee || ctx->S.mediaWavefront;
             for (int c = 0; c < CLS_N; c++) {
                 if (!((ctx->clsMask >> c) & 1u)) continue;
                 E.begin(STG_SHADE);
-                kShadeCls[c]<<<G.cls[c], kBlock, 0, st>>>(A);
+                if (extra) kShadeClsX[c]<<<G.clsX[c], kBlock, 0, st>>>(A);
+                else kShadeCls[c]<<<G.cls[c], kBlock, 0, st>>>(A);
                 E.end();
             }
             E.begin(STG_SHADOW);
@@ -1274,7 +1288,7 @@ cudaError_t enqueue_render(const pt_ctx *ctx, Enqueue &E, WaveArgs A, const pt_r
         if (err == cudaSuccess && e != cudaSuccess) err = e;
     };
     const bool cached = A.cacheOn != 0;
-    const Grids G{gExt, gExtC, gExtM, gShadeI, gShadow, gCls};
+    const Grids G{gExt, gExtC, gExtM, gShadeI, gShadow, gCls, gClsX};
     chk(cudaMemsetAsync(B.counters, 0, kCounterWords * sizeof(uint32_t), st));
     chk(cudaMemsetAsync(ctx->d_err, 0, 4, st));
     if (cached) {  // per-call cache counters: records [2], queries of the call [5], records with targets [6]
@@ -1366,7 +1380,10 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
         gExtM = grid_for(ctx, (const void *)k_extend<true, true>);
         gShadeI = grid_for(ctx, (const void *)k_shade<true, CLS_ANY>);
         gShadow = grid_for(ctx, (const void *)k_shadow);
-        for (int c = 0; c < CLS_N; c++) gCls[c] = grid_for(ctx, (const void *)kShadeCls[c]);
+        for (int c = 0; c < CLS_N; c++) {
+            gCls[c] = grid_for(ctx, (const void *)kShadeCls[c]);
+            gClsX[c] = grid_for(ctx, (const void *)kShadeClsX[c]);
+        }
     }
     WaveArgs A;
     A.S = ctx->S;
@@ -1643,13 +1660,19 @@ int render_batch(pt_ctx *ctx, const pt_request *R, uint32_t n, float *request_ms
         gExtM = grid_for(ctx, (const void *)k_extend<true, true>);
         gShadeI = grid_for(ctx, (const void *)k_shade<true, CLS_ANY>);
         gShadow = grid_for(ctx, (const void *)k_shadow);
-        for (int c = 0; c < CLS_N; c++) gCls[c] = grid_for(ctx, (const void *)kShadeCls[c]);
+        for (int c = 0; c < CLS_N; c++) {
+            gCls[c] = grid_for(ctx, (const void *)kShadeCls[c]);
+            gClsX[c] = grid_for(ctx, (const void *)kShadeClsX[c]);
+        }
     }
     if (gridScale <= 0.0f) gridScale = (Bt.tunedWave && Bt.tunedSceneGen == ctx->sceneGen) ? Bt.tunedGrid : 1.0f;
     auto sc = [&](int g) { return std::max(ctx->numSMs, (int)((float)g * gridScale)); };
-    int clsG[CLS_N];
-    for (int c = 0; c < CLS_N; c++) clsG[c] = sc(gCls[c]);
-    const Grids G{sc(gExt), sc(gExtC), sc(gExtM), sc(gShadeI), sc(gShadow), clsG};
+    int clsG[CLS_N], clsGX[CLS_N];
+    for (int c = 0; c < CLS_N; c++) {
+        clsG[c] = sc(gCls[c]);
+        clsGX[c] = sc(gClsX[c]);
+    }
+    const Grids G{sc(gExt), sc(gExtC), sc(gExtM), sc(gShadeI), sc(gShadow), clsG, clsGX};
 
     const BatchPlan pl = batch_plan(R, n, cap);
     // films: the callers' device films, device copies of host films, or the tuning scratch
