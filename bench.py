@@ -472,6 +472,8 @@ def main():
     ap.add_argument("--wave-paths", type=int, default=0, help="paths in flight per wave (0 = library default)")
     ap.add_argument("--no-ttq", action="store_true", help="skip the time-to-relMSE measurement")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-requests measurement")
+    ap.add_argument("--media-inline", action="store_true",
+                    help="heterogeneous media in the inline form (the reference's draw order) instead of the wavefront")
     ap.add_argument("--cache-kernels-only", action="store_true",
                     help="only the radiance-cache network kernels' roofline (profiling of those kernels)")
     args = ap.parse_args()
@@ -510,11 +512,13 @@ def main():
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > 126 MB L2
     paths_step = W * H * spp
 
+    base_flags = 0 if args.media_inline else pt.PT_RENDER_MEDIA_WAVEFRONT
+
     def step(i, timing=False):
         def params(off):
             return pt.render_params(W, H, spp, cam, max_depth=depth, sample_offset=off, env_sampling=env_mode,
                                     wave_paths=args.wave_paths,
-                                    flags=pt.PT_RENDER_STAGE_TIMING if timing else 0)
+                                    flags=base_flags | (pt.PT_RENDER_STAGE_TIMING if timing else 0))
 
         _, _, st = D.render_shard(ctx, params, film, i, rank, world, spp)
         D.all_reduce_film(film)

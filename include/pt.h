@@ -200,6 +200,10 @@ typedef struct pt_render_params {
 #define PT_RENDER_RADIANCE_CACHE 0x2u /* terminate paths into the radiance cache (pt_cache_init) */
 #define PT_RENDER_RIS_NEE 0x4u /* area-light NEE by resampled importance sampling: the reference's
                                   USE_RIS=1 build (RISDirectIllumination, shaders/Emitter.hlsli:155-271) */
+#define PT_RENDER_MEDIA_WAVEFRONT 0x8u /* heterogeneous media in the wavefront form (deferred NEE shadow
+                                          rays; ratio tracking drawn before visibility is known: the same
+                                          estimator with another order of draws than the reference).
+                                          Scenes whose media are all homogeneous use it always. */
 
 /* Film: per pixel Σ(L, 1) as RGBA float32 (shaders/Shaders.hlsl:632-634)
  * plus the Kahan compensation of the same shape.  location 0 = host

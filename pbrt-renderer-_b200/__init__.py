@@ -31,6 +31,7 @@ PT_SAMPLE_DIMS = 4
 PT_RENDER_STAGE_TIMING = 1
 PT_RENDER_RADIANCE_CACHE = 2
 PT_RENDER_RIS_NEE = 4
+PT_RENDER_MEDIA_WAVEFRONT = 8
 PT_CACHE_PARAMS = 21504
 PT_CACHE_FEATURES = 64
 PT_CACHE_RECORD_FLOATS = 16

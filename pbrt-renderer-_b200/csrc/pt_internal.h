@@ -98,7 +98,7 @@ struct RenderGraph {
     const void *sum = nullptr, *comp = nullptr;
     uint64_t sceneGen = 0, waveGen = 0;
     uint32_t cached = 0, trainOn = 0;  // radiance-cache configuration baked into the launches
-    uint32_t risNee = 0;
+    uint32_t risNee = 0, flags = 0;
     uint64_t cacheGen = 0;
     uint64_t launches = 0;
 };

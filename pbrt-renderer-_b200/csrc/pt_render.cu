@@ -1231,7 +1231,7 @@ struct Grids {
 // Returns the first failing call's status (cudaSuccess if none).
 cudaError_t enqueue_paths(const pt_ctx *ctx, Enqueue &E, WaveArgs &A, uint32_t depth, const Grids &G) {
     const WaveBuffers &B = ctx->W;
-    const bool inl = (ctx->S.numVols > 0 && !ctx->S.mediaWavefront) || ctx->S.hasSubsurface;
+    const bool inl = (ctx->S.numVols > 0 && !A.S.mediaWavefront) || ctx->S.hasSubsurface;
     cudaStream_t st = E.st;
     cudaError_t err = cudaSuccess;
     auto chk = [&](cudaError_t e) {
@@ -1258,12 +1258,13 @@ cudaError_t enqueue_paths(const pt_ctx *ctx, Enqueue &E, WaveArgs &A, uint32_t d
         } else {
             chk(cudaMemsetAsync(A.cntCls, 0, CLS_N * sizeof(uint32_t), st));
             E.begin(STG_EXTEND);
-            if (ctx->S.mediaWavefront) k_extend<true, true><<<G.extM, kBlock, 0, st>>>(A);
+            if (A.S.mediaWavefront) k_extend<true, true><<<G.extM, kBlock, 0, st>>>(A);
             else k_extend<true><<<G.extC, kBlock, 0, st>>>(A);
             E.end();
-            const bool extra = A.risNee || ctx->S.mediaWavefront;
+            const bool extra = A.risNee || A.S.mediaWavefront;
+            const uint32_t mask = ctx->clsMask | (A.S.mediaWavefront ? 1u << CLS_MEDIUM : 0u);
             for (int c = 0; c < CLS_N; c++) {
-                if (!((ctx->clsMask >> c) & 1u)) continue;
+                if (!((mask >> c) & 1u)) continue;
                 E.begin(STG_SHADE);
                 if (extra) kShadeClsX[c]<<<G.clsX[c], kBlock, 0, st>>>(A);
                 else kShadeCls[c]<<<G.cls[c], kBlock, 0, st>>>(A);
@@ -1335,7 +1336,7 @@ bool graph_matches(const pt_ctx *ctx, const pt_render_params *P, size_t cap, con
            G.rngKind == P->rng_kind && G.envSampling == P->env_sampling && G.cap == cap && G.sum == sum &&
            G.comp == comp && G.sceneGen == ctx->sceneGen && G.waveGen == ctx->waveGen &&
            G.cached == A.cacheOn && G.trainOn == A.trainOn && (!A.cacheOn || G.cacheGen == ctx->cache.gen) &&
-           G.risNee == A.risNee &&
+           G.risNee == A.risNee && G.flags == (P->flags & ~PT_RENDER_STAGE_TIMING) &&
            memcmp(&G.cam, &P->camera, sizeof(pt_camera)) == 0;
 }
 }  // namespace
@@ -1403,6 +1404,7 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
     A.shadowCap = (uint32_t)(2 * B.cap);
     A.batch = 0; A.numReqs = 0; A.reqs = nullptr; A.slotInfo = nullptr;
     A.risNee = (P->flags & PT_RENDER_RIS_NEE) ? 1u : 0u;
+    if ((P->flags & PT_RENDER_MEDIA_WAVEFRONT) && A.S.numVols > 0 && !A.S.hasSubsurface) A.S.mediaWavefront = 1u;
     A.cacheOn = (P->flags & PT_RENDER_RADIANCE_CACHE) ? 1u : 0u;
     A.trainOn = A.unbiasedEvery = A.recCap = A.queryCap = 0;
     A.roughThr = 0.0f;
@@ -1450,6 +1452,7 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
             G.cap = cap; G.sum = d_sum; G.comp = d_comp;
             G.sceneGen = ctx->sceneGen; G.waveGen = ctx->waveGen;
             G.cached = A.cacheOn; G.trainOn = A.trainOn; G.cacheGen = ctx->cache.gen; G.risNee = A.risNee;
+            G.flags = P->flags & ~PT_RENDER_STAGE_TIMING;
             G.launches = E.launches;
         } else {  // capture unavailable: issue the launches directly
             cudaGetLastError();
@@ -1738,6 +1741,8 @@ int render_batch(pt_ctx *ctx, const pt_request *R, uint32_t n, float *request_ms
     A.shadowCap = (uint32_t)(2 * B.cap);
     A.batch = 1; A.numReqs = n; A.reqs = (const ReqDev *)Bt.reqs; A.slotInfo = Bt.slotInfo;
     A.risNee = (R[0].params.flags & PT_RENDER_RIS_NEE) ? 1u : 0u;
+    if ((R[0].params.flags & PT_RENDER_MEDIA_WAVEFRONT) && A.S.numVols > 0 && !A.S.hasSubsurface)
+        A.S.mediaWavefront = 1u;
     // the launch graph depends on the batch's shape, not on cameras, offsets or films (device table)
     std::vector<uint64_t> key = {n, pl.cap, R[0].params.rng_kind, R[0].params.env_sampling, R[0].params.flags,
                                  ctx->sceneGen,
