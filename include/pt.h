@@ -363,7 +363,9 @@ int pt_rng_batch(pt_ctx *ctx, uint32_t rng_kind, const uint32_t *pixel_ids, cons
  * LBVH of the uploaded scene.  morton_out: one 30-bit code per triangle in
  * global triangle order (may be NULL); sorted_prims_out: triangle ids in
  * LBVH leaf order; nodes_out: (n-1) internal nodes x 2 child links
- * (a link >= 0 is an internal node, ~link a leaf slot).  Host memory. */
+ * (a link >= 0 is an internal node, ~link a leaf slot) of the radix tree
+ * as built, before the treelet passes that shape the traversed tree.
+ * Host memory. */
 int pt_bvh_info(pt_ctx *ctx, uint32_t *num_triangles, uint32_t *num_wide_nodes);
 int pt_bvh_read(pt_ctx *ctx, uint32_t *morton_out, uint32_t *sorted_prims_out, int32_t *nodes_out);
 

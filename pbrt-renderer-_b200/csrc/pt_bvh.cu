@@ -7,7 +7,14 @@
 //   3. the Karras 2012 binary radix tree over the sorted codes (ties broken by
 //      position, so the topology is a pure function of the input),
 //   4. bottom-up bounds with one atomic per internal node,
-//   5. a top-down collapse into 8-wide nodes: each wide node takes its binary
+//   5. treelet restructuring (Karras & Aila 2013, "Fast Parallel Construction
+//      of High-Quality Bounding Volume Hierarchies"): in bottom-up passes,
+//      every node with >= 7 triangles below grows a treelet of 7 leaves by
+//      opening its largest-area leaf, finds the topology of least surface-area
+//      cost over those leaves by dynamic programming over the 127 leaf
+//      subsets, and rewires the treelet's 6 internal nodes to it when that
+//      lowers the cost,
+//   6. a top-down collapse into 8-wide nodes: each wide node takes its binary
 //      root's two children and repeatedly opens the child with the largest
 //      surface area until it has 8; subtrees of <= 3 triangles become leaves.
 //      Child boxes are quantised to 8 bits per plane against a power-of-two
@@ -165,10 +172,176 @@ __global__ void k_refit(int n, const uint32_t *__restrict__ sorted, const float4
     }
 }
 
+// Triangles under each internal node of the radix tree (its key range).
+__global__ void k_range_count(int n, const uint32_t *__restrict__ rangeFirst, const uint32_t *__restrict__ rangeLast,
+                              uint32_t *cnt) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n - 1) cnt[i] = rangeLast[i] - rangeFirst[i] + 1u;
+}
+
+__device__ __forceinline__ float area(float4 l, float4 h) {
+    float dx = h.x - l.x, dy = h.y - l.y, dz = h.z - l.z;
+    return dx * dy + dy * dz + dz * dx;
+}
+
+// ---- treelet restructuring --------------------------------------------------
+// Surface-area cost of a binary subtree: kCostNode x area of every internal
+// node + kCostTri x area of every triangle leaf (areas of the boxes).
+constexpr float kCostNode = 1.2f, kCostTri = 1.0f;
+constexpr int kTreeletLeaves = 7;
+constexpr uint32_t kTreeletMinTris = 7;
+constexpr int kTreeletPasses = 3;
+
+struct TreeletIn {
+    int n;
+    int32_t *children;                // rewired in place
+    int32_t *intParent, *leafParent;  // rewired in place
+    const float4 *leafLo, *leafHi;
+    float4 *intLo, *intHi;            // treelet internal nodes get the bounds of their new subtrees
+    float *cost;                      // subtree cost of each internal node
+    uint32_t *cnt;                    // triangles under each internal node
+    uint32_t *flags;                  // arrivals per internal node, zero before each pass
+    uint32_t *rewired;                // treelets rewired in this pass
+};
+
+__device__ __forceinline__ void node_box(const TreeletIn &T, int32_t x, float4 &lo, float4 &hi) {
+    lo = x >= 0 ? __ldcg(&T.intLo[x]) : T.leafLo[~x];
+    hi = x >= 0 ? __ldcg(&T.intHi[x]) : T.leafHi[~x];
+}
+
+// Treelet of root R (whose two children are c0, c1 and whose subtree cost is
+// `cur` as the tree stands): returns the subtree cost after the step.
+__device__ float treelet_restructure(const TreeletIn &T, int32_t R, int32_t c0, int32_t c1, float cur) {
+    int32_t L[kTreeletLeaves], I[kTreeletLeaves - 1];
+    float4 lo[kTreeletLeaves], hi[kTreeletLeaves];
+    float la[kTreeletLeaves];
+    int m = 2, ni = 1;
+    I[0] = R;
+    L[0] = c0;
+    L[1] = c1;
+    for (int i = 0; i < 2; i++) {
+        node_box(T, L[i], lo[i], hi[i]);
+        la[i] = area(lo[i], hi[i]);
+    }
+    while (m < kTreeletLeaves) {  // open the internal leaf of largest area
+        int best = -1;
+        float ba = -1.0f;
+        for (int i = 0; i < m; i++)
+            if (L[i] >= 0 && la[i] > ba) { ba = la[i]; best = i; }
+        if (best < 0) break;
+        int32_t x = L[best];
+        I[ni++] = x;
+        L[best] = __ldcg(&T.children[2 * x]);
+        L[m] = __ldcg(&T.children[2 * x + 1]);
+        node_box(T, L[best], lo[best], hi[best]);
+        node_box(T, L[m], lo[m], hi[m]);
+        la[best] = area(lo[best], hi[best]);
+        la[m] = area(lo[m], hi[m]);
+        m++;
+    }
+    if (m < 3) return cur;
+    float copt[1 << kTreeletLeaves];
+    uint8_t part[1 << kTreeletLeaves];
+    const uint32_t full = (1u << m) - 1u;
+    for (int i = 0; i < m; i++)
+        copt[1u << i] = L[i] >= 0 ? __ldcg(&T.cost[L[i]]) : kCostTri * la[i];
+    // subsets in increasing order: every proper subset of S is smaller than S
+    for (uint32_t S = 3; S <= full; S++) {
+        if (__popc(S) < 2) continue;
+        float4 bl = make_float4(3e38f, 3e38f, 3e38f, 0.0f), bh = make_float4(-3e38f, -3e38f, -3e38f, 0.0f);
+        for (uint32_t b = S; b; b &= b - 1) {
+            int i = __ffs(b) - 1;
+            bl = make_float4(fminf(bl.x, lo[i].x), fminf(bl.y, lo[i].y), fminf(bl.z, lo[i].z), 0.0f);
+            bh = make_float4(fmaxf(bh.x, hi[i].x), fmaxf(bh.y, hi[i].y), fmaxf(bh.z, hi[i].z), 0.0f);
+        }
+        const uint32_t low = S & (0u - S);
+        float best = 3e38f;
+        uint32_t bp = low;
+        // splits (P, S \ P) with P holding the lowest leaf of S: each once
+        for (uint32_t P = (S - 1u) & S; P; P = (P - 1u) & S) {
+            if (!(P & low)) continue;
+            float c = copt[P] + copt[S ^ P];
+            if (c < best) { best = c; bp = P; }
+        }
+        copt[S] = kCostNode * area(bl, bh) + best;
+        part[S] = (uint8_t)bp;
+    }
+    if (!(copt[full] < cur * 0.99999f)) return cur;
+    // rewire: the subset of each new internal node, R first
+    uint32_t stS[kTreeletLeaves - 1];
+    int32_t stN[kTreeletLeaves - 1];
+    int sp = 0, used = 1;
+    stS[sp] = full;
+    stN[sp++] = R;
+    while (sp > 0) {
+        --sp;
+        const uint32_t S = stS[sp];
+        const int32_t node = stN[sp];
+        const uint32_t side[2] = {part[S], S ^ part[S]};
+        uint32_t tris = 0;
+        float4 bl = make_float4(3e38f, 3e38f, 3e38f, 0.0f), bh = make_float4(-3e38f, -3e38f, -3e38f, 0.0f);
+        for (int k = 0; k < 2; k++) {
+            int32_t c;
+            if (__popc(side[k]) == 1) {
+                c = L[__ffs(side[k]) - 1];
+            } else {
+                c = I[used++];
+                stS[sp] = side[k];
+                stN[sp++] = c;
+            }
+            T.children[2 * node + k] = c;
+            if (c >= 0) T.intParent[c] = node;
+            else T.leafParent[~c] = node;
+        }
+        for (uint32_t b = S; b; b &= b - 1) {
+            int i = __ffs(b) - 1;
+            bl = make_float4(fminf(bl.x, lo[i].x), fminf(bl.y, lo[i].y), fminf(bl.z, lo[i].z), 0.0f);
+            bh = make_float4(fmaxf(bh.x, hi[i].x), fmaxf(bh.y, hi[i].y), fmaxf(bh.z, hi[i].z), 0.0f);
+            tris += L[i] >= 0 ? __ldcg(&T.cnt[L[i]]) : 1u;
+        }
+        if (node != R) {
+            T.intLo[node] = bl;
+            T.intHi[node] = bh;
+            T.cost[node] = copt[S];
+            T.cnt[node] = tris;
+        }
+    }
+    atomicAdd(T.rewired, 1u);
+    return copt[full];
+}
+
+// One bottom-up pass, one thread per triangle leaf: the second thread to
+// reach an internal node finishes it (both subtrees are final by then).
+__global__ void k_treelet(TreeletIn T) {
+    int leaf = blockIdx.x * blockDim.x + threadIdx.x;
+    if (leaf >= T.n || T.n < 2) return;
+    int32_t node = __ldcg(&T.leafParent[leaf]);
+    for (int guard = 0; node >= 0 && guard < T.n; guard++) {
+        __threadfence();
+        if (atomicAdd(&T.flags[node], 1u) == 0u) return;
+        __threadfence();
+        int32_t c0 = __ldcg(&T.children[2 * node]), c1 = __ldcg(&T.children[2 * node + 1]);
+        float4 l, h;
+        node_box(T, c0, l, h);
+        float k0 = c0 >= 0 ? __ldcg(&T.cost[c0]) : kCostTri * area(l, h);
+        uint32_t n0 = c0 >= 0 ? __ldcg(&T.cnt[c0]) : 1u;
+        node_box(T, c1, l, h);
+        float k1 = c1 >= 0 ? __ldcg(&T.cost[c1]) : kCostTri * area(l, h);
+        uint32_t n1 = c1 >= 0 ? __ldcg(&T.cnt[c1]) : 1u;
+        node_box(T, node, l, h);
+        float c = kCostNode * area(l, h) + k0 + k1;
+        if (n0 + n1 >= kTreeletMinTris) c = treelet_restructure(T, node, c0, c1, c);
+        T.cost[node] = c;
+        T.cnt[node] = n0 + n1;
+        node = __ldcg(&T.intParent[node]);
+    }
+}
+
 struct CollapseIn {
     int n;
     const int32_t *children;
-    const uint32_t *rangeFirst, *rangeLast;
+    const uint32_t *cnt;  // triangles under each internal node
+    uint32_t maxWide;     // capacity of `nodes`
     const float4 *leafLo, *leafHi, *intLo, *intHi;
     const uint32_t *sorted;
     const uint32_t *triMesh, *meshFirstTri;
@@ -177,13 +350,9 @@ struct CollapseIn {
     const float *pos;
     BVH8Node *nodes;
     float4 *tri;
-    uint32_t *counters;  // [0] wide nodes allocated, [1] triangles written, [2] next queue size
+    uint32_t *counters;  // [0] wide nodes allocated, [1] triangles written, [2] next queue size, [3] error
 };
 
-__device__ __forceinline__ float area(float4 l, float4 h) {
-    float dx = h.x - l.x, dy = h.y - l.y, dz = h.z - l.z;
-    return dx * dy + dy * dz + dz * dx;
-}
 // Exponent e (biased) with (hi - lo) / 2^(e-127) <= 255, from an upper bound.
 __device__ __forceinline__ uint32_t quant_exp(float lo, float hi) {
     float r = __fdiv_ru(__fsub_ru(hi, lo), 255.0f);
@@ -210,7 +379,7 @@ __global__ void k_collapse(CollapseIn C, const int2 *__restrict__ qin, uint32_t 
         ch[0] = root;
         cnt = 1;
     }
-    auto openable = [&](int32_t r) { return r >= 0 && (C.rangeLast[r] - C.rangeFirst[r] + 1) > kLeafMax; };
+    auto openable = [&](int32_t r) { return r >= 0 && C.cnt[r] > kLeafMax; };
     while (cnt < 8) {
         int best = -1;
         float ba = -1.0f;
@@ -258,11 +427,18 @@ __global__ void k_collapse(CollapseIn C, const int2 *__restrict__ qin, uint32_t 
         if (child[s] < 0) continue;
         int32_t r = ch[child[s]];
         if (openable(r)) { nInt++; imask |= 1u << s; }
-        else nTri += r >= 0 ? (C.rangeLast[r] - C.rangeFirst[r] + 1) : 1u;
+        else nTri += r >= 0 ? C.cnt[r] : 1u;
     }
     uint32_t childBase = nInt ? atomicAdd(&C.counters[0], nInt) : 0u;
     uint32_t triBase = atomicAdd(&C.counters[1], nTri);
     uint32_t qpos = nInt ? atomicAdd(&C.counters[2], nInt) : 0u;
+    // a malformed tree (more nodes, queue entries or triangles than the
+    // buffers hold) is reported, never written past the buffers
+    if ((uint64_t)childBase + nInt > C.maxWide || (uint64_t)qpos + nInt > (uint64_t)C.n ||
+        (uint64_t)triBase + nTri > (uint64_t)C.n || wide >= C.maxWide) {
+        atomicOr(&C.counters[3], 2u);
+        return;
+    }
     // quantisation grid
     uint32_t ex = quant_exp(nlo.x, nhi.x), ey = quant_exp(nlo.y, nhi.y), ez = quant_exp(nlo.z, nhi.z);
     float ix = __uint_as_float((254u - ex) << 23), iy = __uint_as_float((254u - ey) << 23),
@@ -290,11 +466,28 @@ __global__ void k_collapse(CollapseIn C, const int2 *__restrict__ qin, uint32_t 
             qout[qpos + rank] = make_int2(r, (int)(childBase + rank));
             rank++;
         } else {
-            uint32_t first = r >= 0 ? C.rangeFirst[r] : (uint32_t)(~r);
-            uint32_t count = r >= 0 ? (C.rangeLast[r] - first + 1) : 1u;
+            // the subtree's triangle leaves, left to right (<= kLeafMax)
+            uint32_t lv[kLeafMax], count = 0;
+            int32_t stk[kLeafMax + 1];
+            int sp = 0;
+            stk[sp++] = r;
+            while (sp > 0) {
+                int32_t x = stk[--sp];
+                if (x < 0) {
+                    if (count < kLeafMax) lv[count++] = (uint32_t)(~x);
+                } else if (sp + 2 <= (int)kLeafMax + 1) {
+                    stk[sp++] = C.children[2 * x + 1];
+                    stk[sp++] = C.children[2 * x];
+                }
+            }
+            const uint32_t want = r >= 0 ? C.cnt[r] : 1u;  // the count this node allocated
+            if (count != want || toff + count > nTri) {
+                atomicOr(&C.counters[3], 1u);
+                count = min(min(count, want), nTri - min(toff, nTri));
+            }
             meta[s] = (uint8_t)((((1u << count) - 1u) << 5) | toff);
             for (uint32_t k = 0; k < count; k++) {
-                uint32_t g = C.sorted[first + k];
+                uint32_t g = C.sorted[lv[k]];
                 uint32_t mesh = C.triMesh[g];
                 const pt_material &m = C.mats[mesh];
                 uint32_t base = m.indexOffset + 3u * (g - C.meshFirstTri[mesh]);
@@ -387,6 +580,26 @@ int pt_build_bvh_device(pt_ctx *ctx, const uint32_t *d_meshFirstTri, uint32_t n)
     }
     k_refit<<<G, B, 0, st>>>((int)n, idsS, tlo, thi, children, intParent, leafParent, leafLo, leafHi, intLo, intHi,
                              flags);
+    // the radix tree stays as built in `children` (pt_bvh_read); the
+    // treelet passes rewire a copy
+    uint32_t *cnt, *rewired;
+    int32_t *tch, *tip, *tlp;
+    float *cost;
+    const size_t ni = (size_t)max(n - 1, 1u);
+    TA(cnt, ni * 4); TA(cost, ni * 4); TA(rewired, 4);
+    TA(tch, ni * 8); TA(tip, ni * 4); TA(tlp, (size_t)n * 4);
+    if (n > 1) {
+        k_range_count<<<(n - 1 + B - 1) / B, B, 0, st>>>((int)n, rf, rl, cnt);
+        cudaMemcpyAsync(tch, children, (size_t)(n - 1) * 8, cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(tip, intParent, (size_t)(n - 1) * 4, cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync(tlp, leafParent, (size_t)n * 4, cudaMemcpyDeviceToDevice, st);
+        TreeletIn T{(int)n, tch, tip, tlp, leafLo, leafHi, intLo, intHi, cost, cnt, flags, rewired};
+        for (int pass = 0; pass < kTreeletPasses; pass++) {
+            cudaMemsetAsync(flags, 0, (size_t)(n - 1) * 4, st);
+            cudaMemsetAsync(rewired, 0, 4, st);
+            k_treelet<<<G, B, 0, st>>>(T);
+        }
+    }
     // collapse: wide nodes <= max(1, n - 1); triangles exactly n
     BVH8Node *nodes;
     float4 *tri;
@@ -394,33 +607,47 @@ int pt_build_bvh_device(pt_ctx *ctx, const uint32_t *d_meshFirstTri, uint32_t n)
     cudaError_t e1 = ctx->alloc_scene(&nodes, maxWide);
     cudaError_t e2 = ctx->alloc_scene(&tri, 3 * (size_t)n);
     if (e1 != cudaSuccess || e2 != cudaSuccess) { cleanup(); return ctx->fail(PT_E_NOMEM, "bvh nodes"); }
-    CollapseIn C{(int)n, children, rf, rl, leafLo, leafHi, intLo, intHi, idsS, triMesh, d_meshFirstTri,
-                 S.mats, S.idx, S.pos, nodes, tri, counters};
-    int2 root = make_int2(n > 1 ? 0 : ~0, 0);
-    cudaMemcpyAsync(qa, &root, sizeof(root), cudaMemcpyHostToDevice, st);
-    uint32_t cinit[4] = {1u, 0u, 0u, 0u};
-    cudaMemcpyAsync(counters, cinit, sizeof(cinit), cudaMemcpyHostToDevice, st);
-    uint32_t qn = 1;
-    int levels = 0;
-    while (qn > 0) {
-        cudaMemsetAsync(counters + 2, 0, 4, st);
-        k_collapse<<<(qn + 127) / 128, 128, 0, st>>>(C, qa, qn, qb);
-        PT_CUDA(cudaMemcpyAsync(&qn, counters + 2, 4, cudaMemcpyDeviceToHost, st));
-        PT_CUDA(cudaStreamSynchronize(st));
-        std::swap(qa, qb);
-        if (++levels > 64) { cleanup(); return ctx->fail(PT_E_DEVICE, "bvh collapse did not terminate"); }
+    // A wide tree deeper than the traversal stack falls back to the radix
+    // tree (its depth is bounded by the key bits plus the index bits of
+    // equal keys); the restructured tree is used whenever it fits.
+    uint32_t cnt4[4];
+    for (int attempt = 0; attempt < 2; attempt++) {
+        const bool radix = attempt == 1 || n == 1;
+        if (attempt == 1) {  // restore the radix tree's bounds and counts
+            cudaMemsetAsync(flags, 0, (size_t)(n - 1) * 4, st);
+            k_refit<<<G, B, 0, st>>>((int)n, idsS, tlo, thi, children, intParent, leafParent, leafLo, leafHi, intLo,
+                                     intHi, flags);
+            k_range_count<<<(n - 1 + B - 1) / B, B, 0, st>>>((int)n, rf, rl, cnt);
+        }
+        CollapseIn C{(int)n, radix ? children : tch, cnt, maxWide, leafLo, leafHi, intLo, intHi, idsS, triMesh,
+                     d_meshFirstTri, S.mats, S.idx, S.pos, nodes, tri, counters};
+        int2 root = make_int2(n > 1 ? 0 : ~0, 0);
+        cudaMemcpyAsync(qa, &root, sizeof(root), cudaMemcpyHostToDevice, st);
+        uint32_t cinit[4] = {1u, 0u, 0u, 0u};
+        cudaMemcpyAsync(counters, cinit, sizeof(cinit), cudaMemcpyHostToDevice, st);
+        uint32_t qn = 1;
+        int levels = 0;
+        while (qn > 0) {
+            cudaMemsetAsync(counters + 2, 0, 4, st);
+            k_collapse<<<(qn + 127) / 128, 128, 0, st>>>(C, qa, qn, qb);
+            PT_CUDA(cudaMemcpyAsync(&qn, counters + 2, 4, cudaMemcpyDeviceToHost, st));
+            PT_CUDA(cudaStreamSynchronize(st));
+            std::swap(qa, qb);
+            if (++levels > 64) { cleanup(); return ctx->fail(PT_E_DEVICE, "bvh collapse did not terminate"); }
+        }
+        PT_CUDA(cudaMemcpyAsync(cnt4, counters, sizeof(cnt4), cudaMemcpyDeviceToHost, st));
+        cudaError_t se = cudaStreamSynchronize(st);
+        if (se != cudaSuccess) { cleanup(); return ctx->fail(PT_E_CUDA, "bvh build", cudaGetErrorString(se)); }
+        if (levels <= kTraversalStack || radix) break;
     }
-    uint32_t cnt[4];
-    PT_CUDA(cudaMemcpyAsync(cnt, counters, sizeof(cnt), cudaMemcpyDeviceToHost, st));
-    cudaError_t se = cudaStreamSynchronize(st);
     cleanup();
-    if (se != cudaSuccess) return ctx->fail(PT_E_CUDA, "bvh build", cudaGetErrorString(se));
-    if (cnt[1] != n) return ctx->fail(PT_E_DEVICE, "bvh collapse lost triangles");
+    if (cnt4[3] != 0u) return ctx->fail(PT_E_DEVICE, "bvh collapse: leaf triangle count mismatch");
+    if (cnt4[1] != n) return ctx->fail(PT_E_DEVICE, "bvh collapse lost triangles");
     S.tri = tri;
     S.nodes = nodes;
-    S.numNodes = cnt[0];
+    S.numNodes = cnt4[0];
     S.triMesh = triMesh;
-    ctx->numWide = cnt[0];
+    ctx->numWide = cnt4[0];
     ctx->d_morton = codes;
     ctx->d_sorted = idsS;
     ctx->d_binChildren = children;
