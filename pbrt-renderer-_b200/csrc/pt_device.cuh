@@ -716,8 +716,24 @@ struct Trav {
     uint32_t visits;
     int sp;
 };
-struct TravStack {
+// An entry is (child base, internal mask << 8 | pending hit bits).
+struct TravStack {  // all entries in local memory
     uint32_t base[kTraversalStack], mask[kTraversalStack];
+    __device__ __forceinline__ void put(int i, uint32_t b, uint32_t m) { base[i] = b; mask[i] = m; }
+    __device__ __forceinline__ uint2 get(int i) const { return make_uint2(base[i], mask[i]); }
+};
+// The first SH entries in shared memory, the rest in local memory.  `col`
+// is this thread's column of a block-wide [SH][STRIDE] uint2 array: entry i
+// of the block's threads lies in consecutive words (no bank conflicts).
+template <int SH, int STRIDE>
+struct SplitStack {
+    uint2 *col;
+    uint2 spill[kTraversalStack - SH];
+    __device__ __forceinline__ void put(int i, uint32_t b, uint32_t m) {
+        if (i < SH) col[i * STRIDE] = make_uint2(b, m);
+        else spill[i - SH] = make_uint2(b, m);
+    }
+    __device__ __forceinline__ uint2 get(int i) const { return i < SH ? col[i * STRIDE] : spill[i - SH]; }
 };
 __device__ __forceinline__ void trav_init(Trav &T, const DevScene &S, float3 o, float3 d, float tmin, float tmax,
                                           uint32_t seed = 0u, uint32_t key = 0u) {
@@ -734,13 +750,15 @@ __device__ __forceinline__ void trav_init(Trav &T, const DevScene &S, float3 o, 
 // Next node: pop the nearest pending child (from this node or the stack) and
 // intersect it.  Returns false when nothing is left (or on an error, which
 // is flagged in *err).
-__device__ __forceinline__ bool trav_next_node(Trav &T, TravStack &K, const DevScene &S, float tmax, uint32_t *err) {
+template <class Stack>
+__device__ __forceinline__ bool trav_next_node(Trav &T, Stack &K, const DevScene &S, float tmax, uint32_t *err) {
     if (T.gHits == 0) {
         if (T.sp == 0) return false;
         --T.sp;
-        T.gBase = K.base[T.sp];
-        T.gImask = K.mask[T.sp] >> 8;
-        T.gHits = K.mask[T.sp] & 0xFFu;
+        const uint2 e = K.get(T.sp);
+        T.gBase = e.x;
+        T.gImask = e.y >> 8;
+        T.gHits = e.y & 0xFFu;
     }
     uint32_t k = __ffs(T.gHits) - 1;
     T.gHits &= T.gHits - 1;
@@ -755,8 +773,7 @@ __device__ __forceinline__ bool trav_next_node(Trav &T, TravStack &K, const DevS
             if (err) atomicOr(err, 1u);
             return false;
         }
-        K.base[T.sp] = T.gBase;
-        K.mask[T.sp] = (T.gImask << 8) | T.gHits;
+        K.put(T.sp, T.gBase, (T.gImask << 8) | T.gHits);
         ++T.sp;
     }
     intersect_node(S, child, T.r, T.tmin, tmax, T.gBase, T.gImask, T.gHits, T.tBase, T.tHits);
@@ -764,7 +781,8 @@ __device__ __forceinline__ bool trav_next_node(Trav &T, TravStack &K, const DevS
 }
 // Closest-hit step: the current node's triangles, then the next node.
 // Returns true when the traversal has finished.
-__device__ __forceinline__ bool trav_step_closest(Trav &T, TravStack &K, const DevScene &S, Hit &h, uint32_t *err) {
+template <class Stack>
+__device__ __forceinline__ bool trav_step_closest(Trav &T, Stack &K, const DevScene &S, Hit &h, uint32_t *err) {
     while (T.tHits) {
         uint32_t j = __ffs(T.tHits) - 1;
         T.tHits &= T.tHits - 1;
@@ -784,7 +802,8 @@ __device__ __forceinline__ bool trav_step_closest(Trav &T, TravStack &K, const D
 }
 // Any-hit step (shadow rays).  Sets `occluded` and returns true at the first
 // opaque hit; mirror/dielectric hits multiply `trans` by (1 - Fr).
-__device__ __forceinline__ bool trav_step_shadow(Trav &T, TravStack &K, const DevScene &S, float3 &trans,
+template <class Stack>
+__device__ __forceinline__ bool trav_step_shadow(Trav &T, Stack &K, const DevScene &S, float3 &trans,
                                                  bool &occluded, uint32_t *err) {
     while (T.tHits) {
         uint32_t j = __ffs(T.tHits) - 1;
@@ -812,33 +831,44 @@ __device__ __forceinline__ bool trav_step_shadow(Trav &T, TravStack &K, const De
 
 // Closest hit (TraceClosestInline semantics for opaque geometry).  Sets *err
 // on stack overflow or a runaway visit count.
-__device__ __forceinline__ Hit trace_closest(const DevScene &S, float3 o, float3 d, float tmin, float tmax,
-                                             uint32_t *err, uint32_t seed = 0u, uint32_t key = 0u) {
+template <class Stack>
+__device__ __forceinline__ Hit trace_closest_on(Stack &K, const DevScene &S, float3 o, float3 d, float tmin,
+                                                float tmax, uint32_t *err, uint32_t seed = 0u, uint32_t key = 0u) {
     Hit h;
     h.t = tmax; h.u = 0.0f; h.v = 0.0f; h.gid = 0xFFFFFFFFu;
     if (S.numNodes == 0) return h;
     Trav T;
-    TravStack K;
     trav_init(T, S, o, d, tmin, tmax, seed, key);
     while (!trav_step_closest(T, K, S, h, err)) {
     }
     return h;
 }
+__device__ __forceinline__ Hit trace_closest(const DevScene &S, float3 o, float3 d, float tmin, float tmax,
+                                             uint32_t *err, uint32_t seed = 0u, uint32_t key = 0u) {
+    TravStack K;
+    return trace_closest_on(K, S, o, d, tmin, tmax, err, seed, key);
+}
 
 // Occlusion (TraceShadowInline, shaders/RayQueryTrace.hlsli:88-129, for
 // scenes without alpha textures): the first opaque hit in [tmin, tmax]
 // occludes; mirror/dielectric surfaces multiply `trans` by (1 - Fr).
-__device__ __forceinline__ bool trace_shadow(const DevScene &S, float3 o, float3 d, float tmin, float tmax,
-                                             float3 &trans, uint32_t *err, uint32_t seed = 0u, uint32_t key = 0u) {
+template <class Stack>
+__device__ __forceinline__ bool trace_shadow_on(Stack &K, const DevScene &S, float3 o, float3 d, float tmin,
+                                                float tmax, float3 &trans, uint32_t *err, uint32_t seed = 0u,
+                                                uint32_t key = 0u) {
     trans = v3(1.0f);
     if (S.numNodes == 0) return false;
     Trav T;
-    TravStack K;
     trav_init(T, S, o, d, tmin, tmax, seed, key);
     bool occ = false;
     while (!trav_step_shadow(T, K, S, trans, occ, err)) {
     }
     return occ;
+}
+__device__ __forceinline__ bool trace_shadow(const DevScene &S, float3 o, float3 d, float tmin, float tmax,
+                                             float3 &trans, uint32_t *err, uint32_t seed = 0u, uint32_t key = 0u) {
+    TravStack K;
+    return trace_shadow_on(K, S, o, d, tmin, tmax, trans, err, seed, key);
 }
 
 }  // namespace pt

@@ -59,9 +59,13 @@ __host__ __device__ inline int shade_class(bool hit, bool emitter, uint32_t type
     return textured ? c + CLS_TEX : c;
 }
 
-// Words of the per-wave counter block (WaveBuffers::counters).
+// Words of the per-wave counter block (WaveBuffers::counters).  The claim
+// positions of the work-stealing traversal kernels sit right after the
+// counts that are zeroed together with them each bounce: the shadow count
+// (word 2) and the class counts (words 8 .. 8 + CLS_N).
 constexpr int kCounterWords = 32;
-static_assert(8 + CLS_N <= kCounterWords, "class queue counts must fit the counter block");
+constexpr int kCntShadow = 2, kCntStealExt = 3, kCntClass = 8, kCntStealShadow = kCntClass + CLS_N;
+static_assert(kCntStealShadow + 1 <= kCounterWords, "class queue counts must fit the counter block");
 
 // Per-wave buffers of the wavefront integrator (structure of arrays).
 struct WaveBuffers {
@@ -81,9 +85,10 @@ struct WaveBuffers {
     // shadow queue (two per path per bounce at most)
     uint32_t *sslot = nullptr;           // slot | kind << 31
     float4 *so = nullptr, *sd = nullptr, *sX = nullptr, *sthr = nullptr;
-    // counters: [0] ray count q0, [1] ray count q1, [2] shadow count,
-    // [4..7] total extension / shadow rays (two uint64), [8 .. 8+CLS_N) class
-    // queue counts; kCounterWords words in all
+    // counters: [0] ray count q0, [1] ray count q1, [2] shadow count, [3]
+    // k_extend claim position, [4..7] total extension / shadow rays (two
+    // uint64), [8 .. 8+CLS_N) class queue counts, [8+CLS_N] k_shadow claim
+    // position; kCounterWords words in all
     uint32_t *counters = nullptr;
 };
 

@@ -63,6 +63,7 @@ struct WaveArgs {
     uint32_t *sslot;
     float4 *so, *sd, *sX, *sthr;
     uint32_t *cntIn, *cntOut, *cntShadow;
+    uint32_t *stealExt, *stealShadow;  // next unclaimed queue position of k_extend / k_shadow
     uint32_t *cls, *cntCls;  // shading-class queues (CLS_N x clsStride) and their counts
     uint32_t clsStride;
     unsigned long long *rayTotals;  // [0] extension, [1] shadow
@@ -229,81 +230,128 @@ __device__ __forceinline__ void finish_extend(const WaveArgs &A, uint32_t i, con
         class_append(A, c, i);
     }
 }
+// Traversal stacks of k_extend / k_shadow: the first kSharedStack entries of
+// each thread in shared memory (kSharedStack x kBlock x 8 bytes per block),
+// deeper entries in local memory.
+#ifndef PT_SHARED_STACK
+#define PT_SHARED_STACK 0
+#endif
+constexpr int kSharedStack = PT_SHARED_STACK;
+template <int SH>
+struct QueueStack {
+    using type = SplitStack<SH, kBlock>;
+};
+template <>
+struct QueueStack<0> {
+    using type = TravStack;
+};
+template <int SH, int STRIDE>
+__device__ __forceinline__ void bind_stack(SplitStack<SH, STRIDE> &K, uint2 *col) {
+    K.col = col;
+}
+__device__ __forceinline__ void bind_stack(TravStack &, uint2 *) {}
+#define PT_QUEUE_STACK(K)                                                \
+    __shared__ uint2 stk_[kSharedStack > 0 ? kSharedStack : 1][kBlock]; \
+    QueueStack<kSharedStack>::type K;                                    \
+    bind_stack(K, &stk_[0][threadIdx.x]);
+
+// Persistent work-stealing over a ray queue: each warp claims the next 32
+// queue positions with one atomic (so a warp's rays stay neighbours in the
+// queue) until the queue is exhausted.  Returns the claimed base, uniform
+// across the warp; all 32 lanes must call it together.
+__device__ __forceinline__ uint32_t claim32(uint32_t *next) {
+    uint32_t base = 0;
+    if (lane_id() == 0) base = atomicAdd(next, 32u);
+    return __shfl_sync(0xFFFFFFFFu, base, 0);
+}
+
 // MEDIA: the free flight of Shaders.hlsl:133-179 follows the closest hit here
 // (draws from the path's stream in the shader's order); a scattering event
 // goes to the medium class with (t, volume | 1 << 31) in the hit record and
 // the throughput gets the flight's weight.  Homogeneous media only: their
 // shadow-ray transmittance draws nothing, so NEE can be deferred.
+template <bool CLASSIFY, bool MEDIA, class Stack>
+__device__ __forceinline__ void extend_one(const WaveArgs &A, uint32_t i, Stack &K) {
+    float4 o = A.qoIn[i], d = A.qdIn[i];
+    uint32_t aseed = 0, akey = 0;
+    if (A.S.hasAlpha) {  // alpha tests: the path's seed, key of this bounce's extension ray
+        uint32_t slot = A.qslotIn[i];
+        Rng r = load_rng(A, slot, A.rng[slot]);
+        aseed = alpha_seed(r.pixelSeed, r.sampleIndex);
+        akey = alpha_key(A.rng[slot].z, 0u);
+    }
+    Hit h = trace_closest_on(K, A.S, make_float3(o.x, o.y, o.z), make_float3(d.x, d.y, d.z), o.w, d.w, A.err, aseed,
+                             akey);
+    if (MEDIA) {
+        const uint32_t slot = A.qslotIn[i];
+        uint4 st = A.rng[slot];
+        Rng r = load_rng(A, slot, st);
+        float3 vw = v3(1.0f);
+        float tsc;
+        uint32_t svi;
+        bool sc = sample_free_flight(A.S, make_float3(o.x, o.y, o.z), make_float3(d.x, d.y, d.z),
+                                     h.gid != 0xFFFFFFFFu ? h.t : 1e20f, r, vw, tsc, svi);
+        if (r.dim != st.x || r.white != st.y) {
+            st.x = r.dim;
+            st.y = r.white;
+            A.rng[slot] = st;
+        }
+        if (vw.x != 1.0f || vw.y != 1.0f || vw.z != 1.0f) {
+            float4 tp = A.thr_pdf[slot];
+            float3 t3 = make_float3(tp.x, tp.y, tp.z) * vw;
+            A.thr_pdf[slot] = make_float4(t3.x, t3.y, t3.z, tp.w);
+        }
+        if (sc) {
+            A.qhit[i] = make_float4(tsc, __uint_as_float(svi | 0x80000000u), 0.0f, 0.0f);
+            class_append(A, CLS_MEDIUM, i);
+            return;
+        }
+    }
+    finish_extend<CLASSIFY>(A, i, h);
+}
 template <bool CLASSIFY, bool MEDIA = false>
 __global__ void __launch_bounds__(kBlock) k_extend(WaveArgs A) {
-    // grid-stride over the queue in order: the 32 rays of a warp are
-    // neighbours in the queue (coherent traversal), and the class queues and
-    // the next ray queue keep that order for the kernels that follow
+    // warps claim the queue in order: the 32 rays of a warp are neighbours in
+    // the queue (coherent traversal), and the class queues and the next ray
+    // queue keep that order for the kernels that follow
     const uint32_t n = *(volatile uint32_t *)A.cntIn;
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&A.rayTotals[0], (unsigned long long)n);
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        float4 o = A.qoIn[i], d = A.qdIn[i];
-        uint32_t aseed = 0, akey = 0;
-        if (A.S.hasAlpha) {  // alpha tests: the path's seed, key of this bounce's extension ray
-            uint32_t slot = A.qslotIn[i];
-            Rng r = load_rng(A, slot, A.rng[slot]);
-            aseed = alpha_seed(r.pixelSeed, r.sampleIndex);
-            akey = alpha_key(A.rng[slot].z, 0u);
-        }
-        Hit h = trace_closest(A.S, make_float3(o.x, o.y, o.z), make_float3(d.x, d.y, d.z), o.w, d.w, A.err, aseed,
-                              akey);
-        if (MEDIA) {
-            const uint32_t slot = A.qslotIn[i];
-            uint4 st = A.rng[slot];
-            Rng r = load_rng(A, slot, st);
-            float3 vw = v3(1.0f);
-            float tsc;
-            uint32_t svi;
-            bool sc = sample_free_flight(A.S, make_float3(o.x, o.y, o.z), make_float3(d.x, d.y, d.z),
-                                         h.gid != 0xFFFFFFFFu ? h.t : 1e20f, r, vw, tsc, svi);
-            if (r.dim != st.x || r.white != st.y) {
-                st.x = r.dim;
-                st.y = r.white;
-                A.rng[slot] = st;
-            }
-            if (vw.x != 1.0f || vw.y != 1.0f || vw.z != 1.0f) {
-                float4 tp = A.thr_pdf[slot];
-                float3 t3 = make_float3(tp.x, tp.y, tp.z) * vw;
-                A.thr_pdf[slot] = make_float4(t3.x, t3.y, t3.z, tp.w);
-            }
-            if (sc) {
-                A.qhit[i] = make_float4(tsc, __uint_as_float(svi | 0x80000000u), 0.0f, 0.0f);
-                class_append(A, CLS_MEDIUM, i);
-                continue;
-            }
-        }
-        finish_extend<CLASSIFY>(A, i, h);
+    PT_QUEUE_STACK(K)
+    for (uint32_t base; (base = claim32(A.stealExt)) < n;) {
+        const uint32_t i = base + lane_id();
+        if (i < n) extend_one<CLASSIFY, MEDIA>(A, i, K);
     }
 }
 
 // ---- shadow: any hit -> pending NEE contribution ---------------------------
+template <class Stack>
+__device__ __forceinline__ void shadow_one(const WaveArgs &A, uint32_t i, Stack &K) {
+    float4 o = A.so[i], d = A.sd[i];
+    float3 tr;
+    uint32_t aseed = 0, akey = 0;
+    if (A.S.hasAlpha) {  // the shading kernel already advanced the path's bounce counter
+        uint32_t s = A.sslot[i], slot = s & 0x7FFFFFFFu;
+        Rng r = load_rng(A, slot, A.rng[slot]);
+        aseed = alpha_seed(r.pixelSeed, r.sampleIndex);
+        akey = alpha_key(A.rng[slot].z - 1u, (s >> 31) ? 2u : 1u);
+    }
+    bool occ = trace_shadow_on(K, A.S, make_float3(o.x, o.y, o.z), make_float3(d.x, d.y, d.z), o.w, d.w, tr, A.err,
+                               aseed, akey);
+    float4 X = A.sX[i], Th = A.sthr[i];
+    uint32_t s = A.sslot[i];
+    float3 thr = make_float3(Th.x, Th.y, Th.z);
+    float3 R = occ ? thr * v3(0.0f) : thr * (make_float3(X.x, X.y, X.z) * tr);
+    float4 out = make_float4(R.x, R.y, R.z, 0.0f);
+    if (s >> 31) A.pendE[s & 0x7FFFFFFFu] = out;
+    else A.pendA[s] = out;
+}
 __global__ void __launch_bounds__(kBlock) k_shadow(WaveArgs A) {
     const uint32_t n = *(volatile uint32_t *)A.cntShadow;
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&A.rayTotals[1], (unsigned long long)n);
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        float4 o = A.so[i], d = A.sd[i];
-        float3 tr;
-        uint32_t aseed = 0, akey = 0;
-        if (A.S.hasAlpha) {  // the shading kernel already advanced the path's bounce counter
-            uint32_t s = A.sslot[i], slot = s & 0x7FFFFFFFu;
-            Rng r = load_rng(A, slot, A.rng[slot]);
-            aseed = alpha_seed(r.pixelSeed, r.sampleIndex);
-            akey = alpha_key(A.rng[slot].z - 1u, (s >> 31) ? 2u : 1u);
-        }
-        bool occ = trace_shadow(A.S, make_float3(o.x, o.y, o.z), make_float3(d.x, d.y, d.z), o.w, d.w, tr, A.err,
-                                aseed, akey);
-        float4 X = A.sX[i], Th = A.sthr[i];
-        uint32_t s = A.sslot[i];
-        float3 thr = make_float3(Th.x, Th.y, Th.z);
-        float3 R = occ ? thr * v3(0.0f) : thr * (make_float3(X.x, X.y, X.z) * tr);
-        float4 out = make_float4(R.x, R.y, R.z, 0.0f);
-        if (s >> 31) A.pendE[s & 0x7FFFFFFFu] = out;
-        else A.pendA[s] = out;
+    PT_QUEUE_STACK(K)
+    for (uint32_t base; (base = claim32(A.stealShadow)) < n;) {
+        const uint32_t i = base + lane_id();
+        if (i < n) shadow_one(A, i, K);
     }
 }
 
@@ -1247,7 +1295,7 @@ cudaError_t enqueue_paths(const pt_ctx *ctx, Enqueue &E, WaveArgs &A, uint32_t d
         A.qslotOut = B.qslot[1 - cur]; A.qoOut = B.qo[1 - cur]; A.qdOut = B.qd[1 - cur];
         A.cntOut = B.counters + (1 - cur);
         chk(cudaMemsetAsync(A.cntOut, 0, 4, st));
-        chk(cudaMemsetAsync(A.cntShadow, 0, 4, st));
+        chk(cudaMemsetAsync(A.cntShadow, 0, 8, st));  // shadow count and the extend claim position
         if (inl) {
             E.begin(STG_EXTEND);
             k_extend<false><<<G.ext, kBlock, 0, st>>>(A);
@@ -1256,7 +1304,8 @@ cudaError_t enqueue_paths(const pt_ctx *ctx, Enqueue &E, WaveArgs &A, uint32_t d
             k_shade<true, CLS_ANY><<<G.shadeI, kBlock, 0, st>>>(A);
             E.end();
         } else {
-            chk(cudaMemsetAsync(A.cntCls, 0, CLS_N * sizeof(uint32_t), st));
+            // class counts and the shadow claim position after them
+            chk(cudaMemsetAsync(A.cntCls, 0, (CLS_N + 1) * sizeof(uint32_t), st));
             E.begin(STG_EXTEND);
             if (A.S.mediaWavefront) k_extend<true, true><<<G.extM, kBlock, 0, st>>>(A);
             else k_extend<true><<<G.extC, kBlock, 0, st>>>(A);
@@ -1395,8 +1444,10 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
     A.thr_pdf = B.thr_pdf; A.lo_eta = B.lo_eta; A.pendA = B.pendA; A.pendE = B.pendE; A.rng = B.rng;
     A.qhit = B.qhit;
     A.sslot = B.sslot; A.so = B.so; A.sd = B.sd; A.sX = B.sX; A.sthr = B.sthr;
-    A.cntShadow = B.counters + 2;
-    A.cntCls = B.counters + 8;
+    A.cntShadow = B.counters + kCntShadow;
+    A.stealExt = B.counters + kCntStealExt;
+    A.stealShadow = B.counters + kCntStealShadow;
+    A.cntCls = B.counters + kCntClass;
     A.cls = B.cls;
     A.clsStride = (uint32_t)B.cap;
     A.rayTotals = (unsigned long long *)(B.counters + 4);
@@ -1732,8 +1783,10 @@ int render_batch(pt_ctx *ctx, const pt_request *R, uint32_t n, float *request_ms
     A.thr_pdf = B.thr_pdf; A.lo_eta = B.lo_eta; A.pendA = B.pendA; A.pendE = B.pendE; A.rng = B.rng;
     A.qhit = B.qhit;
     A.sslot = B.sslot; A.so = B.so; A.sd = B.sd; A.sX = B.sX; A.sthr = B.sthr;
-    A.cntShadow = B.counters + 2;
-    A.cntCls = B.counters + 8;
+    A.cntShadow = B.counters + kCntShadow;
+    A.stealExt = B.counters + kCntStealExt;
+    A.stealShadow = B.counters + kCntStealShadow;
+    A.cntCls = B.counters + kCntClass;
     A.cls = B.cls;
     A.clsStride = (uint32_t)B.cap;
     A.rayTotals = (unsigned long long *)(B.counters + 4);
