@@ -537,6 +537,7 @@ int pt_upload_scene(pt_ctx *ctx, const pt_scene_desc *d) {
         for (uint32_t v = 0; v < d->num_volumes; v++)
             if (d->volumes[v].flags & PT_VOLUME_HETEROGENEOUS) homog = false;
         S.mediaWavefront = (homog && !hasSubsurface) ? 1u : 0u;
+        S.mediaTrDeferred = 0u;
         if (S.mediaWavefront) clsMask |= 1u << CLS_MEDIUM;
     }
     S.pos = dpos; S.nrm = dnrm; S.uv = duv; S.tan = dtan; S.idx = didx;

@@ -74,6 +74,9 @@ struct DevScene {
     uint32_t hasSubsurface;     // any subsurface (type 6) mesh: shading traces its walks inline
     uint32_t mediaWavefront;    // media, all homogeneous, no subsurface: free flights in the closest-hit
                                 // kernel, medium events as their own shading class, NEE deferred
+    uint32_t mediaTrDeferred;   // heterogeneous media in the wavefront (on request): the medium
+                                // transmittance of an NEE ray is estimated in the shadow kernel, only
+                                // when the ray is unoccluded, from its own random stream
 };
 
 // One texture's mip chain in DevScene::texels (level l: max(w >> l, 1) x

@@ -32,6 +32,8 @@
 namespace pt {
 
 constexpr uint32_t kFlagPending = 1u;
+// Shadow queue entries: path slot (< 2^30) | kShadowTrLater | NEE kind << 31.
+constexpr uint32_t kShadowTrLater = 1u << 30, kShadowSlotMask = kShadowTrLater - 1u;
 // radiance-cache path flags (rng.w); the record index of a training path sits above bit 8
 constexpr uint32_t kFlagRough = 2u;     // the last bounce scattered off a rough surface or a medium
 constexpr uint32_t kFlagTrain = 4u;     // training path
@@ -324,13 +326,14 @@ __global__ void __launch_bounds__(kBlock) k_extend(WaveArgs A) {
 }
 
 // ---- shadow: any hit -> pending NEE contribution ---------------------------
-template <class Stack>
+// Shadow queue entry: path slot | kShadowTrLater | kind (0 area, 1 envmap) << 31.
+template <bool MEDIA_TR, class Stack>
 __device__ __forceinline__ void shadow_one(const WaveArgs &A, uint32_t i, Stack &K) {
     float4 o = A.so[i], d = A.sd[i];
     float3 tr;
     uint32_t aseed = 0, akey = 0;
     if (A.S.hasAlpha) {  // the shading kernel already advanced the path's bounce counter
-        uint32_t s = A.sslot[i], slot = s & 0x7FFFFFFFu;
+        uint32_t s = A.sslot[i], slot = s & kShadowSlotMask;
         Rng r = load_rng(A, slot, A.rng[slot]);
         aseed = alpha_seed(r.pixelSeed, r.sampleIndex);
         akey = alpha_key(A.rng[slot].z - 1u, (s >> 31) ? 2u : 1u);
@@ -339,19 +342,40 @@ __device__ __forceinline__ void shadow_one(const WaveArgs &A, uint32_t i, Stack 
                                aseed, akey);
     float4 X = A.sX[i], Th = A.sthr[i];
     uint32_t s = A.sslot[i];
+    const uint32_t slot = s & kShadowSlotMask;
+    if (MEDIA_TR && !occ && (s & kShadowTrLater)) {
+        // the ray's medium transmittance (ratio tracking, Volume.hlsl:326-372),
+        // estimated only now that the ray is known to be unoccluded: its own
+        // white-noise stream, keyed by pixel, sample, bounce and NEE kind.  The
+        // shading kernel integrated to the light (area: tmax + 0.001)
+        Rng r = load_rng(A, slot, A.rng[slot]);
+        Rng t;
+        t.kind = PT_RNG_PCG_HASH;
+        t.pixelSeed = r.pixelSeed;
+        t.sampleIndex = r.sampleIndex;
+        t.dim = 0u;
+        t.white = pcg_hash(r.pixelSeed ^ pcg_hash(r.sampleIndex ^ pcg_hash(((A.rng[slot].z - 1u) << 1) + (s >> 31) +
+                                                                          0x3C6EF372u)));
+        const float tm = d.w < 1e19f ? d.w + 0.001f : d.w;
+        tr = tr * multi_volume_tr(A.S, make_float3(o.x, o.y, o.z), make_float3(d.x, d.y, d.z), tm, t);
+    }
     float3 thr = make_float3(Th.x, Th.y, Th.z);
     float3 R = occ ? thr * v3(0.0f) : thr * (make_float3(X.x, X.y, X.z) * tr);
     float4 out = make_float4(R.x, R.y, R.z, 0.0f);
-    if (s >> 31) A.pendE[s & 0x7FFFFFFFu] = out;
-    else A.pendA[s] = out;
+    if (s >> 31) A.pendE[slot] = out;
+    else A.pendA[slot] = out;
 }
+// MEDIA_TR: the instantiation for heterogeneous media in the wavefront
+// (transmittance of unoccluded rays); the default one carries none of that
+// code.
+template <bool MEDIA_TR = false>
 __global__ void __launch_bounds__(kBlock) k_shadow(WaveArgs A) {
     const uint32_t n = *(volatile uint32_t *)A.cntShadow;
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&A.rayTotals[1], (unsigned long long)n);
     PT_QUEUE_STACK(K)
     for (uint32_t base; (base = claim32(A.stealShadow)) < n;) {
         const uint32_t i = base + lane_id();
-        if (i < n) shadow_one(A, i, K);
+        if (i < n) shadow_one<MEDIA_TR>(A, i, K);
     }
 }
 
@@ -360,6 +384,7 @@ __global__ void __launch_bounds__(kBlock) k_shadow(WaveArgs A) {
 // the final thr * 0 written straight to the pending slot.
 struct NeeOut {
     bool ray;
+    bool trLater;  // medium transmittance left to the shadow kernel (not in X)
     float3 o, d, X;
     float tmin, tmax;
 };
@@ -371,6 +396,7 @@ __device__ __forceinline__ float3 nee_area(const WaveArgs &A, float3 hp, float3 
                                            NeeOut &out, uint32_t aseed, uint32_t bounce) {
     const DevScene &S = A.S;
     out.ray = false;
+    out.trLater = false;
     EmitterSample es = sample_emitter(S, rng);
     if (!es.valid) return v3(0.0f);
     float3 tl = es.pos - hp;
@@ -391,7 +417,8 @@ __device__ __forceinline__ float3 nee_area(const WaveArgs &A, float3 hp, float3 
     material_eval_pdf_t(type, wil, to_local(ww, T, B, N), m, h, f, pb);
     float pe = es.pdfArea * dist * dist / cl;
     float w = balance(pe, pb);
-    float3 vt = (INLINE || (MEDIA && S.mediaWavefront)) ? multi_volume_tr(S, so, ww, dist, rng) : v3(1.0f);
+    out.trLater = !INLINE && MEDIA && S.mediaTrDeferred;
+    float3 vt = (INLINE || (MEDIA && S.mediaWavefront && !out.trLater)) ? multi_volume_tr(S, so, ww, dist, rng) : v3(1.0f);
     float3 X = es.rad * f * act / v3(mx(pe, 1e-20f)) * w * vt;
     if (INLINE) return X * trans;
     out.ray = true;
@@ -435,6 +462,7 @@ __device__ __forceinline__ float3 nee_ris(const WaveArgs &A, float3 hp, float3 N
                                           NeeOut &out, uint32_t aseed, uint32_t bounce) {
     const DevScene &S = A.S;
     out.ray = false;
+    out.trLater = false;
     EmitterSample y;
     y.valid = false;
     float wSum = 0.0f, pHatY = 0.0f;
@@ -467,7 +495,8 @@ __device__ __forceinline__ float3 nee_ris(const WaveArgs &A, float3 hp, float3 N
     float pdfBsdf;
     material_eval_pdf_t(type, wil, to_local(wiw, T, B, N), m, h, fu, pdfBsdf);
     float wMis = balance(pSA, pdfBsdf);
-    float3 vt = (INLINE || (MEDIA && S.mediaWavefront)) ? multi_volume_tr(S, so, wiw, dist, rng) : v3(1.0f);
+    out.trLater = !INLINE && MEDIA && S.mediaTrDeferred;
+    float3 vt = (INLINE || (MEDIA && S.mediaWavefront && !out.trLater)) ? multi_volume_tr(S, so, wiw, dist, rng) : v3(1.0f);
     float3 X = integ * v3(W) * v3(wMis) * vt;
     if (INLINE) return X * trans;
     out.ray = true;
@@ -481,6 +510,7 @@ __device__ __forceinline__ float3 nee_env(const WaveArgs &A, float3 hp, float3 N
                                           NeeOut &out, uint32_t aseed, uint32_t bounce) {
     const DevScene &S = A.S;
     out.ray = false;
+    out.trLater = false;
     float u1 = next_float(rng, S.sobol1), u2 = next_float(rng, S.sobol1);
     float3 ww, Le;
     float pe;
@@ -500,7 +530,8 @@ __device__ __forceinline__ float3 nee_env(const WaveArgs &A, float3 hp, float3 N
     float pb;
     material_eval_pdf_t(type, wil, to_local(ww, T, B, N), m, h, f, pb);
     float w = balance(pe, pb);
-    float3 vt = (INLINE || (MEDIA && S.mediaWavefront)) ? multi_volume_tr(S, so, ww, 1e20f, rng) : v3(1.0f);
+    out.trLater = !INLINE && MEDIA && S.mediaTrDeferred;
+    float3 vt = (INLINE || (MEDIA && S.mediaWavefront && !out.trLater)) ? multi_volume_tr(S, so, ww, 1e20f, rng) : v3(1.0f);
     float3 X = Le * f * act / v3(mx(pe, 1e-20f)) * w * vt;
     if (INLINE) return X * trans;
     out.ray = true;
@@ -524,6 +555,7 @@ __device__ float3 vol_nee_area(const WaveArgs &A, float3 sp, float3 wo, uint32_t
                                uint32_t bounce, NeeOut &out) {
     const DevScene &S = A.S;
     out.ray = false;
+    out.trLater = false;
     const pt_volume &v = S.vols[vi];
     if (vol_nee_skip(v, sp)) return v3(0.0f);
     EmitterSample es = sample_emitter(S, rng);
@@ -539,7 +571,8 @@ __device__ float3 vol_nee_area(const WaveArgs &A, float3 sp, float3 wo, uint32_t
     float fp = hg(dot(wo, wi), v.phase_g);
     float pe = es.pdfArea * dist * dist / cl;
     float w = balance(pe, fp);
-    float3 vt = multi_volume_tr(S, sp, wi, dist, rng);
+    out.trLater = !INLINE && S.mediaTrDeferred;
+    float3 vt = out.trLater ? v3(1.0f) : multi_volume_tr(S, sp, wi, dist, rng);
     float3 X = es.rad * fp / v3(mx(pe, 1e-20f)) * w * vt;
     if (INLINE) return X * trans;
     out.ray = true;
@@ -551,6 +584,7 @@ __device__ float3 vol_nee_env(const WaveArgs &A, float3 sp, float3 wo, uint32_t 
                               uint32_t bounce, NeeOut &out) {
     const DevScene &S = A.S;
     out.ray = false;
+    out.trLater = false;
     const pt_volume &v = S.vols[vi];
     if (vol_nee_skip(v, sp)) return v3(0.0f);
     float u1 = next_float(rng, S.sobol1), u2 = next_float(rng, S.sobol1);
@@ -563,7 +597,8 @@ __device__ float3 vol_nee_env(const WaveArgs &A, float3 sp, float3 wo, uint32_t 
         return v3(0.0f);
     float fp = hg(dot(wo, wi), v.phase_g);
     float w = balance(pe, fp);
-    float3 vt = multi_volume_tr(S, sp, wi, 1e20f, rng);
+    out.trLater = !INLINE && S.mediaTrDeferred;
+    float3 vt = out.trLater ? v3(1.0f) : multi_volume_tr(S, sp, wi, 1e20f, rng);
     float3 X = Le * fp / v3(mx(pe, 1e-20f)) * w * vt;
     if (INLINE) return X * trans;
     out.ray = true;
@@ -576,7 +611,7 @@ __device__ __forceinline__ void push_shadow(const WaveArgs &A, bool pred, uint32
     uint32_t pos = warp_append(A.cntShadow, pred);
     if (!pred) return;
     if (pos >= A.shadowCap) { atomicOr(A.err, (uint32_t)PT_DEVERR_QUEUE); return; }
-    A.sslot[pos] = slot | (kind << 31);
+    A.sslot[pos] = slot | (kind << 31) | (o.trLater ? kShadowTrLater : 0u);
     A.so[pos] = make_float4(o.o.x, o.o.y, o.o.z, o.tmin);
     A.sd[pos] = make_float4(o.d.x, o.d.y, o.d.z, o.tmax);
     A.sX[pos] = make_float4(o.X.x, o.X.y, o.X.z, 0.0f);
@@ -761,6 +796,7 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
         float ntmin = 0.0f;
         NeeOut neeA, neeE;
         neeA.ray = neeE.ray = false;
+        neeA.trLater = neeE.trLater = false;
         float3 thrNee = v3(0.0f);
         Rng rng;
         if (active) {
@@ -1243,7 +1279,7 @@ struct ShadeTable {
 // per class: the default kernels, and the EXTRA ones (RIS NEE, media in the wavefront)
 const Kernel *const kShadeCls = ShadeTable<false>::k;
 const Kernel *const kShadeClsX = ShadeTable<true>::k;
-int gExt = 0, gExtC = 0, gExtM = 0, gShadeI = 0, gShadow = 0, gCls[CLS_N], gClsX[CLS_N];
+int gExt = 0, gExtC = 0, gExtM = 0, gShadeI = 0, gShadow = 0, gShadowM = 0, gCls[CLS_N], gClsX[CLS_N];
 
 enum { STG_RAYGEN, STG_EXTEND, STG_SHADE, STG_SHADOW, STG_FILM, STG_CACHE, STG_N };
 struct Mark { int stage; cudaEvent_t a, b; };
@@ -1271,7 +1307,7 @@ struct Enqueue {
 
 // Grid sizes of the traversal and shading kernels (grid-stride loops).
 struct Grids {
-    int ext, extC, extM, shadeI, shadow;
+    int ext, extC, extM, shadeI, shadow, shadowM;
     const int *cls, *clsX;
 };
 
@@ -1320,7 +1356,8 @@ cudaError_t enqueue_paths(const pt_ctx *ctx, Enqueue &E, WaveArgs &A, uint32_t d
                 E.end();
             }
             E.begin(STG_SHADOW);
-            k_shadow<<<G.shadow, kBlock, 0, st>>>(A);
+            if (A.S.mediaTrDeferred) k_shadow<true><<<G.shadowM, kBlock, 0, st>>>(A);
+            else k_shadow<<<G.shadow, kBlock, 0, st>>>(A);
             E.end();
         }
         cur = 1 - cur;
@@ -1338,7 +1375,7 @@ cudaError_t enqueue_render(const pt_ctx *ctx, Enqueue &E, WaveArgs A, const pt_r
         if (err == cudaSuccess && e != cudaSuccess) err = e;
     };
     const bool cached = A.cacheOn != 0;
-    const Grids G{gExt, gExtC, gExtM, gShadeI, gShadow, gCls, gClsX};
+    const Grids G{gExt, gExtC, gExtM, gShadeI, gShadow, gShadowM, gCls, gClsX};
     chk(cudaMemsetAsync(B.counters, 0, kCounterWords * sizeof(uint32_t), st));
     chk(cudaMemsetAsync(ctx->d_err, 0, 4, st));
     if (cached) {  // per-call cache counters: records [2], queries of the call [5], records with targets [6]
@@ -1429,7 +1466,8 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
         gExtC = grid_for(ctx, (const void *)k_extend<true>);
         gExtM = grid_for(ctx, (const void *)k_extend<true, true>);
         gShadeI = grid_for(ctx, (const void *)k_shade<true, CLS_ANY>);
-        gShadow = grid_for(ctx, (const void *)k_shadow);
+        gShadow = grid_for(ctx, (const void *)k_shadow<false>);
+        gShadowM = grid_for(ctx, (const void *)k_shadow<true>);
         for (int c = 0; c < CLS_N; c++) {
             gCls[c] = grid_for(ctx, (const void *)kShadeCls[c]);
             gClsX[c] = grid_for(ctx, (const void *)kShadeClsX[c]);
@@ -1455,7 +1493,10 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
     A.shadowCap = (uint32_t)(2 * B.cap);
     A.batch = 0; A.numReqs = 0; A.reqs = nullptr; A.slotInfo = nullptr;
     A.risNee = (P->flags & PT_RENDER_RIS_NEE) ? 1u : 0u;
-    if ((P->flags & PT_RENDER_MEDIA_WAVEFRONT) && A.S.numVols > 0 && !A.S.hasSubsurface) A.S.mediaWavefront = 1u;
+    if ((P->flags & PT_RENDER_MEDIA_WAVEFRONT) && A.S.numVols > 0 && !A.S.hasSubsurface && !A.S.mediaWavefront) {
+        A.S.mediaWavefront = 1u;  // heterogeneous media (homogeneous-only scenes have it already)
+        A.S.mediaTrDeferred = 1u;
+    }
     A.cacheOn = (P->flags & PT_RENDER_RADIANCE_CACHE) ? 1u : 0u;
     A.trainOn = A.unbiasedEvery = A.recCap = A.queryCap = 0;
     A.roughThr = 0.0f;
@@ -1713,7 +1754,8 @@ int render_batch(pt_ctx *ctx, const pt_request *R, uint32_t n, float *request_ms
         gExtC = grid_for(ctx, (const void *)k_extend<true>);
         gExtM = grid_for(ctx, (const void *)k_extend<true, true>);
         gShadeI = grid_for(ctx, (const void *)k_shade<true, CLS_ANY>);
-        gShadow = grid_for(ctx, (const void *)k_shadow);
+        gShadow = grid_for(ctx, (const void *)k_shadow<false>);
+        gShadowM = grid_for(ctx, (const void *)k_shadow<true>);
         for (int c = 0; c < CLS_N; c++) {
             gCls[c] = grid_for(ctx, (const void *)kShadeCls[c]);
             gClsX[c] = grid_for(ctx, (const void *)kShadeClsX[c]);
@@ -1726,7 +1768,7 @@ int render_batch(pt_ctx *ctx, const pt_request *R, uint32_t n, float *request_ms
         clsG[c] = sc(gCls[c]);
         clsGX[c] = sc(gClsX[c]);
     }
-    const Grids G{sc(gExt), sc(gExtC), sc(gExtM), sc(gShadeI), sc(gShadow), clsG, clsGX};
+    const Grids G{sc(gExt), sc(gExtC), sc(gExtM), sc(gShadeI), sc(gShadow), sc(gShadowM), clsG, clsGX};
 
     const BatchPlan pl = batch_plan(R, n, cap);
     // films: the callers' device films, device copies of host films, or the tuning scratch
@@ -1794,8 +1836,11 @@ int render_batch(pt_ctx *ctx, const pt_request *R, uint32_t n, float *request_ms
     A.shadowCap = (uint32_t)(2 * B.cap);
     A.batch = 1; A.numReqs = n; A.reqs = (const ReqDev *)Bt.reqs; A.slotInfo = Bt.slotInfo;
     A.risNee = (R[0].params.flags & PT_RENDER_RIS_NEE) ? 1u : 0u;
-    if ((R[0].params.flags & PT_RENDER_MEDIA_WAVEFRONT) && A.S.numVols > 0 && !A.S.hasSubsurface)
-        A.S.mediaWavefront = 1u;
+    if ((R[0].params.flags & PT_RENDER_MEDIA_WAVEFRONT) && A.S.numVols > 0 && !A.S.hasSubsurface &&
+        !A.S.mediaWavefront) {
+        A.S.mediaWavefront = 1u;  // heterogeneous media (homogeneous-only scenes have it already)
+        A.S.mediaTrDeferred = 1u;
+    }
     // the launch graph depends on the batch's shape, not on cameras, offsets or films (device table)
     std::vector<uint64_t> key = {n, pl.cap, R[0].params.rng_kind, R[0].params.env_sampling, R[0].params.flags,
                                  ctx->sceneGen,
