@@ -208,16 +208,20 @@ def progressive(pt, ctx, stream, W, H, ref_img, make_params, spf, warm=0):
 
 
 # Radiance-cache settings of the cached form: 4-spp calls (4 training steps
-# each), the first CACHE_WARM calls training only, up to 65,536 records per
-# call from at most 10 % of the paths that reach a cache vertex, bounces with
-# Disney roughness >= 0.1 end into the cache, no unbiased suffixes; inference
-# uses an exponential average of the weights (decay 0.97), which removes the
-# frame-to-frame flicker of a cache that takes 4 steps per call.
-CACHE_SPF, CACHE_WARM, CACHE_RECORDS, CACHE_LR, CACHE_EMA = 4, 8, 65536, 1e-2, 0.97
+# each), the first CACHE_WARM[workload] calls training only (from sweeps of
+# each scene: the 10 M-triangle fogged scene needs 8, the 64-sphere scene 6),
+# up to 65,536 records per call from at most 10 % of the paths that reach a
+# cache vertex, bounces with Disney roughness >= 0.1 end into the cache, no
+# unbiased suffixes; inference uses an exponential average of the weights
+# (decay 0.97), which removes the frame-to-frame flicker of a cache that takes
+# 4 steps per call.
+CACHE_SPF, CACHE_RECORDS, CACHE_LR, CACHE_EMA = 4, 65536, 1e-2, 0.97
+CACHE_WARM = {"disney_envmap": 6, "radiance_cache": 8}
+CACHE_WARM_DEFAULT = 8
 CACHE_FRACTION, CACHE_ROUGH = 0.1, 0.1
 
 
-def time_to_relmse(pt, ctx, stream, W, H, cam, depth, env_mode, chunk):
+def time_to_relmse(pt, ctx, stream, W, H, cam, depth, env_mode, chunk, warm=CACHE_WARM_DEFAULT):
     """Device time for plain and radiance-cached path tracing to reach relMSE
     <= 1e-2 against a 4096-spp plain render of the same scene, checked at
     accumulated spp 1, 2, 3, 4, 6, 8, 11, ... (~2^(k/2)) in both forms.
@@ -262,9 +266,9 @@ def time_to_relmse(pt, ctx, stream, W, H, cam, depth, env_mode, chunk):
     torch.cuda.synchronize()
     ctx.cache_init(cache_params())
     try:
-        cached = progressive(pt, ctx, stream, W, H, ref_img, cached_params, CACHE_SPF, warm=CACHE_WARM)
+        cached = progressive(pt, ctx, stream, W, H, ref_img, cached_params, CACHE_SPF, warm=warm)
         st = ctx.cache_stats()
-        cached["settings"] = {"spp_per_call": CACHE_SPF, "warmup_calls": CACHE_WARM,
+        cached["settings"] = {"spp_per_call": CACHE_SPF, "warmup_calls": warm,
                               "train_records_per_call": CACHE_RECORDS, "max_train_fraction": CACHE_FRACTION,
                               "rough_threshold": CACHE_ROUGH, "learning_rate": CACHE_LR, "ema": CACHE_EMA,
                               "adam_steps": int(st.steps),
@@ -632,7 +636,8 @@ def main():
         "scene_upload_s": round(upload_s, 3),
     }
     if world == 1 and not args.no_ttq:
-        line["time_to_relmse"] = time_to_relmse(pt, ctx, stream, W, H, cam, depth, env_mode, max(spp, 64))
+        line["time_to_relmse"] = time_to_relmse(pt, ctx, stream, W, H, cam, depth, env_mode, max(spp, 64),
+                                                warm=CACHE_WARM.get(cfg["workload"], CACHE_WARM_DEFAULT))
         line["cache_roofline"] = cache_kernel_roofline(pt, ctx)
     if world == 1 and not args.no_batch:
         line["batched"] = batched_requests_run(pt)
