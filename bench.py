@@ -570,14 +570,14 @@ def main():
         # launch graph for the host-film staging buffers on the first call
         for k in range(args.warmup):
             P = pt.render_params(W, H, spp, cam, max_depth=depth, sample_offset=D.sample_offset(k, rank, world, spp),
-                                 env_sampling=env_mode, wave_paths=args.wave_paths)
+                                 env_sampling=env_mode, wave_paths=args.wave_paths, flags=base_flags)
             ctx.render(P, film_np, comp_np, pt.PT_MEM_HOST)
         torch.cuda.synchronize()
         e2e_ms = 0.0
         for k in range(args.steps):
             P = pt.render_params(W, H, spp, cam, max_depth=depth,
                                  sample_offset=D.sample_offset(k, rank, world, spp), env_sampling=env_mode,
-                                 wave_paths=args.wave_paths)
+                                 wave_paths=args.wave_paths, flags=base_flags)
             flush.zero_()
             torch.cuda.synchronize()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
