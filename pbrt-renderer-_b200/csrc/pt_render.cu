@@ -220,13 +220,13 @@ __device__ __forceinline__ void class_append(const WaveArgs &A, int c, uint32_t 
     uint32_t base = 0;
     if (lane_id() == leader) base = atomicAdd(A.cntCls + c, __popc(peers));
     base = __shfl_sync(peers, base, leader);
-    A.cls[(size_t)c * A.clsStride + base + __popc(peers & ((1u << lane_id()) - 1u))] = i;
+    __stcs(A.cls + (size_t)c * A.clsStride + base + __popc(peers & ((1u << lane_id()) - 1u)), i);
 }
 
 // ---- extend: closest hit (+ sort into shading classes) -----------------------
 template <bool CLASSIFY>
 __device__ __forceinline__ void finish_extend(const WaveArgs &A, uint32_t i, const Hit &h) {
-    A.qhit[i] = make_float4(h.t, __uint_as_float(h.gid), h.u, h.v);
+    __stcs(A.qhit + i, make_float4(h.t, __uint_as_float(h.gid), h.u, h.v));
     if (CLASSIFY) {
         int c = h.gid == 0xFFFFFFFFu ? (int)CLS_MISS : (int)__ldg(A.S.meshClass + __ldg(A.S.triMesh + h.gid));
         class_append(A, c, i);
@@ -274,7 +274,9 @@ __device__ __forceinline__ uint32_t claim32(uint32_t *next) {
 // shadow-ray transmittance draws nothing, so NEE can be deferred.
 template <bool CLASSIFY, bool MEDIA, class Stack>
 __device__ __forceinline__ void extend_one(const WaveArgs &A, uint32_t i, Stack &K) {
-    float4 o = A.qoIn[i], d = A.qdIn[i];
+    // queue data streams through once: evict-first loads and stores keep
+    // the BVH nodes and triangles resident in L2
+    float4 o = __ldcs(A.qoIn + i), d = __ldcs(A.qdIn + i);
     uint32_t aseed = 0, akey = 0;
     if (A.S.hasAlpha) {  // alpha tests: the path's seed, key of this bounce's extension ray
         uint32_t slot = A.qslotIn[i];
@@ -329,7 +331,7 @@ __global__ void __launch_bounds__(kBlock) k_extend(WaveArgs A) {
 // Shadow queue entry: path slot | kShadowTrLater | kind (0 area, 1 envmap) << 31.
 template <bool MEDIA_TR, class Stack>
 __device__ __forceinline__ void shadow_one(const WaveArgs &A, uint32_t i, Stack &K) {
-    float4 o = A.so[i], d = A.sd[i];
+    float4 o = __ldcs(A.so + i), d = __ldcs(A.sd + i);
     float3 tr;
     uint32_t aseed = 0, akey = 0;
     if (A.S.hasAlpha) {  // the shading kernel already advanced the path's bounce counter
@@ -340,8 +342,8 @@ __device__ __forceinline__ void shadow_one(const WaveArgs &A, uint32_t i, Stack 
     }
     bool occ = trace_shadow_on(K, A.S, make_float3(o.x, o.y, o.z), make_float3(d.x, d.y, d.z), o.w, d.w, tr, A.err,
                                aseed, akey);
-    float4 X = A.sX[i], Th = A.sthr[i];
-    uint32_t s = A.sslot[i];
+    float4 X = __ldcs(A.sX + i), Th = __ldcs(A.sthr + i);
+    uint32_t s = __ldcs(A.sslot + i);
     const uint32_t slot = s & kShadowSlotMask;
     if (MEDIA_TR && !occ && (s & kShadowTrLater)) {
         // the ray's medium transmittance (ratio tracking, Volume.hlsl:326-372),
@@ -362,8 +364,8 @@ __device__ __forceinline__ void shadow_one(const WaveArgs &A, uint32_t i, Stack 
     float3 thr = make_float3(Th.x, Th.y, Th.z);
     float3 R = occ ? thr * v3(0.0f) : thr * (make_float3(X.x, X.y, X.z) * tr);
     float4 out = make_float4(R.x, R.y, R.z, 0.0f);
-    if (s >> 31) A.pendE[slot] = out;
-    else A.pendA[slot] = out;
+    if (s >> 31) __stcs(A.pendE + slot, out);
+    else __stcs(A.pendA + slot, out);
 }
 // MEDIA_TR: the instantiation for heterogeneous media in the wavefront
 // (transmittance of unoccluded rays); the default one carries none of that
