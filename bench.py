@@ -142,10 +142,10 @@ def measured_peaks():
 
 
 # k_extend DRAM traffic per extension ray (dram__bytes_read.sum + dram__bytes_write.sum
-# from one ncu capture of this workload at 4 spp: 322.1 MB over the 3,686,400
+# from one ncu capture of this workload at 4 spp: 235.3 MB over the 3,686,400
 # camera rays of bounce 0).  The scene is L2-resident and the queues stream
 # once, so traffic scales with the rays a launch processes.
-EXTEND_DRAM_BYTES_PER_RAY = {"disney_envmap": 87.4}
+EXTEND_DRAM_BYTES_PER_RAY = {"disney_envmap": 63.8}
 
 
 REF_SPP = 4096        # reference image: plain path tracing, samples [0, 4096)
