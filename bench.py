@@ -221,7 +221,7 @@ CACHE_WARM_DEFAULT = 8
 CACHE_FRACTION, CACHE_ROUGH = 0.1, 0.1
 
 
-def time_to_relmse(pt, ctx, stream, W, H, cam, depth, env_mode, chunk, warm=CACHE_WARM_DEFAULT):
+def time_to_relmse(pt, ctx, stream, W, H, cam, depth, env_mode, chunk, warm_calls=CACHE_WARM_DEFAULT):
     """Device time for plain and radiance-cached path tracing to reach relMSE
     <= 1e-2 against a 4096-spp plain render of the same scene, checked at
     accumulated spp 1, 2, 3, 4, 6, 8, 11, ... (~2^(k/2)) in both forms.
@@ -266,9 +266,9 @@ def time_to_relmse(pt, ctx, stream, W, H, cam, depth, env_mode, chunk, warm=CACH
     torch.cuda.synchronize()
     ctx.cache_init(cache_params())
     try:
-        cached = progressive(pt, ctx, stream, W, H, ref_img, cached_params, CACHE_SPF, warm=warm)
+        cached = progressive(pt, ctx, stream, W, H, ref_img, cached_params, CACHE_SPF, warm=warm_calls)
         st = ctx.cache_stats()
-        cached["settings"] = {"spp_per_call": CACHE_SPF, "warmup_calls": warm,
+        cached["settings"] = {"spp_per_call": CACHE_SPF, "warmup_calls": warm_calls,
                               "train_records_per_call": CACHE_RECORDS, "max_train_fraction": CACHE_FRACTION,
                               "rough_threshold": CACHE_ROUGH, "learning_rate": CACHE_LR, "ema": CACHE_EMA,
                               "adam_steps": int(st.steps),
@@ -637,7 +637,7 @@ def main():
     }
     if world == 1 and not args.no_ttq:
         line["time_to_relmse"] = time_to_relmse(pt, ctx, stream, W, H, cam, depth, env_mode, max(spp, 64),
-                                                warm=CACHE_WARM.get(cfg["workload"], CACHE_WARM_DEFAULT))
+                                                warm_calls=CACHE_WARM.get(cfg["workload"], CACHE_WARM_DEFAULT))
         line["cache_roofline"] = cache_kernel_roofline(pt, ctx)
     if world == 1 and not args.no_batch:
         line["batched"] = batched_requests_run(pt)
