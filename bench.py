@@ -207,27 +207,29 @@ def progressive(pt, ctx, stream, W, H, ref_img, make_params, spf, warm=0):
             "spp": None if reached is None else reached[0], "curve": curve}
 
 
-# Radiance-cache settings of the cached form: 4-spp calls (4 training steps
-# each), the first CACHE_WARM[workload] calls training only (from sweeps of
-# each scene: the 10 M-triangle fogged scene needs 8, the 64-sphere scene 6),
-# up to 65,536 records per call from at most 10 % of the paths that reach a
-# cache vertex, bounces with Disney roughness >= 0.1 end into the cache, no
-# unbiased suffixes; inference uses an exponential average of the weights
-# (decay 0.97), which removes the frame-to-frame flicker of a cache that takes
-# 4 steps per call.
-CACHE_SPF, CACHE_RECORDS, CACHE_LR, CACHE_EMA = 4, 65536, 1e-2, 0.97
-CACHE_WARM = {"disney_envmap": 6, "radiance_cache": 8}
-CACHE_WARM_DEFAULT = 8
+# Radiance-cache settings of the cached form: calls of CACHE_CALLS[workload]
+# = (spp per call, training-only warm-up calls) from sweeps of each scene (the
+# 64-sphere scene: 8-spp calls after 3; the 10 M-triangle fogged scene: 4-spp
+# calls after 8), 4 training steps per call, up to 65,536 records per call
+# from at most 10 % of the paths that reach a cache vertex, bounces with
+# Disney roughness >= 0.1 end into the cache, no unbiased suffixes; inference
+# uses an exponential average of the weights (decay 0.97), which removes the
+# frame-to-frame flicker of a cache that takes 4 steps per call.
+CACHE_RECORDS, CACHE_LR, CACHE_EMA = 65536, 1e-2, 0.97
+CACHE_CALLS = {"disney_envmap": (8, 3), "radiance_cache": (4, 8)}
+CACHE_CALLS_DEFAULT = (4, 8)
 CACHE_FRACTION, CACHE_ROUGH = 0.1, 0.1
 
 
-def time_to_relmse(pt, ctx, stream, W, H, cam, depth, env_mode, chunk, warm_calls=CACHE_WARM_DEFAULT):
+def time_to_relmse(pt, ctx, stream, W, H, cam, depth, env_mode, chunk, calls=CACHE_CALLS_DEFAULT):
     """Device time for plain and radiance-cached path tracing to reach relMSE
     <= 1e-2 against a 4096-spp plain render of the same scene, checked at
     accumulated spp 1, 2, 3, 4, 6, 8, 11, ... (~2^(k/2)) in both forms.
     Plain: one render call per check point (calls grow with it).  Cached:
-    CACHE_SPF-spp calls with training steps in each, from an untrained cache
+    calls[0]-spp calls with training steps in each, the first calls[1] of
+    them training only, from an untrained cache
     (training time and the warm-up calls are inside the timed total)."""
+    spf, warm_calls = calls
     ref_img = reference_image(pt, ctx, W, H, cam, depth, env_mode, chunk)
 
     # plain: render calls that bring the accumulated spp to each check point
@@ -254,7 +256,7 @@ def time_to_relmse(pt, ctx, stream, W, H, cam, depth, env_mode, chunk, warm_call
                                max_train_fraction=CACHE_FRACTION, rough_threshold=CACHE_ROUGH)
 
     def cached_params(off):
-        return pt.render_params(W, H, CACHE_SPF, cam, max_depth=depth, sample_offset=off, env_sampling=env_mode,
+        return pt.render_params(W, H, spf, cam, max_depth=depth, sample_offset=off, env_sampling=env_mode,
                                 flags=pt.PT_RENDER_RADIANCE_CACHE)
 
     # one untimed cached call first: the cache kernels' first launch in the
@@ -266,9 +268,9 @@ def time_to_relmse(pt, ctx, stream, W, H, cam, depth, env_mode, chunk, warm_call
     torch.cuda.synchronize()
     ctx.cache_init(cache_params())
     try:
-        cached = progressive(pt, ctx, stream, W, H, ref_img, cached_params, CACHE_SPF, warm=warm_calls)
+        cached = progressive(pt, ctx, stream, W, H, ref_img, cached_params, spf, warm=warm_calls)
         st = ctx.cache_stats()
-        cached["settings"] = {"spp_per_call": CACHE_SPF, "warmup_calls": warm_calls,
+        cached["settings"] = {"spp_per_call": spf, "warmup_calls": warm_calls,
                               "train_records_per_call": CACHE_RECORDS, "max_train_fraction": CACHE_FRACTION,
                               "rough_threshold": CACHE_ROUGH, "learning_rate": CACHE_LR, "ema": CACHE_EMA,
                               "adam_steps": int(st.steps),
@@ -637,7 +639,7 @@ def main():
     }
     if world == 1 and not args.no_ttq:
         line["time_to_relmse"] = time_to_relmse(pt, ctx, stream, W, H, cam, depth, env_mode, max(spp, 64),
-                                                warm_calls=CACHE_WARM.get(cfg["workload"], CACHE_WARM_DEFAULT))
+                                                calls=CACHE_CALLS.get(cfg["workload"], CACHE_CALLS_DEFAULT))
         line["cache_roofline"] = cache_kernel_roofline(pt, ctx)
     if world == 1 and not args.no_batch:
         line["batched"] = batched_requests_run(pt)
