@@ -598,6 +598,14 @@ int pt_build_bvh_device(pt_ctx *ctx, const uint32_t *d_meshFirstTri, uint32_t n)
             cudaMemsetAsync(flags, 0, (size_t)(n - 1) * 4, st);
             cudaMemsetAsync(rewired, 0, 4, st);
             k_treelet<<<G, B, 0, st>>>(T);
+            if (pass + 1 == kTreeletPasses) break;
+            // a pass that rewires nothing leaves the tree as it found it, and
+            // the next pass would decide the same: stop
+            uint32_t changed = 0;
+            cudaError_t ce = cudaMemcpyAsync(&changed, rewired, 4, cudaMemcpyDeviceToHost, st);
+            if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+            if (ce != cudaSuccess) { cleanup(); return ctx->fail(PT_E_CUDA, "bvh treelets", cudaGetErrorString(ce)); }
+            if (changed == 0) break;
         }
     }
     // collapse: wide nodes <= max(1, n - 1); triangles exactly n
