@@ -66,6 +66,7 @@ struct WaveArgs {
     float4 *so, *sd, *sX, *sthr;
     uint32_t *cntIn, *cntOut, *cntShadow;
     uint32_t *stealExt, *stealShadow;  // next unclaimed queue position of k_extend / k_shadow
+    uint32_t bounce;                   // bounce of the kernels of this launch (uniform over the queue)
     uint32_t *cls, *cntCls;  // shading-class queues (CLS_N x clsStride) and their counts
     uint32_t clsStride;
     unsigned long long *rayTotals;  // [0] extension, [1] shadow
@@ -206,8 +207,13 @@ __global__ void k_raygen(WaveArgs A) {
     A.qslotOut[slot] = slot;
     A.qoOut[slot] = make_float4(ro.x, ro.y, ro.z, 0.001f);
     A.qdOut[slot] = make_float4(rd.x, rd.y, rd.z, 1e20f);
-    A.thr_pdf[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-    A.lo_eta[slot] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+    // the first shading pass starts every path from throughput 1 and Lo 0
+    // without loading them; they are stored only where something reads them
+    // first: the film (no bounce) and the medium free flights of k_extend
+    if (A.S.mediaWavefront || path_depth(A, slot) == 0) {
+        A.thr_pdf[slot] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+        A.lo_eta[slot] = make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+    }
     A.rng[slot] = make_uint4(r.dim, r.white, 0u, 0u);
     if (slot == 0) *A.cntOut = A.waveCount;
 }
@@ -803,7 +809,10 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
         Rng rng;
         if (active) {
             slot = A.qslotIn[i];
-            float4 tp = A.thr_pdf[slot], le = A.lo_eta[slot];
+            // bounce 0 outside the medium wavefront: the initial state, known
+            const bool fresh = A.bounce == 0u && !S.mediaWavefront;
+            float4 tp = fresh ? make_float4(1.0f, 1.0f, 1.0f, 0.0f) : A.thr_pdf[slot];
+            float4 le = fresh ? make_float4(0.0f, 0.0f, 0.0f, 1.0f) : A.lo_eta[slot];
             st = A.rng[slot];
             thr = make_float3(tp.x, tp.y, tp.z);
             lastPdf = tp.w;
@@ -1329,6 +1338,7 @@ cudaError_t enqueue_paths(const pt_ctx *ctx, Enqueue &E, WaveArgs &A, uint32_t d
     E.end();
     int cur = 0;
     for (uint32_t b = 0; b < depth; b++) {
+        A.bounce = b;
         A.qslotIn = B.qslot[cur]; A.qoIn = B.qo[cur]; A.qdIn = B.qd[cur]; A.cntIn = B.counters + cur;
         A.qslotOut = B.qslot[1 - cur]; A.qoOut = B.qo[1 - cur]; A.qdOut = B.qd[1 - cur];
         A.cntOut = B.counters + (1 - cur);
