@@ -204,7 +204,8 @@ __global__ void k_raygen(WaveArgs A) {
         ro = cpos + (rr * cosf(th)) * right + (rr * sinf(th)) * up;
         rd = normalize(fp - ro);
     }
-    A.qslotOut[slot] = slot;
+    // the first ray queue is in slot order (its slot index is the position:
+    // the kernels of bounce 0 do not read it)
     A.qoOut[slot] = make_float4(ro.x, ro.y, ro.z, 0.001f);
     A.qdOut[slot] = make_float4(rd.x, rd.y, rd.z, 1e20f);
     // the first shading pass starts every path from throughput 1 and Lo 0
@@ -285,7 +286,7 @@ __device__ __forceinline__ void extend_one(const WaveArgs &A, uint32_t i, Stack 
     float4 o = __ldcs(A.qoIn + i), d = __ldcs(A.qdIn + i);
     uint32_t aseed = 0, akey = 0;
     if (A.S.hasAlpha) {  // alpha tests: the path's seed, key of this bounce's extension ray
-        uint32_t slot = A.qslotIn[i];
+        uint32_t slot = A.bounce == 0u ? i : A.qslotIn[i];
         Rng r = load_rng(A, slot, A.rng[slot]);
         aseed = alpha_seed(r.pixelSeed, r.sampleIndex);
         akey = alpha_key(A.rng[slot].z, 0u);
@@ -293,7 +294,7 @@ __device__ __forceinline__ void extend_one(const WaveArgs &A, uint32_t i, Stack 
     Hit h = trace_closest_on(K, A.S, make_float3(o.x, o.y, o.z), make_float3(d.x, d.y, d.z), o.w, d.w, A.err, aseed,
                              akey);
     if (MEDIA) {
-        const uint32_t slot = A.qslotIn[i];
+        const uint32_t slot = A.bounce == 0u ? i : A.qslotIn[i];
         uint4 st = A.rng[slot];
         Rng r = load_rng(A, slot, st);
         float3 vw = v3(1.0f);
@@ -808,7 +809,7 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
         float3 thrNee = v3(0.0f);
         Rng rng;
         if (active) {
-            slot = A.qslotIn[i];
+            slot = A.bounce == 0u ? i : A.qslotIn[i];
             // bounce 0 outside the medium wavefront: the initial state, known
             const bool fresh = A.bounce == 0u && !S.mediaWavefront;
             float4 tp = fresh ? make_float4(1.0f, 1.0f, 1.0f, 0.0f) : A.thr_pdf[slot];
