@@ -478,7 +478,7 @@ __global__ void __launch_bounds__(1024) k_rc_targets(RcRows<1> rec, float4 *beta
         tgt[r] = make_float4(o[0], o[1], o[2], 0.0f);
         const float4 cv = recCache[r];
         lo_eta[slot] = make_float4(__fadd_rn(l0.x, __fmul_rn(b.x, cv.x)), __fadd_rn(l0.y, __fmul_rn(b.y, cv.y)),
-                                   __fadd_rn(l0.z, __fmul_rn(b.z, cv.z)), le.w);
+                                   __fadd_rn(l0.z, __fmul_rn(b.z, cv.z)), fabsf(le.w));  // nothing pending now
         uint4 st = rng[slot];
         st.w &= ~1u;
         rng[slot] = st;

@@ -818,7 +818,7 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
             thr = make_float3(tp.x, tp.y, tp.z);
             lastPdf = tp.w;
             Lo = make_float3(le.x, le.y, le.z);
-            eta = le.w;
+            eta = fabsf(le.w);  // the sign of w flags pending NEE for the film
             if (st.w & kFlagPending) {  // NEE of the previous bounce, in RayGen's order
                 float4 pa = A.pendA[slot], pe = A.pendE[slot];
                 Lo += make_float3(pa.x, pa.y, pa.z);
@@ -1137,7 +1137,9 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
             st.x = rng.dim;
             st.y = rng.white;
             A.thr_pdf[slot] = make_float4(thr.x, thr.y, thr.z, lastPdf);
-            A.lo_eta[slot] = make_float4(Lo.x, Lo.y, Lo.z, eta);
+            // w = eta, negative while NEE of this bounce is pending: the film
+            // reads the flag here instead of the path's RNG state
+            A.lo_eta[slot] = make_float4(Lo.x, Lo.y, Lo.z, (st.w & kFlagPending) ? -eta : eta);
             A.rng[slot] = st;
         }
         if (!INLINE) {
@@ -1172,7 +1174,7 @@ __global__ void k_film(WaveArgs A, float4 *sum, float4 *comp) {
         uint32_t slot = (uint32_t)(pid - first);
         float4 le = A.lo_eta[slot];
         float3 L = make_float3(le.x, le.y, le.z);
-        if (A.rng[slot].w & kFlagPending) {
+        if (le.w < 0.0f) {  // NEE of the last bounce pending
             float4 pa = A.pendA[slot], pe = A.pendE[slot];
             L += make_float3(pa.x, pa.y, pa.z);
             L += make_float3(pe.x, pe.y, pe.z);
@@ -1203,7 +1205,7 @@ __global__ void k_film_req(WaveArgs A, uint32_t q) {
         uint32_t slot = (uint32_t)(ps + l - ws);
         float4 le = A.lo_eta[slot];
         float3 L = make_float3(le.x, le.y, le.z);
-        if (A.rng[slot].w & kFlagPending) {
+        if (le.w < 0.0f) {  // NEE of the last bounce pending
             float4 pa = A.pendA[slot], pe4 = A.pendE[slot];
             L += make_float3(pa.x, pa.y, pa.z);
             L += make_float3(pe4.x, pe4.y, pe4.z);
