@@ -1136,11 +1136,14 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
             if (st.z >= path_depth(A, slot)) cont = false;
             st.x = rng.dim;
             st.y = rng.white;
-            A.thr_pdf[slot] = make_float4(thr.x, thr.y, thr.z, lastPdf);
+            // a finished path's throughput is read by nothing, and its RNG
+            // state only by the shadow kernel's alpha tests and the cache's
+            // target pass
+            if (cont) A.thr_pdf[slot] = make_float4(thr.x, thr.y, thr.z, lastPdf);
             // w = eta, negative while NEE of this bounce is pending: the film
             // reads the flag here instead of the path's RNG state
             A.lo_eta[slot] = make_float4(Lo.x, Lo.y, Lo.z, (st.w & kFlagPending) ? -eta : eta);
-            A.rng[slot] = st;
+            if (cont || S.hasAlpha || A.cacheOn) A.rng[slot] = st;
         }
         if (!INLINE) {
             push_shadow(A, active && neeA.ray, slot, 0u, neeA, thrNee);
