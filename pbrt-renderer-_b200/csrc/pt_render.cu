@@ -645,7 +645,7 @@ template <int CLS>
 struct ShadeBlocks {
     static constexpr int base = CLS < 0 ? CLS : CLS == CLS_MEDIUM ? CLS : CLS % CLS_TEX;
     static constexpr int value = base == CLS_MISS ? 5 : (base == CLS_EMIT || base == CLS_DELTA) ? 4
-                                                      : (base == CLS_DISNEY || base == CLS_MEDIUM) ? 3 : 2;
+                                                      : base == CLS_DISNEY ? 4 : base == CLS_MEDIUM ? 3 : 2;
 };
 
 // SubsurfaceWalk (Subsurface.hlsli:49-144): random walk inside the closed
