@@ -260,6 +260,10 @@ int pt_create(pt_ctx **out, int device) {
     ctx->stream = ctx->ownStream;
     if (cudaEventCreate(&ctx->ev[0]) != cudaSuccess || cudaEventCreate(&ctx->ev[1]) != cudaSuccess)
         return bail(PT_E_CUDA);
+    if (cudaStreamCreateWithFlags(&ctx->copyStream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->filmReady, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->streamMark, cudaEventDisableTiming) != cudaSuccess)
+        return bail(PT_E_CUDA);
     uint32_t tab[1024];
     for (uint32_t k = 0; k < 4; k++)
         for (uint32_t b = 0; b < 256; b++) tab[256 * k + b] = ptm::sobol1_loop(b << (8 * k));
@@ -285,6 +289,12 @@ int pt_destroy(pt_ctx *ctx) {
     if (ctx->d_err) cudaFree(ctx->d_err);
     for (cudaEvent_t e : ctx->ev)
         if (e) cudaEventDestroy(e);
+    if (ctx->copyStream) {
+        cudaStreamSynchronize(ctx->copyStream);
+        cudaStreamDestroy(ctx->copyStream);
+    }
+    if (ctx->filmReady) cudaEventDestroy(ctx->filmReady);
+    if (ctx->streamMark) cudaEventDestroy(ctx->streamMark);
     if (ctx->ownStream) cudaStreamDestroy(ctx->ownStream);
     delete ctx;
     return PT_OK;
@@ -662,8 +672,16 @@ int pt_render(pt_ctx *ctx, const pt_render_params *p, pt_film *film, pt_stats *s
         if (rc) return rc;
         dsum = (float *)base;
         dcomp = (float *)(base + bytes);
-        PT_CUDA(cudaMemcpyAsync(dsum, film->sum, bytes, cudaMemcpyHostToDevice, ctx->stream));
-        PT_CUDA(cudaMemcpyAsync(dcomp, film->comp, bytes, cudaMemcpyHostToDevice, ctx->stream));
+        // the upload overlaps the render (only its film kernel reads the
+        // film): on the copy stream, after the render stream's earlier work
+        // on the staging memory
+        PT_CUDA(cudaEventRecord(ctx->streamMark, ctx->stream));
+        PT_CUDA(cudaStreamWaitEvent(ctx->copyStream, ctx->streamMark, 0));
+        PT_CUDA(cudaMemcpyAsync(dsum, film->sum, bytes, cudaMemcpyHostToDevice, ctx->copyStream));
+        PT_CUDA(cudaMemcpyAsync(dcomp, film->comp, bytes, cudaMemcpyHostToDevice, ctx->copyStream));
+        PT_CUDA(cudaEventRecord(ctx->filmReady, ctx->copyStream));
+    } else {
+        PT_CUDA(cudaEventRecord(ctx->filmReady, ctx->stream));
     }
     int rc = pt_render_impl(ctx, p, dsum, dcomp, stats);
     if (rc) return rc;

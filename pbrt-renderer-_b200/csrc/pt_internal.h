@@ -156,6 +156,11 @@ struct pt_ctx {
     cudaStream_t stream = nullptr;     // stream all work is issued on
     cudaStream_t ownStream = nullptr;  // created by pt_create, destroyed by pt_destroy
     cudaEvent_t ev[2] = {nullptr, nullptr};  // brackets each render (stats.ms_total)
+    // host films: the upload runs on copyStream beside the render, and the
+    // render's first film kernel waits for filmReady (recorded by pt_render
+    // before every render: after the upload, or on the render stream)
+    cudaStream_t copyStream = nullptr;
+    cudaEvent_t filmReady = nullptr, streamMark = nullptr;
     std::string err;
     std::vector<void *> sceneAllocs;  // freed on re-upload / destroy
     pt::DevScene S{};

@@ -1418,6 +1418,12 @@ cudaError_t enqueue_render(const pt_ctx *ctx, Enqueue &E, WaveArgs A, const pt_r
             E.end();
         }
         uint32_t cover = (uint32_t)std::min<uint64_t>(A.waveCount, npix);
+        if (ws == 0) {  // the film's contents (a host film's upload may still be in flight)
+            cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+            chk(cudaStreamIsCapturing(st, &cs));
+            chk(cudaStreamWaitEvent(st, ctx->filmReady,
+                                    cs == cudaStreamCaptureStatusActive ? cudaEventWaitExternal : 0u));
+        }
         E.begin(STG_FILM);
         k_film<<<(cover + kBlock - 1) / kBlock, kBlock, 0, st>>>(A, (float4 *)d_sum, (float4 *)d_comp);
         E.end();
