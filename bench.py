@@ -439,6 +439,20 @@ def cpu_reference_run(pt, sc, cam, W, H, depth, seconds=15.0, prefer_reference=T
     return paths / t_total / 1e6, kind, cores, f"{frames} frame(s) of {W}x{rows} at 1 spp ({paths} paths, {t_total:.1f} s)"
 
 
+def launch_ranks(n):
+    """`bench.py --gpus N` outside torchrun: start N ranks on this node (one
+    per GPU) with torch.distributed.run and return its exit status."""
+    import socket
+
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", os.path.abspath(__file__), *sys.argv[1:]]
+    return subprocess.call(cmd)
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -483,6 +497,10 @@ def main():
     ap.add_argument("--cache-kernels-only", action="store_true",
                     help="only the radiance-cache network kernels' roofline (profiling of those kernels)")
     args = ap.parse_args()
+    if args.gpus < 1:
+        raise SystemExit("--gpus must be >= 1")
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ and args.impl == "pt":
+        return launch_ranks(args.gpus)
     if args.impl == "reference":
         return run_reference_arm(args)
     if args.cache_kernels_only:
@@ -498,6 +516,8 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus:
+        raise SystemExit(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={world} ranks were started")
     torch.cuda.set_device(local)
     if world > 1:
         from datetime import timedelta
@@ -514,7 +534,9 @@ def main():
     ctx.upload(sc)
     upload_s = time.perf_counter() - t0
     D = importlib.import_module("pbrt_b200.distributed")
-    film = D.new_film(H, W, device="cuda")  # (sum, Kahan compensation)
+    film = D.new_film(H, W, device="cuda")  # accumulated frames (sum, Kahan compensation)
+    shard = D.new_film(H, W, device="cuda") if world > 1 else None  # this rank's part of a frame
+    render_into = D.device_renderer(ctx)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > 126 MB L2
     paths_step = W * H * spp
 
@@ -526,8 +548,7 @@ def main():
                                     wave_paths=args.wave_paths,
                                     flags=base_flags | (pt.PT_RENDER_STAGE_TIMING if timing else 0))
 
-        _, _, st = D.render_shard(ctx, params, film, i, rank, world, spp)
-        D.all_reduce_film(film)
+        _, _, st = D.render_frame(render_into, params, film, i, rank, world, spp, shard=shard)
         return st
 
     def timed_steps(first, timing):
@@ -576,15 +597,24 @@ def main():
             ctx.render(P, film_np, comp_np, pt.PT_MEM_HOST)
         torch.cuda.synchronize()
         e2e_ms = 0.0
+        # with several ranks: rank 0 uploads the accumulated host film into its
+        # shard, every rank renders its samples, one all-reduce sums the
+        # shards and rank 0 downloads the frame (render_frame with host_acc)
+        hfilm = torch.stack([hsum, hcomp]).pin_memory() if world > 1 else None
         for k in range(args.steps):
-            P = pt.render_params(W, H, spp, cam, max_depth=depth,
-                                 sample_offset=D.sample_offset(k, rank, world, spp), env_sampling=env_mode,
-                                 wave_paths=args.wave_paths, flags=base_flags)
+            def e2e_params(off):
+                return pt.render_params(W, H, spp, cam, max_depth=depth, sample_offset=off, env_sampling=env_mode,
+                                        wave_paths=args.wave_paths, flags=base_flags)
             flush.zero_()
+            if world > 1:
+                dist.barrier()
             torch.cuda.synchronize()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
-            ctx.render(P, film_np, comp_np, pt.PT_MEM_HOST)
+            if world > 1:
+                D.render_frame(render_into, e2e_params, None, k, rank, world, spp, shard=shard, host_acc=hfilm)
+            else:
+                ctx.render(e2e_params(D.sample_offset(k, rank, world, spp)), film_np, comp_np, pt.PT_MEM_HOST)
             b.record(stream)
             torch.cuda.synchronize()
             e2e_ms += a.elapsed_time(b)
@@ -632,7 +662,9 @@ def main():
                      "mean_launch_ms": round(ext_ms_per_launch, 4), "dominant_stage": dominant},
         "e2e": None if e2e_value is None else {
             "value": round(e2e_value, 3), "unit": "Mpaths/s", "h2d_bytes_per_step": 2 * W * H * 16,
-            "d2h_bytes_per_step": 2 * W * H * 16},
+            "d2h_bytes_per_step": 2 * W * H * 16,
+            "path": "pt_render with pinned host films" if world == 1 else
+                    "render_frame: host film -> rank-0 shard, render, NCCL all-reduce, shard -> host film"},
         "gpu_launches": int(sum(s.launches for s in stats)),
         "clocks": clk.summary(),
         "scene_upload_s": round(upload_s, 3),

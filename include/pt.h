@@ -324,6 +324,10 @@ int pt_bsdf_eval_batch(pt_ctx *ctx, const pt_material *materials, uint32_t num_m
  *   stream capture.
  * - The array is one per device and process: calls that overlap in time on
  *   the same device (other threads or streams) race on it.  Serialise them.
+ * - The kept address belongs to the device's primary context: after a
+ *   cudaDeviceReset, or from a thread whose current context is not the
+ *   primary one, it no longer names the array.  Callers that reset a device
+ *   must not call this function on it again in the same process.
  * Errors are status codes only (no context to hold a message). */
 #define PT_NOALLOC_MAX_QUERIES 65536u
 #define PT_NOALLOC_MAX_MATERIALS 256u

@@ -39,7 +39,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
 GEN = os.path.join(OUT, "gen")
 SHIM = os.path.join(HERE, "ref_shim")
-DEFAULT_SRC = "/root/reference/shaders"
+# the reference checkout: $PBRT_REFERENCE_ROOT, default /root/reference
+REF_ROOT = os.environ.get("PBRT_REFERENCE_ROOT", "/root/reference")
+DEFAULT_SRC = os.path.join(REF_ROOT, "shaders")
 
 FILES = [
     "Common.hlsli", "RNG.hlsli", "GeometryUtils.hlsli", "RayQueryTrace.hlsli",

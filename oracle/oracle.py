@@ -17,7 +17,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libref.so")
 REF_RIS_SO = os.path.join(HERE, "_ref", "libref_ris.so")  # the reference's USE_RIS=1 build
-REF_SRC = "/root/reference/shaders"
+# the reference checkout (read only where it is present): $PBRT_REFERENCE_ROOT,
+# default /root/reference
+REF_ROOT = os.environ.get("PBRT_REFERENCE_ROOT", "/root/reference")
+REF_SRC = os.path.join(REF_ROOT, "shaders")
 
 
 def build_oracle(quiet=True) -> str:

@@ -684,7 +684,13 @@ int pt_render(pt_ctx *ctx, const pt_render_params *p, pt_film *film, pt_stats *s
         PT_CUDA(cudaEventRecord(ctx->filmReady, ctx->stream));
     }
     int rc = pt_render_impl(ctx, p, dsum, dcomp, stats);
-    if (rc) return rc;
+    if (rc) {
+        // an early error return must not leave the upload in flight: the
+        // staging memory is reused by the next call and the caller may free
+        // the host film once this returns
+        if (host) cudaStreamSynchronize(ctx->copyStream);
+        return rc;
+    }
     if (host) {
         PT_CUDA(cudaMemcpyAsync(film->sum, dsum, bytes, cudaMemcpyDeviceToHost, ctx->stream));
         PT_CUDA(cudaMemcpyAsync(film->comp, dcomp, bytes, cudaMemcpyDeviceToHost, ctx->stream));

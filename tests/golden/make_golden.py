@@ -1,8 +1,9 @@
 """Generate tests/golden/furnace.json from the reference's validation suite.
 
-Run in a checkout that has the reference mounted (default /root/reference):
+Run in a checkout that has the reference mounted (default $PBRT_REFERENCE_ROOT,
+else /root/reference):
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py [--ref <reference checkout>]
 
 For each Disney furnace scene (validation_tests/disney/furnace_*.xml) it
 records the Disney parameters and camera of the XML, and the sphere-masked
@@ -68,7 +69,7 @@ def sphere_mask(W, H, fov_deg=45.0, cam_pos=(0, 0, 4), R=1.0):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("PBRT_REFERENCE_ROOT", "/root/reference"))
     a = ap.parse_args()
     os.environ.setdefault("OPENCV_IO_ENABLE_OPENEXR", "1")
     import cv2

@@ -20,7 +20,9 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PKG = os.path.join(ROOT, "pbrt-renderer-_b200")
 CLI = os.path.join(PKG, "host", "nori_render")
 GOLDEN = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "furnace.json")))
-REF_DISNEY = "/root/reference/validation_tests/disney"
+from oracle.oracle import REF_ROOT  # noqa: E402
+
+REF_DISNEY = os.path.join(REF_ROOT, "validation_tests", "disney")
 
 
 def _mod(name):

@@ -93,6 +93,17 @@ def test_noalloc_matches_staged_entry_point(pt, scenes, ctx):
     g2, q2 = ctx.bsdf_eval(hair, None, wi2, wo2, None)
     assert np.allclose(f2, g2, rtol=1e-6, atol=0) and np.allclose(p2, q2, rtol=1e-6, atol=0)
     assert np.isfinite(f2).all() and np.isfinite(p2).all()
+    # the property the entry point exists for: once warm, calls of any size up
+    # to the limit leave the device's free memory exactly where it was
+    import torch
+
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for n in (17, 4096, MAX_Q, 1):
+        rc, f3, _ = _call(pt, mats, mi[:n], wi[:n], wo[:n], h[:n])
+        assert rc == 0 and np.allclose(f3, g1[:n], rtol=1e-6, atol=0)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
 
 
 @pytest.mark.gpu
