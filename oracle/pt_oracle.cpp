@@ -580,6 +580,30 @@ template <class T> T material_pdf(const V3<T> &wi, const V3<T> &wo, const Mat<T>
         default: return T(0);
     }
 }
+// Mirror / dielectric scattering of the shader's delta branch
+// (shaders/Shaders.hlsl:419-472) restated in the local shading frame of a BSDF
+// query: wi toward the viewer, z the outward normal, wi.z < 0 a query from
+// inside (the shader's hitBackFace, which turns N to the ray's side and swaps
+// the IORs).  u: the dielectric's Fresnel draw.  Weight 1, pdf 0 (discrete).
+template <class T>
+V3<T> delta_sample(const V3<T> &wi, const Mat<T> &m, T u, V3<T> &wo, T &pdf) {
+    bool back = wi.z < T(0);
+    V3<T> I = -wi, N(T(0), T(0), back ? T(-1) : T(1));
+    pdf = T(0);
+    if (m.type == PT_MAT_MIRROR) {
+        wo = reflect(I, N);
+        return V3<T>(T(1));
+    }
+    T etaI = back ? m.intIOR : m.extIOR, etaT = back ? m.extIOR : m.intIOR;
+    T Fr = fresnel_dielectric(dot(-I, N), etaI, etaT);
+    if (u < Fr) wo = reflect(I, N);
+    else {
+        wo = refract(I, N, etaI / etaT);
+        if (dot(wo, wo) < T(0.001)) wo = reflect(I, N);
+    }
+    return V3<T>(T(1));
+}
+
 // u: the uniforms MaterialSample draws, in draw order; *used = how many.
 template <class T>
 V3<T> material_sample(const V3<T> &wi, const T *u, const Mat<T> &m, T h, V3<T> &wo, T &pdf, int *used) {
@@ -2257,7 +2281,8 @@ void or_bsdf_sample(int precision, const pt_material *mats, const uint32_t *mi, 
             V3<double> a(wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]), o;
             double uu[4] = {u[4 * i], u[4 * i + 1], u[4 * i + 2], u[4 * i + 3]};
             double p;
-            V3<double> r = material_sample(a, uu, m, (double)h, o, p, &used);
+            bool delta = pm.type == PT_MAT_MIRROR || pm.type == PT_MAT_DIELECTRIC;
+            V3<double> r = delta ? delta_sample(a, m, uu[0], o, p) : material_sample(a, uu, m, (double)h, o, p, &used);
             wo[3 * i] = (float)o.x; wo[3 * i + 1] = (float)o.y; wo[3 * i + 2] = (float)o.z;
             wt[3 * i] = (float)r.x; wt[3 * i + 1] = (float)r.y; wt[3 * i + 2] = (float)r.z;
             pdf[i] = (float)p;
@@ -2265,7 +2290,8 @@ void or_bsdf_sample(int precision, const pt_material *mats, const uint32_t *mi, 
             Mat<float> m = Mat<float>::from(pm);
             F3 a(wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]), o;
             float p;
-            F3 r = material_sample(a, &u[4 * i], m, h, o, p, &used);
+            bool delta = pm.type == PT_MAT_MIRROR || pm.type == PT_MAT_DIELECTRIC;
+            F3 r = delta ? delta_sample(a, m, u[4 * i], o, p) : material_sample(a, &u[4 * i], m, h, o, p, &used);
             wo[3 * i] = o.x; wo[3 * i + 1] = o.y; wo[3 * i + 2] = o.z;
             wt[3 * i] = r.x; wt[3 * i + 1] = r.y; wt[3 * i + 2] = r.z;
             pdf[i] = p;

@@ -166,7 +166,9 @@ __global__ void k_bsdf_sample(const pt_material *mats, uint32_t nm, const uint32
     float uu[4] = {u[4 * i], u[4 * i + 1], u[4 * i + 2], u[4 * i + 3]};
     float3 o;
     float p;
-    float3 r = material_sample(a, uu, m, hh ? hh[i] : 0.0f, o, p);
+    float3 r = (m.type == PT_MAT_MIRROR || m.type == PT_MAT_DIELECTRIC)
+                   ? delta_sample(a, m, uu[0], o, p)
+                   : material_sample(a, uu, m, hh ? hh[i] : 0.0f, o, p);
     wo[3 * i] = o.x; wo[3 * i + 1] = o.y; wo[3 * i + 2] = o.z;
     wt[3 * i] = r.x; wt[3 * i + 1] = r.y; wt[3 * i + 2] = r.z;
     pdf[i] = p;

@@ -191,6 +191,36 @@ PT_HD float fresnel(float cosI, float etaI, float etaT) {  // :200-219
     float Rp = (etaT * cosI - etaI * cosT) / (etaT * cosI + etaI * cosT);
     return 0.5f * (Rs * Rs + Rp * Rp);
 }
+// Mirror and dielectric (delta BSDFs), shaders/Shaders.hlsl:419-472: the
+// direction a hit scatters into.  rd is the incoming ray's direction, N the
+// shading normal turned to the side the ray arrives from (at a back-face hit
+// the shader flips Ng and N with it), back whether the ray hit the back face.
+// u is the dielectric's Fresnel draw (a mirror draws nothing).  A dielectric
+// reflects with probability Fr, else refracts (reflecting on total internal
+// reflection); etaScale is etaI / etaT after a refraction, else 1.  Delta
+// BSDFs leave the throughput unchanged and have no pdf (lastBsdfPdf = 0).
+PT_HD float3 delta_scatter(uint32_t type, float3 rd, float3 N, bool back, float intIOR, float extIOR, float u,
+                           float &etaScale) {
+    etaScale = 1.0f;
+    if (type == PT_MAT_MIRROR) return reflect(rd, N);
+    float etaI = back ? intIOR : extIOR, etaT = back ? extIOR : intIOR;
+    float Fr = fresnel(dot(-rd, N), etaI, etaT);
+    if (u < Fr) return reflect(rd, N);
+    float3 nd = refract(rd, N, etaI / etaT);
+    if (dot(nd, nd) < 0.001f) return reflect(rd, N);
+    etaScale = etaI / etaT;
+    return nd;
+}
+// The same in the local shading frame (BSDF query convention: wi points to the
+// viewer, z is the outward normal; wi.z < 0 is a query from inside): returns
+// the throughput weight (1), sets wo and pdf = 0 (a discrete measure).
+PT_HD float3 delta_sample(float3 wi, const pt_material &m, float u, float3 &wo, float &pdf) {
+    bool back = wi.z < 0.0f;
+    float es;
+    wo = delta_scatter(m.type, -wi, v3(0.0f, 0.0f, back ? -1.0f : 1.0f), back, m.intIOR, m.extIOR, u, es);
+    pdf = 0.0f;
+    return v3(1.0f);
+}
 PT_HD float luminance(float3 c) { return 0.212671f * c.x + 0.715160f * c.y + 0.072169f * c.z; }  // :225-228
 PT_HD float3 albedo(const pt_material &m) { return v3(m.albedo[0], m.albedo[1], m.albedo[2]); }
 

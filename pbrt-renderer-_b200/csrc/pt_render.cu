@@ -1001,18 +1001,12 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
                         cont = true;
                         st.w &= ~kFlagRough;
                     } else if (type == PT_MAT_DIELECTRIC) {  // Shaders.hlsl:429-472
-                        float etaI = back ? m.intIOR : m.extIOR, etaT = back ? m.extIOR : m.intIOR;
-                        float Fr = fresnel(dot(-rd, N), etaI, etaT);
-                        bool refr = false;
-                        if (next_float(rng, S.sobol1) < Fr) nd = reflect(rd, N);
-                        else {
-                            nd = refract(rd, N, etaI / etaT);
-                            if (dot(nd, nd) < 0.001f) nd = reflect(rd, N);
-                            else refr = true;
-                        }
+                        float es;
+                        nd = delta_scatter(PT_MAT_DIELECTRIC, rd, N, back, m.intIOR, m.extIOR,
+                                           next_float(rng, S.sobol1), es);
                         no = hp + (dot(nd, Ng) > 0.0f ? Ng : -Ng) * 0.001f;
                         lastPdf = 0.0f;
-                        if (refr) eta *= etaI / etaT;
+                        eta *= es;
                         cont = true;
                         st.w &= ~kFlagRough;
                     } else if (C != CLS_DELTA &&

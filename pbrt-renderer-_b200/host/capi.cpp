@@ -48,6 +48,9 @@ int nori_info(void *scene, uint32_t *out8) {
     return 0;
 }
 
+// The scene's envmapScale (no GPU needed).
+float nori_env_scale(void *scene) { return static_cast<const Scene *>(scene)->getEnvmapScale(); }
+
 // Camera constants the GPU integrator uses (no GPU needed).
 int nori_camera(void *scene, pt_camera *out) {
     const Scene *s = static_cast<const Scene *>(scene);

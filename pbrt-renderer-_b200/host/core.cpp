@@ -233,12 +233,16 @@ static std::vector<std::string> &searchPaths() {
     return v;
 }
 void pushSearchPath(const std::string &dir) { searchPaths().insert(searchPaths().begin(), dir); }
-std::string resolvePath(const std::string &name) {
+void popSearchPath() {
+    if (!searchPaths().empty()) searchPaths().erase(searchPaths().begin());
+}
+std::string resolvePath(const std::string &name, const std::string &baseDir) {
     if (!name.empty() && name[0] == '/') return name;
+    auto readable = [](const std::string &p) { return std::ifstream(p).good(); };
+    if (!baseDir.empty() && readable(baseDir + "/" + name)) return baseDir + "/" + name;
     for (const std::string &d : searchPaths()) {
         std::string p = d.empty() ? name : d + "/" + name;
-        std::ifstream f(p);
-        if (f.good()) return p;
+        if (readable(p)) return p;
     }
     return name;
 }
@@ -651,12 +655,23 @@ NoriObject *loadFromXML(const std::string &filename) {
     ss << f.rdbuf();
     std::string text = ss.str();
     size_t slash = filename.find_last_of('/');
-    pushSearchPath(slash == std::string::npos ? std::string(".") : filename.substr(0, slash));
+    const std::string dir = slash == std::string::npos ? std::string(".") : filename.substr(0, slash);
+    // The scene's directory is searched first while its own files load (the
+    // reference's resolver prepends it, src/cpu/parser.cpp), and only then:
+    // a later scene in the same process must not find this one's files.
+    struct Scoped {
+        explicit Scoped(const std::string &d) { pushSearchPath(d); }
+        ~Scoped() { popSearchPath(); }
+    } scoped(dir);
     XmlReader xr(text, filename);
     XNode root = xr.parseDocument();
     Loader L{xr, filename};
     PropertyList list;
-    return L.parse(root, list, TInvalid);
+    NoriObject *obj = L.parse(root, list, TInvalid);
+    // files the scene names but reads later (envmap, textures, volume grids)
+    // resolve against its directory too
+    if (obj && obj->getClassType() == NoriObject::EScene) static_cast<Scene *>(obj)->setBaseDir(dir);
+    return obj;
 }
 
 }  // namespace nori

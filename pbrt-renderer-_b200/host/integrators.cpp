@@ -34,7 +34,7 @@ void flattenScene(const Scene *scene, FlatScene &out) {
     std::unordered_map<std::string, uint32_t> texCache;
     auto texture = [&](const std::string &rel, bool srgb) -> uint32_t {
         if (rel.empty()) return PT_NO_TEXTURE;
-        std::string path = resolvePath(rel);
+        std::string path = resolvePath(rel, scene->getBaseDir());
         auto it = texCache.find(path);
         if (it != texCache.end()) return it->second;
         std::vector<uint8_t> rgba;
@@ -99,7 +99,7 @@ void flattenScene(const Scene *scene, FlatScene &out) {
     }
     for (size_t t = 0; t < out.textures.size(); t++) out.textures[t].rgba8 = out.texData[t].data();
     // envmap: the reference falls back to a 1x1 0.5 grey texel when the HDR cannot be read
-    std::string hdr = resolvePath(scene->getEnvmap());
+    std::string hdr = resolvePath(scene->getEnvmap(), scene->getBaseDir());
     if (!loadHDR(hdr, out.env, out.envW, out.envH)) {
         std::fprintf(stderr, "[envmap] No HDR at '%s' - falling back to flat gray.\n", hdr.c_str());
         out.envW = out.envH = 1;
@@ -121,7 +121,7 @@ void flattenScene(const Scene *scene, FlatScene &out) {
         if (med->isHeterogeneous() && !med->getVolumePath().empty()) {
             std::vector<float> data;
             uint32_t w, h, d;
-            std::string p = resolvePath(med->getVolumePath());
+            std::string p = resolvePath(med->getVolumePath(), scene->getBaseDir());
             if (loadVol(p, data, w, h, d)) {
                 v.density_grid = (uint32_t)out.gridData.size();
                 out.gridData.push_back(std::move(data));

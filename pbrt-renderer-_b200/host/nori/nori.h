@@ -381,6 +381,9 @@ public:
     const std::string &getEnvmap() const { return m_envmap; }
     float getEnvmapScale() const { return m_envmapScale; }
     float getEvCompensation() const { return m_evCompensation; }
+    // directory of the scene file: what the scene names by relative path resolves there first
+    const std::string &getBaseDir() const { return m_baseDir; }
+    void setBaseDir(const std::string &dir) { m_baseDir = dir; }
     void activate() override;
     void addChild(NoriObject *obj) override;
     std::string toString() const override;
@@ -393,7 +396,7 @@ private:
     Camera *m_camera = nullptr;
     Medium *m_medium = nullptr;
     BoundingBox3f m_bbox;
-    std::string m_envmap;
+    std::string m_envmap, m_baseDir;
     float m_envmapScale = 1.0f, m_evCompensation = 0.0f;
 };
 
@@ -474,9 +477,13 @@ void loadImageRGBA8(const std::string &path, uint32_t &width, uint32_t &height, 
 // Camera constants of src/gpu/DXRApp_Camera.cpp:23-112 from a Nori camera.
 pt_camera cameraConstants(const Camera *cam, int width, int height);
 
-// File resolution relative to the scene file (filesystem/resolver.h).
-std::string resolvePath(const std::string &name);
+// File resolution relative to the scene file (filesystem/resolver.h): an
+// absolute name as is, else baseDir/name when readable, else the first
+// readable entry of the search paths (the directory of the XML being loaded
+// while it loads, and any the caller pushed), else the name unchanged.
+std::string resolvePath(const std::string &name, const std::string &baseDir = std::string());
 void pushSearchPath(const std::string &dir);
+void popSearchPath();
 // Radiance .hdr (RGBE) loader; returns false when the file cannot be read.
 bool loadHDR(const std::string &path, std::vector<float> &rgb, uint32_t &w, uint32_t &h);
 // .vol density grid ("VOL1", W, H, D, bbox, float data): src/gpu/DXRApp_Scene.cpp:495-548.

@@ -160,6 +160,44 @@ def test_bsdf_sample_parity(kind_name, pt, scenes, ctx, oracle):
     assert_parity_ill_conditioned(sp)
 
 
+@pytest.mark.parametrize("kind_name", ["MIRROR", "DIELECTRIC"])
+def test_delta_bsdf_sample_parity(kind_name, pt, scenes, ctx, oracle):
+    """Mirror and dielectric scattering: the shading kernels' delta branch
+    (shaders/Shaders.hlsl:419-472, one device function for both) queried in
+    the local frame from both sides, IOR pairs with extIOR above intIOR as
+    well (total internal reflection).  Weight exactly 1 and pdf exactly 0
+    (discrete); the Fresnel pick may flip only where u is within rounding of
+    Fr; directions no further from FP64 than the float32 oracle's."""
+    kind = getattr(pt, "PT_MAT_" + kind_name)
+    rng = np.random.default_rng(53)
+    mats = []
+    for _ in range(64):
+        m = pt.make_material(kind, (1.0, 1.0, 1.0))
+        m.intIOR, m.extIOR = float(rng.uniform(1.0, 2.4)), float(rng.uniform(1.0, 1.8))
+        mats.append(m)
+    n = N_PAIRS
+    wi = scenes.sample_directions(n, 57, upper=False)
+    u = rng.uniform(0, 1, (n, 4)).astype(np.float32)
+    mi = rng.integers(0, len(mats), n).astype(np.uint32)
+    wog, wtg, pg = ctx.bsdf_sample(mats, mi, wi, u, None)
+    wo32, wt32, p32 = oracle.bsdf_sample(mats, mi, wi, u, None)
+    wo64, _, _ = oracle.bsdf_sample(mats, mi, wi, u, None, fp64=True)
+    assert np.all(wtg == 1.0) and np.all(pg == 0.0) and np.all(wt32 == 1.0) and np.all(p32 == 0.0)
+    e_gpu = np.abs(wog - wo64).max(1)
+    e_or = np.abs(wo32 - wo64).max(1)
+    same = e_gpu < 1e-2
+    print(kind_name, "same branch", same.mean(), "max err gpu", e_gpu[same].max(), "oracle", e_or[same].max())
+    assert same.mean() > 0.9999
+    assert (e_gpu <= 4 * e_or + 2e-6)[same].mean() > 0.999
+    assert np.quantile(e_gpu[same], 0.999) <= 1.25 * np.quantile(e_or[same], 0.999) + 1e-6
+    assert e_gpu[same].max() <= max(2e-5, 2 * e_or[same].max())
+    if kind == pt.PT_MAT_MIRROR:  # reflection about z: exact in float
+        assert np.array_equal(wog, wo32)
+    else:
+        refracted = np.sign(wog[:, 2]) != np.sign(wi[:, 2])
+        assert 0.3 < refracted.mean() < 0.99
+
+
 def test_phase_sample_parity(ctx, oracle, scenes):
     n = N_PAIRS
     rng = np.random.default_rng(41)
@@ -238,8 +276,19 @@ def test_envmap_sampler_distribution(mode, pt, ctx, scenes):
     assert np.abs(z).max() < 6.0 and np.mean(z ** 2) < 1.3, (np.abs(z).max(), np.mean(z ** 2))
 
 
-def test_bvh_topology_bit_exact(ctx, oracle, scenes):
-    sc, _ = scenes.disney_spheres(32, 32, grid=3, slices=48, rings=25, env_w=16, env_h=8)
+@pytest.fixture(scope="module")
+def bench_scene(scenes):
+    """The bench's scene: 64 spheres x 20,480 triangles (1,310,720), treelet-
+    restructured 8-wide BVH on the GPU."""
+    return scenes.disney_spheres(1280, 720)
+
+
+@pytest.mark.parametrize("which", ["small", "bench"])
+def test_bvh_topology_bit_exact(which, ctx, oracle, scenes, bench_scene):
+    if which == "small":
+        sc, _ = scenes.disney_spheres(32, 32, grid=3, slices=48, rings=25, env_w=16, env_h=8)
+    else:
+        sc, _ = bench_scene
     ctx.upload(sc)
     oracle.load(sc)
     mg, og, ng, nwide = ctx.bvh()
@@ -250,23 +299,57 @@ def test_bvh_topology_bit_exact(ctx, oracle, scenes):
     assert 0 < nwide < sc.num_triangles
 
 
-@pytest.mark.parametrize("which", ["spheres", "cornell", "hair"])
-def test_trace_parity(which, ctx, oracle, scenes):
+def _surface_rays(sc, rng, n):
+    """Rays leaving random points of random triangles (offset 1e-3 along the
+    face normal, directions over the sphere): bounce-like rays."""
+    P = sc.positions.astype(np.float64)
+    f = sc.indices.reshape(-1, 3)
+    # indices are per mesh: add each mesh's vertex offset
+    off = np.zeros(len(f), np.int64)
+    for m in sc.materials:
+        off[m.indexOffset // 3:(m.indexOffset + m.indexCount) // 3] = m.vertexOffset
+    t = rng.integers(0, len(f), n)
+    a, b, c = (P[f[t, k] + off[t]] for k in range(3))
+    r1, r2 = rng.uniform(0, 1, n), rng.uniform(0, 1, n)
+    s1 = np.sqrt(r1)
+    p = a * (1 - s1)[:, None] + b * (s1 * (1 - r2))[:, None] + c * (s1 * r2)[:, None]
+    nrm = np.cross(b - a, c - a)
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True) + 1e-30
+    d = rng.standard_normal((n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    o = p + nrm * np.where((d * nrm).sum(1) > 0, 1e-3, -1e-3)[:, None]
+    return o.astype(np.float32), d.astype(np.float32)
+
+
+@pytest.mark.parametrize("which", ["spheres", "cornell", "hair", "bench"])
+def test_trace_parity(which, ctx, oracle, scenes, bench_scene):
+    """Closest hits against the oracle's SAH BVH.  The triangle test rounds as
+    the oracle's (bit-identical t, u, v), so a ray may disagree only where
+    traversal decides: an equal-t tie between triangles, or a hit within
+    1e-6 (barycentric) of an edge that one tree's box test grazes.  No other
+    disagreement is allowed.  The bench scene's 1,310,720-triangle tree gets
+    2^20 rays, half from random points in space, half leaving its surfaces."""
+    rng = np.random.default_rng(47)
+    n = 200000
     if which == "spheres":
         sc, _ = scenes.disney_spheres(32, 32, grid=3, slices=48, rings=25, env_w=16, env_h=8)
         lo, hi = -6.0, 6.0
     elif which == "cornell":
         sc, _ = scenes.cornell(32, 32)
         lo, hi = -1.0, 2.0
-    else:
+    elif which == "hair":
         sc, _ = scenes.hair_volume(32, 32, strands=400, segments=8, grid_n=16)
         lo, hi = -1.5, 1.5
+    else:
+        sc, _ = bench_scene
+        n = 1 << 20
+        lo, hi = sc.positions.min(0) - 1.0, sc.positions.max(0) + 1.0
     ctx.upload(sc)
     oracle.load(sc)
-    rng = np.random.default_rng(47)
-    n = 200000
     o = rng.uniform(lo, hi, (n, 3)).astype(np.float32)
     d = scenes.sample_directions(n, 48)
+    if which == "bench":
+        o[n // 2:], d[n // 2:] = _surface_rays(sc, rng, n - n // 2)
     rays = np.zeros((n, 8), np.float32)
     rays[:, 0:3], rays[:, 3], rays[:, 4:7], rays[:, 7] = o, 0.0, d, 1e20
     hg = ctx.trace_closest(rays)
@@ -274,15 +357,24 @@ def test_trace_parity(which, ctx, oracle, scenes):
     same_hit = hg["hit"] == ho["hit"]
     both = (hg["hit"] == 1) & (ho["hit"] == 1)
     same_prim = (hg["mesh"] == ho["mesh"]) & (hg["prim"] == ho["prim"])
-    # disagreements only where the oracle's barycentrics are within 1e-6 of an edge
-    # (or the hit distances tie), i.e. the ray grazes a shared edge or vertex
-    edge = np.minimum(np.minimum(ho["u"], ho["v"]), 1 - ho["u"] - ho["v"]) < 1e-4
+
+    def near_edge(h):
+        return (h["hit"] == 1) & (np.minimum(np.minimum(h["u"], h["v"]), 1 - h["u"] - h["v"]) < 1e-6)
+
+    tie = both & (hg["t"] == ho["t"])
+    exempt = near_edge(hg) | near_edge(ho) | tie
     bad = ~(same_hit & (~both | same_prim))
-    assert (bad & ~edge).sum() <= max(2, n // 100000), int((bad & ~edge).sum())
+    print(which, "rays", n, "hits", int(both.sum()), "disagreements", int(bad.sum()), "ties", int((bad & tie).sum()),
+          "near an edge", int((bad & ~tie).sum()))
+    assert (bad & ~exempt).sum() == 0, int((bad & ~exempt).sum())
+    assert bad.mean() < 1e-4
+    # the same triangle at the same distance, bit for bit
     tt = both & same_prim
-    assert np.abs(hg["t"][tt] - ho["t"][tt]).max() <= 1e-4 * max(1.0, float(np.abs(ho["t"][tt]).max()))
-    # shadow rays: occlusion within the closest-hit distance
+    assert np.array_equal(hg["t"][tt], ho["t"][tt])
+    assert np.array_equal(hg["u"][tt], ho["u"][tt]) and np.array_equal(hg["v"][tt], ho["v"][tt])
+    # shadow rays: occlusion within half the closest-hit distance
     rays[:, 7] = np.where(ho["hit"] == 1, ho["t"] * 0.5, 10.0)
     og, _ = ctx.trace_shadow(rays)
     oo, _ = oracle.trace_shadow(rays)
-    assert (og != oo).mean() < 1e-3
+    print(which, "shadow disagreements", int((og != oo).sum()))
+    assert (og != oo).mean() < 1e-4

@@ -89,8 +89,8 @@ def scene_dir(tmp_path_factory, scenes):
     return d
 
 
-@pytest.fixture(scope="module")
-def nori():
+def nori_lib():
+    """ctypes binding of the Nori host's C surface (host/capi.cpp)."""
     L = C.CDLL(LIBNORI)
     L.nori_load.restype = C.c_void_p
     L.nori_load.argtypes = [C.c_char_p, C.c_char_p, C.c_size_t]
@@ -103,7 +103,14 @@ def nori():
                               C.c_size_t]
     L.nori_flat.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
     L.nori_flat.restype = C.c_uint64
+    L.nori_env_scale.argtypes = [C.c_void_p]
+    L.nori_env_scale.restype = C.c_float
     return L
+
+
+@pytest.fixture(scope="module")
+def nori():
+    return nori_lib()
 
 
 def load(nori, path):
@@ -356,6 +363,34 @@ def flat(nori, h, which):
     return a
 
 
+def scene_from_xml(nori, pt, path):
+    """Load a Nori XML scene through the host (parser, plugins, OBJ loader,
+    flattening, camera conversion) and rebuild the flattened arrays as a
+    pt.Scene, so the oracle, the reference build and libpt all see the scene
+    the host would upload.  Returns (scene, camera, info) with info as
+    nori_info (width, height, spp, meshes, triangles, emitters, medium,
+    max depth).  Scenes with textures or media are not rebuilt here."""
+    h, err = load(nori, path)
+    assert h, err
+    try:
+        info = (C.c_uint32 * 8)()
+        nori.nori_info(h, info)
+        assert info[6] == 0 and int(nori.nori_flat(h, 7, None)) == 0, "textures / media are not rebuilt"
+        n = nori.nori_materials(h, None, 0)
+        mats = (pt.pt_material * n)()
+        nori.nori_materials(h, mats, n)
+        cam = pt.pt_camera()
+        nori.nori_camera(h, C.byref(cam))
+        pos, nrm, uv, tan, idx, env = (flat(nori, h, k) for k in range(6))
+        ew = int(nori.nori_flat(h, 6, None))
+        sc = pt.Scene(pos, idx, list(mats), normals=nrm if nrm.size else None, texcoords=uv if uv.size else None,
+                      tangents=tan if tan.size else None, env_rgb=env.reshape(-1, ew, 3),
+                      env_scale=float(nori.nori_env_scale(h)))
+        return sc, cam, list(info)
+    finally:
+        nori.nori_free(h)
+
+
 SSS_XML = SCENE_XML.replace('''    <bsdf type="disney">
       <color name="baseColor" value="0.8, 0.3, 0.2"/>
       <float name="roughness" value="0.4"/><float name="metallic" value="0.2"/><float name="clearcoat" value="0.5"/>
@@ -406,3 +441,25 @@ def test_subsurface_xml_render_matches_direct_scene(nori, pt, scene_dir):
     ctx.close()
     assert np.array_equal(s, d), np.abs(s - d).max()
     nori.nori_free(h)
+
+
+def test_scene_files_resolve_per_scene(nori, pt, tmp_path):
+    """Relative file names resolve against the scene's own directory: a scene
+    loaded later in the same process does not pick up an earlier scene's
+    files (here the default envmap textures/white_furnace.hdr)."""
+    xml = """<scene><camera type="perspective"><integer name="width" value="8"/>
+      <integer name="height" value="8"/></camera>
+      <mesh type="obj"><string name="filename" value="tri.obj"/></mesh></scene>"""
+    for name, with_env in (("a", True), ("b", False)):
+        d = tmp_path / name
+        (d / "textures").mkdir(parents=True)
+        write_obj(d / "tri.obj", np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], float), np.array([[0, 1, 2]]))
+        if with_env:
+            write_hdr(d / "textures" / "white_furnace.hdr", np.ones((2, 2, 3), np.float32))
+        (d / "scene.xml").write_text(xml)
+    sa, _, _ = scene_from_xml(nori, pt, tmp_path / "a" / "scene.xml")
+    sb, _, _ = scene_from_xml(nori, pt, tmp_path / "b" / "scene.xml")
+    sa2, _, _ = scene_from_xml(nori, pt, tmp_path / "a" / "scene.xml")
+    assert np.array_equal(sa.env_rgb, np.ones((2, 2, 3), np.float32))
+    assert np.array_equal(sb.env_rgb, np.full((1, 1, 3), 0.5, np.float32))
+    assert np.array_equal(sa2.env_rgb, sa.env_rgb)
