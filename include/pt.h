@@ -245,6 +245,21 @@ int pt_destroy(pt_ctx *ctx);
  * ownership of the stream.  No reference counterpart (DXRApp owns its queue,
  * src/gpu/DXRApp_Device.cpp). */
 int pt_set_stream(pt_ctx *ctx, void *stream);
+
+/* Test hooks for the device error paths; no counterpart in the reference.
+ * They make the library's own bounded checks fire without any fault:
+ * - PT_DEBUG_SHADOW_QUEUE_CAP: shadow-ray queue capacity of later pt_render
+ *   calls (0 = the default, two per path).  Below the number of NEE rays a
+ *   render makes, shadow rays beyond it are dropped and the render returns
+ *   PT_E_DEVICE (queue overflow); no memory beyond the queue is touched.
+ * - PT_DEBUG_CACHE_STALL: radiance-cache kernels first wait `value` polls on
+ *   a barrier nothing arrives at, before they issue any copy or tensor-core
+ *   work, then take their error exit (TMEM freed): the call returns
+ *   PT_E_DEVICE.  0 = off.
+ * Setting a hook back to 0 restores normal operation on the same context. */
+#define PT_DEBUG_SHADOW_QUEUE_CAP 1u
+#define PT_DEBUG_CACHE_STALL 2u
+int pt_debug_set(pt_ctx *ctx, uint32_t what, uint64_t value);
 const char *pt_last_error(const pt_ctx *ctx);
 int pt_abi_version(void);
 

@@ -40,7 +40,7 @@ struct HostScene {
     std::vector<uint3> gridDims;
     std::vector<bool> opaque;               // per mesh (instance flags)
     std::vector<uint> triMesh, triPrim;
-    struct Node { float lo[3], hi[3]; uint left, right, start, count; };
+    struct Node { float lo[3], hi[3]; uint left, right, start, count, axis; };
     std::vector<Node> nodes;
     std::vector<uint> prims;
 };
@@ -56,6 +56,13 @@ static void tri_verts(uint g, float3 &p0, float3 &p1, float3 &p2) {
     p0 = V(0); p1 = V(1); p2 = V(2);
 }
 
+// The ray-query stand-in's tree: a binned SAH build with the cost model of
+// the reference's CPU accelerator (src/cpu/accel.cpp:55-324): 16 centroid
+// bins along the node's largest axis, cost 2 C_trav + C_isect (n_L A_L +
+// n_R A_R) / A with both costs 1, against C_isect n for a leaf; nodes of
+// fewer than 32 triangles, or where the bins find no better split, get an
+// exact sweep over the sorted centroids of all three axes.  Leaves where no
+// split is cheaper.  Depth is capped so traversal's 128-entry stack holds.
 static void build_bvh() {
     uint n = (uint)g_host.triMesh.size();
     g_host.prims.resize(n);
@@ -70,30 +77,105 @@ static void build_bvh() {
     }
     g_host.nodes.clear();
     if (!n) return;
-    struct It { uint node, s, e; };
-    std::vector<It> st{{0, 0, n}};
+    struct Box {
+        float3 l{1e30f, 1e30f, 1e30f}, h{-1e30f, -1e30f, -1e30f};
+        void add(const float3 &a, const float3 &b) { l = min(l, a); h = max(h, b); }
+        void add(const Box &o) { l = min(l, o.l); h = max(h, o.h); }
+        float area() const {
+            if (l.x > h.x) return 0.0f;
+            float3 e = h - l;
+            return 2.0f * (e.x * e.y + e.y * e.z + e.z * e.x);
+        }
+    };
+    constexpr int kBins = 16, kSerial = 32, kMaxDepth = 100;
+    struct It { uint node, s, e, depth; };
+    std::vector<It> st{{0, 0, n, 0}};
     g_host.nodes.push_back({});
+    uint *P = g_host.prims.data();
+    std::vector<float> rightArea(n + 1);
     while (!st.empty()) {
         It it = st.back();
         st.pop_back();
         HostScene::Node nd{};
-        float3 bl(1e30f, 1e30f, 1e30f), bh(-1e30f, -1e30f, -1e30f);
-        for (uint i = it.s; i < it.e; i++) { bl = min(bl, lo[g_host.prims[i]]); bh = max(bh, hi[g_host.prims[i]]); }
-        for (int a = 0; a < 3; a++) { nd.lo[a] = bl[a]; nd.hi[a] = bh[a]; }
-        uint cnt = it.e - it.s;
-        if (cnt <= 4) { nd.start = it.s; nd.count = cnt; g_host.nodes[it.node] = nd; continue; }
-        float3 ext = bh - bl;
+        Box bb;
+        for (uint i = it.s; i < it.e; i++) bb.add(lo[P[i]], hi[P[i]]);
+        for (int a = 0; a < 3; a++) { nd.lo[a] = bb.l[a]; nd.hi[a] = bb.h[a]; }
+        const uint cnt = it.e - it.s;
+        const float A = bb.area();
+        float bestCost = (float)cnt;  // a leaf
+        int bestAxis = -1;
+        uint split = 0;  // triangles left of the split, in the order of bestAxis
+        float3 ext = bb.h - bb.l;
         int ax = ext.x > ext.y ? (ext.x > ext.z ? 0 : 2) : (ext.y > ext.z ? 1 : 2);
-        uint mid = it.s + cnt / 2;
-        std::nth_element(g_host.prims.begin() + it.s, g_host.prims.begin() + mid, g_host.prims.begin() + it.e,
-                         [&](uint a, uint b) { return ce[a][ax] < ce[b][ax]; });
+        bool binned = false;
+        if (cnt >= kSerial && A > 0.0f && ext[ax] > 0.0f) {
+            float cmin = bb.l[ax], scale = kBins / ext[ax];
+            uint binCnt[kBins] = {};
+            Box binBox[kBins];
+            auto binOf = [&](uint g) { return std::min(std::max((int)((ce[g][ax] - cmin) * scale), 0), kBins - 1); };
+            for (uint i = it.s; i < it.e; i++) {
+                int b = binOf(P[i]);
+                binCnt[b]++;
+                binBox[b].add(lo[P[i]], hi[P[i]]);
+            }
+            Box left[kBins];
+            uint leftCnt[kBins];
+            left[0] = binBox[0];
+            leftCnt[0] = binCnt[0];
+            for (int b = 1; b < kBins; b++) {
+                left[b] = left[b - 1];
+                left[b].add(binBox[b]);
+                leftCnt[b] = leftCnt[b - 1] + binCnt[b];
+            }
+            Box right = binBox[kBins - 1];
+            int bestBin = -1;
+            for (int b = kBins - 2; b >= 0; b--) {
+                float c = 2.0f + (leftCnt[b] * left[b].area() + (cnt - leftCnt[b]) * right.area()) / A;
+                if (c < bestCost && leftCnt[b] > 0 && leftCnt[b] < cnt) { bestCost = c; bestBin = b; }
+                right.add(binBox[b]);
+            }
+            if (bestBin >= 0) {
+                uint *mid = std::partition(P + it.s, P + it.e, [&](uint g) { return binOf(g) <= bestBin; });
+                split = (uint)(mid - (P + it.s));
+                bestAxis = ax;
+                binned = true;
+            }
+        }
+        if (!binned && cnt > 1 && A > 0.0f) {  // exact sweep, every axis
+            for (int a = 0; a < 3; a++) {
+                std::sort(P + it.s, P + it.e, [&](uint x, uint y) { return ce[x][a] < ce[y][a] || (ce[x][a] == ce[y][a] && x < y); });
+                Box r;
+                for (uint i = cnt; i >= 1; i--) {
+                    r.add(lo[P[it.s + i - 1]], hi[P[it.s + i - 1]]);
+                    rightArea[i - 1] = r.area();
+                }
+                Box l;
+                for (uint i = 1; i < cnt; i++) {
+                    l.add(lo[P[it.s + i - 1]], hi[P[it.s + i - 1]]);
+                    float c = 2.0f + (i * l.area() + (cnt - i) * rightArea[i]) / A;
+                    if (c < bestCost) { bestCost = c; bestAxis = a; split = i; }
+                }
+            }
+            if (bestAxis >= 0 && bestAxis != 2)  // the last sort was along z
+                std::sort(P + it.s, P + it.e, [&](uint x, uint y) {
+                    return ce[x][bestAxis] < ce[y][bestAxis] || (ce[x][bestAxis] == ce[y][bestAxis] && x < y);
+                });
+        }
+        if (bestAxis < 0 || it.depth >= kMaxDepth) {
+            if (bestAxis < 0 || cnt <= 4) { nd.start = it.s; nd.count = cnt; g_host.nodes[it.node] = nd; continue; }
+        }
+        if (it.depth >= kMaxDepth) {  // deep and still large: median split on the largest axis
+            bestAxis = ax;
+            split = cnt / 2;
+            std::nth_element(P + it.s, P + it.s + split, P + it.e, [&](uint x, uint y) { return ce[x][ax] < ce[y][ax]; });
+        }
         uint L = (uint)g_host.nodes.size();
         g_host.nodes.push_back({});
         g_host.nodes.push_back({});
-        nd.left = L; nd.right = L + 1; nd.count = 0;
+        nd.left = L; nd.right = L + 1; nd.count = 0; nd.axis = (uint)bestAxis;
         g_host.nodes[it.node] = nd;
-        st.push_back({L, it.s, mid});
-        st.push_back({L + 1, mid, it.e});
+        st.push_back({L, it.s, it.s + split, it.depth + 1});
+        st.push_back({L + 1, it.s + split, it.e, it.depth + 1});
     }
 }
 
@@ -155,9 +237,10 @@ void collect_candidates(const RayDesc &r, std::vector<Candidate> &out, bool acce
                     out.push_back(c);
                 }
             }
-        } else {
-            stack[sp++] = n.left;
-            stack[sp++] = n.right;
+        } else if (sp + 2 <= 128) {  // near child (along the split axis) on top
+            bool leftNear = r.Direction[(int)n.axis] >= 0.0f;
+            stack[sp++] = leftNear ? n.right : n.left;
+            stack[sp++] = leftNear ? n.left : n.right;
         }
     }
     if (haveOpaque) {

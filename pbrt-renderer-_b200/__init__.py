@@ -37,6 +37,8 @@ PT_CACHE_FEATURES = 64
 PT_CACHE_RECORD_FLOATS = 16
 PT_CACHE_MAX_RECORDS = 262144
 PT_CACHE_NO_TRAIN = 1
+PT_DEBUG_SHADOW_QUEUE_CAP, PT_DEBUG_CACHE_STALL = 1, 2
+PT_E_DEVICE = -5
 
 
 class pt_material(C.Structure):
@@ -273,6 +275,7 @@ def lib():
         L.pt_create.argtypes = [C.POINTER(C.c_void_p), C.c_int]
         L.pt_destroy.argtypes = [P]
         L.pt_set_stream.argtypes = [P, C.c_void_p]
+        L.pt_debug_set.argtypes = [P, C.c_uint32, C.c_uint64]
         L.pt_last_error.argtypes = [P]
         L.pt_last_error.restype = C.c_char_p
         L.pt_upload_scene.argtypes = [P, C.POINTER(pt_scene_desc)]
@@ -317,6 +320,10 @@ class Context:
     def _check(self, rc):
         if rc != 0:
             raise PTError(f"libpt error {rc}: {self.L.pt_last_error(self.h).decode()}")
+
+    def debug_set(self, what, value):
+        """Test hooks of the device error paths (pt_debug_set)."""
+        self._check(self.L.pt_debug_set(self.h, what, value))
 
     def set_stream(self, stream_ptr):
         """Run libpt work on an existing CUDA stream (an int cudaStream_t)."""

@@ -310,6 +310,15 @@ int pt_set_stream(pt_ctx *ctx, void *stream) {
     return PT_OK;
 }
 
+int pt_debug_set(pt_ctx *ctx, uint32_t what, uint64_t value) {
+    if (!ctx) return PT_E_INVALID;
+    if (value > 0xFFFFFFFFull) return ctx->fail(PT_E_INVALID, "debug value out of range");
+    if (what == PT_DEBUG_SHADOW_QUEUE_CAP) ctx->dbgShadowCap = (uint32_t)value;
+    else if (what == PT_DEBUG_CACHE_STALL) ctx->dbgCacheStall = (uint32_t)value;
+    else return ctx->fail(PT_E_INVALID, "unknown debug hook");
+    return PT_OK;
+}
+
 const char *pt_last_error(const pt_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
 // LoadTexture's mip chain (src/gpu/DXRApp_Textures.cpp:49-95): levels halve

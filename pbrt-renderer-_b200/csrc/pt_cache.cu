@@ -38,6 +38,7 @@ struct RcNet {
     const uint8_t *img;  // BF16 weight image
     float bmin[3], binv[3];
     uint32_t *err;
+    uint32_t stallPolls;  // test hook: polls of the up-front stall (0 = none)
 };
 
 // Input of one row: a record (encoded here) or a ready feature vector.
@@ -86,9 +87,10 @@ struct CtaCtl {
     uint32_t mbW, mbM, tbase, tl;
     uint32_t phase;
     bool ok;
+    bool copyIssued, mmaPending;  // what an error exit still has to wait for
 };
 __device__ __forceinline__ void rc_setup(CtaCtl &c, uint8_t *W, uint64_t *bars, uint32_t *tslot, const uint8_t *img,
-                                         uint32_t cols) {
+                                         uint32_t cols, uint32_t stallPolls) {
     const uint32_t t = threadIdx.x, warp = t >> 5;
     c.mbW = smem_u32(bars);
     c.mbM = smem_u32(bars + 1);
@@ -98,10 +100,17 @@ __device__ __forceinline__ void rc_setup(CtaCtl &c, uint8_t *W, uint64_t *bars, 
         mbar_fence_init();
     }
     __syncthreads();
-    if (t == 0) {
+    // Test hook: a wait that runs out.  Nothing arrives at mbM before an MMA
+    // is committed to it, so with no copy or MMA issued yet every thread gives
+    // up after stallPolls polls and the CTA takes the error exit below.
+    bool ok = true;
+    if (stallPolls) ok = __syncthreads_and(mbar_wait(c.mbM, 0, stallPolls)) != 0;
+    if (ok && t == 0) {
         mbar_expect_tx(c.mbW, kRcImageBytes);
         bulk_g2s(smem_u32(W), img, kRcImageBytes, c.mbW);
     }
+    c.copyIssued = ok;
+    c.mmaPending = false;
     __syncwarp();
     if (warp == 0) tmem_alloc(smem_u32(tslot), cols);
     tc_fence_before();
@@ -110,21 +119,22 @@ __device__ __forceinline__ void rc_setup(CtaCtl &c, uint8_t *W, uint64_t *bars, 
     c.tbase = *tslot;
     c.tl = c.tbase + ((warp * 32u) << 16);
     c.phase = 0;
-    c.ok = __syncthreads_and(mbar_wait(c.mbW, 0)) != 0;
+    c.ok = ok && __syncthreads_and(mbar_wait(c.mbW, 0)) != 0;  // ok is uniform across the CTA
 }
 // Wait for the MMAs committed to mbM; uniform across the CTA.
 __device__ __forceinline__ bool rc_wait_mma(CtaCtl &c) {
     bool done = mbar_wait(c.mbM, c.phase);
     bool all = __syncthreads_and(done) != 0;
     if (all) c.phase ^= 1u;
+    else c.mmaPending = true;
     tc_fence_after();
     return all;
 }
 __device__ __forceinline__ void rc_teardown(CtaCtl &c, uint32_t cols, uint32_t *err) {
     if (!c.ok) {
         if (threadIdx.x == 0) atomicOr(err, kDevErrCache);
-        mbar_wait(c.mbW, 0, 1u << 20);        // the weight copy, if it is still in flight
-        mbar_wait(c.mbM, c.phase, 1u << 20);  // MMAs of the wait that gave up
+        if (c.copyIssued) mbar_wait(c.mbW, 0, 1u << 20);          // the weight copy, if still in flight
+        if (c.mmaPending) mbar_wait(c.mbM, c.phase, 1u << 20);  // MMAs of the wait that gave up
     }
     tc_fence_before();
     __syncthreads();
@@ -168,7 +178,7 @@ __global__ void __launch_bounds__(kRcThreads) k_rc_infer(RcInferArgs a) {
     const uint32_t ntiles = (n + kRcTile - 1) / kRcTile;
     if (blockIdx.x >= ntiles) return;  // uniform: before any set-up
     CtaCtl c;
-    rc_setup(c, W, bars, tslot, a.net.img, 64);
+    rc_setup(c, W, bars, tslot, a.net.img, 64, a.net.stallPolls);
     for (uint32_t tile = blockIdx.x; tile < ntiles && c.ok; tile += gridDim.x) {
         const uint32_t row = tile * kRcTile + t;
         const bool valid = row < n;
@@ -256,7 +266,7 @@ __global__ void __launch_bounds__(kRcThreads, 1) k_rc_train(RcTrainArgs a) {
         reinterpret_cast<uint4 *>(dZo)[i] = make_uint4(0, 0, 0, 0);
     fence_async_smem();
     CtaCtl c;
-    rc_setup(c, W, bars, tslot, a.net.img, 512);
+    rc_setup(c, W, bars, tslot, a.net.img, 512, a.net.stallPolls);
     float loss = 0.0f;
     bool first = true;
     for (uint32_t tile = blockIdx.x; tile < ntiles && c.ok; tile += gridDim.x) {
@@ -528,6 +538,7 @@ RcNet rc_net(const pt_ctx *ctx, const uint8_t *img) {
         n.binv[k] = ctx->cache.binv[k];
     }
     n.err = ctx->d_err;
+    n.stallPolls = ctx->dbgCacheStall;
     return n;
 }
 // Cache bounds: the parameters' box, else the scene's vertex bounds.

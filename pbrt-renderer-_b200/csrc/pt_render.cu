@@ -379,7 +379,8 @@ __device__ __forceinline__ void shadow_one(const WaveArgs &A, uint32_t i, Stack 
 // code.
 template <bool MEDIA_TR = false>
 __global__ void __launch_bounds__(kBlock) k_shadow(WaveArgs A) {
-    const uint32_t n = *(volatile uint32_t *)A.cntShadow;
+    // appends past the capacity were dropped (and flagged): only what was stored is read
+    const uint32_t n = min(*(volatile uint32_t *)A.cntShadow, A.shadowCap);
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&A.rayTotals[1], (unsigned long long)n);
     PT_QUEUE_STACK(K)
     for (uint32_t base; (base = claim32(A.stealShadow)) < n;) {
@@ -1441,6 +1442,7 @@ bool graph_matches(const pt_ctx *ctx, const pt_render_params *P, size_t cap, con
            G.comp == comp && G.sceneGen == ctx->sceneGen && G.waveGen == ctx->waveGen &&
            G.cached == A.cacheOn && G.trainOn == A.trainOn && (!A.cacheOn || G.cacheGen == ctx->cache.gen) &&
            G.risNee == A.risNee && G.flags == (P->flags & ~PT_RENDER_STAGE_TIMING) &&
+           G.shadowCap == A.shadowCap && G.cacheStall == ctx->dbgCacheStall &&
            memcmp(&G.cam, &P->camera, sizeof(pt_camera)) == 0;
 }
 }  // namespace
@@ -1509,6 +1511,7 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
     A.rayTotals = (unsigned long long *)(B.counters + 4);
     A.err = ctx->d_err;
     A.shadowCap = (uint32_t)(2 * B.cap);
+    if (ctx->dbgShadowCap) A.shadowCap = std::min(A.shadowCap, ctx->dbgShadowCap);
     A.batch = 0; A.numReqs = 0; A.reqs = nullptr; A.slotInfo = nullptr;
     A.risNee = (P->flags & PT_RENDER_RIS_NEE) ? 1u : 0u;
     if ((P->flags & PT_RENDER_MEDIA_WAVEFRONT) && A.S.numVols > 0 && !A.S.hasSubsurface && !A.S.mediaWavefront) {
@@ -1563,6 +1566,7 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
             G.sceneGen = ctx->sceneGen; G.waveGen = ctx->waveGen;
             G.cached = A.cacheOn; G.trainOn = A.trainOn; G.cacheGen = ctx->cache.gen; G.risNee = A.risNee;
             G.flags = P->flags & ~PT_RENDER_STAGE_TIMING;
+            G.shadowCap = A.shadowCap; G.cacheStall = ctx->dbgCacheStall;
             G.launches = E.launches;
         } else {  // capture unavailable: issue the launches directly
             cudaGetLastError();

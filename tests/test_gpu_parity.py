@@ -10,8 +10,9 @@ FP64 evaluation, on 1M seeded direction pairs per material type:
   FP64 where that is larger (floor 1e-6 of the median magnitude);
 * the GPU is never less accurate than the float32 oracle: its error against
   FP64 is within 4x the oracle's own error + 1e-5 relative for >= 99.9 % of
-  pairs, and its 99.9th-percentile error against FP64 is at most 1.25x the
-  oracle's.
+  pairs, its 99.9th-percentile error against FP64 is at most 1.25x the
+  oracle's, and its 99.99th-percentile and largest errors against FP64 at
+  most 2x the oracle's.
 
 Cancellation in the reference formulas (e.g. pow(1 - cos, 5), GTR1 at low
 gloss) puts the float32 oracle itself ~2e-5 from FP64 at the 99.9th
@@ -58,10 +59,23 @@ def parity_stats(gpu, o32, o64, floor):
     bound = 4.0 * e_or + 1e-5 * np.maximum(np.abs(o64), floor)
     rg = e_gpu / np.maximum(np.abs(o64), floor)
     ro = e_or / np.maximum(np.abs(o64), floor)
-    return {"p99": float(np.quantile(d, 0.99)), "p999": float(np.quantile(d, 0.999)), "max": float(d.max()),
+    return {"p99": float(np.quantile(d, 0.99)), "p999": float(np.quantile(d, 0.999)),
+            "p9999": float(np.quantile(d, 0.9999)), "max": float(d.max()),
             "frac_within_bound": float((e_gpu <= bound).mean()),
             "gpu_vs_fp64_p99": float(np.quantile(rg, 0.99)), "oracle_vs_fp64_p99": float(np.quantile(ro, 0.99)),
-            "gpu_vs_fp64_p999": float(np.quantile(rg, 0.999)), "oracle_vs_fp64_p999": float(np.quantile(ro, 0.999))}
+            "gpu_vs_fp64_p999": float(np.quantile(rg, 0.999)), "oracle_vs_fp64_p999": float(np.quantile(ro, 0.999)),
+            "gpu_vs_fp64_p9999": float(np.quantile(rg, 0.9999)),
+            "oracle_vs_fp64_p9999": float(np.quantile(ro, 0.9999)),
+            "gpu_vs_fp64_max": float(rg.max()), "oracle_vs_fp64_max": float(ro.max())}
+
+
+def assert_tail(st):
+    """The worst pairs: a float32 evaluation of these formulas can itself be
+    far from FP64 on a few pairs (cancellation), so the tail is bounded by
+    the oracle's own: the GPU's 99.99th-percentile and worst errors against
+    FP64 at most twice the oracle's."""
+    assert st["gpu_vs_fp64_p9999"] <= 2.0 * st["oracle_vs_fp64_p9999"] + 1e-6, st
+    assert st["gpu_vs_fp64_max"] <= 2.0 * st["oracle_vs_fp64_max"] + 1e-6, st
 
 
 def assert_parity(st, accuracy_factor=1.25):
@@ -70,6 +84,7 @@ def assert_parity(st, accuracy_factor=1.25):
     assert st["p99"] <= 1e-5 and st["p999"] <= max(5e-5, st["oracle_vs_fp64_p999"]), st
     assert st["frac_within_bound"] >= 0.999, st
     assert st["gpu_vs_fp64_p999"] <= accuracy_factor * st["oracle_vs_fp64_p999"] + 1e-6, st
+    assert_tail(st)
 
 
 def assert_parity_ill_conditioned(st):
@@ -83,6 +98,7 @@ def assert_parity_ill_conditioned(st):
     assert st["p999"] <= max(5e-5, 2 * st["oracle_vs_fp64_p999"]), st
     assert st["gpu_vs_fp64_p99"] <= 1.25 * st["oracle_vs_fp64_p99"] + 1e-6, st
     assert st["gpu_vs_fp64_p999"] <= 1.25 * st["oracle_vs_fp64_p999"] + 1e-6, st
+    assert_tail(st)
 
 
 def test_sample_stream_bit_exact(ctx, oracle):
@@ -365,7 +381,7 @@ def test_trace_parity(which, ctx, oracle, scenes, bench_scene):
     exempt = near_edge(hg) | near_edge(ho) | tie
     bad = ~(same_hit & (~both | same_prim))
     print(which, "rays", n, "hits", int(both.sum()), "disagreements", int(bad.sum()), "ties", int((bad & tie).sum()),
-          "near an edge", int((bad & ~tie).sum()))
+          "within 1e-6 of an edge", int((bad & ~tie & exempt).sum()), "unexplained", int((bad & ~exempt).sum()))
     assert (bad & ~exempt).sum() == 0, int((bad & ~exempt).sum())
     assert bad.mean() < 1e-4
     # the same triangle at the same distance, bit for bit
