@@ -448,6 +448,41 @@ def config5_run(pt, steps=3, warmup=1):
     return out
 
 
+def cache_render_roofline(pt, ctx, W, H, cam, depth, env_mode, spp=8):
+    """Tensor-core roofline of the network kernels as the cached form runs
+    them: the render-mode inference (queries encoded from path records,
+    Lo += throughput x cache) and training (the call's records, 4 steps)
+    inside a cached render of the workload, timed by libpt's events around
+    those launches (PT_RENDER_STAGE_TIMING); three untimed cached calls first
+    so the cache has trained."""
+    import torch
+
+    D = importlib.import_module("pbrt_b200.distributed")
+    pk = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    peak = float(pk.get("bf16_tflops", 1590.0))
+    ctx.cache_init(pt.cache_params(seed=0, train_records=CACHE_RECORDS, learning_rate=CACHE_LR, ema=CACHE_EMA,
+                                   max_train_fraction=CACHE_FRACTION, rough_threshold=CACHE_ROUGH))
+    film = D.new_film(H, W, device="cuda")
+    try:
+        for k in range(4):
+            P = pt.render_params(W, H, spp, cam, max_depth=depth, sample_offset=k * spp, env_sampling=env_mode,
+                                 flags=pt.PT_RENDER_RADIANCE_CACHE | (pt.PT_RENDER_STAGE_TIMING if k == 3 else 0))
+            ctx.render(P, film[0].data_ptr(), film[1].data_ptr(), pt.PT_MEM_DEVICE)
+        torch.cuda.synchronize()
+        st = ctx.cache_stats()
+    finally:
+        ctx.cache_release()
+    out = {"call": f"{W}x{H}, {spp} spp, cached"}
+    for kind, rows, ms, flops in (("infer", int(st.queries), st.last_render_infer_ms, CACHE_FLOPS_INFER),
+                                  ("train", int(st.last_render_train_rows), st.last_render_train_ms,
+                                   CACHE_FLOPS_TRAIN)):
+        tf = rows * flops / (ms / 1e3) / 1e12 if ms > 0 else 0.0
+        out[kind] = {"rows": rows, "flops_per_row": flops, "ms": round(float(ms), 4), "achieved": round(tf, 2),
+                     "peak": peak, "unit": "TFLOP/s", "frac": round(tf / peak, 4)}
+    return out
+
+
 BATCH_STEPS = 3
 
 
@@ -619,9 +654,12 @@ def main():
     if args.impl == "reference":
         return run_reference_arm(args)
     if args.cache_kernels_only:
-        pt = load_pkg()
+        pt, sc, cam, W, H, spp, depth, cfg = workload(args.workload)
         ctx = pt.Context(0)
-        print(json.dumps({"cache_roofline": cache_kernel_roofline(pt, ctx)}), flush=True)
+        out = cache_kernel_roofline(pt, ctx)
+        ctx.upload(sc)
+        out["render_mode"] = cache_render_roofline(pt, ctx, W, H, cam, depth, pt.PT_ENV_CDF)
+        print(json.dumps({"cache_roofline": out}), flush=True)
         ctx.close()
         return 0
 
@@ -788,6 +826,7 @@ def main():
         line["time_to_relmse"] = time_to_relmse(pt, ctx, stream, W, H, cam, depth, env_mode, max(spp, 64),
                                                 calls=CACHE_CALLS.get(cfg["workload"], CACHE_CALLS_DEFAULT))
         line["cache_roofline"] = cache_kernel_roofline(pt, ctx)
+        line["cache_roofline"]["render_mode"] = cache_render_roofline(pt, ctx, W, H, cam, depth, env_mode)
     if world == 1 and not args.no_batch:
         line["batched"] = batched_requests_run(pt)
     if world == 1 and not args.no_configs and cfg["workload"] == "disney_envmap":

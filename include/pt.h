@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define PT_ABI_VERSION 3
+#define PT_ABI_VERSION 4
 
 /* ---- status codes ---------------------------------------------------- */
 #define PT_OK 0
@@ -452,6 +452,13 @@ typedef struct pt_cache_stats {
     float last_loss;       /* mean relative L2 loss of the last step */
     uint64_t queries;      /* cache queries of the last render */
     float last_kernel_ms;  /* device time of the last batch call's network kernel (infer / train) */
+    /* the last cached render made with PT_RENDER_STAGE_TIMING (0 otherwise):
+     * device time of its inference kernels (all waves; `queries` rows) and of
+     * its training kernels (forward, backward, weight gradients of every
+     * step, not the Adam updates), and the rows those processed */
+    float last_render_infer_ms;
+    float last_render_train_ms;
+    uint64_t last_render_train_rows;
 } pt_cache_stats;
 /* (Re)initialise the cache of ctx: weights from params->seed, zero moments. */
 int pt_cache_init(pt_ctx *ctx, const pt_cache_params *params);

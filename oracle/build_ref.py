@@ -81,7 +81,7 @@ def build(src: str = DEFAULT_SRC, quiet: bool = False) -> str:
     lib = os.path.join(OUT, "libref.so")
     for name, extra in (("libref.so", []), ("libref_ris.so", ["-DUSE_RIS=1"])):
         cmd = [
-            "g++", "-std=c++17", "-O2", "-march=x86-64-v2", "-ffp-contract=off",
+            "g++", "-std=c++17", "-O2", "-march=x86-64-v2", "-mfma", "-ffp-contract=off",
             "-fsingle-precision-constant", "-fPIC", "-shared", "-w",
             "-DMAX_BOUNCES=g_max_bounces", *extra,
             "-I", GEN, "-I", SHIM,

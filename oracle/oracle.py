@@ -25,7 +25,7 @@ REF_SRC = os.path.join(REF_ROOT, "shaders")
 
 def build_oracle(quiet=True) -> str:
     """Compile the oracle restatement (FP contraction off: float32 IEEE order)."""
-    cmd = ["g++", "-std=c++17", "-O2", "-march=x86-64-v2", "-ffp-contract=off", "-fPIC", "-shared",
+    cmd = ["g++", "-std=c++17", "-O2", "-march=x86-64-v2", "-mfma", "-ffp-contract=off", "-fPIC", "-shared",
            "-o", ORACLE_SO, os.path.join(HERE, "pt_oracle.cpp"), "-lpthread"]
     if not quiet:
         print(" ".join(cmd))
@@ -44,6 +44,18 @@ def build_ref(quiet=True):
     return mod.build(REF_SRC, quiet=quiet)
 
 
+def require_fma():
+    """The oracle and the reference build use the CPU's fused multiply-add
+    instruction (the triangle test; -mfma, nothing else contracted): fail
+    clearly on a CPU without it rather than on an illegal instruction."""
+    try:
+        flags = open("/proc/cpuinfo").read()
+    except OSError:
+        return
+    if " fma" not in flags:
+        raise RuntimeError("the CPU oracle needs a CPU with fused multiply-add (x86 FMA3)")
+
+
 def _f(a):
     return None if a is None else a.ctypes.data_as(C.POINTER(C.c_float))
 
@@ -56,6 +68,7 @@ class Oracle:
     """The C++ restatement (pt_oracle.cpp)."""
 
     def __init__(self, pt):
+        require_fma()
         src = os.path.join(HERE, "pt_oracle.cpp")
         if not os.path.exists(ORACLE_SO) or os.path.getmtime(src) > os.path.getmtime(ORACLE_SO):
             build_oracle()
@@ -207,6 +220,7 @@ class Reference:
         so = REF_RIS_SO if ris else REF_SO
         if not os.path.exists(so):
             raise FileNotFoundError(so)
+        require_fma()
         self.pt = pt
         L = C.CDLL(so)
         F, U, S = C.POINTER(C.c_float), C.POINTER(C.c_uint32), C.c_size_t

@@ -1310,21 +1310,29 @@ static inline bool box_hit(const F3 &lo, const F3 &hi, const F3 &o, const F3 &in
     }
     return t0 <= t1 * 1.00000024f;
 }
-// Moller-Trumbore (src/cpu/mesh.cpp:51-89)
+// Moller-Trumbore (src/cpu/mesh.cpp:51-89).  The reference's GPU path
+// intersects in ray-tracing hardware whose arithmetic is not published; this
+// restatement fixes one: fused multiply-adds in a set order (a*b - c*d as
+// fma(a, b, -(c*d)), dot products as fma(z, z', fma(y, y', x*x'))), which the
+// kernels and the reference build's ray-query stand-in use too.
+static inline float dot_f(const F3 &a, const F3 &b) { return std::fmaf(a.z, b.z, std::fmaf(a.y, b.y, a.x * b.x)); }
+static inline F3 cross_f(const F3 &a, const F3 &b) {
+    return F3(std::fmaf(a.y, b.z, -(a.z * b.y)), std::fmaf(a.z, b.x, -(a.x * b.z)), std::fmaf(a.x, b.y, -(a.y * b.x)));
+}
 static bool tri_hit(const F3 &p0, const F3 &p1, const F3 &p2, const F3 &o, const F3 &d, float tmin, float tmax,
                     float &u, float &v, float &t) {
     F3 e1 = p1 - p0, e2 = p2 - p0;
-    F3 pv = cross(d, e2);
-    float det = dot(e1, pv);
+    F3 pv = cross_f(d, e2);
+    float det = dot_f(e1, pv);
     if (det > -1e-8f && det < 1e-8f) return false;
     float inv = 1.0f / det;
     F3 tv = o - p0;
-    u = dot(tv, pv) * inv;
+    u = dot_f(tv, pv) * inv;
     if (u < 0.0f || u > 1.0f) return false;
-    F3 qv = cross(tv, e1);
-    v = dot(d, qv) * inv;
+    F3 qv = cross_f(tv, e1);
+    v = dot_f(d, qv) * inv;
     if (v < 0.0f || u + v > 1.0f) return false;
-    t = dot(e2, qv) * inv;
+    t = dot_f(e2, qv) * inv;
     return t >= tmin && t <= tmax;
 }
 static thread_local uint64_t g_ext_rays = 0, g_shadow_rays = 0;

@@ -179,19 +179,29 @@ static void build_bvh() {
     }
 }
 
+// The ray-tracing hardware's triangle test stand-in: Moller-Trumbore with
+// fused multiply-adds in a set order (the arithmetic of the hardware the
+// reference runs on is not published; the oracle and the kernels use this one).
+static inline float dot_f(const float3 &a, const float3 &b) {
+    return std::fmaf(a.z, b.z, std::fmaf(a.y, b.y, a.x * b.x));
+}
+static inline float3 cross_f(const float3 &a, const float3 &b) {
+    return float3(std::fmaf(a.y, b.z, -(a.z * b.y)), std::fmaf(a.z, b.x, -(a.x * b.z)),
+                  std::fmaf(a.x, b.y, -(a.y * b.x)));
+}
 static bool mt(const float3 &p0, const float3 &p1, const float3 &p2, const RayDesc &r, float &u, float &v, float &t) {
     float3 e1 = p1 - p0, e2 = p2 - p0;
-    float3 pv = cross(r.Direction, e2);
-    float det = dot(e1, pv);
+    float3 pv = cross_f(r.Direction, e2);
+    float det = dot_f(e1, pv);
     if (det > -1e-8f && det < 1e-8f) return false;
     float inv = 1.0f / det;
     float3 tv = r.Origin - p0;
-    u = dot(tv, pv) * inv;
+    u = dot_f(tv, pv) * inv;
     if (u < 0.0f || u > 1.0f) return false;
-    float3 qv = cross(tv, e1);
-    v = dot(r.Direction, qv) * inv;
+    float3 qv = cross_f(tv, e1);
+    v = dot_f(r.Direction, qv) * inv;
     if (v < 0.0f || u + v > 1.0f) return false;
-    t = dot(e2, qv) * inv;
+    t = dot_f(e2, qv) * inv;
     return t >= r.TMin && t <= r.TMax;
 }
 

@@ -135,7 +135,8 @@ class pt_cache_params(C.Structure):
 
 class pt_cache_stats(C.Structure):
     _fields_ = [("steps", C.c_uint64), ("last_records", C.c_uint32), ("last_loss", C.c_float),
-                ("queries", C.c_uint64), ("last_kernel_ms", C.c_float)]
+                ("queries", C.c_uint64), ("last_kernel_ms", C.c_float), ("last_render_infer_ms", C.c_float),
+                ("last_render_train_ms", C.c_float), ("last_render_train_rows", C.c_uint64)]
 
 
 def cache_params(train_records=0, unbiased_every=0, rough_threshold=0.0, learning_rate=0.0, ema=0.0, seed=0,

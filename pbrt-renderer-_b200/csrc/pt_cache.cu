@@ -60,6 +60,23 @@ struct RcRows<0> {  // features n x 64, targets n x 3 (training)
     __device__ float3 target(uint32_t row) const {
         return make_float3(targ[3 * row], targ[3 * row + 1], targ[3 * row + 2]);
     }
+    // a row's inputs in flight: fetch issues the loads, decode uses them
+    struct Raw {
+        float4 v[kRcIn / 4];
+        float3 tg;
+    };
+    __device__ void fetch(uint32_t row, bool withTarget, Raw &r) const {
+        const float4 *p = reinterpret_cast<const float4 *>(feat + (size_t)row * kRcIn);
+#pragma unroll
+        for (int k = 0; k < kRcIn / 4; k++) r.v[k] = __ldcs(p + k);
+        if (withTarget) r.tg = target(row);
+    }
+    __device__ void decode(const RcNet &, const Raw &r, float f[kRcIn]) const {
+#pragma unroll
+        for (int k = 0; k < kRcIn / 4; k++) {
+            f[4 * k] = r.v[k].x; f[4 * k + 1] = r.v[k].y; f[4 * k + 2] = r.v[k].z; f[4 * k + 3] = r.v[k].w;
+        }
+    }
 };
 template <>
 struct RcRows<1> {  // records (render queries or training records): rows phase, phase + stride, ...
@@ -79,6 +96,18 @@ struct RcRows<1> {  // records (render queries or training records): rows phase,
     __device__ float3 target(uint32_t row) const {
         float4 t = tgt[row * stride + phase];
         return make_float3(t.x, t.y, t.z);
+    }
+    struct Raw {
+        float4 q[4];
+        float3 tg;
+    };
+    __device__ void fetch(uint32_t row, bool withTarget, Raw &r) const {
+        const uint32_t i = row * stride + phase;
+        r.q[0] = r0[i]; r.q[1] = r1[i]; r.q[2] = r2[i]; r.q[3] = r3[i];
+        if (withTarget) r.tg = target(row);
+    }
+    __device__ void decode(const RcNet &N, const Raw &r, float f[kRcIn]) const {
+        rc_encode(r.q[0], r.q[1], r.q[2], r.q[3], N.bmin, N.binv, f);
     }
 };
 
@@ -167,6 +196,12 @@ struct RcInferArgs {
     float4 *lo_eta;
     float4 *recCache;  // cache value at training-record vertices (queries tagged with bit 31)
 };
+// the row source of each mode: feature arrays (batch entry points) or records
+template <int MODE>
+__device__ __forceinline__ const auto &infer_rows(const RcInferArgs &a) {
+    if constexpr (MODE == 0) return a.feat;
+    else return a.qry;
+}
 template <int MODE>
 __global__ void __launch_bounds__(kRcThreads) k_rc_infer(RcInferArgs a) {
     extern __shared__ __align__(1024) uint8_t sm[];
@@ -178,17 +213,37 @@ __global__ void __launch_bounds__(kRcThreads) k_rc_infer(RcInferArgs a) {
     const uint32_t ntiles = (n + kRcTile - 1) / kRcTile;
     if (blockIdx.x >= ntiles) return;  // uniform: before any set-up
     CtaCtl c;
+    // each tile's inputs are loaded while the tile before it runs its layers:
+    // the first here, the next one right after a tile decodes its own
+    const auto &rows = infer_rows<MODE>(a);
+    typename std::remove_reference_t<decltype(rows)>::Raw raw;
+    if (blockIdx.x * kRcTile + t < n) rows.fetch(blockIdx.x * kRcTile + t, false, raw);
     rc_setup(c, W, bars, tslot, a.net.img, 64, a.net.stallPolls);
     for (uint32_t tile = blockIdx.x; tile < ntiles && c.ok; tile += gridDim.x) {
         const uint32_t row = tile * kRcTile + t;
         const bool valid = row < n;
         float f[kRcIn];
         if (valid) {
-            if (MODE == 0) a.feat.load(a.net, row, f);
-            else a.qry.load(a.net, row, f);
+            rows.decode(a.net, raw, f);
         } else {
 #pragma unroll
             for (int k = 0; k < kRcIn; k++) f[k] = 0.0f;
+        }
+        // render queries: what the last step reads, requested now
+        uint32_t tag = 0;
+        float4 qw = make_float4(0.0f, 0.0f, 0.0f, 0.0f), le = qw;
+        if constexpr (MODE != 0) {
+            if (valid) {
+                tag = __float_as_uint(raw.q[1].w);
+                if (!(tag & 0x80000000u)) {
+                    qw = a.qw[row];
+                    le = a.lo_eta[tag];
+                }
+            }
+        }
+        {
+            const uint32_t nrow = row + gridDim.x * kRcTile;
+            if (nrow < n) rows.fetch(nrow, false, raw);
         }
         store_row_bf16(T, t, f);
         fence_async_smem();
@@ -215,16 +270,14 @@ __global__ void __launch_bounds__(kRcThreads) k_rc_infer(RcInferArgs a) {
                         a.out[3 * (size_t)row + 1] = v[1];
                         a.out[3 * (size_t)row + 2] = v[2];
                     } else {
-                        const uint32_t tag = __float_as_uint(a.qry.r1[row].w);
                         if (tag & 0x80000000u) {  // a training record's vertex: keep the value
                             a.recCache[tag & 0x7FFFFFFFu] =
                                 make_float4(fmaxf(v[0], 0.0f), fmaxf(v[1], 0.0f), fmaxf(v[2], 0.0f), 0.0f);
                         } else {
-                            float4 w = a.qw[row], le = a.lo_eta[tag];
                             // Lo += throughput * cache, rounded as two operations (no FMA)
-                            le.x = __fadd_rn(le.x, __fmul_rn(w.x, fmaxf(v[0], 0.0f)));
-                            le.y = __fadd_rn(le.y, __fmul_rn(w.y, fmaxf(v[1], 0.0f)));
-                            le.z = __fadd_rn(le.z, __fmul_rn(w.z, fmaxf(v[2], 0.0f)));
+                            le.x = __fadd_rn(le.x, __fmul_rn(qw.x, fmaxf(v[0], 0.0f)));
+                            le.y = __fadd_rn(le.y, __fmul_rn(qw.y, fmaxf(v[1], 0.0f)));
+                            le.z = __fadd_rn(le.z, __fmul_rn(qw.z, fmaxf(v[2], 0.0f)));
                             a.lo_eta[tag] = le;
                         }
                     }
@@ -245,6 +298,11 @@ struct RcTrainArgs {
     float *grad;     // kRcParams FP32, added to
     float *lossSum;  // added to
 };
+template <int MODE>
+__device__ __forceinline__ const auto &train_rows(const RcTrainArgs &a) {
+    if constexpr (MODE == 0) return a.feat;
+    else return a.rec;
+}
 // TMEM columns: [0, 64) layer output / input gradient, [64 + 64 l, 128 + 64 l)
 // the weight gradient of layer l.
 template <int MODE>
@@ -266,6 +324,10 @@ __global__ void __launch_bounds__(kRcThreads, 1) k_rc_train(RcTrainArgs a) {
         reinterpret_cast<uint4 *>(dZo)[i] = make_uint4(0, 0, 0, 0);
     fence_async_smem();
     CtaCtl c;
+    // the next tile's inputs load while this tile runs forward and backward
+    const auto &rows = train_rows<MODE>(a);
+    typename std::remove_reference_t<decltype(rows)>::Raw raw;
+    if (blockIdx.x * kRcTile + t < n) rows.fetch(blockIdx.x * kRcTile + t, true, raw);
     rc_setup(c, W, bars, tslot, a.net.img, 512, a.net.stallPolls);
     float loss = 0.0f;
     bool first = true;
@@ -275,11 +337,15 @@ __global__ void __launch_bounds__(kRcThreads, 1) k_rc_train(RcTrainArgs a) {
         float f[kRcIn];
         float3 tg = make_float3(0.0f, 0.0f, 0.0f);
         if (valid) {
-            if (MODE == 0) { a.feat.load(a.net, row, f); tg = a.feat.target(row); }
-            else { a.rec.load(a.net, row, f); tg = a.rec.target(row); }
+            rows.decode(a.net, raw, f);
+            tg = raw.tg;
         } else {
 #pragma unroll
             for (int k = 0; k < kRcIn; k++) f[k] = 0.0f;
+        }
+        {
+            const uint32_t nrow = row + gridDim.x * kRcTile;
+            if (nrow < n) rows.fetch(nrow, true, raw);
         }
         store_row_bf16(Act, t, f);
         fence_async_smem();
@@ -597,13 +663,12 @@ cudaError_t rc_enqueue_targets(pt_ctx *ctx, cudaStream_t st, float4 *lo_eta, uin
                                      pendE);
     return cudaGetLastError();
 }
-// kRcStepsPerCall Adam steps per render call, step s on records s, s + steps,
-// ... (interleaved, so each batch spans the whole frame).
-constexpr uint32_t kRcStepsPerCall = 4;
-cudaError_t rc_enqueue_train(pt_ctx *ctx, cudaStream_t st) {
+// kRcStepsPerCall (pt_internal.h) Adam steps per render call, step s on
+// records s, s + steps, ... (interleaved, so each batch spans the whole frame).
+cudaError_t rc_enqueue_train(pt_ctx *ctx, cudaStream_t st, uint32_t s, bool adam) {
     RadianceCache &C = ctx->cache;
     float *lossDev = reinterpret_cast<float *>(C.ctr + 8);
-    for (uint32_t s = 0; s < kRcStepsPerCall; s++) {
+    if (!adam) {  // the step's gradient over records s, s + kRcStepsPerCall, ...
         cudaError_t e = cudaMemsetAsync(lossDev, 0, 4, st);
         if (e != cudaSuccess) return e;
         RcTrainArgs a{};
@@ -613,6 +678,7 @@ cudaError_t rc_enqueue_train(pt_ctx *ctx, cudaStream_t st) {
         a.grad = C.grad;
         a.lossSum = lossDev;
         k_rc_train<1><<<ctx->numSMs, kRcThreads, kTrainSmem, st>>>(a);
+    } else {
         RcAdamArgs d{C.w, C.m, C.v, C.ema, C.grad, C.imgTrain, C.imgInfer, C.ctr, C.ctr + 2, (uint32_t)C.recCap,
                      kRcStepsPerCall, s, C.params.learning_rate, C.params.ema, lossDev,
                      s + 1 == kRcStepsPerCall ? 1u : 0u, C.params.max_train_fraction};
@@ -847,6 +913,9 @@ int pt_cache_get_stats(pt_ctx *ctx, pt_cache_stats *out) {
     memcpy(&out->last_loss, &c[3], 4);
     out->queries = c[5];
     out->last_kernel_ms = ctx->cache.lastKernelMs;
+    out->last_render_infer_ms = ctx->cache.renderInferMs;
+    out->last_render_train_ms = ctx->cache.renderTrainMs;
+    out->last_render_train_rows = std::min<uint64_t>(c[2], ctx->cache.recCap);
     return PT_OK;
 }
 

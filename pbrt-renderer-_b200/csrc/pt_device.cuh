@@ -603,32 +603,33 @@ struct Hit {
 };
 
 // Moller-Trumbore (src/cpu/mesh.cpp:51-89) on (v0, e1, e2).
-// Products and sums rounded one at a time, in the order the oracle's
-// Moller-Trumbore evaluates them (no FMA contraction), so that the test's
-// decision and its t, u, v are the oracle's bit for bit: hit ids then differ
-// only where traversal order breaks an equal-t tie or a ray grazes a box.
-__device__ __forceinline__ float dot_rn(float3 a, float3 b) {
-    return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
+// Moller-Trumbore with fused multiply-adds in one fixed order, the order
+// the oracle (and the reference build's ray-query stand-in) evaluates it:
+// a*b - c*d as fma(a, b, -(c*d)), dot products as fma(z, z', fma(y, y',
+// x*x')).  Explicit intrinsics, so the compiler contracts nothing else: the
+// decision and t, u, v are the oracle's bit for bit, and hit ids differ only
+// where traversal order breaks an equal-t tie or a ray grazes a box.
+__device__ __forceinline__ float dot_f(float3 a, float3 b) {
+    return __fmaf_rn(a.z, b.z, __fmaf_rn(a.y, b.y, __fmul_rn(a.x, b.x)));
 }
-__device__ __forceinline__ float3 cross_rn(float3 a, float3 b) {
-    return make_float3(__fsub_rn(__fmul_rn(a.y, b.z), __fmul_rn(a.z, b.y)),
-                       __fsub_rn(__fmul_rn(a.z, b.x), __fmul_rn(a.x, b.z)),
-                       __fsub_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
+__device__ __forceinline__ float3 cross_f(float3 a, float3 b) {
+    return make_float3(__fmaf_rn(a.y, b.z, -__fmul_rn(a.z, b.y)), __fmaf_rn(a.z, b.x, -__fmul_rn(a.x, b.z)),
+                       __fmaf_rn(a.x, b.y, -__fmul_rn(a.y, b.x)));
 }
 __device__ __forceinline__ bool tri_test(float3 o, float3 d, float4 a, float4 b, float4 c, float tmin, float tmax,
                                          float &t, float &u, float &v) {
     float3 e1 = make_float3(b.x, b.y, b.z), e2 = make_float3(c.x, c.y, c.z);
-    float3 pv = cross_rn(d, e2);
-    float det = dot_rn(e1, pv);
+    float3 pv = cross_f(d, e2);
+    float det = dot_f(e1, pv);
     if (det > -1e-8f && det < 1e-8f) return false;
     float inv = __frcp_rn(det);  // correctly rounded: the value of 1.0f / det
     float3 tv = o - make_float3(a.x, a.y, a.z);
-    u = __fmul_rn(dot_rn(tv, pv), inv);
+    u = __fmul_rn(dot_f(tv, pv), inv);
     if (u < 0.0f || u > 1.0f) return false;
-    float3 qv = cross_rn(tv, e1);
-    v = __fmul_rn(dot_rn(d, qv), inv);
+    float3 qv = cross_f(tv, e1);
+    v = __fmul_rn(dot_f(d, qv), inv);
     if (v < 0.0f || __fadd_rn(u, v) > 1.0f) return false;
-    t = __fmul_rn(dot_rn(e2, qv), inv);
+    t = __fmul_rn(dot_f(e2, qv), inv);
     return t >= tmin && t <= tmax;
 }
 

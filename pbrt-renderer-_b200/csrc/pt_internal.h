@@ -131,6 +131,7 @@ struct RadianceCache {
     float4 *rec[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     uint64_t gen = 1;  // bumped when buffers move
     float lastKernelMs = 0.0f;  // network kernel of the last batch call (CUDA events)
+    float renderInferMs = 0.0f, renderTrainMs = 0.0f;  // network kernels of the last stage-timed render
 };
 
 // Batched renders (pt_render_batch): the device request table, per-slot
@@ -283,6 +284,8 @@ int rc_render_setup(pt_ctx *ctx, size_t waveCap);     // checks, bounds, query b
 cudaError_t rc_enqueue_resolve(pt_ctx *ctx, cudaStream_t st, float4 *lo_eta);
 cudaError_t rc_enqueue_targets(pt_ctx *ctx, cudaStream_t st, float4 *lo_eta, uint4 *rng, const float4 *pendA,
                                const float4 *pendE);
-cudaError_t rc_enqueue_train(pt_ctx *ctx, cudaStream_t st);
+// one training step s of kRcStepsPerCall: the network kernel (adam = false) or its Adam update (adam = true)
+cudaError_t rc_enqueue_train(pt_ctx *ctx, cudaStream_t st, uint32_t s, bool adam);
+constexpr uint32_t kRcStepsPerCall = 4;  // Adam steps per cached render call, on interleaved quarters of its records
 void pt_graph_free(pt_ctx *ctx);
 void pt_batch_free(pt_ctx *ctx);

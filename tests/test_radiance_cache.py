@@ -93,7 +93,7 @@ def test_constant_weights_in_restatement():
 
 def test_cache_abi_sizes(pt):
     assert C.sizeof(pt.pt_cache_params) == 56
-    assert C.sizeof(pt.pt_cache_stats) == 32
+    assert C.sizeof(pt.pt_cache_stats) == 48
     assert pt.PT_CACHE_PARAMS == rc.PARAMS
 
 
