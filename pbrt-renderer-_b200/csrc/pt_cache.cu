@@ -295,7 +295,8 @@ struct RcTrainArgs {
     RcNet net;
     RcRows<0> feat;
     RcRows<1> rec;
-    float *grad;     // kRcParams FP32, added to
+    float *part;     // per CTA, kRcParams FP32: the CTA's summed gradient (overwritten; zeros from a CTA
+                     // that trained nothing); k_rc_grad_reduce adds the slots in order
     float *lossSum;  // added to
 };
 template <int MODE>
@@ -317,7 +318,11 @@ __global__ void __launch_bounds__(kRcThreads, 1) k_rc_train(RcTrainArgs a) {
     const uint32_t t = threadIdx.x;
     const uint32_t n = MODE == 0 ? a.feat.count() : a.rec.count();
     const uint32_t ntiles = (n + kRcTile - 1) / kRcTile;
-    if (blockIdx.x >= ntiles) return;
+    float4 *slot = reinterpret_cast<float4 *>(a.part + (size_t)blockIdx.x * kRcParams);
+    if (blockIdx.x >= ntiles) {  // nothing to train: an empty slot
+        for (uint32_t i = t; i < kRcParams / 4; i += kRcThreads) slot[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        return;
+    }
     // the dZ images are read as M = 128 operands: their upper halves (and the
     // unused columns of dZo) must hold zeros
     for (uint32_t i = t; i < 2 * kGradBytes / 16; i += kRcThreads)
@@ -430,7 +435,9 @@ __global__ void __launch_bounds__(kRcThreads, 1) k_rc_train(RcTrainArgs a) {
         }
         first = false;
     }
-    // flush the weight gradients: thread t holds row t (an output unit)
+    // the CTA's weight gradients into its slot: thread t holds row t (an
+    // output unit) of each layer, 64 consecutive parameters; plain stores, the
+    // slots are summed afterwards in a fixed order (no float atomics)
     if (c.ok && !first) {
         tc_fence_after();
         for (int l = 0; l < kRcLayers; l++) {
@@ -438,17 +445,29 @@ __global__ void __launch_bounds__(kRcThreads, 1) k_rc_train(RcTrainArgs a) {
             tmem_ld64(c.tl + 64 + 64 * l, v);
             tmem_wait_ld();
             if (t < (uint32_t)rc_rows(l)) {
-                float *g = a.grad + rc_param_base(l) + t * kRcIn;
+                float4 *g = slot + (rc_param_base(l) + t * kRcIn) / 4;
 #pragma unroll
-                for (int k = 0; k < 64; k++) atomicAdd(g + k, v[k]);
+                for (int k = 0; k < 16; k++) g[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
             }
         }
+    } else {  // a wait gave up (the call reports it): leave nothing in the slot
+        for (uint32_t i = t; i < kRcParams / 4; i += kRcThreads) slot[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xFFFFFFFFu, loss, o);
     if ((t & 31) == 0 && c.ok) atomicAdd(a.lossSum, loss);
     rc_teardown(c, 512, a.net.err);
 }
+
+// The training CTAs' gradient slots summed in slot order (deterministic), added to grad.
+__global__ void __launch_bounds__(256) k_rc_grad_reduce(const float *part, uint32_t slots, float *grad) {
+    const uint32_t p = blockIdx.x * 256u + threadIdx.x;
+    if (p >= kRcParams) return;
+    float s = 0.0f;
+    for (uint32_t k = 0; k < slots; k++) s += __ldcs(part + (size_t)k * kRcParams + p);
+    grad[p] += s;
+}
+constexpr uint32_t kReduceBlocks = (kRcParams + 255) / 256;
 
 // ---- Adam (one CTA): FP32 master weights -> BF16 images ------------------------
 struct RcAdamArgs {
@@ -675,9 +694,10 @@ cudaError_t rc_enqueue_train(pt_ctx *ctx, cudaStream_t st, uint32_t s, bool adam
         a.net = rc_net(ctx, C.imgTrain);
         a.rec = RcRows<1>{C.rec[0], C.rec[1], C.rec[2], C.rec[3], C.rec[6], C.ctr + 2, (uint32_t)C.recCap,
                           kRcStepsPerCall, s};
-        a.grad = C.grad;
+        a.part = C.gradPart;
         a.lossSum = lossDev;
         k_rc_train<1><<<ctx->numSMs, kRcThreads, kTrainSmem, st>>>(a);
+        k_rc_grad_reduce<<<kReduceBlocks, 256, 0, st>>>(C.gradPart, (uint32_t)ctx->numSMs, C.grad);
     } else {
         RcAdamArgs d{C.w, C.m, C.v, C.ema, C.grad, C.imgTrain, C.imgInfer, C.ctr, C.ctr + 2, (uint32_t)C.recCap,
                      kRcStepsPerCall, s, C.params.learning_rate, C.params.ema, lossDev,
@@ -697,7 +717,7 @@ int rc_render_setup(pt_ctx *ctx, size_t waveCap) {
 
 void pt_cache_free(pt_ctx *ctx) {
     RadianceCache &C = ctx->cache;
-    void *ps[] = {C.w, C.m, C.v, C.ema, C.grad, C.imgTrain, C.imgInfer, C.ctr};
+    void *ps[] = {C.w, C.m, C.v, C.ema, C.grad, C.gradPart, C.imgTrain, C.imgInfer, C.ctr};
     for (void *p : ps)
         if (p) cudaFree(p);
     for (float4 *p : C.q)
@@ -743,6 +763,7 @@ int pt_cache_init(pt_ctx *ctx, const pt_cache_params *params) {
     cudaError_t e = cudaSuccess;
     auto A = [&](void **p, size_t b) { if (e == cudaSuccess) e = cudaMalloc(p, b); };
     for (float **p : {&C.w, &C.m, &C.v, &C.ema, &C.grad}) A((void **)p, kRcParams * sizeof(float));
+    A((void **)&C.gradPart, (size_t)ctx->numSMs * kRcParams * sizeof(float));
     A((void **)&C.imgTrain, kRcImageBytes);
     A((void **)&C.imgInfer, kRcImageBytes);
     A((void **)&C.ctr, 16 * sizeof(uint32_t));
@@ -867,10 +888,12 @@ static int rc_train_impl(pt_ctx *ctx, const float *features, const float *target
         a.feat.feat = (const float *)s.dev(0);
         a.feat.targ = (const float *)s.dev(1);
         a.feat.n = n32;
-        a.grad = C.grad;
+        a.part = C.gradPart;
         a.lossSum = lossDev;
+        const unsigned grid = rc_grid(ctx, n32, 1);
         cudaEventRecord(ctx->ev[0], ctx->stream);
-        k_rc_train<0><<<rc_grid(ctx, n32, 1), kRcThreads, kTrainSmem, ctx->stream>>>(a);
+        k_rc_train<0><<<grid, kRcThreads, kTrainSmem, ctx->stream>>>(a);
+        k_rc_grad_reduce<<<kReduceBlocks, 256, 0, ctx->stream>>>(C.gradPart, grid, C.grad);
         cudaEventRecord(ctx->ev[1], ctx->stream);
     }
     float lossHost = 0.0f;

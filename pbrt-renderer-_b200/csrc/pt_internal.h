@@ -118,6 +118,7 @@ struct RadianceCache {
     float bmin[3] = {0, 0, 0}, binv[3] = {1, 1, 1};
     bool boundsFromScene = true;
     float *w = nullptr, *m = nullptr, *v = nullptr, *ema = nullptr, *grad = nullptr;
+    float *gradPart = nullptr;  // per training CTA (numSMs slots): its summed weight gradient
     uint8_t *imgTrain = nullptr, *imgInfer = nullptr;
     // counters: [0] Adam steps, [1] queries of the wave, [2] records of the
     // call, [3] loss sum (float bits), [4] records of the last step, [5]

@@ -66,7 +66,8 @@ def test_cache_wait_timeout_reported_then_recovers(pt):
         y1 = ctx.cache_infer(f)
         g1, l1 = ctx.cache_gradient(f, t)
         assert np.array_equal(y0, y1)
-        # gradient sums use float atomics: same up to summation order
-        assert np.allclose(g0, g1, rtol=1e-4, atol=1e-6) and abs(l0 - l1) <= 1e-4 * abs(l0)
+        # gradient sums use float atomics: the same up to summation order (a
+        # few near-cancelling components move by more than their own size)
+        assert np.linalg.norm(g1 - g0) <= 1e-5 * np.linalg.norm(g0) and abs(l0 - l1) <= 1e-4 * abs(l0)
     finally:
         ctx.close()
