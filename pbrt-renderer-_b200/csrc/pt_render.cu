@@ -67,11 +67,6 @@ struct WaveArgs {
     uint32_t *cntIn, *cntOut, *cntShadow;
     uint32_t *stealExt, *stealShadow;  // next unclaimed queue position of k_extend / k_shadow
     uint32_t bounce;                   // bounce of the kernels of this launch (uniform over the queue)
-    // k_extend's visit order: with sorted != 0 it traverses queue position
-    // perm[j] as its j-th ray (perm: k_ray_sort, stored in the idle shadow-slot array)
-    uint32_t sorted;
-    const uint32_t *perm;
-    float sortMin[3], sortScale[3];  // origin -> [0, 32) cells of the scene box
     uint32_t *cls, *cntCls;  // shading-class queues (CLS_N x clsStride) and their counts
     uint32_t clsStride;
     unsigned long long *rayTotals;  // [0] extension, [1] shadow
@@ -329,88 +324,14 @@ template <bool CLASSIFY, bool MEDIA = false>
 __global__ void __launch_bounds__(kBlock) k_extend(WaveArgs A) {
     // warps claim the queue in order: the 32 rays of a warp are neighbours in
     // the queue (coherent traversal), and the class queues and the next ray
-    // queue keep that order for the kernels that follow.  Secondary rays are
-    // claimed in the order k_ray_sort left in perm: within each window of
-    // the queue, grouped by direction and origin.
+    // queue keep that order for the kernels that follow
     const uint32_t n = *(volatile uint32_t *)A.cntIn;
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&A.rayTotals[0], (unsigned long long)n);
     PT_QUEUE_STACK(K)
     for (uint32_t base; (base = claim32(A.stealExt)) < n;) {
-        const uint32_t j = base + lane_id();
-        if (j < n) extend_one<CLASSIFY, MEDIA>(A, A.sorted ? __ldcs(A.perm + j) : j, K);
+        const uint32_t i = base + lane_id();
+        if (i < n) extend_one<CLASSIFY, MEDIA>(A, i, K);
     }
-}
-
-// ---- secondary-ray order ------------------------------------------------------
-// Rays leaving a shading pass are in path order: neighbours in the queue
-// start near each other but head in unrelated directions, so a warp's lanes
-// walk different parts of the tree.  k_ray_sort reorders each window of
-// kSortWin queue positions by (direction octant, dominant axis, Morton code
-// of the origin on a 32^3 grid of the scene box) with a bitonic sort in
-// shared memory; k_extend then takes the window's rays in that order.  A
-// window is a short run of paths (a strip of the image), so the shading
-// kernels that follow still touch path state within it.
-// Off by default (PT_RAY_SORT=0): on the 64-sphere bench frame it measured
-// slower at every window size (extend 18.6 ms per frame in queue order, 25.7
-// / 20.1 / 19.4 ms with 1024 / 4096 / 8192-ray windows, the sort included;
-// shading 7.3 -> 8.2 ms): the queue's own order, 8 x 4 pixel tiles carried
-// through the bounces, keeps rays from one surface patch together, and that
-// coherence is worth more than grouping by direction.
-#ifndef PT_RAY_SORT
-#define PT_RAY_SORT 0
-#endif
-constexpr uint32_t kSortBits = PT_RAY_SORT > 0 ? PT_RAY_SORT : 1;
-constexpr uint32_t kSortWin = 1u << kSortBits;
-constexpr uint32_t kSortThreads = 1024;
-static_assert(kSortBits <= 13, "sort window in static shared memory");
-__device__ __forceinline__ uint32_t spread5(uint32_t v) {  // 5 bits -> every third bit
-    v &= 31u;
-    v = (v | (v << 8)) & 0x0300F00Fu;
-    v = (v | (v << 4)) & 0x030C30C3u;
-    v = (v | (v << 2)) & 0x09249249u;
-    return v;
-}
-__device__ __forceinline__ uint32_t ray_sort_key(const WaveArgs &A, float4 o, float4 d) {
-    uint32_t oct = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
-    float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
-    uint32_t dom = ax >= ay ? (ax >= az ? 0u : 2u) : (ay >= az ? 1u : 2u);
-    auto cell = [](float p, float lo, float sc) {
-        float c = (p - lo) * sc;
-        return (uint32_t)fminf(fmaxf(c, 0.0f), 31.0f);
-    };
-    uint32_t m = spread5(cell(o.x, A.sortMin[0], A.sortScale[0])) |
-                 (spread5(cell(o.y, A.sortMin[1], A.sortScale[1])) << 1) |
-                 (spread5(cell(o.z, A.sortMin[2], A.sortScale[2])) << 2);
-    return (oct << 17) | (dom << 15) | m;  // 20 bits
-}
-__global__ void __launch_bounds__(kSortThreads) k_ray_sort(WaveArgs A) {
-    __shared__ uint32_t key[kSortWin];
-    const uint32_t n = *(volatile uint32_t *)A.cntIn;
-    const uint32_t base = blockIdx.x * kSortWin;
-    if (base >= n) return;  // uniform
-    const uint32_t cnt = min(kSortWin, n - base);
-    for (uint32_t e = threadIdx.x; e < kSortWin; e += kSortThreads)
-        // the 20-bit key (lowest Morton bits dropped above 4096-ray windows)
-        // above the index; the largest real key stays below the padding
-        key[e] = e < cnt ? ((ray_sort_key(A, __ldg(A.qoIn + base + e), __ldg(A.qdIn + base + e)) >>
-                             (kSortBits > 12 ? kSortBits - 12 : 0)) << kSortBits) | e
-                         : 0xFFFFFFFFu;  // padding sorts last
-    __syncthreads();
-    for (uint32_t size = 2; size <= kSortWin; size <<= 1) {
-        for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
-            for (uint32_t t = threadIdx.x; t < kSortWin / 2; t += kSortThreads) {
-                const uint32_t a = 2 * t - (t & (stride - 1)), b = a + stride;
-                const uint32_t x = key[a], y = key[b];
-                if ((x > y) == ((a & size) == 0)) {
-                    key[a] = y;
-                    key[b] = x;
-                }
-            }
-            __syncthreads();
-        }
-    }
-    uint32_t *perm = const_cast<uint32_t *>(A.perm);
-    for (uint32_t e = threadIdx.x; e < cnt; e += kSortThreads) perm[base + e] = base + (key[e] & (kSortWin - 1));
 }
 
 // ---- shadow: any hit -> pending NEE contribution ---------------------------
@@ -1428,7 +1349,6 @@ cudaError_t enqueue_paths(const pt_ctx *ctx, Enqueue &E, WaveArgs &A, uint32_t d
         chk(cudaMemsetAsync(A.cntOut, 0, 4, st));
         chk(cudaMemsetAsync(A.cntShadow, 0, 8, st));  // shadow count and the extend claim position
         if (inl) {
-            A.sorted = 0;
             E.begin(STG_EXTEND);
             k_extend<false><<<G.ext, kBlock, 0, st>>>(A);
             E.end();
@@ -1438,15 +1358,10 @@ cudaError_t enqueue_paths(const pt_ctx *ctx, Enqueue &E, WaveArgs &A, uint32_t d
         } else {
             // class counts and the shadow claim position after them
             chk(cudaMemsetAsync(A.cntCls, 0, (CLS_N + 1) * sizeof(uint32_t), st));
-            A.sorted = (PT_RAY_SORT > 0 && b > 0) ? 1u : 0u;
-            A.perm = B.sslot;  // free until the shading kernels queue shadow rays
             E.begin(STG_EXTEND);
-            if (A.sorted)
-                k_ray_sort<<<(A.waveCount + kSortWin - 1) / kSortWin, kSortThreads, 0, st>>>(A);
             if (A.S.mediaWavefront) k_extend<true, true><<<G.extM, kBlock, 0, st>>>(A);
             else k_extend<true><<<G.extC, kBlock, 0, st>>>(A);
             E.end();
-            A.sorted = 0;
             const bool extra = A.risNee || A.S.mediaWavefront;
             const uint32_t mask = ctx->clsMask | (A.S.mediaWavefront ? 1u << CLS_MEDIUM : 0u);
             for (int c = 0; c < CLS_N; c++) {
@@ -1527,16 +1442,6 @@ cudaError_t enqueue_render(const pt_ctx *ctx, Enqueue &E, WaveArgs A, const pt_r
 
 __global__ void k_set_u32(uint32_t *p, uint32_t v) { *p = v; }
 
-// k_ray_sort's origin grid: 32 cells per axis over the scene's vertex bounds.
-void set_sort_box(WaveArgs &A, const pt_ctx *ctx) {
-    A.sorted = 0;
-    A.perm = nullptr;
-    for (int k = 0; k < 3; k++) {
-        float ext = ctx->sceneMax[k] - ctx->sceneMin[k];
-        A.sortMin[k] = ctx->sceneMin[k];
-        A.sortScale[k] = ext > 0.0f ? 32.0f / ext : 0.0f;
-    }
-}
 
 bool graph_matches(const pt_ctx *ctx, const pt_render_params *P, size_t cap, const float *sum, const float *comp,
                    const WaveArgs &A) {
@@ -1617,7 +1522,6 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
     A.shadowCap = (uint32_t)(2 * B.cap);
     if (ctx->dbgShadowCap) A.shadowCap = std::min(A.shadowCap, ctx->dbgShadowCap);
     A.batch = 0; A.numReqs = 0; A.reqs = nullptr; A.slotInfo = nullptr;
-    set_sort_box(A, ctx);
     A.risNee = (P->flags & PT_RENDER_RIS_NEE) ? 1u : 0u;
     if ((P->flags & PT_RENDER_MEDIA_WAVEFRONT) && A.S.numVols > 0 && !A.S.hasSubsurface && !A.S.mediaWavefront) {
         A.S.mediaWavefront = 1u;  // heterogeneous media (homogeneous-only scenes have it already)
@@ -1966,7 +1870,6 @@ int render_batch(pt_ctx *ctx, const pt_request *R, uint32_t n, float *request_ms
     A.err = ctx->d_err;
     A.shadowCap = (uint32_t)(2 * B.cap);
     A.batch = 1; A.numReqs = n; A.reqs = (const ReqDev *)Bt.reqs; A.slotInfo = Bt.slotInfo;
-    set_sort_box(A, ctx);
     A.risNee = (R[0].params.flags & PT_RENDER_RIS_NEE) ? 1u : 0u;
     if ((R[0].params.flags & PT_RENDER_MEDIA_WAVEFRONT) && A.S.numVols > 0 && !A.S.hasSubsurface &&
         !A.S.mediaWavefront) {

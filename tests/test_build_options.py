@@ -4,11 +4,8 @@ PT_SHARED_STACK=k keeps the first k traversal-stack entries of each thread of
 k_extend / k_shadow in shared memory (one column per thread) and the deeper
 ones in local memory.  The default (0) keeps the whole stack in local memory,
 which measured faster on B200; the option stays buildable so the choice can
-be re-measured.  PT_RAY_SORT=b reorders each window of 2^b secondary rays
-by direction and origin before closest-hit traversal (k_ray_sort); the
-default (0) traverses in queue order, which measured faster.  This
-cross-compiles the render kernels with both options (nvcc needs no GPU) and
-checks the shared memory the traversal and sort kernels then declare."""
+be re-measured.  This cross-compiles the traversal kernels with the option
+(nvcc needs no GPU) and checks the shared memory they then declare."""
 
 import os
 import re
@@ -30,8 +27,7 @@ def test_shared_stack_variant_compiles(depth):
     with tempfile.TemporaryDirectory() as tmp:
         out = os.path.join(tmp, "pt_render_shared_stack.o")
         cmd = [nvcc, "-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-c", src, "-o", out,
-               "-I", os.path.join(ROOT, "include"), f"-DPT_SHARED_STACK={depth}", "-DPT_RAY_SORT=12",
-               "-Xptxas", "-v"]
+               "-I", os.path.join(ROOT, "include"), f"-DPT_SHARED_STACK={depth}", "-Xptxas", "-v"]
         r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
         assert r.returncode == 0, r.stderr[-2000:]
         assert os.path.getsize(out) > 0
@@ -50,5 +46,3 @@ def test_shared_stack_variant_compiles(depth):
     traversal = {k: v for k, v in smem.items() if "k_extend" in k or "k_shadow" in k}
     assert traversal, "no traversal kernels in the ptxas report"
     assert all(v >= stack_bytes for v in traversal.values()), traversal
-    sort = {k: v for k, v in smem.items() if "k_ray_sort" in k}
-    assert sort and all(v >= 4096 * 4 for v in sort.values()), sort  # one 4096-key window
