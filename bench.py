@@ -142,10 +142,10 @@ def measured_peaks():
 
 
 # k_extend DRAM traffic per extension ray (dram__bytes_read.sum + dram__bytes_write.sum
-# from one ncu capture of this workload at 4 spp: 235.3 MB over the 3,686,400
+# from one ncu capture of this workload at 4 spp: 233.6 MB over the 3,686,400
 # camera rays of bounce 0).  The scene is L2-resident and the queues stream
 # once, so traffic scales with the rays a launch processes.
-EXTEND_DRAM_BYTES_PER_RAY = {"disney_envmap": 63.8}
+EXTEND_DRAM_BYTES_PER_RAY = {"disney_envmap": 63.4}
 
 
 REF_SPP = 4096        # reference image: plain path tracing, samples [0, 4096)
@@ -779,19 +779,21 @@ def main():
 
     ext = sum(s.extension_rays for s in stats)
     sh = sum(s.shadow_rays for s in stats)
-    stage_ms = {k: sum(getattr(s, "ms_" + k) for s in tstats) for k in ("raygen", "extend", "shade", "shadow", "film")}
+    stage_ms = {k: sum(getattr(s, "ms_" + k) for s in tstats)
+                for k in ("raygen", "extend", "shade", "shadow", "tail", "film")}
     launches = {"extend": sum(s.bounces for s in tstats)}
+    # k_extend's own rays (the tail kernel traces the last bounces' rays itself)
+    ext_k = sum(s.extension_rays - s.tail_extension_rays for s in tstats)
     peak, peak_src = measured_peaks()
     dominant = max(stage_ms, key=stage_ms.get)
-    alg = {"extend": ext * BYTES_PER_EXT_RAY, "shadow": sh * BYTES_PER_SHADOW_RAY}
     # roofline of the closest-hit traversal kernel: algorithmic bytes per launch / mean launch time
     n_ext_launch = max(1, launches["extend"])
-    ext_bytes_per_launch = ext * BYTES_PER_EXT_RAY / n_ext_launch
+    ext_bytes_per_launch = ext_k * BYTES_PER_EXT_RAY / n_ext_launch
     ext_ms_per_launch = stage_ms["extend"] / n_ext_launch
     achieved = ext_bytes_per_launch / (ext_ms_per_launch / 1e3) / 1e9 if ext_ms_per_launch > 0 else 0.0
     traffic = None
     if cfg["workload"] in EXTEND_DRAM_BYTES_PER_RAY:
-        traffic = round(EXTEND_DRAM_BYTES_PER_RAY[cfg["workload"]] * ext / n_ext_launch, 1)
+        traffic = round(EXTEND_DRAM_BYTES_PER_RAY[cfg["workload"]] * ext_k / n_ext_launch, 1)
     n_ext = ext / (paths_step * args.steps)
     n_sh = sh / (paths_step * args.steps)
     b_path = BYTES_PER_PATH_FILM + BYTES_PER_EXT_RAY * n_ext + BYTES_PER_SHADOW_RAY * n_sh

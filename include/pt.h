@@ -222,7 +222,7 @@ typedef struct pt_stats {
     uint64_t extension_rays;
     uint64_t shadow_rays;
     uint64_t waves;
-    uint64_t bounces;  /* wavefront iterations launched */
+    uint64_t bounces;  /* wavefront iterations launched (closest-hit kernel launches) */
     uint64_t launches; /* kernels this call launched */
     float ms_total;    /* device time of the render, CUDA events on the context's stream */
     /* per stage, with PT_RENDER_STAGE_TIMING (0 otherwise): */
@@ -232,6 +232,12 @@ typedef struct pt_stats {
     float ms_shadow;   /* any-hit traversal */
     float ms_film;     /* film accumulation */
     float ms_cache;    /* radiance-cache inference, training targets, training step */
+    /* The last bounces of a wave, once few paths are left, run as one kernel
+     * (each path to its end: closest hit, shading, NEE): its device time
+     * (with PT_RENDER_STAGE_TIMING) and the extension rays it traced (part of
+     * extension_rays; its shadow rays are part of shadow_rays). */
+    float ms_tail;
+    uint64_t tail_extension_rays;
 } pt_stats;
 
 typedef struct pt_ctx pt_ctx;

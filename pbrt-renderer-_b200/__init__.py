@@ -109,7 +109,8 @@ class pt_stats(C.Structure):
     _fields_ = [("paths", C.c_uint64), ("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
                 ("waves", C.c_uint64), ("bounces", C.c_uint64), ("launches", C.c_uint64), ("ms_total", C.c_float),
                 ("ms_raygen", C.c_float), ("ms_extend", C.c_float), ("ms_shade", C.c_float),
-                ("ms_shadow", C.c_float), ("ms_film", C.c_float), ("ms_cache", C.c_float)]
+                ("ms_shadow", C.c_float), ("ms_film", C.c_float), ("ms_cache", C.c_float), ("ms_tail", C.c_float),
+                ("tail_extension_rays", C.c_uint64)]
 
 
 class pt_hit(C.Structure):

@@ -65,7 +65,9 @@ __host__ __device__ inline int shade_class(bool hit, bool emitter, uint32_t type
 // (word 2) and the class counts (words 8 .. 8 + CLS_N).
 constexpr int kCounterWords = 32;
 constexpr int kCntShadow = 2, kCntStealExt = 3, kCntClass = 8, kCntStealShadow = kCntClass + CLS_N;
-static_assert(kCntStealShadow + 1 <= kCounterWords, "class queue counts must fit the counter block");
+constexpr int kCntTailRays = 24;  // uint64: extension rays of the tail kernel
+static_assert(kCntStealShadow + 1 <= kCntTailRays && kCntTailRays + 2 <= kCounterWords,
+              "class queue counts and the tail's ray count must fit the counter block");
 
 // Per-wave buffers of the wavefront integrator (structure of arrays).
 struct WaveBuffers {

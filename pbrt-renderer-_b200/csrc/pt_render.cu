@@ -70,6 +70,7 @@ struct WaveArgs {
     uint32_t *cls, *cntCls;  // shading-class queues (CLS_N x clsStride) and their counts
     uint32_t clsStride;
     unsigned long long *rayTotals;  // [0] extension, [1] shadow
+    unsigned long long *tailRays;   // extension rays of k_tail (also in rayTotals[0])
     uint32_t *err;
     uint32_t shadowCap;
     // radiance cache (cacheOn == 0: plain path tracing)
@@ -88,6 +89,13 @@ struct WaveArgs {
 };
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// Add this thread's count of rays of kind k (0 extension, 1 shadow) to the
+// render's totals: one atomic per warp.
+__device__ __forceinline__ void add_rays(const WaveArgs &A, int k, uint32_t c) {
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
+    if (lane_id() == 0 && c) atomicAdd(&A.rayTotals[k], (unsigned long long)c);
+}
 
 // Warp-aggregated append: returns this lane's slot in the queue.
 __device__ __forceinline__ uint32_t warp_append(uint32_t *counter, bool pred) {
@@ -394,6 +402,7 @@ __global__ void __launch_bounds__(kBlock) k_shadow(WaveArgs A) {
 // the final thr * 0 written straight to the pending slot.
 struct NeeOut {
     bool ray;
+    bool traced;   // the inline form traced its shadow ray (ray counts)
     bool trLater;  // medium transmittance left to the shadow kernel (not in X)
     float3 o, d, X;
     float tmin, tmax;
@@ -420,6 +429,7 @@ __device__ __forceinline__ float3 nee_area(const WaveArgs &A, float3 hp, float3 
     float3 so = offset_origin(hp, sng, sng);
     float3 trans = v3(1.0f);
     if (INLINE) {
+        out.traced = true;
         if (trace_shadow(S, so, ww, 0.0f, dist - 0.001f, trans, A.err, aseed, alpha_key(bounce, 1u))) return v3(0.0f);
     }
     float3 f;
@@ -499,6 +509,7 @@ __device__ __forceinline__ float3 nee_ris(const WaveArgs &A, float3 hp, float3 N
     float3 so = offset_origin(hp, sng, sng);
     float3 trans = v3(1.0f);
     if (INLINE) {
+        out.traced = true;
         if (trace_shadow(S, so, wiw, 0.0f, dist - 0.001f, trans, A.err, aseed, alpha_key(bounce, 1u))) return v3(0.0f);
     }
     float3 fu;
@@ -534,6 +545,7 @@ __device__ __forceinline__ float3 nee_env(const WaveArgs &A, float3 hp, float3 N
     float3 so = offset_origin(hp, sng, sng);
     float3 trans = v3(1.0f);
     if (INLINE) {
+        out.traced = true;
         if (trace_shadow(S, so, ww, 0.0f, 1e20f, trans, A.err, aseed, alpha_key(bounce, 2u))) return v3(0.0f);
     }
     float3 f;
@@ -576,6 +588,7 @@ __device__ float3 vol_nee_area(const WaveArgs &A, float3 sp, float3 wo, uint32_t
     float cl = dot(es.nrm, -wi);
     if (cl <= 0.0f) return v3(0.0f);
     float3 trans = v3(1.0f);
+    if (INLINE) out.traced = true;
     if (INLINE && trace_shadow(S, sp, wi, 0.001f, dist - 0.001f, trans, A.err, aseed, alpha_key(bounce, 1u)))
         return v3(0.0f);
     float fp = hg(dot(wo, wi), v.phase_g);
@@ -603,6 +616,7 @@ __device__ float3 vol_nee_env(const WaveArgs &A, float3 sp, float3 wo, uint32_t 
     env_sample(S, A.envMode, u1, u2, wi, Le, pe);
     if (pe <= 0.0f) return v3(0.0f);
     float3 trans = v3(1.0f);
+    if (INLINE) out.traced = true;
     if (INLINE && trace_shadow(S, sp, wi, 0.001f, 1e20f, trans, A.err, aseed, alpha_key(bounce, 2u)))
         return v3(0.0f);
     float fp = hg(dot(wo, wi), v.phase_g);
@@ -785,89 +799,73 @@ __device__ __forceinline__ bool rough_bounce(const WaveArgs &A, uint32_t type, c
 // CLS + CLS_TEX: the kernel of class CLS for materials with shading textures.
 // EXTRA: the instantiation for RIS NEE and homogeneous media in the wavefront;
 // the default one carries neither (their code would raise register pressure).
-template <bool INLINE, int CLS, bool EXTRA = false>
-__global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveArgs A) {
+// What one shading event leaves for the kernel around it: whether the path
+// goes on and with which ray, and its deferred NEE rays.
+struct ShadeOut {
+    bool cont;
+    uint32_t slot;
+    float3 no, nd;
+    float ntmin;
+    NeeOut neeA, neeE;
+    float3 thrNee;
+};
+// The shading event of ray-queue position i (active: i is a real entry).
+template <bool INLINE, int CLS, bool EXTRA>
+__device__ __forceinline__ void shade_item(const WaveArgs &A, bool active, uint32_t i, ShadeOut &O) {
     constexpr int C = ShadeBlocks<CLS>::base;    // the event / material class
     constexpr bool TEX = CLS >= (int)CLS_TEX && CLS != (int)CLS_MEDIUM;  // shading textures present
     const DevScene &S = A.S;
-    uint32_t n = CLS == CLS_ANY ? *(volatile uint32_t *)A.cntIn : *(volatile uint32_t *)(A.cntCls + CLS);
-    uint32_t iters = (n + gridDim.x * blockDim.x - 1) / (gridDim.x * blockDim.x);
-    for (uint32_t it = 0; it < iters; it++) {
-        uint32_t q = (it * gridDim.x + blockIdx.x) * blockDim.x + threadIdx.x;
-        bool active = q < n;
-        uint32_t i = q;
-        if (CLS != CLS_ANY && active) i = A.cls[(size_t)(CLS < 0 ? 0 : CLS) * A.clsStride + q];
-        bool cont = false;
-        uint32_t slot = 0;
-        float3 thr = v3(1.0f), Lo = v3(0.0f);
-        float lastPdf = 0.0f, eta = 1.0f;
-        uint4 st = make_uint4(0, 0, 0, 0);
-        float3 no = v3(0.0f), nd = v3(0.0f);
-        float ntmin = 0.0f;
-        NeeOut neeA, neeE;
-        neeA.ray = neeE.ray = false;
-        neeA.trLater = neeE.trLater = false;
-        float3 thrNee = v3(0.0f);
-        Rng rng;
-        if (active) {
-            slot = A.bounce == 0u ? i : A.qslotIn[i];
-            // bounce 0 outside the medium wavefront: the initial state, known
-            const bool fresh = A.bounce == 0u && !S.mediaWavefront;
-            float4 tp = fresh ? make_float4(1.0f, 1.0f, 1.0f, 0.0f) : A.thr_pdf[slot];
-            float4 le = fresh ? make_float4(0.0f, 0.0f, 0.0f, 1.0f) : A.lo_eta[slot];
-            st = A.rng[slot];
-            thr = make_float3(tp.x, tp.y, tp.z);
-            lastPdf = tp.w;
-            Lo = make_float3(le.x, le.y, le.z);
-            eta = fabsf(le.w);  // the sign of w flags pending NEE for the film
-            if (st.w & kFlagPending) {  // NEE of the previous bounce, in RayGen's order
-                float4 pa = A.pendA[slot], pe = A.pendE[slot];
-                Lo += make_float3(pa.x, pa.y, pa.z);
-                Lo += make_float3(pe.x, pe.y, pe.z);
-                st.w &= ~kFlagPending;
-            }
-            rng = load_rng(A, slot, st);
-            const uint32_t aseed = S.hasAlpha ? alpha_seed(rng.pixelSeed, rng.sampleIndex) : 0u;
-            float4 o4 = A.qoIn[i], d4 = A.qdIn[i], h4 = A.qhit[i];
-            float3 ro = make_float3(o4.x, o4.y, o4.z), rd = make_float3(d4.x, d4.y, d4.z);
-            uint32_t gid = __float_as_uint(h4.y);
-            bool hit = gid != 0xFFFFFFFFu;
-            bool volScat = false;
-            if (INLINE && S.numVols > 0) {  // Shaders.hlsl:133-179
-                float tSurf = hit ? h4.x : 1e20f;
-                float tsc;
-                uint32_t svi;
-                float3 vw = v3(1.0f);
-                bool sc = sample_free_flight(S, ro, rd, tSurf, rng, vw, tsc, svi);
-                thr *= vw;
-                if (sc) {
-                    volScat = true;
-                    const pt_volume &v = S.vols[svi];
-                    float3 spos = xpos(ro, rd, tsc);
-                    thr *= make_float3(v.sigma_s[0], v.sigma_s[1], v.sigma_s[2]) / vmax(vsigma_t(v), v3(1e-20f));
-                    Lo += thr * vol_nee_area<true>(A, spos, rd, svi, rng, aseed, st.z, neeA);
-                    Lo += thr * vol_nee_env<true>(A, spos, rd, svi, rng, aseed, st.z, neeE);
-                    float x1 = next_float(rng, S.sobol1), x2 = next_float(rng, S.sobol1);
-                    float pp;
-                    nd = sample_hg(rd, v.phase_g, x1, x2, pp);
-                    no = spos;
-                    ntmin = 0.0f;
-                    lastPdf = mx(pp, 1e-20f);
-                    cont = true;
-                    st.w |= kFlagRough;
-                }
-            }
-            if (EXTRA && C == CLS_MEDIUM) {  // scattering in a homogeneous medium (Shaders.hlsl:149-178), NEE deferred
-                const uint32_t svi = gid & 0x7FFFFFFFu;
+    bool cont = false;
+    uint32_t slot = 0;
+    float3 thr = v3(1.0f), Lo = v3(0.0f);
+    float lastPdf = 0.0f, eta = 1.0f;
+    uint4 st = make_uint4(0, 0, 0, 0);
+    float3 no = v3(0.0f), nd = v3(0.0f);
+    float ntmin = 0.0f;
+    NeeOut neeA, neeE;
+    neeA.ray = neeE.ray = false;
+    neeA.traced = neeE.traced = false;
+    neeA.trLater = neeE.trLater = false;
+    float3 thrNee = v3(0.0f);
+    Rng rng;
+    if (active) {
+        slot = A.bounce == 0u ? i : A.qslotIn[i];
+        // bounce 0 outside the medium wavefront: the initial state, known
+        const bool fresh = A.bounce == 0u && !S.mediaWavefront;
+        float4 tp = fresh ? make_float4(1.0f, 1.0f, 1.0f, 0.0f) : A.thr_pdf[slot];
+        float4 le = fresh ? make_float4(0.0f, 0.0f, 0.0f, 1.0f) : A.lo_eta[slot];
+        st = A.rng[slot];
+        thr = make_float3(tp.x, tp.y, tp.z);
+        lastPdf = tp.w;
+        Lo = make_float3(le.x, le.y, le.z);
+        eta = fabsf(le.w);  // the sign of w flags pending NEE for the film
+        if (st.w & kFlagPending) {  // NEE of the previous bounce, in RayGen's order
+            float4 pa = A.pendA[slot], pe = A.pendE[slot];
+            Lo += make_float3(pa.x, pa.y, pa.z);
+            Lo += make_float3(pe.x, pe.y, pe.z);
+            st.w &= ~kFlagPending;
+        }
+        rng = load_rng(A, slot, st);
+        const uint32_t aseed = S.hasAlpha ? alpha_seed(rng.pixelSeed, rng.sampleIndex) : 0u;
+        float4 o4 = A.qoIn[i], d4 = A.qdIn[i], h4 = A.qhit[i];
+        float3 ro = make_float3(o4.x, o4.y, o4.z), rd = make_float3(d4.x, d4.y, d4.z);
+        uint32_t gid = __float_as_uint(h4.y);
+        bool hit = gid != 0xFFFFFFFFu;
+        bool volScat = false;
+        if (INLINE && S.numVols > 0) {  // Shaders.hlsl:133-179
+            float tSurf = hit ? h4.x : 1e20f;
+            float tsc;
+            uint32_t svi;
+            float3 vw = v3(1.0f);
+            bool sc = sample_free_flight(S, ro, rd, tSurf, rng, vw, tsc, svi);
+            thr *= vw;
+            if (sc) {
+                volScat = true;
                 const pt_volume &v = S.vols[svi];
-                float3 spos = xpos(ro, rd, h4.x);
+                float3 spos = xpos(ro, rd, tsc);
                 thr *= make_float3(v.sigma_s[0], v.sigma_s[1], v.sigma_s[2]) / vmax(vsigma_t(v), v3(1e-20f));
-                vol_nee_area<false>(A, spos, rd, svi, rng, aseed, st.z, neeA);
-                vol_nee_env<false>(A, spos, rd, svi, rng, aseed, st.z, neeE);
-                thrNee = thr;
-                if (!neeA.ray) A.pendA[slot] = make_float4(thr.x * 0.0f, thr.y * 0.0f, thr.z * 0.0f, 0.0f);
-                if (!neeE.ray) A.pendE[slot] = make_float4(thr.x * 0.0f, thr.y * 0.0f, thr.z * 0.0f, 0.0f);
-                st.w |= kFlagPending;
+                Lo += thr * vol_nee_area<true>(A, spos, rd, svi, rng, aseed, st.z, neeA);
+                Lo += thr * vol_nee_env<true>(A, spos, rd, svi, rng, aseed, st.z, neeE);
                 float x1 = next_float(rng, S.sobol1), x2 = next_float(rng, S.sobol1);
                 float pp;
                 nd = sample_hg(rd, v.phase_g, x1, x2, pp);
@@ -876,75 +874,86 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
                 lastPdf = mx(pp, 1e-20f);
                 cont = true;
                 st.w |= kFlagRough;
-            } else if (volScat) {
-            } else if (C == CLS_MISS || (C == CLS_ANY && !hit)) {  // Shaders.hlsl:188-212
-                float3 env = eval_env(S, rd);
-                if (lastPdf == 0.0f) Lo += thr * env;
-                else Lo += thr * env * balance(lastPdf, env_pdf(S, A.envMode, rd));
-            } else if (C != CLS_MISS) {
-                uint32_t mesh = __ldg(S.triMesh + gid);
-                uint32_t prim = gid - __ldg(S.meshFirstTri + mesh);
-                pt_material m = S.mats[mesh];
-                const uint32_t type = C >= CLS_DIFFUSE ? class_type(C) : m.type;
-                uint32_t i0, i1, i2;
-                tri_vidx(S, mesh, prim, i0, i1, i2);
-                float bx = h4.z, by = h4.w, w0 = 1.0f - bx - by;
-                float3 hp = ro + rd * h4.x;
-                float3 p0 = ld3(S.pos, i0), p1 = ld3(S.pos, i1), p2 = ld3(S.pos, i2);
-                float3 Ng = normalize(normalize(cross(p1 - p0, p2 - p0)));
-                float3 nn = ld3(S.nrm, i0) * w0 + ld3(S.nrm, i1) * bx + ld3(S.nrm, i2) * by;
-                float l2 = dot(nn, nn);
-                float3 N = normalize(l2 < 1e-8f ? normalize(cross(p1 - p0, p2 - p0)) : nn * (1.0f / sqrtf(l2)));
-                bool back = dot(Ng, rd) > 0.0f;
-                if (back) Ng = -Ng;
-                if (dot(N, Ng) < 0.0f) N = -N;
-                if (TEX || (C == CLS_ANY && has_shading_textures(m)))
-                {
-                    const uint2 wh = path_image(A, slot);
-                    apply_textures(S, m, mesh, prim, h4.x, i0, i1, i2, bx, by, N, wh.x, wh.y);
-                }
-                // Radiance cache: the first surface vertex after a rough bounce ends
-                // the path (a query, resolved after the wave), or, with probability
-                // *trainProb, records its state there and the path goes on as a
-                // training path (its suffix ends at its own next cache vertex, or
-                // for one in unbiasedEvery, runs without the cache).
-                bool cacheStop = false;
-                if (A.cacheOn && (st.w & kFlagRough) && !(C == CLS_EMIT || (C == CLS_ANY && m.isEmitter))) {
-                    bool train = (st.w & kFlagTrain) != 0;
-                    if (!train && A.trainOn) {
-                        const uint32_t hsh = pcg_hash(pcg_hash(rng.pixelSeed ^ (rng.sampleIndex * 0x9E3779B9u)) ^ st.z);
-                        if ((float)(hsh >> 8) * (1.0f / 16777216.0f) < __ldg(A.trainProb)) {
-                            uint32_t r = warp_append(A.crCount, true);
-                            if (r < A.recCap) {
-                                cache_record(A.cr, r, hp, -rd, N, m, type, slot);
-                                A.cr[4][r] = make_float4(thr.x, thr.y, thr.z, 0.0f);
-                                A.cr[5][r] = make_float4(Lo.x, Lo.y, Lo.z, 0.0f);
-                                st.w |= kFlagTrain | kFlagHasRec | (r << 8);
-                                if (A.unbiasedEvery && pcg_hash(hsh) % A.unbiasedEvery == 0) st.w |= kFlagUnbiased;
-                                train = true;
-                                // the image takes this path as it takes the others (prefix +
-                                // throughput x cache here); its suffix only feeds training
-                                uint32_t q = warp_append(A.cqCount, true);
-                                if (q < A.queryCap) {
-                                    cache_record(A.cq, q, hp, -rd, N, m, type, r | 0x80000000u);
-                                    A.cq[4][q] = make_float4(thr.x, thr.y, thr.z, 0.0f);
-                                } else {
-                                    atomicOr(A.err, (uint32_t)PT_DEVERR_QUEUE);
-                                }
-                            }
-                        }
-                        if (train) {
-                        } else {
+            }
+        }
+        if (EXTRA && C == CLS_MEDIUM) {  // scattering in a homogeneous medium (Shaders.hlsl:149-178), NEE deferred
+            const uint32_t svi = gid & 0x7FFFFFFFu;
+            const pt_volume &v = S.vols[svi];
+            float3 spos = xpos(ro, rd, h4.x);
+            thr *= make_float3(v.sigma_s[0], v.sigma_s[1], v.sigma_s[2]) / vmax(vsigma_t(v), v3(1e-20f));
+            vol_nee_area<false>(A, spos, rd, svi, rng, aseed, st.z, neeA);
+            vol_nee_env<false>(A, spos, rd, svi, rng, aseed, st.z, neeE);
+            thrNee = thr;
+            if (!neeA.ray) A.pendA[slot] = make_float4(thr.x * 0.0f, thr.y * 0.0f, thr.z * 0.0f, 0.0f);
+            if (!neeE.ray) A.pendE[slot] = make_float4(thr.x * 0.0f, thr.y * 0.0f, thr.z * 0.0f, 0.0f);
+            st.w |= kFlagPending;
+            float x1 = next_float(rng, S.sobol1), x2 = next_float(rng, S.sobol1);
+            float pp;
+            nd = sample_hg(rd, v.phase_g, x1, x2, pp);
+            no = spos;
+            ntmin = 0.0f;
+            lastPdf = mx(pp, 1e-20f);
+            cont = true;
+            st.w |= kFlagRough;
+        } else if (volScat) {
+        } else if (C == CLS_MISS || (C == CLS_ANY && !hit)) {  // Shaders.hlsl:188-212
+            float3 env = eval_env(S, rd);
+            if (lastPdf == 0.0f) Lo += thr * env;
+            else Lo += thr * env * balance(lastPdf, env_pdf(S, A.envMode, rd));
+        } else if (C != CLS_MISS) {
+            uint32_t mesh = __ldg(S.triMesh + gid);
+            uint32_t prim = gid - __ldg(S.meshFirstTri + mesh);
+            pt_material m = S.mats[mesh];
+            const uint32_t type = C >= CLS_DIFFUSE ? class_type(C) : m.type;
+            uint32_t i0, i1, i2;
+            tri_vidx(S, mesh, prim, i0, i1, i2);
+            float bx = h4.z, by = h4.w, w0 = 1.0f - bx - by;
+            float3 hp = ro + rd * h4.x;
+            float3 p0 = ld3(S.pos, i0), p1 = ld3(S.pos, i1), p2 = ld3(S.pos, i2);
+            float3 Ng = normalize(normalize(cross(p1 - p0, p2 - p0)));
+            float3 nn = ld3(S.nrm, i0) * w0 + ld3(S.nrm, i1) * bx + ld3(S.nrm, i2) * by;
+            float l2 = dot(nn, nn);
+            float3 N = normalize(l2 < 1e-8f ? normalize(cross(p1 - p0, p2 - p0)) : nn * (1.0f / sqrtf(l2)));
+            bool back = dot(Ng, rd) > 0.0f;
+            if (back) Ng = -Ng;
+            if (dot(N, Ng) < 0.0f) N = -N;
+            if (TEX || (C == CLS_ANY && has_shading_textures(m)))
+            {
+                const uint2 wh = path_image(A, slot);
+                apply_textures(S, m, mesh, prim, h4.x, i0, i1, i2, bx, by, N, wh.x, wh.y);
+            }
+            // Radiance cache: the first surface vertex after a rough bounce ends
+            // the path (a query, resolved after the wave), or, with probability
+            // *trainProb, records its state there and the path goes on as a
+            // training path (its suffix ends at its own next cache vertex, or
+            // for one in unbiasedEvery, runs without the cache).
+            bool cacheStop = false;
+            if (A.cacheOn && (st.w & kFlagRough) && !(C == CLS_EMIT || (C == CLS_ANY && m.isEmitter))) {
+                bool train = (st.w & kFlagTrain) != 0;
+                if (!train && A.trainOn) {
+                    const uint32_t hsh = pcg_hash(pcg_hash(rng.pixelSeed ^ (rng.sampleIndex * 0x9E3779B9u)) ^ st.z);
+                    if ((float)(hsh >> 8) * (1.0f / 16777216.0f) < __ldg(A.trainProb)) {
+                        uint32_t r = warp_append(A.crCount, true);
+                        if (r < A.recCap) {
+                            cache_record(A.cr, r, hp, -rd, N, m, type, slot);
+                            A.cr[4][r] = make_float4(thr.x, thr.y, thr.z, 0.0f);
+                            A.cr[5][r] = make_float4(Lo.x, Lo.y, Lo.z, 0.0f);
+                            st.w |= kFlagTrain | kFlagHasRec | (r << 8);
+                            if (A.unbiasedEvery && pcg_hash(hsh) % A.unbiasedEvery == 0) st.w |= kFlagUnbiased;
+                            train = true;
+                            // the image takes this path as it takes the others (prefix +
+                            // throughput x cache here); its suffix only feeds training
                             uint32_t q = warp_append(A.cqCount, true);
                             if (q < A.queryCap) {
-                                cache_record(A.cq, q, hp, -rd, N, m, type, slot);
+                                cache_record(A.cq, q, hp, -rd, N, m, type, r | 0x80000000u);
                                 A.cq[4][q] = make_float4(thr.x, thr.y, thr.z, 0.0f);
                             } else {
                                 atomicOr(A.err, (uint32_t)PT_DEVERR_QUEUE);
                             }
-                            cacheStop = true;
                         }
-                    } else if (!(train && (st.w & kFlagUnbiased))) {
+                    }
+                    if (train) {
+                    } else {
                         uint32_t q = warp_append(A.cqCount, true);
                         if (q < A.queryCap) {
                             cache_record(A.cq, q, hp, -rd, N, m, type, slot);
@@ -954,203 +963,275 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
                         }
                         cacheStop = true;
                     }
-                }
-                if (C == CLS_EMIT || (C == CLS_ANY && m.isEmitter)) {  // Shaders.hlsl:317-335
-                    float3 rad = make_float3(m.radiance[0], m.radiance[1], m.radiance[2]);
-                    if (lastPdf == 0.0f) Lo += thr * rad;
-                    else Lo += thr * rad * balance(lastPdf, emitter_pdf_sa(S, m, hp, ro, N));
-                } else if (C != CLS_EMIT && !cacheStop) {
-                    float3 T, B;
-                    float h = 0.0f;
-                    if (type == PT_MAT_HAIR) {  // Shaders.hlsl:340-387
-                        float hu = __ldg(S.uv + 2 * i0) * w0 + __ldg(S.uv + 2 * i1) * bx + __ldg(S.uv + 2 * i2) * by;
-                        float hv = __ldg(S.uv + 2 * i0 + 1) * w0 + __ldg(S.uv + 2 * i1 + 1) * bx +
-                                   __ldg(S.uv + 2 * i2 + 1) * by;
-                        float3 ht = ld3(S.tan, i0) * w0 + ld3(S.tan, i1) * bx + ld3(S.tan, i2) * by;
-                        float tl2 = dot(ht, ht);
-                        ht = tl2 > 1e-8f ? ht * (1.0f / sqrtf(tl2)) : v3(0.0f);
-                        if (dot(ht, ht) > 1e-8f) {
-                            ht = normalize(ht);
-                            h = hv * 2.0f - 1.0f;
-                        } else {
-                            float a0u = __ldg(S.uv + 2 * i0), a0v = __ldg(S.uv + 2 * i0 + 1);
-                            float d1u = __ldg(S.uv + 2 * i1) - a0u, d1v = __ldg(S.uv + 2 * i1 + 1) - a0v;
-                            float d2u = __ldg(S.uv + 2 * i2) - a0u, d2v = __ldg(S.uv + 2 * i2 + 1) - a0v;
-                            float det = d1u * d2v - d2u * d1v;
-                            if (fabsf(det) > 1e-8f) ht = normalize((-d1u * (p1 - p0) + d2u * (p2 - p0)) * (1.0f / det));
-                            else build_onb(N, ht, B);
-                            h = hu * 2.0f - 1.0f;
-                        }
-                        T = normalize(ht - N * dot(ht, N));
-                        B = cross(N, T);
+                } else if (!(train && (st.w & kFlagUnbiased))) {
+                    uint32_t q = warp_append(A.cqCount, true);
+                    if (q < A.queryCap) {
+                        cache_record(A.cq, q, hp, -rd, N, m, type, slot);
+                        A.cq[4][q] = make_float4(thr.x, thr.y, thr.z, 0.0f);
                     } else {
+                        atomicOr(A.err, (uint32_t)PT_DEVERR_QUEUE);
+                    }
+                    cacheStop = true;
+                }
+            }
+            if (C == CLS_EMIT || (C == CLS_ANY && m.isEmitter)) {  // Shaders.hlsl:317-335
+                float3 rad = make_float3(m.radiance[0], m.radiance[1], m.radiance[2]);
+                if (lastPdf == 0.0f) Lo += thr * rad;
+                else Lo += thr * rad * balance(lastPdf, emitter_pdf_sa(S, m, hp, ro, N));
+            } else if (C != CLS_EMIT && !cacheStop) {
+                float3 T, B;
+                float h = 0.0f;
+                if (type == PT_MAT_HAIR) {  // Shaders.hlsl:340-387
+                    float hu = __ldg(S.uv + 2 * i0) * w0 + __ldg(S.uv + 2 * i1) * bx + __ldg(S.uv + 2 * i2) * by;
+                    float hv = __ldg(S.uv + 2 * i0 + 1) * w0 + __ldg(S.uv + 2 * i1 + 1) * bx +
+                               __ldg(S.uv + 2 * i2 + 1) * by;
+                    float3 ht = ld3(S.tan, i0) * w0 + ld3(S.tan, i1) * bx + ld3(S.tan, i2) * by;
+                    float tl2 = dot(ht, ht);
+                    ht = tl2 > 1e-8f ? ht * (1.0f / sqrtf(tl2)) : v3(0.0f);
+                    if (dot(ht, ht) > 1e-8f) {
+                        ht = normalize(ht);
+                        h = hv * 2.0f - 1.0f;
+                    } else {
+                        float a0u = __ldg(S.uv + 2 * i0), a0v = __ldg(S.uv + 2 * i0 + 1);
+                        float d1u = __ldg(S.uv + 2 * i1) - a0u, d1v = __ldg(S.uv + 2 * i1 + 1) - a0v;
+                        float d2u = __ldg(S.uv + 2 * i2) - a0u, d2v = __ldg(S.uv + 2 * i2 + 1) - a0v;
+                        float det = d1u * d2v - d2u * d1v;
+                        if (fabsf(det) > 1e-8f) ht = normalize((-d1u * (p1 - p0) + d2u * (p2 - p0)) * (1.0f / det));
+                        else build_onb(N, ht, B);
+                        h = hu * 2.0f - 1.0f;
+                    }
+                    T = normalize(ht - N * dot(ht, N));
+                    B = cross(N, T);
+                } else {
+                    build_onb(N, T, B);
+                }
+                {  // terminator bend, Shaders.hlsl:402-411
+                    float3 V = -rd;
+                    float ndv = dot(N, V);
+                    if (ndv <= 0.0f && dot(V, Ng) > 0.0f) {
+                        N = normalize(N + V * (1e-3f - ndv));
                         build_onb(N, T, B);
                     }
-                    {  // terminator bend, Shaders.hlsl:402-411
-                        float3 V = -rd;
-                        float ndv = dot(N, V);
-                        if (ndv <= 0.0f && dot(V, Ng) > 0.0f) {
-                            N = normalize(N + V * (1e-3f - ndv));
-                            build_onb(N, T, B);
-                        }
+                }
+                float3 wil = to_local(-rd, T, B, N);
+                if (type == PT_MAT_MIRROR) {  // Shaders.hlsl:419-427
+                    nd = reflect(rd, N);
+                    no = hp + Ng * 0.001f;
+                    lastPdf = 0.0f;
+                    cont = true;
+                    st.w &= ~kFlagRough;
+                } else if (type == PT_MAT_DIELECTRIC) {  // Shaders.hlsl:429-472
+                    float es;
+                    nd = delta_scatter(PT_MAT_DIELECTRIC, rd, N, back, m.intIOR, m.extIOR,
+                                       next_float(rng, S.sobol1), es);
+                    no = hp + (dot(nd, Ng) > 0.0f ? Ng : -Ng) * 0.001f;
+                    lastPdf = 0.0f;
+                    eta *= es;
+                    cont = true;
+                    st.w &= ~kFlagRough;
+                } else if (C != CLS_DELTA &&
+                           (type == PT_MAT_DIFFUSE || type == PT_MAT_MICROFACET || type == PT_MAT_DISNEY ||
+                            type == PT_MAT_HAIR)) {  // Shaders.hlsl:473-511
+                    float3 ra = ((INLINE || EXTRA) && A.risNee)
+                                    ? nee_ris<INLINE, EXTRA>(A, hp, N, Ng, T, B, wil, type, m, h, rng, neeA, aseed, st.z)
+                                    : nee_area<INLINE, EXTRA>(A, hp, N, Ng, T, B, wil, type, m, h, rng, neeA, aseed, st.z);
+                    float3 re = nee_env<INLINE, EXTRA>(A, hp, N, Ng, T, B, wil, type, m, h, rng, neeE, aseed, st.z);
+                    if (INLINE) {
+                        Lo += thr * ra;
+                        Lo += thr * re;
+                    } else {
+                        thrNee = thr;
+                        if (!neeA.ray) A.pendA[slot] = make_float4(thr.x * 0.0f, thr.y * 0.0f, thr.z * 0.0f, 0.0f);
+                        if (!neeE.ray) A.pendE[slot] = make_float4(thr.x * 0.0f, thr.y * 0.0f, thr.z * 0.0f, 0.0f);
+                        st.w |= kFlagPending;
                     }
-                    float3 wil = to_local(-rd, T, B, N);
-                    if (type == PT_MAT_MIRROR) {  // Shaders.hlsl:419-427
-                        nd = reflect(rd, N);
-                        no = hp + Ng * 0.001f;
-                        lastPdf = 0.0f;
+                    float u[4];
+                    int k = material_sample_dims_t(type, wil);
+                    for (int j = 0; j < k; j++) u[j] = next_float(rng, S.sobol1);
+                    float3 wol;
+                    float bp;
+                    float3 wt = material_sample_t(type, wil, u, m, h, wol, bp);
+                    if (!(bp <= 0.0f || (wt.x == 0.0f && wt.y == 0.0f && wt.z == 0.0f))) {
+                        float3 ww = to_world(wol, T, B, N);
+                        float3 on = type == PT_MAT_HAIR ? (dot(ww, Ng) >= 0.0f ? Ng : -Ng) : Ng;
+                        no = offset_origin(hp, on, on);
+                        nd = ww;
+                        thr *= wt;
+                        lastPdf = mx(bp, 1e-20f);
                         cont = true;
-                        st.w &= ~kFlagRough;
-                    } else if (type == PT_MAT_DIELECTRIC) {  // Shaders.hlsl:429-472
-                        float es;
-                        nd = delta_scatter(PT_MAT_DIELECTRIC, rd, N, back, m.intIOR, m.extIOR,
-                                           next_float(rng, S.sobol1), es);
-                        no = hp + (dot(nd, Ng) > 0.0f ? Ng : -Ng) * 0.001f;
-                        lastPdf = 0.0f;
-                        eta *= es;
-                        cont = true;
-                        st.w &= ~kFlagRough;
-                    } else if (C != CLS_DELTA &&
-                               (type == PT_MAT_DIFFUSE || type == PT_MAT_MICROFACET || type == PT_MAT_DISNEY ||
-                                type == PT_MAT_HAIR)) {  // Shaders.hlsl:473-511
-                        float3 ra = ((INLINE || EXTRA) && A.risNee)
-                                        ? nee_ris<INLINE, EXTRA>(A, hp, N, Ng, T, B, wil, type, m, h, rng, neeA, aseed, st.z)
-                                        : nee_area<INLINE, EXTRA>(A, hp, N, Ng, T, B, wil, type, m, h, rng, neeA, aseed, st.z);
-                        float3 re = nee_env<INLINE, EXTRA>(A, hp, N, Ng, T, B, wil, type, m, h, rng, neeE, aseed, st.z);
-                        if (INLINE) {
-                            Lo += thr * ra;
-                            Lo += thr * re;
-                        } else {
-                            thrNee = thr;
-                            if (!neeA.ray) A.pendA[slot] = make_float4(thr.x * 0.0f, thr.y * 0.0f, thr.z * 0.0f, 0.0f);
-                            if (!neeE.ray) A.pendE[slot] = make_float4(thr.x * 0.0f, thr.y * 0.0f, thr.z * 0.0f, 0.0f);
-                            st.w |= kFlagPending;
-                        }
-                        float u[4];
-                        int k = material_sample_dims_t(type, wil);
-                        for (int j = 0; j < k; j++) u[j] = next_float(rng, S.sobol1);
-                        float3 wol;
-                        float bp;
-                        float3 wt = material_sample_t(type, wil, u, m, h, wol, bp);
-                        if (!(bp <= 0.0f || (wt.x == 0.0f && wt.y == 0.0f && wt.z == 0.0f))) {
-                            float3 ww = to_world(wol, T, B, N);
-                            float3 on = type == PT_MAT_HAIR ? (dot(ww, Ng) >= 0.0f ? Ng : -Ng) : Ng;
-                            no = offset_origin(hp, on, on);
-                            nd = ww;
-                            thr *= wt;
-                            lastPdf = mx(bp, 1e-20f);
+                        if (A.cacheOn) st.w = rough_bounce(A, type, m) ? (st.w | kFlagRough) : (st.w & ~kFlagRough);
+                    }
+                } else if (C == CLS_ANY && type == PT_MAT_SUBSURFACE) {  // Shaders.hlsl:515-611
+                    // rough dielectric entry (Beckmann half vector, Fresnel choice),
+                    // NEE with the entry lobe, then reflect or walk the interior
+                    const float3 I = rd;
+                    m.roughness = m.roughness * (1.0f + sat(m.specular * 2.0f) * (0.65f - 1.0f));
+                    const float rough = m.roughness;
+                    const float aR = mx(rough * rough, 1e-4f);
+                    float3 wmL = make_float3(0.0f, 0.0f, 1.0f);
+                    if (rough > 1e-3f) {
+                        float u0 = next_float(rng, S.sobol1), u1 = next_float(rng, S.sobol1);
+                        wmL = beckmann_sample(u0, u1, aR);
+                    }
+                    float3 wm = normalize(to_world(wmL, T, B, N));
+                    float cosThetaM = dot(-I, wm);
+                    if (cosThetaM <= 0.0f) {
+                        wm = N;
+                        wmL = make_float3(0.0f, 0.0f, 1.0f);
+                        cosThetaM = dot(-I, N);
+                    }
+                    const float G1i = rough > 1e-3f ? smith_g1(wil, wmL, aR) : 1.0f;
+                    const float Fr = fresnel(cosThetaM, m.extIOR, m.intIOR);
+                    Lo += thr * nee_area<INLINE>(A, hp, N, Ng, T, B, wil, type, m, h, rng, neeA, aseed, st.z);
+                    Lo += thr * nee_env<INLINE>(A, hp, N, Ng, T, B, wil, type, m, h, rng, neeE, aseed, st.z);
+                    if (next_float(rng, S.sobol1) < Fr) {
+                        float3 refl = reflect(I, wm);
+                        float3 woL = to_local(refl, T, B, N);
+                        if (woL.z > 0.0f) {  // else reflected below the surface: the path ends
+                            float weight = rough > 1e-3f ? G1i * smith_g1(woL, wmL, aR) * cosThetaM /
+                                                               mx(wil.z * wmL.z, 1e-6f)
+                                                         : 1.0f;
+                            float pdfSpec = rough > 1e-3f
+                                                ? Fr * beckmann_d_cos(wmL, aR) / mx(4.0f * cosThetaM, 1e-6f)
+                                                : 0.0f;
+                            no = hp + Ng * 0.001f;
+                            nd = refl;
+                            thr = thr * weight;
+                            lastPdf = pdfSpec;
                             cont = true;
-                            if (A.cacheOn) st.w = rough_bounce(A, type, m) ? (st.w | kFlagRough) : (st.w & ~kFlagRough);
                         }
-                    } else if (C == CLS_ANY && type == PT_MAT_SUBSURFACE) {  // Shaders.hlsl:515-611
-                        // rough dielectric entry (Beckmann half vector, Fresnel choice),
-                        // NEE with the entry lobe, then reflect or walk the interior
-                        const float3 I = rd;
-                        m.roughness = m.roughness * (1.0f + sat(m.specular * 2.0f) * (0.65f - 1.0f));
-                        const float rough = m.roughness;
-                        const float aR = mx(rough * rough, 1e-4f);
-                        float3 wmL = make_float3(0.0f, 0.0f, 1.0f);
-                        if (rough > 1e-3f) {
-                            float u0 = next_float(rng, S.sobol1), u1 = next_float(rng, S.sobol1);
-                            wmL = beckmann_sample(u0, u1, aR);
-                        }
-                        float3 wm = normalize(to_world(wmL, T, B, N));
-                        float cosThetaM = dot(-I, wm);
-                        if (cosThetaM <= 0.0f) {
-                            wm = N;
-                            wmL = make_float3(0.0f, 0.0f, 1.0f);
-                            cosThetaM = dot(-I, N);
-                        }
-                        const float G1i = rough > 1e-3f ? smith_g1(wil, wmL, aR) : 1.0f;
-                        const float Fr = fresnel(cosThetaM, m.extIOR, m.intIOR);
-                        Lo += thr * nee_area<INLINE>(A, hp, N, Ng, T, B, wil, type, m, h, rng, neeA, aseed, st.z);
-                        Lo += thr * nee_env<INLINE>(A, hp, N, Ng, T, B, wil, type, m, h, rng, neeE, aseed, st.z);
-                        if (next_float(rng, S.sobol1) < Fr) {
-                            float3 refl = reflect(I, wm);
-                            float3 woL = to_local(refl, T, B, N);
-                            if (woL.z > 0.0f) {  // else reflected below the surface: the path ends
-                                float weight = rough > 1e-3f ? G1i * smith_g1(woL, wmL, aR) * cosThetaM /
-                                                                   mx(wil.z * wmL.z, 1e-6f)
-                                                             : 1.0f;
-                                float pdfSpec = rough > 1e-3f
-                                                    ? Fr * beckmann_d_cos(wmL, aR) / mx(4.0f * cosThetaM, 1e-6f)
-                                                    : 0.0f;
-                                no = hp + Ng * 0.001f;
-                                nd = refl;
-                                thr = thr * weight;
-                                lastPdf = pdfSpec;
-                                cont = true;
-                            }
+                    } else {
+                        float3 refr = refract(I, wm, m.extIOR / m.intIOR);
+                        if (dot(refr, refr) < 1e-8f) {
+                            no = hp + Ng * 0.001f;
+                            nd = reflect(I, wm);
+                            lastPdf = 0.0f;
+                            cont = true;
                         } else {
-                            float3 refr = refract(I, wm, m.extIOR / m.intIOR);
-                            if (dot(refr, refr) < 1e-8f) {
-                                no = hp + Ng * 0.001f;
-                                nd = reflect(I, wm);
+                            const float3 tint = make_float3(m.sheen, m.sheenTint, m.clearcoat);
+                            const float3 aSharp = make_float3(m.albedo[0], m.albedo[1], m.albedo[2]);
+                            float3 aBlur = aSharp, detail = v3(1.0f);
+                            if (m.albedoTexIndex != PT_NO_TEXTURE) {  // albedo blurred 4 mip levels up
+                                const uint2 wh = path_image(A, slot);
+                                const float foot = uv_footprint(S, mesh, prim, h4.x, wh.x, wh.y);
+                                const float2 tuv = interp_uv(S, i0, i1, i2, bx, by);
+                                float4 cb = tex_sample(S, m.albedoTexIndex, tuv.x, tuv.y,
+                                                       tex_lod(S, m.albedoTexIndex, foot) + 4.0f);
+                                aBlur = make_float3(cb.x, cb.y, cb.z);
+                                float3 r = aSharp / vmax(aBlur, v3(1e-3f));
+                                detail = make_float3(clampf(r.x, 0.5f, 2.0f), clampf(r.y, 0.5f, 2.0f),
+                                                     clampf(r.z, 0.5f, 2.0f));
+                            }
+                            float sigmaT;
+                            float3 alb;
+                            subsurface_params(aBlur * tint, m.subsurface, sigmaT, alb);
+                            float3 ep, ed, en, tm;
+                            if (subsurface_walk(A, hp - Ng * 0.001f, normalize(refr), mesh, sigmaT, alb,
+                                                m.anisotropic, m.intIOR, m.extIOR, rng, aseed, st.z, ep, ed, en,
+                                                tm)) {
+                                thr *= tm * detail;
+                                no = offset_origin(ep, en, en);
+                                nd = ed;
                                 lastPdf = 0.0f;
                                 cont = true;
-                            } else {
-                                const float3 tint = make_float3(m.sheen, m.sheenTint, m.clearcoat);
-                                const float3 aSharp = make_float3(m.albedo[0], m.albedo[1], m.albedo[2]);
-                                float3 aBlur = aSharp, detail = v3(1.0f);
-                                if (m.albedoTexIndex != PT_NO_TEXTURE) {  // albedo blurred 4 mip levels up
-                                    const uint2 wh = path_image(A, slot);
-                                    const float foot = uv_footprint(S, mesh, prim, h4.x, wh.x, wh.y);
-                                    const float2 tuv = interp_uv(S, i0, i1, i2, bx, by);
-                                    float4 cb = tex_sample(S, m.albedoTexIndex, tuv.x, tuv.y,
-                                                           tex_lod(S, m.albedoTexIndex, foot) + 4.0f);
-                                    aBlur = make_float3(cb.x, cb.y, cb.z);
-                                    float3 r = aSharp / vmax(aBlur, v3(1e-3f));
-                                    detail = make_float3(clampf(r.x, 0.5f, 2.0f), clampf(r.y, 0.5f, 2.0f),
-                                                         clampf(r.z, 0.5f, 2.0f));
-                                }
-                                float sigmaT;
-                                float3 alb;
-                                subsurface_params(aBlur * tint, m.subsurface, sigmaT, alb);
-                                float3 ep, ed, en, tm;
-                                if (subsurface_walk(A, hp - Ng * 0.001f, normalize(refr), mesh, sigmaT, alb,
-                                                    m.anisotropic, m.intIOR, m.extIOR, rng, aseed, st.z, ep, ed, en,
-                                                    tm)) {
-                                    thr *= tm * detail;
-                                    no = offset_origin(ep, en, en);
-                                    nd = ed;
-                                    lastPdf = 0.0f;
-                                    cont = true;
-                                }
                             }
                         }
                     }
                 }
             }
-            // Russian roulette after bounce 3 (Shaders.hlsl:620-626)
-            if (cont && st.z >= 3u) {
-                float q = mn(maxc(thr) * eta * eta, 0.95f);
-                if (next_float(rng, S.sobol1) >= q) cont = false;
-                else thr = thr / v3(q);
-            }
-            st.z += 1u;
-            if (st.z >= path_depth(A, slot)) cont = false;
-            st.x = rng.dim;
-            st.y = rng.white;
-            // a finished path's throughput is read by nothing, and its RNG
-            // state only by the shadow kernel's alpha tests and the cache's
-            // target pass
-            if (cont) A.thr_pdf[slot] = make_float4(thr.x, thr.y, thr.z, lastPdf);
-            // w = eta, negative while NEE of this bounce is pending: the film
-            // reads the flag here instead of the path's RNG state
-            A.lo_eta[slot] = make_float4(Lo.x, Lo.y, Lo.z, (st.w & kFlagPending) ? -eta : eta);
-            if (cont || S.hasAlpha || A.cacheOn) A.rng[slot] = st;
         }
+        // Russian roulette after bounce 3 (Shaders.hlsl:620-626)
+        if (cont && st.z >= 3u) {
+            float q = mn(maxc(thr) * eta * eta, 0.95f);
+            if (next_float(rng, S.sobol1) >= q) cont = false;
+            else thr = thr / v3(q);
+        }
+        st.z += 1u;
+        if (st.z >= path_depth(A, slot)) cont = false;
+        st.x = rng.dim;
+        st.y = rng.white;
+        // a finished path's throughput is read by nothing, and its RNG
+        // state only by the shadow kernel's alpha tests and the cache's
+        // target pass
+        if (cont) A.thr_pdf[slot] = make_float4(thr.x, thr.y, thr.z, lastPdf);
+        // w = eta, negative while NEE of this bounce is pending: the film
+        // reads the flag here instead of the path's RNG state
+        A.lo_eta[slot] = make_float4(Lo.x, Lo.y, Lo.z, (st.w & kFlagPending) ? -eta : eta);
+        if (cont || S.hasAlpha || A.cacheOn) A.rng[slot] = st;
+    }
+    O.cont = cont;
+    O.slot = slot;
+    O.no = no;
+    O.nd = nd;
+    O.ntmin = ntmin;
+    O.neeA = neeA;
+    O.neeE = neeE;
+    O.thrNee = thrNee;
+}
+template <bool INLINE, int CLS, bool EXTRA = false>
+__global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveArgs A) {
+    uint32_t n = CLS == CLS_ANY ? *(volatile uint32_t *)A.cntIn : *(volatile uint32_t *)(A.cntCls + CLS);
+    uint32_t iters = (n + gridDim.x * blockDim.x - 1) / (gridDim.x * blockDim.x);
+    uint32_t traced = 0;
+    for (uint32_t it = 0; it < iters; it++) {
+        uint32_t q = (it * gridDim.x + blockIdx.x) * blockDim.x + threadIdx.x;
+        bool active = q < n;
+        uint32_t i = q;
+        if (CLS != CLS_ANY && active) i = A.cls[(size_t)(CLS < 0 ? 0 : CLS) * A.clsStride + q];
+        ShadeOut O;
+        shade_item<INLINE, CLS, EXTRA>(A, active, i, O);
         if (!INLINE) {
-            push_shadow(A, active && neeA.ray, slot, 0u, neeA, thrNee);
-            push_shadow(A, active && neeE.ray, slot, 1u, neeE, thrNee);
+            push_shadow(A, active && O.neeA.ray, O.slot, 0u, O.neeA, O.thrNee);
+            push_shadow(A, active && O.neeE.ray, O.slot, 1u, O.neeE, O.thrNee);
+        } else if (active) {
+            traced += (O.neeA.traced ? 1u : 0u) + (O.neeE.traced ? 1u : 0u);
         }
-        uint32_t pos = warp_append(A.cntOut, active && cont);
-        if (active && cont) {
-            A.qslotOut[pos] = slot;
-            A.qoOut[pos] = make_float4(no.x, no.y, no.z, ntmin);
-            A.qdOut[pos] = make_float4(nd.x, nd.y, nd.z, 1e20f);
+        uint32_t pos = warp_append(A.cntOut, active && O.cont);
+        if (active && O.cont) {
+            A.qslotOut[pos] = O.slot;
+            A.qoOut[pos] = make_float4(O.no.x, O.no.y, O.no.z, O.ntmin);
+            A.qdOut[pos] = make_float4(O.nd.x, O.nd.y, O.nd.z, 1e20f);
         }
     }
+    if (INLINE) add_rays(A, 1, traced);
+}
+
+// ---- the tail of a wave: its remaining bounces in one launch --------------------
+// From bounce PT_TAIL_BOUNCE on a wave carries few paths, but every bounce's
+// kernels still last as long as their slowest ray (about 0.23 ms per bounce
+// of the bench frame, 12 bounces of 16).  k_tail runs each path left at that
+// bounce to its end in one thread: closest hit, then the inline shading of
+// the run-time dispatched class (NEE traced inline: the numbers the deferred
+// form draws, in the same order), the next ray kept in the path's own queue
+// position.  0 = the wavefront to the last bounce.
+#ifndef PT_TAIL_BOUNCE
+#define PT_TAIL_BOUNCE 4
+#endif
+constexpr uint32_t kTailBounce = PT_TAIL_BOUNCE;
+__global__ void __launch_bounds__(kBlock, 2) k_tail(WaveArgs A) {
+    const uint32_t n = *(volatile uint32_t *)A.cntIn;
+    PT_QUEUE_STACK(K)
+    uint32_t ext = 0, traced = 0;
+    for (uint32_t base; (base = claim32(A.stealExt)) < n;) {
+        const uint32_t i = base + lane_id();
+        bool live = i < n;
+        while (live) {  // each lane its own path
+            extend_one<false, false>(A, i, K);
+            ++ext;
+            ShadeOut O;
+            shade_item<true, CLS_ANY, false>(A, true, i, O);
+            traced += (O.neeA.traced ? 1u : 0u) + (O.neeE.traced ? 1u : 0u);
+            live = O.cont;
+            if (live) {
+                A.qoIn[i] = make_float4(O.no.x, O.no.y, O.no.z, O.ntmin);
+                A.qdIn[i] = make_float4(O.nd.x, O.nd.y, O.nd.z, 1e20f);
+            }
+        }
+    }
+    add_rays(A, 0, ext);
+    add_rays(A, 1, traced);
+    for (int o = 16; o > 0; o >>= 1) ext += __shfl_xor_sync(0xFFFFFFFFu, ext, o);
+    if (lane_id() == 0 && ext) atomicAdd(A.tailRays, (unsigned long long)ext);
 }
 
 // ---- film: Kahan-compensated accumulation of (L, 1), samples in order -------
@@ -1292,11 +1373,19 @@ struct ShadeTable {
 const Kernel *const kShadeCls = ShadeTable<false>::k;
 const Kernel *const kShadeClsX = ShadeTable<true>::k;
 int gExt = 0, gExtC = 0, gExtM = 0, gShadeI = 0, gShadow = 0, gShadowM = 0, gCls[CLS_N], gClsX[CLS_N];
+int gTail = 0;
 
 // STG_CACHE_INFER / STG_CACHE_TRAIN: the cache's network kernels, reported
 // in ms_cache with the rest of the cache's work and on their own in the
 // cache statistics
-enum { STG_RAYGEN, STG_EXTEND, STG_SHADE, STG_SHADOW, STG_FILM, STG_CACHE, STG_CACHE_INFER, STG_CACHE_TRAIN, STG_N };
+enum {
+    STG_RAYGEN, STG_EXTEND, STG_SHADE, STG_SHADOW, STG_FILM, STG_CACHE, STG_CACHE_INFER, STG_CACHE_TRAIN, STG_TAIL,
+    STG_N
+};
+// The bounce from which a wave's remaining paths run in k_tail (depth: never).
+__host__ __device__ inline uint32_t tail_bounce(uint32_t depth, const WaveArgs &A) {
+    return (kTailBounce > 0 && kTailBounce < depth && !A.cacheOn && !A.S.mediaWavefront) ? kTailBounce : depth;
+}
 struct Mark { int stage; cudaEvent_t a, b; };
 
 // Issues one render's work on a stream: directly (optionally with an event
@@ -1324,6 +1413,7 @@ struct Enqueue {
 struct Grids {
     int ext, extC, extM, shadeI, shadow, shadowM;
     const int *cls, *clsX;
+    int tail;
 };
 
 // Raygen and `depth` bounces of one wave (A.waveStart / A.waveCount set).
@@ -1348,6 +1438,12 @@ cudaError_t enqueue_paths(const pt_ctx *ctx, Enqueue &E, WaveArgs &A, uint32_t d
         A.cntOut = B.counters + (1 - cur);
         chk(cudaMemsetAsync(A.cntOut, 0, 4, st));
         chk(cudaMemsetAsync(A.cntShadow, 0, 8, st));  // shadow count and the extend claim position
+        if (b == tail_bounce(depth, A)) {  // the remaining bounces of every path in one launch
+            E.begin(STG_TAIL);
+            k_tail<<<G.tail, kBlock, 0, st>>>(A);
+            E.end();
+            break;
+        }
         if (inl) {
             E.begin(STG_EXTEND);
             k_extend<false><<<G.ext, kBlock, 0, st>>>(A);
@@ -1391,7 +1487,7 @@ cudaError_t enqueue_render(const pt_ctx *ctx, Enqueue &E, WaveArgs A, const pt_r
         if (err == cudaSuccess && e != cudaSuccess) err = e;
     };
     const bool cached = A.cacheOn != 0;
-    const Grids G{gExt, gExtC, gExtM, gShadeI, gShadow, gShadowM, gCls, gClsX};
+    const Grids G{gExt, gExtC, gExtM, gShadeI, gShadow, gShadowM, gCls, gClsX, gTail};
     chk(cudaMemsetAsync(B.counters, 0, kCounterWords * sizeof(uint32_t), st));
     chk(cudaMemsetAsync(ctx->d_err, 0, 4, st));
     if (cached) {  // per-call cache counters: records [2], queries of the call [5], records with targets [6]
@@ -1501,6 +1597,7 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
             gCls[c] = grid_for(ctx, (const void *)kShadeCls[c]);
             gClsX[c] = grid_for(ctx, (const void *)kShadeClsX[c]);
         }
+        gTail = grid_for(ctx, (const void *)k_tail);
     }
     WaveArgs A;
     A.S = ctx->S;
@@ -1518,6 +1615,7 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
     A.cls = B.cls;
     A.clsStride = (uint32_t)B.cap;
     A.rayTotals = (unsigned long long *)(B.counters + 4);
+    A.tailRays = (unsigned long long *)(B.counters + kCntTailRays);
     A.err = ctx->d_err;
     A.shadowCap = (uint32_t)(2 * B.cap);
     if (ctx->dbgShadowCap) A.shadowCap = std::min(A.shadowCap, ctx->dbgShadowCap);
@@ -1628,7 +1726,7 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
         stats->extension_rays = tot[0];
         stats->shadow_rays = tot[1];
         stats->waves = waves;
-        stats->bounces = waves * P->max_depth;
+        stats->bounces = waves * tail_bounce(P->max_depth, A);
         stats->launches = launches;
         stats->ms_total = ms;
         stats->ms_raygen = stage[STG_RAYGEN];
@@ -1637,6 +1735,8 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
         stats->ms_shadow = stage[STG_SHADOW];
         stats->ms_film = stage[STG_FILM];
         stats->ms_cache = stage[STG_CACHE] + stage[STG_CACHE_INFER] + stage[STG_CACHE_TRAIN];
+        stats->ms_tail = stage[STG_TAIL];
+        memcpy(&stats->tail_extension_rays, hostCnt + kCntTailRays, 8);
         if (timing && A.cacheOn) {
             ctx->cache.renderInferMs = stage[STG_CACHE_INFER];
             ctx->cache.renderTrainMs = stage[STG_CACHE_TRAIN];
@@ -1795,6 +1895,7 @@ int render_batch(pt_ctx *ctx, const pt_request *R, uint32_t n, float *request_ms
             gCls[c] = grid_for(ctx, (const void *)kShadeCls[c]);
             gClsX[c] = grid_for(ctx, (const void *)kShadeClsX[c]);
         }
+        gTail = grid_for(ctx, (const void *)k_tail);
     }
     if (gridScale <= 0.0f) gridScale = (Bt.tunedWave && Bt.tunedSceneGen == ctx->sceneGen) ? Bt.tunedGrid : 1.0f;
     auto sc = [&](int g) { return std::max(ctx->numSMs, (int)((float)g * gridScale)); };
@@ -1803,7 +1904,7 @@ int render_batch(pt_ctx *ctx, const pt_request *R, uint32_t n, float *request_ms
         clsG[c] = sc(gCls[c]);
         clsGX[c] = sc(gClsX[c]);
     }
-    const Grids G{sc(gExt), sc(gExtC), sc(gExtM), sc(gShadeI), sc(gShadow), sc(gShadowM), clsG, clsGX};
+    const Grids G{sc(gExt), sc(gExtC), sc(gExtM), sc(gShadeI), sc(gShadow), sc(gShadowM), clsG, clsGX, sc(gTail)};
 
     const BatchPlan pl = batch_plan(R, n, cap);
     // films: the callers' device films, device copies of host films, or the tuning scratch
@@ -1867,6 +1968,7 @@ int render_batch(pt_ctx *ctx, const pt_request *R, uint32_t n, float *request_ms
     A.cls = B.cls;
     A.clsStride = (uint32_t)B.cap;
     A.rayTotals = (unsigned long long *)(B.counters + 4);
+    A.tailRays = (unsigned long long *)(B.counters + kCntTailRays);
     A.err = ctx->d_err;
     A.shadowCap = (uint32_t)(2 * B.cap);
     A.batch = 1; A.numReqs = n; A.reqs = (const ReqDev *)Bt.reqs; A.slotInfo = Bt.slotInfo;
@@ -1959,10 +2061,11 @@ int render_batch(pt_ctx *ctx, const pt_request *R, uint32_t n, float *request_ms
         stats->shadow_rays = tot[1];
         stats->waves = pl.waveStart.size();
         uint64_t bounces = 0;
-        for (uint32_t d : pl.waveDepth) bounces += d;
+        for (uint32_t d : pl.waveDepth) bounces += tail_bounce(d, A);
         stats->bounces = bounces;
         stats->launches = Bt.launches;
         stats->ms_total = ms;
+        memcpy(&stats->tail_extension_rays, hostCnt + kCntTailRays, 8);
     }
     return PT_OK;
 }
