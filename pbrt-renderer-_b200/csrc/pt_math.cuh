@@ -199,15 +199,45 @@ PT_HD float fresnel(float cosI, float etaI, float etaT) {  // :200-219
 // reflects with probability Fr, else refracts (reflecting on total internal
 // reflection); etaScale is etaI / etaT after a refraction, else 1.  Delta
 // BSDFs leave the throughput unchanged and have no pdf (lastBsdfPdf = 0).
+// Every product and sum of the delta branch rounded on its own, in the
+// oracle's order (no contraction): the result is the oracle's float32 value,
+// and the same in every kernel that inlines it.
+PT_HD float dot_nf(float3 a, float3 b) { return radd(radd(rmul(a.x, b.x), rmul(a.y, b.y)), rmul(a.z, b.z)); }
+PT_HD float3 axpy_nf(float s, float3 x, float3 y) {  // s * x + y
+    return make_float3(radd(rmul(s, x.x), y.x), radd(rmul(s, x.y), y.y), radd(rmul(s, x.z), y.z));
+}
+PT_HD float3 reflect_nf(float3 i, float3 n) {  // i - 2 dot(n, i) n
+    const float k = rmul(2.0f, dot_nf(n, i));
+    return make_float3(rsub(i.x, rmul(k, n.x)), rsub(i.y, rmul(k, n.y)), rsub(i.z, rmul(k, n.z)));
+}
+PT_HD float3 refract_nf(float3 i, float3 n, float eta) {  // eta i - (eta dot(n, i) + sqrt(k)) n
+    const float ndi = dot_nf(n, i);
+    const float k = rsub(1.0f, rmul(rmul(eta, eta), rsub(1.0f, rmul(ndi, ndi))));
+    if (k < 0.0f) return v3(0.0f);
+    const float c = radd(rmul(eta, ndi), sqrtf(k));
+    return make_float3(rsub(rmul(eta, i.x), rmul(c, n.x)), rsub(rmul(eta, i.y), rmul(c, n.y)),
+                       rsub(rmul(eta, i.z), rmul(c, n.z)));
+}
+PT_HD float fresnel_nf(float cosI, float etaI, float etaT) {  // :200-219
+    if (etaI == etaT) return 0.0f;
+    if (cosI < 0.0f) { float t = etaI; etaI = etaT; etaT = t; cosI = -cosI; }
+    float eta = etaI / etaT;
+    float s2 = rmul(rmul(eta, eta), rsub(1.0f, rmul(cosI, cosI)));
+    if (s2 > 1.0f) return 1.0f;
+    float cosT = sqrtf(rsub(1.0f, s2));
+    float Rs = rsub(rmul(etaI, cosI), rmul(etaT, cosT)) / radd(rmul(etaI, cosI), rmul(etaT, cosT));
+    float Rp = rsub(rmul(etaT, cosI), rmul(etaI, cosT)) / radd(rmul(etaT, cosI), rmul(etaI, cosT));
+    return rmul(0.5f, radd(rmul(Rs, Rs), rmul(Rp, Rp)));
+}
 PT_HD float3 delta_scatter(uint32_t type, float3 rd, float3 N, bool back, float intIOR, float extIOR, float u,
                            float &etaScale) {
     etaScale = 1.0f;
-    if (type == PT_MAT_MIRROR) return reflect(rd, N);
+    if (type == PT_MAT_MIRROR) return reflect_nf(rd, N);
     float etaI = back ? intIOR : extIOR, etaT = back ? extIOR : intIOR;
-    float Fr = fresnel(dot(-rd, N), etaI, etaT);
-    if (u < Fr) return reflect(rd, N);
-    float3 nd = refract(rd, N, etaI / etaT);
-    if (dot(nd, nd) < 0.001f) return reflect(rd, N);
+    float Fr = fresnel_nf(dot_nf(-rd, N), etaI, etaT);
+    if (u < Fr) return reflect_nf(rd, N);
+    float3 nd = refract_nf(rd, N, etaI / etaT);
+    if (dot_nf(nd, nd) < 0.001f) return reflect_nf(rd, N);
     etaScale = etaI / etaT;
     return nd;
 }

@@ -71,6 +71,7 @@ struct WaveArgs {
     uint32_t clsStride;
     unsigned long long *rayTotals;  // [0] extension, [1] shadow
     unsigned long long *tailRays;   // extension rays of k_tail (also in rayTotals[0])
+    uint32_t tailMax;               // k_tail takes a wave's paths when at most this many are left
     uint32_t *err;
     uint32_t shadowCap;
     // radiance cache (cacheOn == 0: plain path tracing)
@@ -1015,8 +1016,9 @@ __device__ __forceinline__ void shade_item(const WaveArgs &A, bool active, uint3
                 }
                 float3 wil = to_local(-rd, T, B, N);
                 if (type == PT_MAT_MIRROR) {  // Shaders.hlsl:419-427
-                    nd = reflect(rd, N);
-                    no = hp + Ng * 0.001f;
+                    float es;
+                    nd = delta_scatter(PT_MAT_MIRROR, rd, N, back, m.intIOR, m.extIOR, 0.0f, es);
+                    no = axpy_nf(0.001f, Ng, hp);
                     lastPdf = 0.0f;
                     cont = true;
                     st.w &= ~kFlagRough;
@@ -1024,7 +1026,7 @@ __device__ __forceinline__ void shade_item(const WaveArgs &A, bool active, uint3
                     float es;
                     nd = delta_scatter(PT_MAT_DIELECTRIC, rd, N, back, m.intIOR, m.extIOR,
                                        next_float(rng, S.sobol1), es);
-                    no = hp + (dot(nd, Ng) > 0.0f ? Ng : -Ng) * 0.001f;
+                    no = axpy_nf(0.001f, dot_nf(nd, Ng) > 0.0f ? Ng : -Ng, hp);
                     lastPdf = 0.0f;
                     eta *= es;
                     cont = true;
@@ -1197,19 +1199,81 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
 }
 
 // ---- the tail of a wave: its remaining bounces in one launch --------------------
-// From bounce PT_TAIL_BOUNCE on a wave carries few paths, but every bounce's
+// From bounce PT_TAIL_BOUNCE on a wave may carry few paths, but every bounce's
 // kernels still last as long as their slowest ray (about 0.23 ms per bounce
-// of the bench frame, 12 bounces of 16).  k_tail runs each path left at that
-// bounce to its end in one thread: closest hit, then the inline shading of
-// the run-time dispatched class (NEE traced inline: the numbers the deferred
-// form draws, in the same order), the next ray kept in the path's own queue
-// position.  0 = the wavefront to the last bounce.
+// of the bench frame, 12 bounces of 16).  When at most kTailMaxPaths paths
+// are left, k_tail runs each to its end in one thread, its next ray kept in
+// the path's own queue position, and k_tail_close empties the queue so the
+// per-bounce kernels that follow (launched either way) find nothing; with
+// more paths left k_tail returns at once and the per-bounce kernels go on.
+// The result does not depend on which runs: the tail calls the same shading
+// instantiations as the per-bounce kernels — the class-specialized ones, with
+// each deferred NEE ray resolved in place with k_shadow's arithmetic, or for
+// scenes shaded inline the inline one — in the same order per path.
+// 0 = no tail.
 #ifndef PT_TAIL_BOUNCE
 #define PT_TAIL_BOUNCE 4
 #endif
 constexpr uint32_t kTailBounce = PT_TAIL_BOUNCE;
+constexpr uint32_t kTailMaxPaths = 1u << 18;
+
+// A deferred NEE ray of a shading event, resolved here as k_shadow resolves a
+// queued one (its default instantiation): the pending record for the path's
+// next shading event or the film.
+template <class Stack>
+__device__ __forceinline__ void tail_shadow(const WaveArgs &A, Stack &K, uint32_t slot, uint32_t kind, const NeeOut &ne,
+                                            float3 thr) {
+    uint32_t aseed = 0, akey = 0;
+    if (A.S.hasAlpha) {  // the shading event already advanced the path's bounce counter
+        Rng r = load_rng(A, slot, A.rng[slot]);
+        aseed = alpha_seed(r.pixelSeed, r.sampleIndex);
+        akey = alpha_key(A.rng[slot].z - 1u, kind ? 2u : 1u);
+    }
+    float3 tr;
+    bool occ = trace_shadow_on(K, A.S, ne.o, ne.d, ne.tmin, ne.tmax, tr, A.err, aseed, akey);
+    float3 R = occ ? thr * v3(0.0f) : thr * (ne.X * tr);
+    float4 out = make_float4(R.x, R.y, R.z, 0.0f);
+    if (kind) __stcs(A.pendE + slot, out);
+    else __stcs(A.pendA + slot, out);
+}
+// One shading event of queue position i with the per-bounce kernels' code.
+template <bool INLINE, class Stack>
+__device__ __forceinline__ void tail_shade(const WaveArgs &A, Stack &K, uint32_t i, ShadeOut &O, uint32_t &traced) {
+    if (INLINE) {
+        shade_item<true, CLS_ANY, false>(A, true, i, O);
+        traced += (O.neeA.traced ? 1u : 0u) + (O.neeE.traced ? 1u : 0u);
+        return;
+    }
+    const uint32_t gid = __float_as_uint(A.qhit[i].y);
+    const int c = gid == 0xFFFFFFFFu ? (int)CLS_MISS : (int)__ldg(A.S.meshClass + __ldg(A.S.triMesh + gid));
+    switch (c) {
+        case CLS_MISS: shade_item<false, CLS_MISS, false>(A, true, i, O); break;
+        case CLS_EMIT: shade_item<false, CLS_EMIT, false>(A, true, i, O); break;
+        case CLS_DELTA: shade_item<false, CLS_DELTA, false>(A, true, i, O); break;
+        case CLS_DIFFUSE: shade_item<false, CLS_DIFFUSE, false>(A, true, i, O); break;
+        case CLS_MICRO: shade_item<false, CLS_MICRO, false>(A, true, i, O); break;
+        case CLS_DISNEY: shade_item<false, CLS_DISNEY, false>(A, true, i, O); break;
+        case CLS_HAIR: shade_item<false, CLS_HAIR, false>(A, true, i, O); break;
+        case CLS_TEX + CLS_EMIT: shade_item<false, CLS_TEX + CLS_EMIT, false>(A, true, i, O); break;
+        case CLS_TEX + CLS_DELTA: shade_item<false, CLS_TEX + CLS_DELTA, false>(A, true, i, O); break;
+        case CLS_TEX + CLS_DIFFUSE: shade_item<false, CLS_TEX + CLS_DIFFUSE, false>(A, true, i, O); break;
+        case CLS_TEX + CLS_MICRO: shade_item<false, CLS_TEX + CLS_MICRO, false>(A, true, i, O); break;
+        case CLS_TEX + CLS_DISNEY: shade_item<false, CLS_TEX + CLS_DISNEY, false>(A, true, i, O); break;
+        default: shade_item<false, CLS_TEX + CLS_HAIR, false>(A, true, i, O); break;
+    }
+    if (O.neeA.ray) {
+        tail_shadow(A, K, O.slot, 0u, O.neeA, O.thrNee);
+        ++traced;
+    }
+    if (O.neeE.ray) {
+        tail_shadow(A, K, O.slot, 1u, O.neeE, O.thrNee);
+        ++traced;
+    }
+}
+template <bool INLINE>
 __global__ void __launch_bounds__(kBlock, 2) k_tail(WaveArgs A) {
     const uint32_t n = *(volatile uint32_t *)A.cntIn;
+    if (n > A.tailMax) return;  // uniform: the per-bounce kernels take the rest
     PT_QUEUE_STACK(K)
     uint32_t ext = 0, traced = 0;
     for (uint32_t base; (base = claim32(A.stealExt)) < n;) {
@@ -1219,8 +1283,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_tail(WaveArgs A) {
             extend_one<false, false>(A, i, K);
             ++ext;
             ShadeOut O;
-            shade_item<true, CLS_ANY, false>(A, true, i, O);
-            traced += (O.neeA.traced ? 1u : 0u) + (O.neeE.traced ? 1u : 0u);
+            tail_shade<INLINE>(A, K, i, O, traced);
             live = O.cont;
             if (live) {
                 A.qoIn[i] = make_float4(O.no.x, O.no.y, O.no.z, O.ntmin);
@@ -1232,6 +1295,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_tail(WaveArgs A) {
     add_rays(A, 1, traced);
     for (int o = 16; o > 0; o >>= 1) ext += __shfl_xor_sync(0xFFFFFFFFu, ext, o);
     if (lane_id() == 0 && ext) atomicAdd(A.tailRays, (unsigned long long)ext);
+}
+// After k_tail: if it ran, its paths are done and the queue is empty.
+__global__ void k_tail_close(WaveArgs A) {
+    if (*A.cntIn <= A.tailMax) *A.cntIn = 0u;
 }
 
 // ---- film: Kahan-compensated accumulation of (L, 1), samples in order -------
@@ -1373,7 +1440,7 @@ struct ShadeTable {
 const Kernel *const kShadeCls = ShadeTable<false>::k;
 const Kernel *const kShadeClsX = ShadeTable<true>::k;
 int gExt = 0, gExtC = 0, gExtM = 0, gShadeI = 0, gShadow = 0, gShadowM = 0, gCls[CLS_N], gClsX[CLS_N];
-int gTail = 0;
+int gTail = 0, gTailI = 0;
 
 // STG_CACHE_INFER / STG_CACHE_TRAIN: the cache's network kernels, reported
 // in ms_cache with the rest of the cache's work and on their own in the
@@ -1382,9 +1449,12 @@ enum {
     STG_RAYGEN, STG_EXTEND, STG_SHADE, STG_SHADOW, STG_FILM, STG_CACHE, STG_CACHE_INFER, STG_CACHE_TRAIN, STG_TAIL,
     STG_N
 };
-// The bounce from which a wave's remaining paths run in k_tail (depth: never).
+// The bounce at which k_tail may take a wave's remaining paths (depth: never).
+// Not for cached renders, RIS NEE or media in the wavefront form (other
+// shading instantiations).
 __host__ __device__ inline uint32_t tail_bounce(uint32_t depth, const WaveArgs &A) {
-    return (kTailBounce > 0 && kTailBounce < depth && !A.cacheOn && !A.S.mediaWavefront) ? kTailBounce : depth;
+    return (kTailBounce > 0 && kTailBounce < depth && !A.cacheOn && !A.risNee && !A.S.mediaWavefront) ? kTailBounce
+                                                                                                     : depth;
 }
 struct Mark { int stage; cudaEvent_t a, b; };
 
@@ -1413,7 +1483,7 @@ struct Enqueue {
 struct Grids {
     int ext, extC, extM, shadeI, shadow, shadowM;
     const int *cls, *clsX;
-    int tail;
+    int tail, tailI;
 };
 
 // Raygen and `depth` bounces of one wave (A.waveStart / A.waveCount set).
@@ -1438,11 +1508,12 @@ cudaError_t enqueue_paths(const pt_ctx *ctx, Enqueue &E, WaveArgs &A, uint32_t d
         A.cntOut = B.counters + (1 - cur);
         chk(cudaMemsetAsync(A.cntOut, 0, 4, st));
         chk(cudaMemsetAsync(A.cntShadow, 0, 8, st));  // shadow count and the extend claim position
-        if (b == tail_bounce(depth, A)) {  // the remaining bounces of every path in one launch
+        if (b == tail_bounce(depth, A)) {  // the remaining bounces of every path in one launch, when few are left
             E.begin(STG_TAIL);
-            k_tail<<<G.tail, kBlock, 0, st>>>(A);
+            if (inl) k_tail<true><<<G.tailI, kBlock, 0, st>>>(A);
+            else k_tail<false><<<G.tail, kBlock, 0, st>>>(A);
+            k_tail_close<<<1, 1, 0, st>>>(A);
             E.end();
-            break;
         }
         if (inl) {
             E.begin(STG_EXTEND);
@@ -1487,7 +1558,7 @@ cudaError_t enqueue_render(const pt_ctx *ctx, Enqueue &E, WaveArgs A, const pt_r
         if (err == cudaSuccess && e != cudaSuccess) err = e;
     };
     const bool cached = A.cacheOn != 0;
-    const Grids G{gExt, gExtC, gExtM, gShadeI, gShadow, gShadowM, gCls, gClsX, gTail};
+    const Grids G{gExt, gExtC, gExtM, gShadeI, gShadow, gShadowM, gCls, gClsX, gTail, gTailI};
     chk(cudaMemsetAsync(B.counters, 0, kCounterWords * sizeof(uint32_t), st));
     chk(cudaMemsetAsync(ctx->d_err, 0, 4, st));
     if (cached) {  // per-call cache counters: records [2], queries of the call [5], records with targets [6]
@@ -1547,7 +1618,7 @@ bool graph_matches(const pt_ctx *ctx, const pt_render_params *P, size_t cap, con
            G.comp == comp && G.sceneGen == ctx->sceneGen && G.waveGen == ctx->waveGen &&
            G.cached == A.cacheOn && G.trainOn == A.trainOn && (!A.cacheOn || G.cacheGen == ctx->cache.gen) &&
            G.risNee == A.risNee && G.flags == (P->flags & ~PT_RENDER_STAGE_TIMING) &&
-           G.shadowCap == A.shadowCap && G.cacheStall == ctx->dbgCacheStall &&
+           G.shadowCap == A.shadowCap && G.cacheStall == ctx->dbgCacheStall && G.tailMax == A.tailMax &&
            memcmp(&G.cam, &P->camera, sizeof(pt_camera)) == 0;
 }
 }  // namespace
@@ -1597,7 +1668,8 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
             gCls[c] = grid_for(ctx, (const void *)kShadeCls[c]);
             gClsX[c] = grid_for(ctx, (const void *)kShadeClsX[c]);
         }
-        gTail = grid_for(ctx, (const void *)k_tail);
+        gTail = grid_for(ctx, (const void *)k_tail<false>);
+        gTailI = grid_for(ctx, (const void *)k_tail<true>);
     }
     WaveArgs A;
     A.S = ctx->S;
@@ -1616,6 +1688,7 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
     A.clsStride = (uint32_t)B.cap;
     A.rayTotals = (unsigned long long *)(B.counters + 4);
     A.tailRays = (unsigned long long *)(B.counters + kCntTailRays);
+    A.tailMax = ctx->dbgTailOff ? 0u : kTailMaxPaths;
     A.err = ctx->d_err;
     A.shadowCap = (uint32_t)(2 * B.cap);
     if (ctx->dbgShadowCap) A.shadowCap = std::min(A.shadowCap, ctx->dbgShadowCap);
@@ -1673,7 +1746,7 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
             G.sceneGen = ctx->sceneGen; G.waveGen = ctx->waveGen;
             G.cached = A.cacheOn; G.trainOn = A.trainOn; G.cacheGen = ctx->cache.gen; G.risNee = A.risNee;
             G.flags = P->flags & ~PT_RENDER_STAGE_TIMING;
-            G.shadowCap = A.shadowCap; G.cacheStall = ctx->dbgCacheStall;
+            G.shadowCap = A.shadowCap; G.cacheStall = ctx->dbgCacheStall; G.tailMax = A.tailMax;
             G.launches = E.launches;
         } else {  // capture unavailable: issue the launches directly
             cudaGetLastError();
@@ -1726,7 +1799,7 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
         stats->extension_rays = tot[0];
         stats->shadow_rays = tot[1];
         stats->waves = waves;
-        stats->bounces = waves * tail_bounce(P->max_depth, A);
+        stats->bounces = waves * P->max_depth;
         stats->launches = launches;
         stats->ms_total = ms;
         stats->ms_raygen = stage[STG_RAYGEN];
@@ -1895,7 +1968,8 @@ int render_batch(pt_ctx *ctx, const pt_request *R, uint32_t n, float *request_ms
             gCls[c] = grid_for(ctx, (const void *)kShadeCls[c]);
             gClsX[c] = grid_for(ctx, (const void *)kShadeClsX[c]);
         }
-        gTail = grid_for(ctx, (const void *)k_tail);
+        gTail = grid_for(ctx, (const void *)k_tail<false>);
+        gTailI = grid_for(ctx, (const void *)k_tail<true>);
     }
     if (gridScale <= 0.0f) gridScale = (Bt.tunedWave && Bt.tunedSceneGen == ctx->sceneGen) ? Bt.tunedGrid : 1.0f;
     auto sc = [&](int g) { return std::max(ctx->numSMs, (int)((float)g * gridScale)); };
@@ -1904,7 +1978,8 @@ int render_batch(pt_ctx *ctx, const pt_request *R, uint32_t n, float *request_ms
         clsG[c] = sc(gCls[c]);
         clsGX[c] = sc(gClsX[c]);
     }
-    const Grids G{sc(gExt), sc(gExtC), sc(gExtM), sc(gShadeI), sc(gShadow), sc(gShadowM), clsG, clsGX, sc(gTail)};
+    const Grids G{sc(gExt), sc(gExtC), sc(gExtM), sc(gShadeI), sc(gShadow), sc(gShadowM), clsG, clsGX, sc(gTail),
+                  sc(gTailI)};
 
     const BatchPlan pl = batch_plan(R, n, cap);
     // films: the callers' device films, device copies of host films, or the tuning scratch
@@ -1969,6 +2044,7 @@ int render_batch(pt_ctx *ctx, const pt_request *R, uint32_t n, float *request_ms
     A.clsStride = (uint32_t)B.cap;
     A.rayTotals = (unsigned long long *)(B.counters + 4);
     A.tailRays = (unsigned long long *)(B.counters + kCntTailRays);
+    A.tailMax = ctx->dbgTailOff ? 0u : kTailMaxPaths;
     A.err = ctx->d_err;
     A.shadowCap = (uint32_t)(2 * B.cap);
     A.batch = 1; A.numReqs = n; A.reqs = (const ReqDev *)Bt.reqs; A.slotInfo = Bt.slotInfo;
@@ -1982,7 +2058,7 @@ int render_batch(pt_ctx *ctx, const pt_request *R, uint32_t n, float *request_ms
     std::vector<uint64_t> key = {n, pl.cap, R[0].params.rng_kind, R[0].params.env_sampling, R[0].params.flags,
                                  ctx->sceneGen,
                                  ctx->waveGen, (uint64_t)(uintptr_t)Bt.slotInfo, (uint64_t)(uint32_t)G.extC,
-                                 (uint64_t)(uint32_t)G.shadow, (uint64_t)(uint32_t)clsG[CLS_DISNEY]};
+                                 (uint64_t)(uint32_t)G.shadow, (uint64_t)(uint32_t)clsG[CLS_DISNEY], A.tailMax};
     for (uint32_t k = 0; k < n; k++) {
         key.push_back(hostReqs[k].width | ((uint64_t)hostReqs[k].height << 32));
         key.push_back(hostReqs[k].spp | ((uint64_t)hostReqs[k].maxDepth << 32));
@@ -2061,7 +2137,7 @@ int render_batch(pt_ctx *ctx, const pt_request *R, uint32_t n, float *request_ms
         stats->shadow_rays = tot[1];
         stats->waves = pl.waveStart.size();
         uint64_t bounces = 0;
-        for (uint32_t d : pl.waveDepth) bounces += tail_bounce(d, A);
+        for (uint32_t d : pl.waveDepth) bounces += d;
         stats->bounces = bounces;
         stats->launches = Bt.launches;
         stats->ms_total = ms;

@@ -212,3 +212,49 @@ def test_heterogeneous_media_wavefront(pt, scenes, ctx, oracle):
     for Q, (s, c) in zip(reqs, films):
         s1, c1, _ = ctx.render(Q)
         assert np.array_equal(s, s1) and np.array_equal(c, c1)
+
+
+@pytest.mark.parametrize("name", ["cornell", "spheres", "cool_scene1", "textured", "subsurface"])
+def test_tail_kernel_leaves_no_trace(name, pt, scenes):
+    """From bounce 4 on, a wave with at most 2^18 live paths runs its paths to
+    the end in one kernel; with more it stays in the per-bounce kernels.  Both
+    run the same shading code per path (the class-specialized kernels' code
+    with NEE resolved as the shadow kernel does, or the inline form for
+    subsurface scenes), so the film may not depend on which ran: the same
+    render with the tail and, through the PT_DEBUG_TAIL_OFF hook, without it,
+    equal bit for bit (and the tail checked to have traced rays).  The
+    classes covered: miss, emitter, diffuse, Disney (Cornell, spheres),
+    delta (mirror and glass), textured Disney and diffuse with an alpha
+    cut-out, and the inline form (subsurface)."""
+    if name == "cornell":
+        sc, cam = scenes.cornell(128, 128)
+        W = H = 128
+    elif name == "spheres":
+        sc, cam = scenes.disney_spheres(160, 90, grid=4, slices=32, rings=17, env_w=256, env_h=128)
+        W, H = 160, 90
+    elif name == "cool_scene1":
+        from test_reference_scenes import load_scene
+        sc, cam, _ = load_scene(pt, "cool_scene1")
+        W = H = 128
+    elif name == "textured":
+        sc, cam = scenes.textured_scene(128, 96)
+        W, H = 128, 96
+    else:
+        sc, cam = scenes.subsurface_scene(128, 128)
+        W = H = 128
+    ctx = pt.Context(0)
+    try:
+        ctx.upload(sc)
+        P = pt.render_params(W, H, 16, cam, max_depth=16, sample_offset=5)
+        a, ca, sa = ctx.render(P)
+        ctx.debug_set(pt.PT_DEBUG_TAIL_OFF, 1)
+        b, cb, sb = ctx.render(P)
+        ctx.debug_set(pt.PT_DEBUG_TAIL_OFF, 0)
+        c, cc, sc2 = ctx.render(P)
+    finally:
+        ctx.close()
+    print(name, "tail extension rays", sa.tail_extension_rays, "of", sa.extension_rays)
+    assert sa.tail_extension_rays > 0 and sb.tail_extension_rays == 0 and sc2.tail_extension_rays > 0
+    assert sa.extension_rays == sb.extension_rays and sa.shadow_rays == sb.shadow_rays
+    assert np.array_equal(a, b) and np.array_equal(ca, cb)
+    assert np.array_equal(a, c)
