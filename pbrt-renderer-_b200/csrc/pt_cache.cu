@@ -6,14 +6,17 @@
 // Kernel structure (one CTA = 128 threads = one 128-row tile per pass):
 // * the BF16 weight image (43 KB) is placed in shared memory by one bulk
 //   copy per CTA and stays there for all of the CTA's tiles;
-// * each thread encodes one row (query) into the BF16 activation tile;
+// * each thread encodes one row (query);
 // * per layer one thread issues 4 MMAs (K = 64 in steps of 16) into TMEM
 //   and commits them to an mbarrier; the 4 warps read their 32 TMEM lanes
-//   back (tcgen05.ld), apply ReLU and write the next activation tile;
-// * training keeps all six activation tiles, runs the backward pass with the
-//   same MMAs on transposed views of the same shared-memory images
-//   (K-major for dZ.W, MN-major for dZ^T.A), and accumulates the weight
-//   gradients in TMEM across the CTA's tiles before one atomic flush.
+//   back (tcgen05.ld) and apply ReLU;
+// * inference writes each layer's BF16 input to tensor memory (tcgen05.st)
+//   and reads A from there, so only the weights are read from shared memory;
+// * training keeps all six activation tiles in shared memory, runs the
+//   backward pass with the same MMAs on transposed views of the same images
+//   (K-major for dZ.W, MN-major for dZ^T.A), accumulates the weight
+//   gradients in TMEM across the CTA's tiles and stores the sum in the CTA's
+//   own slot, which a reduce kernel adds in slot order.
 // Every mbarrier wait is bounded; a timeout raises an error flag and the CTA
 // frees its tensor memory and returns.
 #include <algorithm>
@@ -29,7 +32,6 @@ namespace pt {
 constexpr int kRcThreads = 128;
 constexpr uint32_t kTileBytes = kRcTile * kRcIn * 2;  // 16 KB: one 128 x 64 BF16 tile
 constexpr uint32_t kGradBytes = 2 * kTileBytes;       // dZ tiles carry a zero upper half (M = 128 views)
-constexpr uint32_t kInferSmem = kRcImageBytes + kTileBytes + 64;
 constexpr uint32_t kTrainSmem = kRcImageBytes + 6 * kTileBytes + 2 * kGradBytes + 64;
 static_assert(kTrainSmem <= 227 * 1024, "training kernel shared memory");
 constexpr uint32_t kDevErrCache = PT_DEVERR_CACHE;
@@ -113,7 +115,7 @@ struct RcRows<1> {  // records (render queries or training records): rows phase,
 
 // ---- weight staging and TMEM set-up shared by the kernels -------------------
 struct CtaCtl {
-    uint32_t mbW, mbM, tbase, tl;
+    uint32_t mbW, mbM, tbase, td, tl;  // td: the accumulator (lane 0), tl: this warp's lanes of TMEM
     uint32_t phase;
     bool ok;
     bool copyIssued, mmaPending;  // what an error exit still has to wait for
@@ -146,6 +148,7 @@ __device__ __forceinline__ void rc_setup(CtaCtl &c, uint8_t *W, uint64_t *bars, 
     __syncthreads();
     tc_fence_after();
     c.tbase = *tslot;
+    c.td = c.tbase;
     c.tl = c.tbase + ((warp * 32u) << 16);
     c.phase = 0;
     c.ok = ok && __syncthreads_and(mbar_wait(c.mbW, 0)) != 0;  // ok is uniform across the CTA
@@ -179,7 +182,7 @@ __device__ __forceinline__ void rc_issue_forward(const CtaCtl &c, const uint8_t 
     for (int s = 0; s < 4; s++) {
         uint64_t ad = umma_desc(smem_u32(A) + s * 2 * (kRcTile * 16), kRcTile * 16, 128);
         uint64_t bd = umma_desc(smem_u32(W) + rc_image_base(l) + s * 2 * (N * 16), N * 16, 128);
-        umma_bf16(c.tbase, ad, bd, idesc, s > 0 ? 1u : 0u);
+        umma_bf16(c.td, ad, bd, idesc, s > 0 ? 1u : 0u);
     }
     umma_commit(c.mbM);
 }
@@ -202,11 +205,39 @@ __device__ __forceinline__ const auto &infer_rows(const RcInferArgs &a) {
     if constexpr (MODE == 0) return a.feat;
     else return a.qry;
 }
+// Inference keeps each layer's input in tensor memory: the epilogue reads the
+// FP32 accumulator (TMEM columns [0, 64)), applies ReLU, rounds to BF16 and
+// writes the packed pairs to columns [64, 96) with tcgen05.st, and the next
+// layer's MMAs read A from there (only the weights come from shared memory).
+// No activation tile in shared memory: a CTA holds the 43 KB weight image and
+// 128 TMEM columns.  CTAs per SM (measured): 3 for feature arrays, whose
+// 256-byte rows are prefetched in registers, 4 for render queries.
 template <int MODE>
-__global__ void __launch_bounds__(kRcThreads) k_rc_infer(RcInferArgs a) {
+constexpr uint32_t kRcInferCtasPerSm = MODE == 0 ? 3u : 4u;
+constexpr uint32_t kRcInferCols = 128;
+constexpr uint32_t kRcInferA = 64;  // first TMEM column of the layer input
+constexpr uint32_t kInferSmem = kRcImageBytes + 64;  // + mbarriers, TMEM slot
+static_assert(4 * (kInferSmem + 1024) <= 228 * 1024, "inference CTAs per SM: shared memory");
+static_assert(4 * kRcInferCols <= 512, "inference CTAs per SM: tensor memory");
+
+// Forward MMAs of layer l with A in tensor memory: D[0:N) = A . W_l^T.
+__device__ __forceinline__ void rc_issue_forward_ts(const CtaCtl &c, const uint8_t *W, int l) {
+    const uint32_t N = rc_rows(l);
+    tc_fence_after();
+    const uint32_t idesc = umma_idesc(128, N, 0, 0);
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+        uint64_t bd = umma_desc(smem_u32(W) + rc_image_base(l) + s * 2 * (N * 16), N * 16, 128);
+        umma_bf16_ts(c.td, c.tbase + kRcInferA + 8 * s, bd, idesc, s > 0 ? 1u : 0u);
+    }
+    umma_commit(c.mbM);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kRcThreads, kRcInferCtasPerSm<MODE>) k_rc_infer(RcInferArgs a) {
     extern __shared__ __align__(1024) uint8_t sm[];
-    uint8_t *W = sm, *T = sm + kRcImageBytes;
-    uint64_t *bars = reinterpret_cast<uint64_t *>(sm + kRcImageBytes + kTileBytes);
+    uint8_t *W = sm;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sm + kRcImageBytes);
     uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2);
     const uint32_t t = threadIdx.x;
     const uint32_t n = MODE == 0 ? a.feat.count() : a.qry.count();
@@ -218,16 +249,23 @@ __global__ void __launch_bounds__(kRcThreads) k_rc_infer(RcInferArgs a) {
     const auto &rows = infer_rows<MODE>(a);
     typename std::remove_reference_t<decltype(rows)>::Raw raw;
     if (blockIdx.x * kRcTile + t < n) rows.fetch(blockIdx.x * kRcTile + t, false, raw);
-    rc_setup(c, W, bars, tslot, a.net.img, 64, a.net.stallPolls);
+    rc_setup(c, W, bars, tslot, a.net.img, kRcInferCols, a.net.stallPolls);
+    const uint32_t aIn = c.tl + kRcInferA;  // this warp's lanes of the layer input
     for (uint32_t tile = blockIdx.x; tile < ntiles && c.ok; tile += gridDim.x) {
         const uint32_t row = tile * kRcTile + t;
         const bool valid = row < n;
-        float f[kRcIn];
-        if (valid) {
-            rows.decode(a.net, raw, f);
-        } else {
+        {
+            float f[kRcIn];
+            if (valid) {
+                rows.decode(a.net, raw, f);
+            } else {
 #pragma unroll
-            for (int k = 0; k < kRcIn; k++) f[k] = 0.0f;
+                for (int k = 0; k < kRcIn; k++) f[k] = 0.0f;
+            }
+            uint32_t pk[32];
+#pragma unroll
+            for (int k = 0; k < 32; k++) pk[k] = pack_bf16(f[2 * k], f[2 * k + 1]);
+            tmem_st32(aIn, pk);
         }
         // render queries: what the last step reads, requested now
         uint32_t tag = 0;
@@ -245,21 +283,22 @@ __global__ void __launch_bounds__(kRcThreads) k_rc_infer(RcInferArgs a) {
             const uint32_t nrow = row + gridDim.x * kRcTile;
             if (nrow < n) rows.fetch(nrow, false, raw);
         }
-        store_row_bf16(T, t, f);
-        fence_async_smem();
+        tmem_wait_st();
         tc_fence_before();
         __syncthreads();
         for (int l = 0; l < kRcLayers && c.ok; l++) {
-            if (t == 0) rc_issue_forward(c, T, W, l);
+            if (t == 0) rc_issue_forward_ts(c, W, l);
             if (!(c.ok = rc_wait_mma(c))) break;
             if (l < kRcLayers - 1) {
                 float v[64];
-                tmem_ld64(c.tl, v);
+                tmem_ld32(c.tl, v);
+                tmem_ld32(c.tl + 32, v + 32);
                 tmem_wait_ld();
+                uint32_t pk[32];
 #pragma unroll
-                for (int k = 0; k < 64; k++) v[k] = fmaxf(v[k], 0.0f);
-                store_row_bf16(T, t, v);
-                fence_async_smem();
+                for (int k = 0; k < 32; k++) pk[k] = pack_bf16_relu(v[2 * k], v[2 * k + 1]);
+                tmem_st32(aIn, pk);
+                tmem_wait_st();
             } else {
                 float v[16];
                 tmem_ld16(c.tl, v);
@@ -287,7 +326,7 @@ __global__ void __launch_bounds__(kRcThreads) k_rc_infer(RcInferArgs a) {
             __syncthreads();
         }
     }
-    rc_teardown(c, 64, a.net.err);
+    rc_teardown(c, kRcInferCols, a.net.err);
 }
 
 // ---- training: forward, relative L2 loss, backward, weight gradients ---------
@@ -671,7 +710,7 @@ cudaError_t rc_enqueue_resolve(pt_ctx *ctx, cudaStream_t st, float4 *lo_eta) {
     a.qw = C.q[4];
     a.lo_eta = lo_eta;
     a.recCache = C.rec[7];
-    k_rc_infer<1><<<ctx->numSMs * 3, kRcThreads, kInferSmem, st>>>(a);
+    k_rc_infer<1><<<ctx->numSMs * kRcInferCtasPerSm<1>, kRcThreads, kInferSmem, st>>>(a);
     return cudaGetLastError();
 }
 cudaError_t rc_enqueue_targets(pt_ctx *ctx, cudaStream_t st, float4 *lo_eta, uint4 *rng, const float4 *pendA,
@@ -859,7 +898,7 @@ int pt_cache_infer_batch(pt_ctx *ctx, const float *features, size_t n, float *ou
     a.feat.n = (uint32_t)n;
     a.out = (float *)s.dev(1);
     cudaEventRecord(ctx->ev[0], ctx->stream);
-    k_rc_infer<0><<<rc_grid(ctx, (uint32_t)n, 3), kRcThreads, kInferSmem, ctx->stream>>>(a);
+    k_rc_infer<0><<<rc_grid(ctx, (uint32_t)n, kRcInferCtasPerSm<0>), kRcThreads, kInferSmem, ctx->stream>>>(a);
     cudaEventRecord(ctx->ev[1], ctx->stream);
     if ((rc = s.finish())) return rc;
     cudaEventElapsedTime(&ctx->cache.lastKernelMs, ctx->ev[0], ctx->ev[1]);
