@@ -522,22 +522,31 @@ struct Loader {
             throw NoriException("Error while parsing \"" + fn + "\": unexpected tag \"" + node.name + "\" at " +
                                 xr.where(node.offset));
         int tag = it->second;
-        bool hasParent = parentTag != TInvalid;
-        bool parentIsObject = hasParent && parentTag < NoriObject::EClassTypeCount;
-        bool currentIsObject = tag < NoriObject::EClassTypeCount;
-        bool parentIsTransform = parentTag == TTransform;
-        bool currentIsTransformOp = tag == TTranslate || tag == TRotate || tag == TScale || tag == TLookAt ||
-                                    tag == TMatrix;
-        if (!hasParent && !currentIsObject)
-            throw NoriException("Error while parsing \"" + fn + "\": root element \"" + node.name +
-                                "\" must be a Nori object (at " + xr.where(node.offset) + ")");
-        if (parentIsTransform != currentIsTransformOp)
-            throw NoriException("Error while parsing \"" + fn +
-                                "\": transform nodes can only contain transform operations (at " +
+        // The format's nesting rules: the document element is a scene
+        // object; a <transform> holds transform steps and nothing else, and
+        // a transform step appears only there; every other element sits
+        // inside a scene object.
+        enum Kind { KObject, KStep, KOther };
+        auto kind = [](int t) {
+            if (t < NoriObject::EClassTypeCount) return KObject;
+            if (t == TTranslate || t == TRotate || t == TScale || t == TLookAt || t == TMatrix) return KStep;
+            return KOther;
+        };
+        const Kind self = kind(tag);
+        const char *misplaced = nullptr;
+        if (parentTag == TInvalid) {
+            if (self != KObject) misplaced = "is not a scene object, so it cannot be the document element";
+        } else if (parentTag == TTransform) {
+            if (self != KStep) misplaced = "cannot appear inside <transform>, which holds transform steps only";
+        } else if (self == KStep) {
+            misplaced = "is a transform step and must appear inside <transform>";
+        } else if (kind(parentTag) != KObject) {
+            misplaced = "must appear inside a scene object";
+        }
+        if (misplaced)
+            throw NoriException("Error while parsing \"" + fn + "\": <" + node.name + "> " + misplaced + " (at " +
                                 xr.where(node.offset) + ")");
-        if (hasParent && !parentIsObject && !(parentIsTransform && currentIsTransformOp))
-            throw NoriException("Error while parsing \"" + fn + "\": node \"" + node.name +
-                                "\" requires a Nori object as parent (at " + xr.where(node.offset) + ")");
+        const bool currentIsObject = self == KObject;
         if (tag == TTransform) transform = Transform();
         PropertyList propList;
         std::vector<NoriObject *> children;

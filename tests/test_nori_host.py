@@ -161,6 +161,15 @@ def test_load_and_flatten(nori, pt, scene_dir):
     ("<scene><integrator type='nonexistent'/></scene>", "could not be found"),
     ("<scene></scene>", "No camera"),
     ("<scene><float name='x' value='1' extra='2'/></scene>", "unexpected attribute"),
+    # nesting rules of the format
+    ("<float name='x' value='1'/>", "cannot be the document element"),
+    ("<scene><mesh type='obj'><transform name='toWorld'><float name='x' value='1'/></transform></mesh></scene>",
+     "holds transform steps only"),
+    ("<scene><mesh type='obj'><scale value='2'/></mesh></scene>", "must appear inside <transform>"),
+    ("<scene><float name='x' value='1'><float name='y' value='2'/></float></scene>",
+     "must appear inside a scene object"),
+    ("<scene><mesh type='obj'><transform name='toWorld'><mesh type='obj'/></transform></mesh></scene>",
+     "holds transform steps only"),
 ])
 def test_parse_errors_are_reported(nori, tmp_path, bad, msg):
     p = tmp_path / "bad.xml"
