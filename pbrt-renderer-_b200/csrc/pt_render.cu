@@ -273,6 +273,15 @@ __device__ __forceinline__ void bind_stack(TravStack &, uint2 *) {}
     QueueStack<kSharedStack>::type K;                                    \
     bind_stack(K, &stk_[0][threadIdx.x]);
 
+// Traversal kernels run 4 blocks of 256 threads per SM (64 registers).  The
+// opaque-scene forms fit that by themselves (and are left to the compiler:
+// the same bound stated explicitly schedules them worse); the media forms
+// (free flight after the closest hit, ratio tracking on shadow rays) would
+// take 80 registers and 3 blocks, so their entry points state the bound —
+// their traversal waits on DRAM in large scenes and wants the warps more than
+// those registers.
+constexpr int kTraversalBlocksPerSm = 4;
+
 // Persistent work-stealing over a ray queue: each warp claims the next 32
 // queue positions with one atomic (so a warp's rays stay neighbours in the
 // queue) until the queue is exhausted.  Returns the claimed base, uniform
@@ -329,8 +338,8 @@ __device__ __forceinline__ void extend_one(const WaveArgs &A, uint32_t i, Stack 
     }
     finish_extend<CLASSIFY>(A, i, h);
 }
-template <bool CLASSIFY, bool MEDIA = false>
-__global__ void __launch_bounds__(kBlock) k_extend(WaveArgs A) {
+template <bool CLASSIFY, bool MEDIA>
+__device__ __forceinline__ void extend_queue(const WaveArgs &A) {
     // warps claim the queue in order: the 32 rays of a warp are neighbours in
     // the queue (coherent traversal), and the class queues and the next ray
     // queue keep that order for the kernels that follow
@@ -341,6 +350,13 @@ __global__ void __launch_bounds__(kBlock) k_extend(WaveArgs A) {
         const uint32_t i = base + lane_id();
         if (i < n) extend_one<CLASSIFY, MEDIA>(A, i, K);
     }
+}
+template <bool CLASSIFY>
+__global__ void __launch_bounds__(kBlock) k_extend(WaveArgs A) {
+    extend_queue<CLASSIFY, false>(A);
+}
+__global__ void __launch_bounds__(kBlock, kTraversalBlocksPerSm) k_extend_media(WaveArgs A) {
+    extend_queue<true, true>(A);
 }
 
 // ---- shadow: any hit -> pending NEE contribution ---------------------------
@@ -383,11 +399,11 @@ __device__ __forceinline__ void shadow_one(const WaveArgs &A, uint32_t i, Stack 
     if (s >> 31) __stcs(A.pendE + slot, out);
     else __stcs(A.pendA + slot, out);
 }
-// MEDIA_TR: the instantiation for heterogeneous media in the wavefront
-// (transmittance of unoccluded rays); the default one carries none of that
-// code.
-template <bool MEDIA_TR = false>
-__global__ void __launch_bounds__(kBlock) k_shadow(WaveArgs A) {
+// MEDIA_TR: the form for heterogeneous media in the wavefront
+// (transmittance of unoccluded rays, k_shadow_media); k_shadow carries none
+// of that code.
+template <bool MEDIA_TR>
+__device__ __forceinline__ void shadow_queue(const WaveArgs &A) {
     // appends past the capacity were dropped (and flagged): only what was stored is read
     const uint32_t n = min(*(volatile uint32_t *)A.cntShadow, A.shadowCap);
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&A.rayTotals[1], (unsigned long long)n);
@@ -396,6 +412,10 @@ __global__ void __launch_bounds__(kBlock) k_shadow(WaveArgs A) {
         const uint32_t i = base + lane_id();
         if (i < n) shadow_one<MEDIA_TR>(A, i, K);
     }
+}
+__global__ void __launch_bounds__(kBlock) k_shadow(WaveArgs A) { shadow_queue<false>(A); }
+__global__ void __launch_bounds__(kBlock, kTraversalBlocksPerSm) k_shadow_media(WaveArgs A) {
+    shadow_queue<true>(A);
 }
 
 // One NEE estimate, deferred: either a shadow ray carrying X (everything but
@@ -1526,7 +1546,7 @@ cudaError_t enqueue_paths(const pt_ctx *ctx, Enqueue &E, WaveArgs &A, uint32_t d
             // class counts and the shadow claim position after them
             chk(cudaMemsetAsync(A.cntCls, 0, (CLS_N + 1) * sizeof(uint32_t), st));
             E.begin(STG_EXTEND);
-            if (A.S.mediaWavefront) k_extend<true, true><<<G.extM, kBlock, 0, st>>>(A);
+            if (A.S.mediaWavefront) k_extend_media<<<G.extM, kBlock, 0, st>>>(A);
             else k_extend<true><<<G.extC, kBlock, 0, st>>>(A);
             E.end();
             const bool extra = A.risNee || A.S.mediaWavefront;
@@ -1539,7 +1559,7 @@ cudaError_t enqueue_paths(const pt_ctx *ctx, Enqueue &E, WaveArgs &A, uint32_t d
                 E.end();
             }
             E.begin(STG_SHADOW);
-            if (A.S.mediaTrDeferred) k_shadow<true><<<G.shadowM, kBlock, 0, st>>>(A);
+            if (A.S.mediaTrDeferred) k_shadow_media<<<G.shadowM, kBlock, 0, st>>>(A);
             else k_shadow<<<G.shadow, kBlock, 0, st>>>(A);
             E.end();
         }
@@ -1660,10 +1680,10 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
     if (!gExt) {
         gExt = grid_for(ctx, (const void *)k_extend<false>);
         gExtC = grid_for(ctx, (const void *)k_extend<true>);
-        gExtM = grid_for(ctx, (const void *)k_extend<true, true>);
+        gExtM = grid_for(ctx, (const void *)k_extend_media);
         gShadeI = grid_for(ctx, (const void *)k_shade<true, CLS_ANY>);
-        gShadow = grid_for(ctx, (const void *)k_shadow<false>);
-        gShadowM = grid_for(ctx, (const void *)k_shadow<true>);
+        gShadow = grid_for(ctx, (const void *)k_shadow);
+        gShadowM = grid_for(ctx, (const void *)k_shadow_media);
         for (int c = 0; c < CLS_N; c++) {
             gCls[c] = grid_for(ctx, (const void *)kShadeCls[c]);
             gClsX[c] = grid_for(ctx, (const void *)kShadeClsX[c]);
@@ -1960,10 +1980,10 @@ int render_batch(pt_ctx *ctx, const pt_request *R, uint32_t n, float *request_ms
     if (!gExt) {
         gExt = grid_for(ctx, (const void *)k_extend<false>);
         gExtC = grid_for(ctx, (const void *)k_extend<true>);
-        gExtM = grid_for(ctx, (const void *)k_extend<true, true>);
+        gExtM = grid_for(ctx, (const void *)k_extend_media);
         gShadeI = grid_for(ctx, (const void *)k_shade<true, CLS_ANY>);
-        gShadow = grid_for(ctx, (const void *)k_shadow<false>);
-        gShadowM = grid_for(ctx, (const void *)k_shadow<true>);
+        gShadow = grid_for(ctx, (const void *)k_shadow);
+        gShadowM = grid_for(ctx, (const void *)k_shadow_media);
         for (int c = 0; c < CLS_N; c++) {
             gCls[c] = grid_for(ctx, (const void *)kShadeCls[c]);
             gClsX[c] = grid_for(ctx, (const void *)kShadeClsX[c]);
