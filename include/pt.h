@@ -445,7 +445,14 @@ int pt_trace_shadow(pt_ctx *ctx, const float *rays, size_t n, uint32_t *occluded
 #define PT_CACHE_MAX_RECORDS 262144u
 #define PT_CACHE_NO_TRAIN 0x1u /* render with the cache, take no training paths and no steps */
 typedef struct pt_cache_params {
-    uint32_t train_records;  /* training paths per render call (0 = 65536; <= PT_CACHE_MAX_RECORDS) */
+    /* training paths a render call aims at (0 = 65536; <= PT_CACHE_MAX_RECORDS).
+     * The record buffers hold twice that; the training chance of a call is
+     * set from the cache vertices of the call before (the first call: from
+     * its path count), and each wave's records are ordered by path slot
+     * before training, so a cached render sequence repeats bit for bit unless
+     * a call's cache vertices more than double from the call before (records
+     * past the buffers are dropped in scheduling order). */
+    uint32_t train_records;
     uint32_t unbiased_every; /* one training path in this many runs without the cache (0 = none) */
     float rough_threshold;   /* microfacet alpha / Disney roughness counted as rough (0 = 0.3) */
     float learning_rate;     /* Adam step size (0 = 5e-3); beta1 0.9, beta2 0.99, eps 1e-8 */

@@ -514,7 +514,9 @@ struct RcAdamArgs {
     uint8_t *imgTrain, *imgInfer;
     uint32_t *ctr;           // [0] steps (read, incremented), [4] records of the step (written)
     const uint32_t *nrec;    // records of the call; this step's gradient sums over rows phase + k stride
-    uint32_t nrecCap, stride, phase;
+    uint32_t nrecCap;     // capacity of the record buffers
+    uint32_t nrecTarget;  // records a render call aims at (train_records)
+    uint32_t stride, phase;
     float lr, emaDecay;
     float *lossSum;          // mean loss of the step -> ctr[3] as float bits; reset
     uint32_t updateProb;     // last step of a render call: set ctr[7] for the next call
@@ -534,10 +536,11 @@ __global__ void __launch_bounds__(1024) k_rc_adam(RcAdamArgs a) {
         uint32_t tot = min(*a.nrec, a.nrecCap);
         sN = tot > a.phase ? (tot - a.phase + a.stride - 1) / a.stride : 0u;
         if (a.updateProb) {
-            // training chance of the next call: about nrecCap records out of
-            // this call's cache vertices (queries + records)
+            // training chance of the next call: about nrecTarget records out
+            // of this call's cache vertices (queries + records)
             float verts = (float)a.ctr[5];  // every cache vertex made a query (training ones too)
-            reinterpret_cast<float *>(a.ctr)[7] = verts > 0.0f ? fminf(a.maxFrac, (float)a.nrecCap / verts) : a.maxFrac;
+            reinterpret_cast<float *>(a.ctr)[7] =
+                verts > 0.0f ? fminf(a.maxFrac, (float)a.nrecTarget / verts) : a.maxFrac;
         }
     }
     __syncthreads();
@@ -620,7 +623,90 @@ __global__ void __launch_bounds__(1024) k_rc_targets(RcRows<1> rec, float4 *beta
     __syncthreads();
     if (threadIdx.x == 0) {
         ctr[6] = s1;
+        ctr[9] = s0;
         ctr[5] += ctr[1];
+    }
+}
+
+// ---- the records of a wave in a fixed order ------------------------------------
+// Records are appended by the shading kernels in whatever order their warps
+// run, and an Adam step's batch and its gradient sums follow record order.
+// Each wave's records [ctr[9], ctr[6]) are therefore put in path-slot order
+// (a path leaves at most one record per wave, so slots are distinct): counted
+// into kRcOrdBuckets buckets of consecutive slots, scanned, scattered, and
+// each bucket (a few records) sorted by slot; the training inputs and
+// targets are copied into recOrd in that order.  Training reads recOrd, and
+// cached renders repeat bit for bit.
+constexpr uint32_t kRcOrdBuckets = 4096;
+__device__ __forceinline__ uint32_t rc_ord_slot(const float4 *r1, uint32_t r) {
+    return __float_as_uint(__ldg(reinterpret_cast<const float *>(r1 + r) + 3));
+}
+__device__ __forceinline__ uint32_t rc_ord_bucket(uint32_t slot, uint32_t waveCount) {
+    // slots lie below waveCount; the clamp keeps any other value in bounds
+    return min((uint32_t)(((uint64_t)slot * kRcOrdBuckets) / waveCount), kRcOrdBuckets - 1u);
+}
+__global__ void __launch_bounds__(256) k_rc_ord_count(const float4 *r1, const uint32_t *ctr, uint32_t waveCount,
+                                                      uint32_t *cnt) {
+    const uint32_t s0 = ctr[9], s1 = ctr[6];
+    for (uint32_t r = s0 + blockIdx.x * blockDim.x + threadIdx.x; r < s1; r += gridDim.x * blockDim.x)
+        atomicAdd(cnt + rc_ord_bucket(rc_ord_slot(r1, r), waveCount), 1u);
+}
+// One block: exclusive scan of the bucket counts into off (kRcOrdBuckets + 1
+// entries) and the scatter cursors.
+__global__ void __launch_bounds__(1024) k_rc_ord_scan(const uint32_t *cnt, uint32_t *off, uint32_t *cur) {
+    constexpr uint32_t kPer = kRcOrdBuckets / 1024;
+    __shared__ uint32_t part[1024];
+    const uint32_t t = threadIdx.x;
+    uint32_t c[kPer], sum = 0;
+#pragma unroll
+    for (uint32_t k = 0; k < kPer; k++) {
+        c[k] = cnt[kPer * t + k];
+        sum += c[k];
+    }
+    part[t] = sum;
+    __syncthreads();
+    for (uint32_t o = 1; o < 1024; o <<= 1) {
+        const uint32_t v = t >= o ? part[t - o] : 0u;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    uint32_t base = part[t] - sum;
+#pragma unroll
+    for (uint32_t k = 0; k < kPer; k++) {
+        off[kPer * t + k] = base;
+        cur[kPer * t + k] = base;
+        base += c[k];
+    }
+    if (t == 1023) off[kRcOrdBuckets] = part[1023];
+}
+__global__ void __launch_bounds__(256) k_rc_ord_scatter(const float4 *r1, const uint32_t *ctr, uint32_t waveCount,
+                                                        uint32_t *cur, uint32_t *tmp) {
+    const uint32_t s0 = ctr[9], s1 = ctr[6];
+    for (uint32_t r = s0 + blockIdx.x * blockDim.x + threadIdx.x; r < s1; r += gridDim.x * blockDim.x)
+        tmp[atomicAdd(cur + rc_ord_bucket(rc_ord_slot(r1, r), waveCount), 1u)] = r;
+}
+struct RcOrdCopy {
+    const float4 *src[5];  // inputs x 4, target
+    float4 *dst[5];
+};
+// One thread per bucket: insertion sort of its record indices by slot, then
+// the records copied to positions ctr[9] + (rank within the wave).
+__global__ void __launch_bounds__(256) k_rc_ord_gather(RcOrdCopy a, const uint32_t *ctr, const uint32_t *off,
+                                                       uint32_t *tmp) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= kRcOrdBuckets) return;
+    const uint32_t s0 = ctr[9], lo = off[b], hi = off[b + 1];
+    for (uint32_t i = lo + 1; i < hi; i++) {
+        const uint32_t x = tmp[i], kx = rc_ord_slot(a.src[1], x);
+        uint32_t j = i;
+        for (; j > lo && rc_ord_slot(a.src[1], tmp[j - 1]) > kx; j--) tmp[j] = tmp[j - 1];
+        tmp[j] = x;
+    }
+    for (uint32_t i = lo; i < hi; i++) {
+        const uint32_t r = tmp[i];
+#pragma unroll
+        for (int k = 0; k < 5; k++) a.dst[k][s0 + i] = a.src[k][r];
     }
 }
 
@@ -714,11 +800,23 @@ cudaError_t rc_enqueue_resolve(pt_ctx *ctx, cudaStream_t st, float4 *lo_eta) {
     return cudaGetLastError();
 }
 cudaError_t rc_enqueue_targets(pt_ctx *ctx, cudaStream_t st, float4 *lo_eta, uint4 *rng, const float4 *pendA,
-                               const float4 *pendE) {
+                               const float4 *pendE, uint32_t waveCount) {
     const RadianceCache &C = ctx->cache;
     RcRows<1> rec{C.rec[0], C.rec[1], C.rec[2], C.rec[3], C.rec[6], C.ctr + 2, (uint32_t)C.recCap, 1u, 0u};
     k_rc_targets<<<1, 1024, 0, st>>>(rec, C.rec[4], C.rec[5], C.rec[6], C.rec[7], C.ctr, lo_eta, rng, pendA,
                                      pendE);
+    // the wave's records in slot order (scratch: counts, offsets, cursors, indices)
+    uint32_t *cnt = C.ordScratch, *off = cnt + kRcOrdBuckets, *cur = off + kRcOrdBuckets + 1,
+             *tmp = cur + kRcOrdBuckets;
+    cudaError_t e = cudaMemsetAsync(cnt, 0, kRcOrdBuckets * sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    const unsigned g = (unsigned)ctx->numSMs;
+    k_rc_ord_count<<<g, 256, 0, st>>>(C.rec[1], C.ctr, waveCount, cnt);
+    k_rc_ord_scan<<<1, 1024, 0, st>>>(cnt, off, cur);
+    k_rc_ord_scatter<<<g, 256, 0, st>>>(C.rec[1], C.ctr, waveCount, cur, tmp);
+    RcOrdCopy oc{{C.rec[0], C.rec[1], C.rec[2], C.rec[3], C.rec[6]},
+                 {C.recOrd[0], C.recOrd[1], C.recOrd[2], C.recOrd[3], C.recOrd[4]}};
+    k_rc_ord_gather<<<kRcOrdBuckets / 256, 256, 0, st>>>(oc, C.ctr, off, tmp);
     return cudaGetLastError();
 }
 // kRcStepsPerCall (pt_internal.h) Adam steps per render call, step s on
@@ -731,7 +829,7 @@ cudaError_t rc_enqueue_train(pt_ctx *ctx, cudaStream_t st, uint32_t s, bool adam
         if (e != cudaSuccess) return e;
         RcTrainArgs a{};
         a.net = rc_net(ctx, C.imgTrain);
-        a.rec = RcRows<1>{C.rec[0], C.rec[1], C.rec[2], C.rec[3], C.rec[6], C.ctr + 2, (uint32_t)C.recCap,
+        a.rec = RcRows<1>{C.recOrd[0], C.recOrd[1], C.recOrd[2], C.recOrd[3], C.recOrd[4], C.ctr + 2, (uint32_t)C.recCap,
                           kRcStepsPerCall, s};
         a.part = C.gradPart;
         a.lossSum = lossDev;
@@ -739,16 +837,27 @@ cudaError_t rc_enqueue_train(pt_ctx *ctx, cudaStream_t st, uint32_t s, bool adam
         k_rc_grad_reduce<<<kReduceBlocks, 256, 0, st>>>(C.gradPart, (uint32_t)ctx->numSMs, C.grad);
     } else {
         RcAdamArgs d{C.w, C.m, C.v, C.ema, C.grad, C.imgTrain, C.imgInfer, C.ctr, C.ctr + 2, (uint32_t)C.recCap,
-                     kRcStepsPerCall, s, C.params.learning_rate, C.params.ema, lossDev,
+                     C.params.train_records, kRcStepsPerCall, s, C.params.learning_rate, C.params.ema, lossDev,
                      s + 1 == kRcStepsPerCall ? 1u : 0u, C.params.max_train_fraction};
         k_rc_adam<<<1, 1024, 0, st>>>(d);
     }
     return cudaGetLastError();
 }
-int rc_render_setup(pt_ctx *ctx, size_t waveCap) {
+int rc_render_setup(pt_ctx *ctx, size_t waveCap, uint64_t callPaths) {
     int rc = rc_check(ctx);
     if (rc) return rc;
     rc_bounds(ctx);
+    RadianceCache &C = ctx->cache;
+    if (C.firstCall && callPaths) {
+        // no call before to count cache vertices: a path has at most one, so
+        // 1.5 x train_records / paths keeps the first call's records well
+        // inside the buffers (twice the target) and their choice repeatable
+        const float p = std::min(C.params.max_train_fraction, 1.5f * (float)C.params.train_records / (float)callPaths);
+        if (cudaMemcpyAsync(C.ctr + 7, &p, 4, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess ||
+            cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+            return ctx->fail(PT_E_CUDA, "cache training chance");
+        C.firstCall = false;
+    }
     // a path makes at most two queries per wave: at its cache vertex and, as a
     // training path, at the end of its suffix
     return pt_cache_prepare(ctx, 2 * waveCap);
@@ -756,12 +865,14 @@ int rc_render_setup(pt_ctx *ctx, size_t waveCap) {
 
 void pt_cache_free(pt_ctx *ctx) {
     RadianceCache &C = ctx->cache;
-    void *ps[] = {C.w, C.m, C.v, C.ema, C.grad, C.gradPart, C.imgTrain, C.imgInfer, C.ctr};
+    void *ps[] = {C.w, C.m, C.v, C.ema, C.grad, C.gradPart, C.imgTrain, C.imgInfer, C.ctr, C.ordScratch};
     for (void *p : ps)
         if (p) cudaFree(p);
     for (float4 *p : C.q)
         if (p) cudaFree(p);
     for (float4 *p : C.rec)
+        if (p) cudaFree(p);
+    for (float4 *p : C.recOrd)
         if (p) cudaFree(p);
     uint64_t gen = C.gen + 1;
     C = RadianceCache{};
@@ -806,8 +917,13 @@ int pt_cache_init(pt_ctx *ctx, const pt_cache_params *params) {
     A((void **)&C.imgTrain, kRcImageBytes);
     A((void **)&C.imgInfer, kRcImageBytes);
     A((void **)&C.ctr, 16 * sizeof(uint32_t));
-    C.recCap = C.params.train_records;
+    // record buffers hold twice the target: a call overflows them only when
+    // its cache vertices more than double from the call before
+    C.recCap = 2 * (size_t)C.params.train_records;
+    C.firstCall = true;
     for (float4 *&p : C.rec) A((void **)&p, C.recCap * sizeof(float4));
+    for (float4 *&p : C.recOrd) A((void **)&p, C.recCap * sizeof(float4));
+    A((void **)&C.ordScratch, (3 * kRcOrdBuckets + 1 + C.recCap) * sizeof(uint32_t));
     if (e != cudaSuccess) {
         pt_cache_free(ctx);
         return ctx->fail(PT_E_NOMEM, "radiance cache", cudaGetErrorString(e));
@@ -828,8 +944,7 @@ int pt_cache_init(pt_ctx *ctx, const pt_cache_params *params) {
     cudaMemset(C.imgTrain, 0, kRcImageBytes);
     cudaMemset(C.imgInfer, 0, kRcImageBytes);
     cudaMemset(C.ctr, 0, 16 * sizeof(uint32_t));
-    // the first call trains on the first records it finds, up to the cap
-    cudaMemcpy(C.ctr + 7, &C.params.max_train_fraction, 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(C.ctr + 7, &C.params.max_train_fraction, 4, cudaMemcpyHostToDevice);  // see rc_render_setup
     k_rc_images<<<21, 1024>>>(C.w, C.imgTrain, C.imgInfer, C.ema);
     e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return ctx->fail(PT_E_CUDA, "cache initialisation", cudaGetErrorString(e));
@@ -858,6 +973,7 @@ int pt_cache_weights(pt_ctx *ctx, float *get, const float *set) {
         for (float *p : {C.m, C.v, C.grad}) cudaMemset(p, 0, kRcParams * sizeof(float));
         cudaMemset(C.ctr, 0, 16 * sizeof(uint32_t));
         cudaMemcpy(C.ctr + 7, &C.params.max_train_fraction, 4, cudaMemcpyHostToDevice);
+        C.firstCall = true;
         k_rc_images<<<21, 1024>>>(C.w, C.imgTrain, C.imgInfer, C.ema);
         cudaError_t e = cudaDeviceSynchronize();
         if (e != cudaSuccess) return ctx->fail(PT_E_CUDA, "cache weights", cudaGetErrorString(e));
@@ -939,7 +1055,7 @@ static int rc_train_impl(pt_ctx *ctx, const float *features, const float *target
     cudaMemcpyAsync(&lossHost, lossDev, 4, cudaMemcpyDeviceToHost, ctx->stream);
     if (step) {
         RcAdamArgs d{C.w, C.m, C.v, C.ema, C.grad, C.imgTrain, C.imgInfer, C.ctr, nDev, PT_CACHE_MAX_RECORDS,
-                     1u, 0u, C.params.learning_rate, C.params.ema, lossDev, 0u, 1.0f};
+                     PT_CACHE_MAX_RECORDS, 1u, 0u, C.params.learning_rate, C.params.ema, lossDev, 0u, 1.0f};
         k_rc_adam<<<1, 1024, 0, ctx->stream>>>(d);
     } else if (grad) {
         cudaMemcpyAsync(grad, C.grad, kRcParams * 4, cudaMemcpyDeviceToHost, ctx->stream);

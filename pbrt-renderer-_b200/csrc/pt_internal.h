@@ -125,13 +125,20 @@ struct RadianceCache {
     // counters: [0] Adam steps, [1] queries of the wave, [2] records of the
     // call, [3] loss sum (float bits), [4] records of the last step, [5]
     // queries of the call, [6] first record not yet given a target, [7] the
-    // chance (float) that a path at a cache vertex trains, set after each call
+    // chance (float) that a path at a cache vertex trains, set after each call,
+    // [8] loss of the step being trained (float), [9] first record of the
+    // wave whose targets were set last
     uint32_t *ctr = nullptr;
     size_t queryCap = 0;
     float4 *q[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // record float4 x 4, weight
-    size_t recCap = 0;
+    size_t recCap = 0;       // record buffers: twice params.train_records
+    bool firstCall = true;   // no cached render yet: rc_render_setup sets the training chance
     // x 4, throughput, Lo so far, target, cache value at the vertex
     float4 *rec[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    // the training inputs (x 4) and targets of the call's records in a fixed
+    // order (each wave's records by path slot), and the ordering's scratch
+    float4 *recOrd[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    uint32_t *ordScratch = nullptr;
     uint64_t gen = 1;  // bumped when buffers move
     float lastKernelMs = 0.0f;  // network kernel of the last batch call (CUDA events)
     float renderInferMs = 0.0f, renderTrainMs = 0.0f;  // network kernels of the last stage-timed render
@@ -283,10 +290,11 @@ int pt_wave_free(pt_ctx *ctx);
 // pt_cache.cu
 void pt_cache_free(pt_ctx *ctx);
 int pt_cache_prepare(pt_ctx *ctx, size_t queryCap);  // query buffers for a cached render
-int rc_render_setup(pt_ctx *ctx, size_t waveCap);     // checks, bounds, query buffers
+int rc_render_setup(pt_ctx *ctx, size_t waveCap, uint64_t callPaths);  // checks, bounds, query buffers
 cudaError_t rc_enqueue_resolve(pt_ctx *ctx, cudaStream_t st, float4 *lo_eta);
+// the wave's records: training targets, then their fixed order (waveCount: the wave's paths)
 cudaError_t rc_enqueue_targets(pt_ctx *ctx, cudaStream_t st, float4 *lo_eta, uint4 *rng, const float4 *pendA,
-                               const float4 *pendE);
+                               const float4 *pendE, uint32_t waveCount);
 // one training step s of kRcStepsPerCall: the network kernel (adam = false) or its Adam update (adam = true)
 cudaError_t rc_enqueue_train(pt_ctx *ctx, cudaStream_t st, uint32_t s, bool adam);
 constexpr uint32_t kRcStepsPerCall = 4;  // Adam steps per cached render call, on interleaved quarters of its records

@@ -1599,7 +1599,7 @@ cudaError_t enqueue_render(const pt_ctx *ctx, Enqueue &E, WaveArgs A, const pt_r
             // training targets from the suffixes, then the training paths' image
             // values (prefix + throughput x cache); counts the wave's queries
             E.begin(STG_CACHE);
-            chk(rc_enqueue_targets(const_cast<pt_ctx *>(ctx), st, A.lo_eta, A.rng, A.pendA, A.pendE));
+            chk(rc_enqueue_targets(const_cast<pt_ctx *>(ctx), st, A.lo_eta, A.rng, A.pendA, A.pendE, A.waveCount));
             E.end();
         }
         uint32_t cover = (uint32_t)std::min<uint64_t>(A.waveCount, npix);
@@ -1726,7 +1726,7 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
     for (float4 *&r : A.cr) r = nullptr;
     A.cqCount = A.crCount = nullptr;
     if (A.cacheOn) {
-        if ((rc = rc_render_setup(ctx, B.cap))) return rc;
+        if ((rc = rc_render_setup(ctx, B.cap, total))) return rc;
         const RadianceCache &C = ctx->cache;
         A.roughThr = C.params.rough_threshold;
         A.unbiasedEvery = C.params.unbiased_every;

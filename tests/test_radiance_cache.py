@@ -248,8 +248,7 @@ def test_cached_render_trains(pt, scenes, ctx):
     chance (about train_records per call), record that vertex and continue;
     each call takes 4 Adam steps on interleaved quarters of its records, and
     the cached image approaches the plain converged image: much closer than
-    the same cache before training.  Training is not bit-reproducible (the
-    weight gradients of the CTAs are summed with float atomics), and its loss
+    the same cache before training.  Its loss
     (relative L2 against one-sample targets) stays at the targets' noise
     level with spikes, so learning is judged on the image: relMSE against a
     1024-spp plain render falls from ~0.29 before training to 0.009-0.02
@@ -290,7 +289,8 @@ def test_cached_render_trains(pt, scenes, ctx):
             print("seed", seed, "cached vs plain relMSE", rel, "before training", rel0, "records median",
                   np.median(records[-50:]))
             assert st.steps == 4 * 200
-            assert 100 <= np.median(records[-50:]) <= 256, records[-50:]
+            # about train_records / 4 per step (the buffers hold twice the target)
+            assert 100 <= np.median(records[-50:]) <= 320, records[-50:]
             assert np.all(np.isfinite(losses)) and min(losses) > 0.0
             return rel
         finally:
@@ -300,3 +300,39 @@ def test_cached_render_trains(pt, scenes, ctx):
     if not (rel < 0.05 and rel < 0.25 * rel0):
         rel = min(rel, train(4))
     assert rel < 0.05 and rel < 0.25 * rel0, (rel, rel0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("wave_paths", [0, 3000])
+def test_cached_render_repeats_bit_for_bit(pt, scenes, ctx, wave_paths):
+    """A cached render sequence is deterministic: records are put in path-slot
+    order per wave before training (the shading kernels append them in warp
+    order), and each step's gradient is summed from per-CTA slots in slot
+    order.  Two fresh caches with the same seed, given the same calls, end
+    with the same films and weights bit for bit; wave_paths=3000 splits each
+    64x64 call into two waves whose records are ordered separately."""
+    sc, cam = scenes.cornell(64, 64)
+    ctx.upload(sc)
+
+    def run():
+        ctx.cache_init(pt.cache_params(seed=7, train_records=1024, learning_rate=1e-2, ema=0.97))
+        try:
+            P = pt.render_params(64, 64, 1, cam, max_depth=8, wave_paths=wave_paths,
+                                 flags=pt.PT_RENDER_RADIANCE_CACHE)
+            films = []
+            for k in range(24):
+                P.sample_offset = k
+                img, _, _ = ctx.render(P)
+                films.append(img.copy())
+            st = ctx.cache_stats()
+            return films, ctx.cache_weights().copy(), int(st.steps), int(st.last_records)
+        finally:
+            ctx.cache_release()
+
+    f0, w0, s0, r0 = run()
+    f1, w1, s1, r1 = run()
+    assert s0 == s1 == 4 * 24 and r0 == r1 and r0 > 0
+    assert np.array_equal(w0, w1)
+    for a, b in zip(f0, f1):
+        assert np.array_equal(a, b)
+
