@@ -472,7 +472,8 @@ typedef struct pt_cache_stats {
     /* the last cached render made with PT_RENDER_STAGE_TIMING (0 otherwise):
      * device time of its inference kernels (all waves; `queries` rows) and of
      * its training kernels (forward, backward, weight gradients of every
-     * step, not the Adam updates), and the rows those processed */
+     * step; not the launches that sum the CTAs' gradients and apply Adam),
+     * and the rows those processed */
     float last_render_infer_ms;
     float last_render_train_ms;
     uint64_t last_render_train_rows;

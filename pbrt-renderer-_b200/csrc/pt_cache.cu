@@ -573,6 +573,60 @@ __global__ void __launch_bounds__(1024) k_rc_adam(RcAdamArgs a) {
     }
 }
 
+// A render call's training step, second half: the CTAs' gradient slots
+// summed in slot order (the same sums as k_rc_grad_reduce) and the Adam
+// update of k_rc_adam, one thread per parameter over the whole GPU.  Every
+// CTA reads the step counter first; the last CTA to finish (a ticket in
+// ctr[11]) writes the step's counters and, on the call's last step, the
+// next call's training chance.
+__global__ void __launch_bounds__(256) k_rc_adam_slots(RcAdamArgs a, const float *part, uint32_t slots) {
+    const uint32_t step = a.ctr[0] + 1u;
+    const uint32_t tot = min(*a.nrec, a.nrecCap);
+    const uint32_t n = tot > a.phase ? (tot - a.phase + a.stride - 1) / a.stride : 0u;
+    auto updateProb = [&]() {
+        // training chance of the next call: about nrecTarget records out of
+        // this call's cache vertices (queries + records)
+        float verts = (float)a.ctr[5];  // every cache vertex made a query (training ones too)
+        reinterpret_cast<float *>(a.ctr)[7] = verts > 0.0f ? fminf(a.maxFrac, (float)a.nrecTarget / verts) : a.maxFrac;
+    };
+    if (n == 0) {  // no records in this step: no update
+        if (a.updateProb && blockIdx.x == 0 && threadIdx.x == 0) updateProb();
+        return;
+    }
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < kRcParams) {
+        float sum = 0.0f;
+        for (uint32_t k = 0; k < slots; k++) sum += __ldcs(part + (size_t)k * kRcParams + i);
+        const float b1 = 0.9f, b2 = 0.99f, eps = 1e-8f;
+        const float gs = 1.0f / (3.0f * (float)n);
+        const float bc1 = 1.0f - powf(b1, (float)step), bc2 = 1.0f - powf(b2, (float)step);
+        float g = sum * gs;
+        if (!isfinite(g)) g = 0.0f;
+        float m = b1 * a.m[i] + (1.0f - b1) * g;
+        float v = b2 * a.v[i] + (1.0f - b2) * g * g;
+        a.m[i] = m;
+        a.v[i] = v;
+        float w = a.w[i] - a.lr * (m / bc1) / (sqrtf(v / bc2) + eps);
+        a.w[i] = w;
+        float e = (step == 1u || a.emaDecay == 0.0f) ? w : a.emaDecay * a.ema[i] + (1.0f - a.emaDecay) * w;
+        a.ema[i] = e;
+        put_bf16(a.imgTrain, i, w);
+        put_bf16(a.imgInfer, i, e);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(a.ctr + 11, 1u) == gridDim.x - 1) {  // every CTA has read ctr[0]
+            a.ctr[11] = 0u;
+            a.ctr[0] = step;
+            a.ctr[4] = n;
+            a.ctr[3] = __float_as_uint(*a.lossSum / (3.0f * (float)n));
+            *a.lossSum = 0.0f;
+            if (a.updateProb) updateProb();
+        }
+    }
+}
+
 // Images from the FP32 weights (initialisation, pt_cache_weights).
 __global__ void k_rc_images(const float *w, uint8_t *imgTrain, uint8_t *imgInfer, float *ema) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kRcParams; i += gridDim.x * blockDim.x) {
@@ -584,19 +638,15 @@ __global__ void k_rc_images(const float *w, uint8_t *imgTrain, uint8_t *imgInfer
 
 // Training targets of the records written in this wave: the radiance the
 // path gathered after its record vertex, divided by the throughput there.
-// One CTA; records [ctr[6], count) belong to the wave that just ended.
-// The training path then takes the value a terminated path would have there,
-// prefix + throughput x cache (lo_eta), with its pending NEE dropped.
-__global__ void __launch_bounds__(1024) k_rc_targets(RcRows<1> rec, float4 *beta, float4 *lo0, float4 *tgt,
-                                                    const float4 *recCache, uint32_t *ctr, float4 *lo_eta,
-                                                    uint4 *rng, const float4 *pendA, const float4 *pendE) {
-    __shared__ uint32_t s0, s1;
-    if (threadIdx.x == 0) {
-        s0 = ctr[6];
-        s1 = rec.total();
-    }
-    __syncthreads();
-    for (uint32_t r = s0 + threadIdx.x; r < s1; r += blockDim.x) {
+// Records [ctr[6], count) belong to the wave that just ended (ctr[6] moves
+// on in k_rc_ord_scan, after every kernel that reads it here).  The training
+// path then takes the value a terminated path would have there, prefix +
+// throughput x cache (lo_eta), with its pending NEE dropped.
+__global__ void __launch_bounds__(256) k_rc_targets(RcRows<1> rec, float4 *beta, float4 *lo0, float4 *tgt,
+                                                   const float4 *recCache, const uint32_t *ctr, float4 *lo_eta,
+                                                   uint4 *rng, const float4 *pendA, const float4 *pendE) {
+    const uint32_t s0 = ctr[6], s1 = rec.total();
+    for (uint32_t r = s0 + blockIdx.x * blockDim.x + threadIdx.x; r < s1; r += gridDim.x * blockDim.x) {
         uint32_t slot = __float_as_uint(rec.r1[r].w);
         float4 le = lo_eta[slot];
         float L[3] = {le.x, le.y, le.z};
@@ -620,23 +670,19 @@ __global__ void __launch_bounds__(1024) k_rc_targets(RcRows<1> rec, float4 *beta
         st.w &= ~1u;
         rng[slot] = st;
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        ctr[6] = s1;
-        ctr[9] = s0;
-        ctr[5] += ctr[1];
-    }
 }
 
 // ---- the records of a wave in a fixed order ------------------------------------
 // Records are appended by the shading kernels in whatever order their warps
 // run, and an Adam step's batch and its gradient sums follow record order.
-// Each wave's records [ctr[9], ctr[6]) are therefore put in path-slot order
-// (a path leaves at most one record per wave, so slots are distinct): counted
-// into kRcOrdBuckets buckets of consecutive slots, scanned, scattered, and
-// each bucket (a few records) sorted by slot; the training inputs and
-// targets are copied into recOrd in that order.  Training reads recOrd, and
-// cached renders repeat bit for bit.
+// Each wave's records are therefore put in path-slot order (a path leaves
+// at most one record per wave, so slots are distinct): counted into
+// kRcOrdBuckets buckets of consecutive slots, scanned, scattered with their
+// slots, and each record placed at its bucket's offset plus its rank by slot
+// among the bucket's few records; the training inputs and targets are copied
+// to recOrd there.  Training reads recOrd, and cached renders repeat bit for
+// bit.  The wave's records are [ctr[6], count) until k_rc_ord_scan records
+// that range in ctr[9], ctr[10] and moves ctr[6] on.
 constexpr uint32_t kRcOrdBuckets = 4096;
 __device__ __forceinline__ uint32_t rc_ord_slot(const float4 *r1, uint32_t r) {
     return __float_as_uint(__ldg(reinterpret_cast<const float *>(r1 + r) + 3));
@@ -645,15 +691,17 @@ __device__ __forceinline__ uint32_t rc_ord_bucket(uint32_t slot, uint32_t waveCo
     // slots lie below waveCount; the clamp keeps any other value in bounds
     return min((uint32_t)(((uint64_t)slot * kRcOrdBuckets) / waveCount), kRcOrdBuckets - 1u);
 }
-__global__ void __launch_bounds__(256) k_rc_ord_count(const float4 *r1, const uint32_t *ctr, uint32_t waveCount,
+__global__ void __launch_bounds__(256) k_rc_ord_count(RcRows<1> rec, const uint32_t *ctr, uint32_t waveCount,
                                                       uint32_t *cnt) {
-    const uint32_t s0 = ctr[9], s1 = ctr[6];
+    const uint32_t s0 = ctr[6], s1 = rec.total();
     for (uint32_t r = s0 + blockIdx.x * blockDim.x + threadIdx.x; r < s1; r += gridDim.x * blockDim.x)
-        atomicAdd(cnt + rc_ord_bucket(rc_ord_slot(r1, r), waveCount), 1u);
+        atomicAdd(cnt + rc_ord_bucket(rc_ord_slot(rec.r1, r), waveCount), 1u);
 }
 // One block: exclusive scan of the bucket counts into off (kRcOrdBuckets + 1
-// entries) and the scatter cursors.
-__global__ void __launch_bounds__(1024) k_rc_ord_scan(const uint32_t *cnt, uint32_t *off, uint32_t *cur) {
+// entries) and the scatter cursors; then the wave's record range moves to
+// ctr[9], ctr[10], ctr[6] to its end, and the wave's queries join the call's.
+__global__ void __launch_bounds__(1024) k_rc_ord_scan(RcRows<1> rec, const uint32_t *cnt, uint32_t *off,
+                                                      uint32_t *cur, uint32_t *ctr) {
     constexpr uint32_t kPer = kRcOrdBuckets / 1024;
     __shared__ uint32_t part[1024];
     const uint32_t t = threadIdx.x;
@@ -679,34 +727,42 @@ __global__ void __launch_bounds__(1024) k_rc_ord_scan(const uint32_t *cnt, uint3
         base += c[k];
     }
     if (t == 1023) off[kRcOrdBuckets] = part[1023];
+    if (t == 0) {
+        const uint32_t s0 = ctr[6], s1 = rec.total();
+        ctr[9] = s0;
+        ctr[10] = s1;
+        ctr[6] = s1;
+        ctr[5] += ctr[1];
+    }
 }
+// Record indices and their slots into bucket order (order within a bucket:
+// whatever the atomics give; the place kernel ranks by slot).
 __global__ void __launch_bounds__(256) k_rc_ord_scatter(const float4 *r1, const uint32_t *ctr, uint32_t waveCount,
-                                                        uint32_t *cur, uint32_t *tmp) {
-    const uint32_t s0 = ctr[9], s1 = ctr[6];
-    for (uint32_t r = s0 + blockIdx.x * blockDim.x + threadIdx.x; r < s1; r += gridDim.x * blockDim.x)
-        tmp[atomicAdd(cur + rc_ord_bucket(rc_ord_slot(r1, r), waveCount), 1u)] = r;
+                                                        uint32_t *cur, uint2 *tmp) {
+    const uint32_t s0 = ctr[9], s1 = ctr[10];
+    for (uint32_t r = s0 + blockIdx.x * blockDim.x + threadIdx.x; r < s1; r += gridDim.x * blockDim.x) {
+        const uint32_t slot = rc_ord_slot(r1, r);
+        tmp[atomicAdd(cur + rc_ord_bucket(slot, waveCount), 1u)] = make_uint2(r, slot);
+    }
 }
 struct RcOrdCopy {
     const float4 *src[5];  // inputs x 4, target
     float4 *dst[5];
 };
-// One thread per bucket: insertion sort of its record indices by slot, then
-// the records copied to positions ctr[9] + (rank within the wave).
-__global__ void __launch_bounds__(256) k_rc_ord_gather(RcOrdCopy a, const uint32_t *ctr, const uint32_t *off,
-                                                       uint32_t *tmp) {
-    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= kRcOrdBuckets) return;
-    const uint32_t s0 = ctr[9], lo = off[b], hi = off[b + 1];
-    for (uint32_t i = lo + 1; i < hi; i++) {
-        const uint32_t x = tmp[i], kx = rc_ord_slot(a.src[1], x);
-        uint32_t j = i;
-        for (; j > lo && rc_ord_slot(a.src[1], tmp[j - 1]) > kx; j--) tmp[j] = tmp[j - 1];
-        tmp[j] = x;
-    }
-    for (uint32_t i = lo; i < hi; i++) {
-        const uint32_t r = tmp[i];
+// One thread per scattered record: its position is its bucket's offset plus
+// the number of the bucket's records with a smaller slot; the record's
+// training inputs and target are copied to ctr[9] + that position.
+__global__ void __launch_bounds__(256) k_rc_ord_place(RcOrdCopy a, const uint32_t *ctr, uint32_t waveCount,
+                                                      const uint32_t *off, const uint2 *tmp) {
+    const uint32_t s0 = ctr[9], n = ctr[10] - s0;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+        const uint2 e = tmp[j];
+        const uint32_t b = rc_ord_bucket(e.y, waveCount), lo = off[b], hi = off[b + 1];
+        uint32_t rank = 0;
+        for (uint32_t i = lo; i < hi; i++) rank += tmp[i].y < e.y ? 1u : 0u;
+        const uint32_t d = s0 + lo + rank;
 #pragma unroll
-        for (int k = 0; k < 5; k++) a.dst[k][s0 + i] = a.src[k][r];
+        for (int k = 0; k < 5; k++) a.dst[k][d] = a.src[k][e.x];
     }
 }
 
@@ -803,20 +859,20 @@ cudaError_t rc_enqueue_targets(pt_ctx *ctx, cudaStream_t st, float4 *lo_eta, uin
                                const float4 *pendE, uint32_t waveCount) {
     const RadianceCache &C = ctx->cache;
     RcRows<1> rec{C.rec[0], C.rec[1], C.rec[2], C.rec[3], C.rec[6], C.ctr + 2, (uint32_t)C.recCap, 1u, 0u};
-    k_rc_targets<<<1, 1024, 0, st>>>(rec, C.rec[4], C.rec[5], C.rec[6], C.rec[7], C.ctr, lo_eta, rng, pendA,
-                                     pendE);
-    // the wave's records in slot order (scratch: counts, offsets, cursors, indices)
-    uint32_t *cnt = C.ordScratch, *off = cnt + kRcOrdBuckets, *cur = off + kRcOrdBuckets + 1,
-             *tmp = cur + kRcOrdBuckets;
+    k_rc_targets<<<(unsigned)ctx->numSMs, 256, 0, st>>>(rec, C.rec[4], C.rec[5], C.rec[6], C.rec[7], C.ctr, lo_eta,
+                                                         rng, pendA, pendE);
+    // the wave's records in slot order (scratch: counts, offsets, cursors, (record, slot) pairs)
+    uint32_t *cnt = C.ordScratch, *off = cnt + kRcOrdBuckets, *cur = off + kRcOrdBuckets + 1;
+    uint2 *tmp = reinterpret_cast<uint2 *>(cur + kRcOrdBuckets + 1);  // 8-byte aligned: 3 x 4096 + 2 words before
     cudaError_t e = cudaMemsetAsync(cnt, 0, kRcOrdBuckets * sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
     const unsigned g = (unsigned)ctx->numSMs;
-    k_rc_ord_count<<<g, 256, 0, st>>>(C.rec[1], C.ctr, waveCount, cnt);
-    k_rc_ord_scan<<<1, 1024, 0, st>>>(cnt, off, cur);
+    k_rc_ord_count<<<g, 256, 0, st>>>(rec, C.ctr, waveCount, cnt);
+    k_rc_ord_scan<<<1, 1024, 0, st>>>(rec, cnt, off, cur, C.ctr);
     k_rc_ord_scatter<<<g, 256, 0, st>>>(C.rec[1], C.ctr, waveCount, cur, tmp);
     RcOrdCopy oc{{C.rec[0], C.rec[1], C.rec[2], C.rec[3], C.rec[6]},
                  {C.recOrd[0], C.recOrd[1], C.recOrd[2], C.recOrd[3], C.recOrd[4]}};
-    k_rc_ord_gather<<<kRcOrdBuckets / 256, 256, 0, st>>>(oc, C.ctr, off, tmp);
+    k_rc_ord_place<<<g, 256, 0, st>>>(oc, C.ctr, waveCount, off, tmp);
     return cudaGetLastError();
 }
 // kRcStepsPerCall (pt_internal.h) Adam steps per render call, step s on
@@ -834,12 +890,11 @@ cudaError_t rc_enqueue_train(pt_ctx *ctx, cudaStream_t st, uint32_t s, bool adam
         a.part = C.gradPart;
         a.lossSum = lossDev;
         k_rc_train<1><<<ctx->numSMs, kRcThreads, kTrainSmem, st>>>(a);
-        k_rc_grad_reduce<<<kReduceBlocks, 256, 0, st>>>(C.gradPart, (uint32_t)ctx->numSMs, C.grad);
-    } else {
+    } else {  // the slots' sum and the Adam update in one launch
         RcAdamArgs d{C.w, C.m, C.v, C.ema, C.grad, C.imgTrain, C.imgInfer, C.ctr, C.ctr + 2, (uint32_t)C.recCap,
                      C.params.train_records, kRcStepsPerCall, s, C.params.learning_rate, C.params.ema, lossDev,
                      s + 1 == kRcStepsPerCall ? 1u : 0u, C.params.max_train_fraction};
-        k_rc_adam<<<1, 1024, 0, st>>>(d);
+        k_rc_adam_slots<<<kReduceBlocks, 256, 0, st>>>(d, C.gradPart, (uint32_t)ctx->numSMs);
     }
     return cudaGetLastError();
 }
@@ -923,7 +978,7 @@ int pt_cache_init(pt_ctx *ctx, const pt_cache_params *params) {
     C.firstCall = true;
     for (float4 *&p : C.rec) A((void **)&p, C.recCap * sizeof(float4));
     for (float4 *&p : C.recOrd) A((void **)&p, C.recCap * sizeof(float4));
-    A((void **)&C.ordScratch, (3 * kRcOrdBuckets + 1 + C.recCap) * sizeof(uint32_t));
+    A((void **)&C.ordScratch, (3 * kRcOrdBuckets + 2 + 2 * C.recCap) * sizeof(uint32_t));
     if (e != cudaSuccess) {
         pt_cache_free(ctx);
         return ctx->fail(PT_E_NOMEM, "radiance cache", cudaGetErrorString(e));

@@ -126,8 +126,9 @@ struct RadianceCache {
     // call, [3] loss sum (float bits), [4] records of the last step, [5]
     // queries of the call, [6] first record not yet given a target, [7] the
     // chance (float) that a path at a cache vertex trains, set after each call,
-    // [8] loss of the step being trained (float), [9] first record of the
-    // wave whose targets were set last
+    // [8] loss of the step being trained (float), [9] / [10] first / end
+    // record of the wave whose targets were set last, [11] CTAs finished in
+    // the current Adam launch (reset by the last)
     uint32_t *ctr = nullptr;
     size_t queryCap = 0;
     float4 *q[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // record float4 x 4, weight

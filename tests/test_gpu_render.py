@@ -41,13 +41,22 @@ def test_per_path_parity(name, pt, scenes, ctx, oracle):
     oracle.load(sc)
     P = pt.render_params(W, H, 1, cam, max_depth=depth, sample_offset=3)
     sg, _, st = ctx.render(P)
-    so, per, _ = oracle.render(P, per_path=True)
+    so, per, (o_ext, o_nee) = oracle.render(P, per_path=True)
     assert np.all(sg[..., 3] == 1.0)
     g, o = sg[..., :3], per[0]
     close = np.abs(g - o) <= 1e-3 * np.maximum(np.abs(o), 1e-2)
     frac = float(close.all(-1).mean())
-    print(name, "pixels matching the oracle path:", frac, "rays", st.extension_rays, st.shadow_rays)
+    print(name, "pixels matching the oracle path:", frac, "rays", st.extension_rays, st.shadow_rays,
+          "oracle", o_ext, o_nee)
     assert frac > 0.97, frac
+    # The per-path ray counts of the bench's algorithmic bytes, checked against
+    # the oracle: one closest-hit trace per bounce on both sides (equal up to
+    # the few paths that differ); the oracle counts every NEE estimate, the
+    # device only the shadow rays it traces (an estimate already zero is not
+    # traced; the Cornell box's black envmap yields no envmap NEE rays), so
+    # that count is at most the oracle's.
+    assert abs(int(st.extension_rays) - int(o_ext)) <= 0.01 * o_ext, (st.extension_rays, o_ext)
+    assert 0.2 * o_nee <= st.shadow_rays <= o_nee, (st.shadow_rays, o_nee)
 
 
 @pytest.mark.parametrize("name", ["cornell", "spheres"])
