@@ -262,13 +262,14 @@ int pt_set_stream(pt_ctx *ctx, void *stream);
  *   a barrier nothing arrives at, before they issue any copy or tensor-core
  *   work, then take their error exit (TMEM freed): the call returns
  *   PT_E_DEVICE.  0 = off.
- * - PT_DEBUG_TAIL_OFF: value 1 keeps later renders in the per-bounce kernels
- *   to their last bounce (the tail kernel never takes the remaining paths),
- *   so that tests can compare both forms; 0 = the default.
+ * - PT_DEBUG_TAIL: which bounces the tail kernel takes, so that tests can
+ *   compare both forms: 0 = the default rule, 1 = never (the per-bounce
+ *   kernels run every render to its last bounce), 2 = whenever few paths are
+ *   left at bounce 4, however few bounces remain.
  * Setting a hook back to 0 restores normal operation on the same context. */
 #define PT_DEBUG_SHADOW_QUEUE_CAP 1u
 #define PT_DEBUG_CACHE_STALL 2u
-#define PT_DEBUG_TAIL_OFF 3u
+#define PT_DEBUG_TAIL 3u
 int pt_debug_set(pt_ctx *ctx, uint32_t what, uint64_t value);
 const char *pt_last_error(const pt_ctx *ctx);
 int pt_abi_version(void);

@@ -107,7 +107,7 @@ struct RenderGraph {
     uint32_t cached = 0, trainOn = 0;  // radiance-cache configuration baked into the launches
     uint32_t risNee = 0, flags = 0;
     uint64_t cacheGen = 0;
-    uint32_t shadowCap = 0, cacheStall = 0, tailMax = 0;  // test hooks baked into the launches
+    uint32_t shadowCap = 0, cacheStall = 0, tailMax = 0, tailMode = 0;  // test hooks baked into the launches
     uint64_t launches = 0;
 };
 
@@ -168,7 +168,7 @@ struct pt_ctx {
     int numSMs = 148;
     // test hooks (pt_debug_set): shadow-queue capacity override (0 = default)
     // and the polls of the cache kernels' up-front stall (0 = off)
-    uint32_t dbgShadowCap = 0, dbgCacheStall = 0, dbgTailOff = 0;
+    uint32_t dbgShadowCap = 0, dbgCacheStall = 0, dbgTail = 0;
     cudaStream_t stream = nullptr;     // stream all work is issued on
     cudaStream_t ownStream = nullptr;  // created by pt_create, destroyed by pt_destroy
     cudaEvent_t ev[2] = {nullptr, nullptr};  // brackets each render (stats.ms_total)

@@ -1226,6 +1226,15 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
 // the path's own queue position, and k_tail_close empties the queue so the
 // per-bounce kernels that follow (launched either way) find nothing; with
 // more paths left k_tail returns at once and the per-bounce kernels go on.
+// It is launched only when at least kTailMinRemaining bounces remain: one
+// thread per path keeps a warp's finished lanes idle until its longest path
+// ends (the per-bounce kernels compact them away every bounce), so the tail
+// pays only where it saves many per-bounce latency floors.  Measured with
+// the tail forced on (Mpaths/s): the 64-sphere scene at depth 16, 4 / 16 / 64
+// spp: 901 -> 1054, 1463 -> 1614, 1779 -> 1853; the Cornell box at depth 8,
+// 2 / 4 / 16 spp: 124 -> 100, 210 -> 155, 390 -> 196.  2^18 live paths let
+// the tail take the Cornell box at 16 spp; 2^17 does not, and keeps the
+// 64-sphere scene's gain.
 // The result does not depend on which runs: the tail calls the same shading
 // instantiations as the per-bounce kernels — the class-specialized ones, with
 // each deferred NEE ray resolved in place with k_shadow's arithmetic, or for
@@ -1235,7 +1244,8 @@ __global__ void __launch_bounds__(kBlock, ShadeBlocks<CLS>::value) k_shade(WaveA
 #define PT_TAIL_BOUNCE 4
 #endif
 constexpr uint32_t kTailBounce = PT_TAIL_BOUNCE;
-constexpr uint32_t kTailMaxPaths = 1u << 18;
+constexpr uint32_t kTailMaxPaths = 1u << 17;
+constexpr uint32_t kTailMinRemaining = 8;
 
 // A deferred NEE ray of a shading event, resolved here as k_shadow resolves a
 // queued one (its default instantiation): the pending record for the path's
@@ -1469,12 +1479,15 @@ enum {
     STG_RAYGEN, STG_EXTEND, STG_SHADE, STG_SHADOW, STG_FILM, STG_CACHE, STG_CACHE_INFER, STG_CACHE_TRAIN, STG_TAIL,
     STG_N
 };
-// The bounce at which k_tail may take a wave's remaining paths (depth: never).
-// Not for cached renders, RIS NEE or media in the wavefront form (other
-// shading instantiations).
-__host__ __device__ inline uint32_t tail_bounce(uint32_t depth, const WaveArgs &A) {
-    return (kTailBounce > 0 && kTailBounce < depth && !A.cacheOn && !A.risNee && !A.S.mediaWavefront) ? kTailBounce
-                                                                                                     : depth;
+// The bounce at which k_tail may take a wave's remaining paths (depth: never):
+// with at least kTailMinRemaining bounces after it, or any (tail mode 2:
+// tests).  Not for cached renders, RIS NEE or media in the wavefront form
+// (other shading instantiations).
+inline uint32_t tail_bounce(uint32_t depth, const WaveArgs &A, uint32_t tailMode) {
+    const bool enough = depth >= kTailBounce + kTailMinRemaining || tailMode == 2u;
+    return (kTailBounce > 0 && kTailBounce < depth && enough && !A.cacheOn && !A.risNee && !A.S.mediaWavefront)
+               ? kTailBounce
+               : depth;
 }
 struct Mark { int stage; cudaEvent_t a, b; };
 
@@ -1528,7 +1541,7 @@ cudaError_t enqueue_paths(const pt_ctx *ctx, Enqueue &E, WaveArgs &A, uint32_t d
         A.cntOut = B.counters + (1 - cur);
         chk(cudaMemsetAsync(A.cntOut, 0, 4, st));
         chk(cudaMemsetAsync(A.cntShadow, 0, 8, st));  // shadow count and the extend claim position
-        if (b == tail_bounce(depth, A)) {  // the remaining bounces of every path in one launch, when few are left
+        if (b == tail_bounce(depth, A, ctx->dbgTail)) {  // the remaining bounces of every path in one launch, when few are left
             E.begin(STG_TAIL);
             if (inl) k_tail<true><<<G.tailI, kBlock, 0, st>>>(A);
             else k_tail<false><<<G.tail, kBlock, 0, st>>>(A);
@@ -1639,6 +1652,7 @@ bool graph_matches(const pt_ctx *ctx, const pt_render_params *P, size_t cap, con
            G.cached == A.cacheOn && G.trainOn == A.trainOn && (!A.cacheOn || G.cacheGen == ctx->cache.gen) &&
            G.risNee == A.risNee && G.flags == (P->flags & ~PT_RENDER_STAGE_TIMING) &&
            G.shadowCap == A.shadowCap && G.cacheStall == ctx->dbgCacheStall && G.tailMax == A.tailMax &&
+           G.tailMode == ctx->dbgTail &&
            memcmp(&G.cam, &P->camera, sizeof(pt_camera)) == 0;
 }
 }  // namespace
@@ -1708,7 +1722,7 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
     A.clsStride = (uint32_t)B.cap;
     A.rayTotals = (unsigned long long *)(B.counters + 4);
     A.tailRays = (unsigned long long *)(B.counters + kCntTailRays);
-    A.tailMax = ctx->dbgTailOff ? 0u : kTailMaxPaths;
+    A.tailMax = ctx->dbgTail == 1u ? 0u : kTailMaxPaths;
     A.err = ctx->d_err;
     A.shadowCap = (uint32_t)(2 * B.cap);
     if (ctx->dbgShadowCap) A.shadowCap = std::min(A.shadowCap, ctx->dbgShadowCap);
@@ -1767,6 +1781,7 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
             G.cached = A.cacheOn; G.trainOn = A.trainOn; G.cacheGen = ctx->cache.gen; G.risNee = A.risNee;
             G.flags = P->flags & ~PT_RENDER_STAGE_TIMING;
             G.shadowCap = A.shadowCap; G.cacheStall = ctx->dbgCacheStall; G.tailMax = A.tailMax;
+            G.tailMode = ctx->dbgTail;
             G.launches = E.launches;
         } else {  // capture unavailable: issue the launches directly
             cudaGetLastError();
@@ -2064,7 +2079,7 @@ int render_batch(pt_ctx *ctx, const pt_request *R, uint32_t n, float *request_ms
     A.clsStride = (uint32_t)B.cap;
     A.rayTotals = (unsigned long long *)(B.counters + 4);
     A.tailRays = (unsigned long long *)(B.counters + kCntTailRays);
-    A.tailMax = ctx->dbgTailOff ? 0u : kTailMaxPaths;
+    A.tailMax = ctx->dbgTail == 1u ? 0u : kTailMaxPaths;
     A.err = ctx->d_err;
     A.shadowCap = (uint32_t)(2 * B.cap);
     A.batch = 1; A.numReqs = n; A.reqs = (const ReqDev *)Bt.reqs; A.slotInfo = Bt.slotInfo;
@@ -2078,7 +2093,8 @@ int render_batch(pt_ctx *ctx, const pt_request *R, uint32_t n, float *request_ms
     std::vector<uint64_t> key = {n, pl.cap, R[0].params.rng_kind, R[0].params.env_sampling, R[0].params.flags,
                                  ctx->sceneGen,
                                  ctx->waveGen, (uint64_t)(uintptr_t)Bt.slotInfo, (uint64_t)(uint32_t)G.extC,
-                                 (uint64_t)(uint32_t)G.shadow, (uint64_t)(uint32_t)clsG[CLS_DISNEY], A.tailMax};
+                                 (uint64_t)(uint32_t)G.shadow, (uint64_t)(uint32_t)clsG[CLS_DISNEY], A.tailMax,
+                                 ctx->dbgTail};
     for (uint32_t k = 0; k < n; k++) {
         key.push_back(hostReqs[k].width | ((uint64_t)hostReqs[k].height << 32));
         key.push_back(hostReqs[k].spp | ((uint64_t)hostReqs[k].maxDepth << 32));

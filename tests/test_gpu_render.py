@@ -225,16 +225,18 @@ def test_heterogeneous_media_wavefront(pt, scenes, ctx, oracle):
 
 @pytest.mark.parametrize("name", ["cornell", "spheres", "cool_scene1", "textured", "subsurface"])
 def test_tail_kernel_leaves_no_trace(name, pt, scenes):
-    """From bounce 4 on, a wave with at most 2^18 live paths runs its paths to
-    the end in one kernel; with more it stays in the per-bounce kernels.  Both
-    run the same shading code per path (the class-specialized kernels' code
-    with NEE resolved as the shadow kernel does, or the inline form for
-    subsurface scenes), so the film may not depend on which ran: the same
-    render with the tail and, through the PT_DEBUG_TAIL_OFF hook, without it,
-    equal bit for bit (and the tail checked to have traced rays).  The
-    classes covered: miss, emitter, diffuse, Disney (Cornell, spheres),
-    delta (mirror and glass), textured Disney and diffuse with an alpha
-    cut-out, and the inline form (subsurface)."""
+    """From bounce 4 on, a wave with at most 2^17 live paths and at least 8
+    bounces left runs its paths to the end in one kernel; otherwise it stays
+    in the per-bounce kernels.  Both run the same shading code per path (the
+    class-specialized kernels' code with NEE resolved as the shadow kernel
+    does, or the inline form for subsurface scenes), so the film may not
+    depend on which ran: the same render with the tail and, through the
+    PT_DEBUG_TAIL hook, without it, equal bit for bit (and the tail checked
+    to have traced rays).  At depth 8 the default rule keeps the per-bounce
+    kernels, and mode 2 forces the tail: again the same film.  The classes
+    covered: miss, emitter, diffuse, Disney (Cornell, spheres), delta
+    (mirror and glass), textured Disney and diffuse with an alpha cut-out,
+    and the inline form (subsurface)."""
     if name == "cornell":
         sc, cam = scenes.cornell(128, 128)
         W = H = 128
@@ -256,12 +258,19 @@ def test_tail_kernel_leaves_no_trace(name, pt, scenes):
         ctx.upload(sc)
         P = pt.render_params(W, H, 16, cam, max_depth=16, sample_offset=5)
         a, ca, sa = ctx.render(P)
-        ctx.debug_set(pt.PT_DEBUG_TAIL_OFF, 1)
+        ctx.debug_set(pt.PT_DEBUG_TAIL, 1)
         b, cb, sb = ctx.render(P)
-        ctx.debug_set(pt.PT_DEBUG_TAIL_OFF, 0)
+        ctx.debug_set(pt.PT_DEBUG_TAIL, 0)
         c, cc, sc2 = ctx.render(P)
+        P8 = pt.render_params(W, H, 16, cam, max_depth=8, sample_offset=5)
+        d, cd, sd = ctx.render(P8)
+        ctx.debug_set(pt.PT_DEBUG_TAIL, 2)
+        e, ce, se = ctx.render(P8)
+        ctx.debug_set(pt.PT_DEBUG_TAIL, 0)
     finally:
         ctx.close()
+    assert sd.tail_extension_rays == 0 and se.tail_extension_rays > 0
+    assert np.array_equal(d, e) and np.array_equal(cd, ce)
     print(name, "tail extension rays", sa.tail_extension_rays, "of", sa.extension_rays)
     assert sa.tail_extension_rays > 0 and sb.tail_extension_rays == 0 and sc2.tail_extension_rays > 0
     assert sa.extension_rays == sb.extension_rays and sa.shadow_rays == sb.shadow_rays
