@@ -57,6 +57,18 @@ __global__ void k_env_marginal(uint32_t H, const float *__restrict__ rowSums, fl
         for (uint32_t y = 0; y <= H; y++) marg[y] = __fdiv_rn((float)y, (float)H);
     }
 }
+// Guide tables of the CDF search (cdf_search_guided): for every conditional
+// row and the marginal, the search index at u = k / kCdfGuide, k = 0 .. kCdfGuide.
+__global__ void k_env_guides(uint32_t W, uint32_t H, const float *marg, const float *cond, uint16_t *margGuide,
+                             uint16_t *condGuide) {
+    const uint32_t per = kCdfGuide + 1, total = (H + 1) * per;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const uint32_t r = i / per, k = i % per;
+        const float u = (float)k / (float)kCdfGuide;  // exact
+        if (r < H) condGuide[i] = (uint16_t)cdf_upper(cond + (size_t)r * (W + 1), 0, W, u);
+        else margGuide[k] = (uint16_t)cdf_upper(marg, 0, H, u);
+    }
+}
 // FP64 texel weights and row sums of the alias tables.
 __global__ void k_alias_weights(uint32_t W, uint32_t H, const float4 *__restrict__ env, const float *__restrict__ sinRow,
                                 double *wall, double *rowSum) {
@@ -597,6 +609,11 @@ int pt_upload_scene(pt_ctx *ctx, const pt_scene_desc *d) {
     PT_CUDA(ctx->alloc_scene(&dcolProb, WH));
     PT_CUDA(ctx->alloc_scene(&dcolAlias, WH));
     PT_CUDA(ctx->alloc_scene(&dapdf, WH));
+    uint16_t *dmguide = nullptr, *dcguide = nullptr;  // 16-bit indices: rows up to 65,535 texels
+    if (W < 65536u && H < 65536u) {
+        PT_CUDA(ctx->alloc_scene(&dmguide, kCdfGuide + 1));
+        PT_CUDA(ctx->alloc_scene(&dcguide, (size_t)H * (kCdfGuide + 1)));
+    }
     if ((rc = h2d(denv, env4.data(), WH * sizeof(float4)))) return rc;
     {
         // temporaries: sin table, row sums, FP64 weights, Vose scratch
@@ -616,6 +633,7 @@ int pt_upload_scene(pt_ctx *ctx, const pt_scene_desc *d) {
         cudaMemcpyAsync(dsin, sinRow.data(), H * 4, cudaMemcpyHostToDevice, st);
         k_env_rows<<<blocks_for(H, 64), 64, 0, st>>>(W, H, denv, dsin, dcond, drowsum);
         k_env_marginal<<<1, 1, 0, st>>>(H, drowsum, dmarg);
+        if (dmguide) k_env_guides<<<256, 256, 0, st>>>(W, H, dmarg, dcond, dmguide, dcguide);
         k_alias_weights<<<blocks_for(H, 64), 64, 0, st>>>(W, H, denv, dsin, wall, rowSum);
         k_alias_marginal<<<1, 1, 0, st>>>(H, rowSum, drowProb, drowAlias, q, stk, total);
         k_alias_rows<<<blocks_for(H, 64), 64, 0, st>>>(W, H, wall, rowSum, dcolProb, dcolAlias, dapdf, q, stk, total);
@@ -625,6 +643,7 @@ int pt_upload_scene(pt_ctx *ctx, const pt_scene_desc *d) {
     }
     S.env = denv; S.envW = W; S.envH = H; S.envScale = d->env_scale;
     S.marg = dmarg; S.cond = dcond;
+    S.margGuide = dmguide; S.condGuide = dcguide;
     S.rowProb = drowProb; S.rowAlias = drowAlias; S.colProb = dcolProb; S.colAlias = dcolAlias; S.aliasPdf = dapdf;
     // --- volumes ------------------------------------------------------------------
     S.numVols = d->num_volumes;

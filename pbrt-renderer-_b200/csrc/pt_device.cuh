@@ -57,6 +57,7 @@ struct DevScene {
     uint32_t envW, envH;
     float envScale;
     const float *marg, *cond;
+    const uint16_t *margGuide, *condGuide;  // guide tables of the CDFs (null: rows wider than 65,535)
     const float *rowProb, *colProb, *aliasPdf;
     const uint32_t *rowAlias, *colAlias;
     // volumes
@@ -158,14 +159,28 @@ __device__ __forceinline__ float3 eval_env(const DevScene &S, float3 dir) {  // 
     dir_to_uv(dir, u, v, st);
     return env_bilinear(S, u, v) * S.envScale;
 }
-__device__ __forceinline__ uint32_t cdf_search(const float *buf, uint32_t n, float u) {  // Envmap.hlsli:31-45
-    uint32_t lo = 0, hi = n - 1;
+// The first index in [lo, hi) whose CDF value exceeds u, else hi.
+__device__ __forceinline__ uint32_t cdf_upper(const float *buf, uint32_t lo, uint32_t hi, float u) {
     while (lo < hi) {
         uint32_t mid = (lo + hi) >> 1;
         if (__ldg(buf + mid) <= u) lo = mid + 1;
         else hi = mid;
     }
-    return (uint32_t)max(0, (int)lo - 1);
+    return lo;
+}
+__device__ __forceinline__ uint32_t cdf_search(const float *buf, uint32_t n, float u) {  // Envmap.hlsli:31-45
+    return (uint32_t)max(0, (int)cdf_upper(buf, 0, n - 1, u) - 1);
+}
+// The same search narrowed by a guide table (Chen and Asau's cutpoint
+// method): guide[k] = cdf_upper(buf, 0, n - 1, k / kCdfGuide) for k = 0 ..
+// kCdfGuide.  For u in [k, k + 1) / kCdfGuide (exact: kCdfGuide is a power of
+// two) the search result is monotone in u, so it lies in [guide[k],
+// guide[k + 1]], and the loop over that range returns the same index as over
+// the whole CDF; a few steps instead of log2(n).
+constexpr uint32_t kCdfGuide = 256;
+__device__ __forceinline__ uint32_t cdf_search_guided(const float *buf, const uint16_t *guide, float u) {
+    const uint32_t k = min((uint32_t)(u * (float)kCdfGuide), kCdfGuide - 1u);
+    return (uint32_t)max(0, (int)cdf_upper(buf, __ldg(guide + k), __ldg(guide + k + 1), u) - 1);
 }
 __device__ __forceinline__ float3 env_dir_from_uv(float u, float v, float &st) {
     float phi = 2.0f * kPi * u, theta = kPi * v;
@@ -178,12 +193,13 @@ __device__ __forceinline__ float3 env_dir_from_uv(float u, float v, float &st) {
 __device__ __forceinline__ void env_sample_cdf(const DevScene &S, float u1, float u2, float3 &dir, float3 &rad,
                                                float &pdf) {  // Envmap.hlsli:58-101
     const uint32_t W = S.envW, H = S.envH;
-    uint32_t y = cdf_search(S.marg, H + 1, u1);
+    uint32_t y = S.margGuide ? cdf_search_guided(S.marg, S.margGuide, u1) : cdf_search(S.marg, H + 1, u1);
     float m0 = __ldg(S.marg + y), m1 = __ldg(S.marg + y + 1);
     float pMar = m1 - m0;
     float jv = pMar > 1e-20f ? sat((u1 - m0) / pMar) : 0.5f;
     const float *row = S.cond + (size_t)y * (W + 1);
-    uint32_t x = cdf_search(row, W + 1, u2);
+    uint32_t x = S.condGuide ? cdf_search_guided(row, S.condGuide + (size_t)y * (kCdfGuide + 1), u2)
+                             : cdf_search(row, W + 1, u2);
     float c0 = __ldg(row + x), c1 = __ldg(row + x + 1);
     float pCon = c1 - c0;
     float ju = pCon > 1e-20f ? sat((u2 - c0) / pCon) : 0.5f;

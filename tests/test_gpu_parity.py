@@ -270,6 +270,41 @@ def test_envmap_sample_pdf_parity(mode, ctx, oracle, sky_scene):
     assert float(np.quantile(rel_err(pg2, po2, 1e-6), 0.999)) <= 1e-5
 
 
+def test_envmap_guided_search_edges(ctx, oracle, sky_scene):
+    """The CDF sampler narrows each binary search with a 256-cell guide table;
+    the chosen texel must be the plain search's for every u, including the
+    points where the narrowing could go wrong: the cell boundaries k / 256
+    (and their float neighbours), and u equal to a CDF entry (the search's
+    tie rule), for the marginal and for the conditional rows.  The oracle
+    searches the whole CDF."""
+    sc, _ = sky_scene
+    ctx.upload(sc)
+    oracle.load(sc)
+    mg, cg = ctx.env_cdf()
+    H = mg.size - 1
+    cg = cg.reshape(H, -1)
+    rng = np.random.default_rng(61)
+    k = np.arange(257, dtype=np.float32) / np.float32(256)
+    edges = np.concatenate([k, np.nextafter(k, np.float32(0)), np.nextafter(k, np.float32(1))])
+    edges = edges[(edges >= 0) & (edges < 1)].astype(np.float32)
+    ties_m = mg[(mg >= 0) & (mg < 1)].astype(np.float32)
+    # marginal: boundaries and ties, with random column draws
+    u1a = np.concatenate([edges, ties_m])
+    u2a = rng.uniform(0, 1, u1a.size).astype(np.float32)
+    # conditional: random rows, u2 a CDF entry of the row u1 selects, or a boundary
+    # (the row as the search picks it: the last entry <= u among all but the last)
+    u1b = rng.uniform(0, 1, 20000).astype(np.float32)
+    y = np.maximum(np.searchsorted(mg[:-1], u1b, side="right") - 1, 0)
+    u2b = cg[y, rng.integers(0, cg.shape[1], y.size)].astype(np.float32)
+    u2b = np.where((u2b >= 0) & (u2b < 1), u2b, rng.choice(edges, y.size)).astype(np.float32)
+    u2b[::3] = rng.choice(edges, u2b[::3].size)
+    u = np.concatenate([np.stack([u1a, u2a], 1), np.stack([u1b, u2b], 1)]).astype(np.float32)
+    dg, rg, pg = ctx.env_sample(0, u)
+    do, ro, po = oracle.env_sample(0, u)
+    assert np.abs(dg - do).max() < 1e-5
+    assert float(np.quantile(rel_err(pg, po, 1e-6), 0.999)) <= 1e-5
+
+
 @pytest.mark.parametrize("mode", [0, 1])
 def test_envmap_sampler_distribution(mode, pt, ctx, scenes):
     """Sampled texels follow lum * sin(theta) (the density both tables encode):
