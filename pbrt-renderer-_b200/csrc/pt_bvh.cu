@@ -3,7 +3,8 @@
 // Replaces the driver's BLAS/TLAS build (src/gpu/DXRApp_Scene.cpp:37-170 of
 // gracejinsotrue/PBRT-renderer-) with:
 //   1. per-triangle bounds and 30-bit Morton codes of the centroids,
-//   2. a stable radix sort of (code, triangle id) (CUB),
+//   2. a stable radix sort of (code, triangle id): four 8-bit passes of
+//      per-tile digit counts, one scan, and an order-keeping scatter,
 //   3. the Karras 2012 binary radix tree over the sorted codes (ties broken by
 //      position, so the topology is a pure function of the input),
 //   4. bottom-up bounds with one atomic per internal node,
@@ -19,13 +20,92 @@
 //      surface area until it has 8; subtrees of <= 3 triangles become leaves.
 //      Child boxes are quantised to 8 bits per plane against a power-of-two
 //      grid with directed rounding, so every stored box contains its child.
-#include <cub/device/device_radix_sort.cuh>
-
 #include "pt_internal.h"
 
 namespace pt {
 
 constexpr uint32_t kLeafMax = 3;
+
+// ---- stable LSD radix sort of (code, id) pairs, 8-bit digits -------------------
+// One pass per digit (shift 0, 8, 16, 24).  k_rs_hist counts each tile's
+// digits, stored digit-major (hist[d * tiles + tile]) so that one exclusive
+// scan gives every (digit, tile) its first output position; k_rs_scatter
+// walks its tile in rounds of 256 keys in input order and places each key at
+// its digit's next position plus its rank among the round's equal digits
+// (earlier warps, then earlier lanes: __match_any_sync), so equal keys keep
+// their order and the result is the unique stable sort.
+constexpr uint32_t kRsThreads = 256, kRsRounds = 64, kRsTile = kRsThreads * kRsRounds;  // 16,384 keys per tile
+__global__ void __launch_bounds__(kRsThreads) k_rs_hist(const uint32_t *keys, uint32_t n, uint32_t shift,
+                                                        uint32_t tiles, uint32_t *hist) {
+    __shared__ uint32_t h[256];
+    h[threadIdx.x] = 0u;
+    __syncthreads();
+    const uint32_t base = blockIdx.x * kRsTile;
+    for (uint32_t i = threadIdx.x; i < kRsTile; i += kRsThreads) {
+        const uint32_t j = base + i;
+        if (j < n) atomicAdd(&h[(keys[j] >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    hist[threadIdx.x * tiles + blockIdx.x] = h[threadIdx.x];
+}
+// One block: exclusive scan of m counts in place (contiguous runs per thread).
+__global__ void __launch_bounds__(1024) k_rs_scan(uint32_t *a, uint32_t m) {
+    __shared__ uint32_t part[1024];
+    const uint32_t t = threadIdx.x, per = (m + 1023) / 1024, lo = min(m, t * per), hi = min(m, lo + per);
+    uint32_t sum = 0;
+    for (uint32_t i = lo; i < hi; i++) sum += a[i];
+    part[t] = sum;
+    __syncthreads();
+    for (uint32_t o = 1; o < 1024; o <<= 1) {
+        const uint32_t v = t >= o ? part[t - o] : 0u;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    uint32_t run = part[t] - sum;
+    for (uint32_t i = lo; i < hi; i++) {
+        const uint32_t c = a[i];
+        a[i] = run;
+        run += c;
+    }
+}
+__global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const uint32_t *keys, const uint32_t *vals, uint32_t n,
+                                                           uint32_t shift, uint32_t tiles, const uint32_t *off,
+                                                           uint32_t *keysOut, uint32_t *valsOut) {
+    constexpr uint32_t kWarps = kRsThreads / 32;
+    __shared__ uint32_t next[256];          // this tile's next output position of each digit
+    __shared__ uint32_t wcnt[kWarps][256];  // the current round's count of each digit per warp
+    const uint32_t t = threadIdx.x, lane = t & 31u, w = t >> 5;
+    next[t] = off[t * tiles + blockIdx.x];
+    const uint32_t base = blockIdx.x * kRsTile;
+    for (uint32_t r = 0; r < kRsRounds; r++) {
+#pragma unroll
+        for (uint32_t k = 0; k < kWarps; k++) wcnt[k][t] = 0u;  // thread t owns column t
+        __syncthreads();
+        const uint32_t j = base + r * kRsThreads + t;
+        const bool valid = j < n;
+        uint32_t key = 0u, val = 0u, d = 256u + lane;  // past the end: a digit no other lane has
+        if (valid) {
+            key = keys[j];
+            val = vals[j];
+            d = (key >> shift) & 255u;
+        }
+        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
+        if (valid && lane == (uint32_t)__ffs(peers) - 1u) wcnt[w][d] = __popc(peers);
+        __syncthreads();
+        if (valid) {
+            uint32_t pos = next[d] + __popc(peers & ((1u << lane) - 1u));
+            for (uint32_t k = 0; k < w; k++) pos += wcnt[k][d];
+            keysOut[pos] = key;
+            valsOut[pos] = val;
+        }
+        __syncthreads();
+        uint32_t tot = 0u;
+#pragma unroll
+        for (uint32_t k = 0; k < kWarps; k++) tot += wcnt[k][t];
+        next[t] += tot;  // read by other threads only after the next round's first barrier
+    }
+}
 
 __device__ __forceinline__ uint32_t expand_bits(uint32_t v) {
     v = (v * 0x00010001u) & 0xFF0000FFu;
@@ -569,11 +649,22 @@ int pt_build_bvh_device(pt_ctx *ctx, const uint32_t *d_meshFirstTri, uint32_t n)
     cudaMemcpyAsync(bounds, binit, sizeof(binit), cudaMemcpyHostToDevice, st);
     k_centroid_bounds<<<min(G, 1024u), B, 0, st>>>(n, cen, bounds);
     k_morton<<<G, B, 0, st>>>(n, cen, bounds, codes, ids);
-    size_t tb = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, tb, codes, codesS, ids, idsS, (int)n, 0, 30, st);
-    void *dtmp;
-    TA(dtmp, tb);
-    cub::DeviceRadixSort::SortPairs(dtmp, tb, codes, codesS, ids, idsS, (int)n, 0, 30, st);
+    {  // (codes, ids) -> (codesS, idsS) by the 30-bit code; `codes` stays unsorted (read back for parity)
+        const uint32_t tiles = (n + kRsTile - 1) / kRsTile;
+        uint32_t *rsHist, *kA, *vA;
+        TA(rsHist, (size_t)256 * tiles * 4);
+        TA(kA, (size_t)n * 4);
+        TA(vA, (size_t)n * 4);
+        const uint32_t *kin = codes, *vin = ids;
+        uint32_t *kout[4] = {kA, codesS, kA, codesS}, *vout[4] = {vA, idsS, vA, idsS};
+        for (int p = 0; p < 4; p++) {
+            k_rs_hist<<<tiles, kRsThreads, 0, st>>>(kin, n, 8u * p, tiles, rsHist);
+            k_rs_scan<<<1, 1024, 0, st>>>(rsHist, 256u * tiles);
+            k_rs_scatter<<<tiles, kRsThreads, 0, st>>>(kin, vin, n, 8u * p, tiles, rsHist, kout[p], vout[p]);
+            kin = kout[p];
+            vin = vout[p];
+        }
+    }
     if (n > 1) {
         k_karras<<<(n - 1 + B - 1) / B, B, 0, st>>>((int)n, codesS, children, intParent, leafParent, rf, rl);
         cudaMemsetAsync(flags, 0, (size_t)(n - 1) * 4, st);

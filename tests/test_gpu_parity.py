@@ -305,6 +305,24 @@ def test_envmap_guided_search_edges(ctx, oracle, sky_scene):
     assert float(np.quantile(rel_err(pg, po, 1e-6), 0.999)) <= 1e-5
 
 
+def test_envmap_wide_rows_plain_search(pt, ctx, oracle, scenes):
+    """Rows of 65,536 texels or more do not fit the guide tables' 16-bit
+    indices: such an envmap keeps the plain binary search, with the same
+    samples as the oracle."""
+    env = scenes.sky_envmap(65536, 2, sun_peak=40.0, sun_sigma_deg=4.0)
+    m = pt.make_material(pt.PT_MAT_DIFFUSE)
+    tri = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32)
+    m.vertexCount, m.indexCount = 3, 3
+    sc = pt.Scene(tri, np.array([0, 1, 2]), [m], env_rgb=env)
+    ctx.upload(sc)
+    oracle.load(sc)
+    u = np.random.default_rng(62).uniform(0, 1, (1 << 16, 2)).astype(np.float32)
+    dg, rg, pg = ctx.env_sample(0, u)
+    do, ro, po = oracle.env_sample(0, u)
+    assert np.abs(dg - do).max() < 1e-5
+    assert float(np.quantile(rel_err(pg, po, 1e-6), 0.999)) <= 1e-5
+
+
 @pytest.mark.parametrize("mode", [0, 1])
 def test_envmap_sampler_distribution(mode, pt, ctx, scenes):
     """Sampled texels follow lum * sin(theta) (the density both tables encode):
