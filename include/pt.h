@@ -266,10 +266,14 @@ int pt_set_stream(pt_ctx *ctx, void *stream);
  *   compare both forms: 0 = the default rule, 1 = never (the per-bounce
  *   kernels run every render to its last bounce), 2 = whenever few paths are
  *   left at bounce 4, however few bounces remain.
+ * - PT_DEBUG_WIDE_PLAN: value 1 makes later scene uploads collapse the BVH
+ *   by the least-area plan, which by default only trees too large for the
+ *   L2 use, so that tests can check those trees on small scenes.
  * Setting a hook back to 0 restores normal operation on the same context. */
 #define PT_DEBUG_SHADOW_QUEUE_CAP 1u
 #define PT_DEBUG_CACHE_STALL 2u
 #define PT_DEBUG_TAIL 3u
+#define PT_DEBUG_WIDE_PLAN 4u
 int pt_debug_set(pt_ctx *ctx, uint32_t what, uint64_t value);
 const char *pt_last_error(const pt_ctx *ctx);
 int pt_abi_version(void);

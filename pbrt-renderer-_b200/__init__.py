@@ -37,7 +37,7 @@ PT_CACHE_FEATURES = 64
 PT_CACHE_RECORD_FLOATS = 16
 PT_CACHE_MAX_RECORDS = 262144
 PT_CACHE_NO_TRAIN = 1
-PT_DEBUG_SHADOW_QUEUE_CAP, PT_DEBUG_CACHE_STALL, PT_DEBUG_TAIL = 1, 2, 3
+PT_DEBUG_SHADOW_QUEUE_CAP, PT_DEBUG_CACHE_STALL, PT_DEBUG_TAIL, PT_DEBUG_WIDE_PLAN = 1, 2, 3, 4
 PT_E_DEVICE = -5
 
 

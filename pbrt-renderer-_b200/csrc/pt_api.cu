@@ -327,6 +327,7 @@ int pt_debug_set(pt_ctx *ctx, uint32_t what, uint64_t value) {
     if (value > 0xFFFFFFFFull) return ctx->fail(PT_E_INVALID, "debug value out of range");
     if (what == PT_DEBUG_SHADOW_QUEUE_CAP) ctx->dbgShadowCap = (uint32_t)value;
     else if (what == PT_DEBUG_CACHE_STALL) ctx->dbgCacheStall = (uint32_t)value;
+    else if (what == PT_DEBUG_WIDE_PLAN) ctx->dbgWidePlan = value ? 1u : 0u;
     else if (what == PT_DEBUG_TAIL) {
         if (value > 2) return ctx->fail(PT_E_INVALID, "tail mode: 0, 1 or 2");
         ctx->dbgTail = (uint32_t)value;

@@ -20,6 +20,10 @@
 //      surface area until it has 8; subtrees of <= 3 triangles become leaves.
 //      Child boxes are quantised to 8 bits per plane against a power-of-two
 //      grid with directed rounding, so every stored box contains its child.
+//      Trees too large for the L2 are collapsed instead by a least-area
+//      plan (dynamic programming over the binary tree); a result deeper than
+//      the traversal stack is collapsed the other way, then, if still too
+//      deep, from the radix tree.
 #include "pt_internal.h"
 
 namespace pt {
@@ -417,6 +421,66 @@ __global__ void k_treelet(TreeletIn T) {
     }
 }
 
+// ---- collapse plan: least summed area of the wide nodes (Ylitie, Karras and
+// Laine 2017, "Efficient Incoherent Ray Traversal on GPUs Through Compressed
+// Wide BVHs", section 3) -------------------------------------------------------
+// Leaf slots are the maximal subtrees of <= kLeafMax triangles, a fixed set,
+// so the tree's cost that the collapse can change is the summed box area of
+// its wide nodes.  cost[8 node + i - 1]: the least such sum over node's
+// subtree when it takes at most i child slots of the wide node above it
+// (leaf slots: 0).  plan[8 node + i - 1]: 0 = node fills one slot itself (a
+// leaf slot or a wide node of its own), k > 0 = node is opened, k slots to
+// its first child and i - k to its second.  planW[node]: the split of node's
+// own 8 slots when it is a wide node.  Bottom-up like k_refit.
+__global__ void k_wide_plan(int n, const int32_t *__restrict__ children, const int32_t *__restrict__ intParent,
+                            const int32_t *__restrict__ leafParent, const uint32_t *__restrict__ cnt,
+                            const float4 *__restrict__ intLo, const float4 *__restrict__ intHi, float *cost,
+                            uint8_t *plan, uint8_t *planW, uint32_t *flags) {
+    int leaf = blockIdx.x * blockDim.x + threadIdx.x;
+    if (leaf >= n || n == 1) return;
+    int node = leafParent[leaf];
+    for (int guard = 0; node >= 0 && guard < n; guard++) {
+        __threadfence();
+        if (atomicAdd(&flags[node], 1u) == 0u) return;  // first arrival: sibling finishes the node
+        float *cn = cost + 8 * (size_t)node;
+        uint8_t *pn = plan + 8 * (size_t)node;
+        if (cnt[node] <= kLeafMax) {
+            for (int i = 0; i < 8; i++) { cn[i] = 0.0f; pn[i] = 0; }
+            planW[node] = 0;
+        } else {
+            const int32_t c0 = children[2 * node], c1 = children[2 * node + 1];
+            float d0[8], d1[8];
+            const bool w0 = c0 >= 0 && cnt[c0] > kLeafMax, w1 = c1 >= 0 && cnt[c1] > kLeafMax;
+            for (int i = 0; i < 8; i++) {
+                d0[i] = w0 ? __ldcg(cost + 8 * (size_t)c0 + i) : 0.0f;
+                d1[i] = w1 ? __ldcg(cost + 8 * (size_t)c1 + i) : 0.0f;
+            }
+            // j slots split between the children, each at least one: the least sum, first k on ties
+            auto split = [&](int j, int &bk) {
+                float b = 3.0e38f;
+                bk = 1;
+                for (int k = 1; k < j; k++) {
+                    const float v = d0[k - 1] + d1[j - k - 1];
+                    if (v < b) { b = v; bk = k; }
+                }
+                return b;
+            };
+            int kw;
+            const float single = area(intLo[node], intHi[node]) + split(8, kw);
+            planW[node] = (uint8_t)kw;
+            cn[0] = single;
+            pn[0] = 0;
+            for (int j = 2; j <= 8; j++) {
+                int k;
+                const float sj = split(j, k);
+                if (sj < single) { cn[j - 1] = sj; pn[j - 1] = (uint8_t)k; }
+                else { cn[j - 1] = single; pn[j - 1] = 0; }
+            }
+        }
+        node = intParent[node];
+    }
+}
+
 struct CollapseIn {
     int n;
     const int32_t *children;
@@ -431,6 +495,7 @@ struct CollapseIn {
     BVH8Node *nodes;
     float4 *tri;
     uint32_t *counters;  // [0] wide nodes allocated, [1] triangles written, [2] next queue size, [3] error
+    const uint8_t *plan, *planW;  // k_wide_plan's choices (null: open the largest child until 8)
 };
 
 // Exponent e (biased) with (hi - lo) / 2^(e-127) <= 255, from an upper bound.
@@ -460,7 +525,25 @@ __global__ void k_collapse(CollapseIn C, const int2 *__restrict__ qin, uint32_t 
         cnt = 1;
     }
     auto openable = [&](int32_t r) { return r >= 0 && C.cnt[r] > kLeafMax; };
-    while (cnt < 8) {
+    if (root >= 0 && C.plan && openable(root)) {  // (a root of <= kLeafMax triangles keeps its two children)
+        // the plan's children: (binary node, slots) pairs, first child first;
+        // the slots on the stack sum to at most 8, one or more each
+        int32_t stn[8];
+        int sts[8], sp = 0;
+        const int kw = C.planW[root];
+        stn[sp] = ch[1]; sts[sp++] = 8 - kw;
+        stn[sp] = ch[0]; sts[sp++] = kw;
+        cnt = 0;
+        while (sp > 0) {
+            const int32_t m = stn[--sp];
+            const int j = sts[sp];
+            const int k = openable(m) ? C.plan[8 * (size_t)m + j - 1] : 0;
+            if (k <= 0 || k >= j) { ch[cnt++] = m; continue; }
+            stn[sp] = C.children[2 * m + 1]; sts[sp++] = j - k;
+            stn[sp] = C.children[2 * m]; sts[sp++] = k;
+        }
+    }
+    while (!C.plan && cnt < 8) {
         int best = -1;
         float ba = -1.0f;
         for (int i = 0; i < cnt; i++)
@@ -679,6 +762,9 @@ int pt_build_bvh_device(pt_ctx *ctx, const uint32_t *d_meshFirstTri, uint32_t n)
     const size_t ni = (size_t)max(n - 1, 1u);
     TA(cnt, ni * 4); TA(cost, ni * 4); TA(rewired, 4);
     TA(tch, ni * 8); TA(tip, ni * 4); TA(tlp, (size_t)n * 4);
+    float *planCost;
+    uint8_t *planSlots, *planWide;
+    TA(planCost, ni * 8 * 4); TA(planSlots, ni * 8); TA(planWide, ni);
     if (n > 1) {
         k_range_count<<<(n - 1 + B - 1) / B, B, 0, st>>>((int)n, rf, rl, cnt);
         cudaMemcpyAsync(tch, children, (size_t)(n - 1) * 8, cudaMemcpyDeviceToDevice, st);
@@ -706,20 +792,41 @@ int pt_build_bvh_device(pt_ctx *ctx, const uint32_t *d_meshFirstTri, uint32_t n)
     cudaError_t e1 = ctx->alloc_scene(&nodes, maxWide);
     cudaError_t e2 = ctx->alloc_scene(&tri, 3 * (size_t)n);
     if (e1 != cudaSuccess || e2 != cudaSuccess) { cleanup(); return ctx->fail(PT_E_NOMEM, "bvh nodes"); }
-    // A wide tree deeper than the traversal stack falls back to the radix
-    // tree (its depth is bounded by the key bits plus the index bits of
-    // equal keys); the restructured tree is used whenever it fits.
+    // Two collapses of the restructured tree: greedy (the largest child
+    // opened until 8) and k_wide_plan's least-area plan.  Which goes first
+    // depends on whether the tree's nodes and triangles (~71 bytes per
+    // triangle) fit in the L2.  If they do, traversal runs from L2 and the
+    // greedy tree is the faster one: the 64-sphere scene at 1866 vs 1846
+    // Mpaths/s, the Cornell box at 390 vs 382.  If they do not, traversal
+    // waits on DRAM for each node, and the plan's fewer node visits win:
+    // the 10 M-triangle scene at 467 vs 458.  A result deeper than the
+    // traversal stack is collapsed the other way, and only then does the
+    // build fall back to the radix tree (its depth is bounded by the key
+    // bits plus the index bits of equal keys).
+    int l2 = 0;
+    cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, ctx->device);
+    const bool planFirst = ctx->dbgWidePlan || (uint64_t)n * 71u > (uint64_t)(l2 > 0 ? l2 : 126 << 20);
     uint32_t cnt4[4];
-    for (int attempt = 0; attempt < 2; attempt++) {
-        const bool radix = attempt == 1 || n == 1;
-        if (attempt == 1) {  // restore the radix tree's bounds and counts
+    for (int attempt = 0; attempt < 3; attempt++) {
+        const bool radix = attempt == 2 || n == 1;
+        const bool usePlan = attempt == (planFirst ? 0 : 1);
+        if (attempt == 2) {  // restore the radix tree's bounds and counts
             cudaMemsetAsync(flags, 0, (size_t)(n - 1) * 4, st);
             k_refit<<<G, B, 0, st>>>((int)n, idsS, tlo, thi, children, intParent, leafParent, leafLo, leafHi, intLo,
                                      intHi, flags);
             k_range_count<<<(n - 1 + B - 1) / B, B, 0, st>>>((int)n, rf, rl, cnt);
         }
+        const uint8_t *plan = nullptr, *planW = nullptr;
+        if (usePlan && n > 1) {  // the collapse plan of the restructured tree
+            cudaMemsetAsync(flags, 0, (size_t)(n - 1) * 4, st);
+            k_wide_plan<<<G, B, 0, st>>>((int)n, radix ? children : tch, radix ? intParent : tip,
+                                         radix ? leafParent : tlp, cnt, intLo, intHi, planCost, planSlots,
+                                         planWide, flags);
+            plan = planSlots;
+            planW = planWide;
+        }
         CollapseIn C{(int)n, radix ? children : tch, cnt, maxWide, leafLo, leafHi, intLo, intHi, idsS, triMesh,
-                     d_meshFirstTri, S.mats, S.idx, S.pos, nodes, tri, counters};
+                     d_meshFirstTri, S.mats, S.idx, S.pos, nodes, tri, counters, plan, planW};
         int2 root = make_int2(n > 1 ? 0 : ~0, 0);
         cudaMemcpyAsync(qa, &root, sizeof(root), cudaMemcpyHostToDevice, st);
         uint32_t cinit[4] = {1u, 0u, 0u, 0u};

@@ -168,7 +168,7 @@ struct pt_ctx {
     int numSMs = 148;
     // test hooks (pt_debug_set): shadow-queue capacity override (0 = default)
     // and the polls of the cache kernels' up-front stall (0 = off)
-    uint32_t dbgShadowCap = 0, dbgCacheStall = 0, dbgTail = 0;
+    uint32_t dbgShadowCap = 0, dbgCacheStall = 0, dbgTail = 0, dbgWidePlan = 0;
     cudaStream_t stream = nullptr;     // stream all work is issued on
     cudaStream_t ownStream = nullptr;  // created by pt_create, destroyed by pt_destroy
     cudaEvent_t ev[2] = {nullptr, nullptr};  // brackets each render (stats.ms_total)

@@ -395,16 +395,20 @@ def _surface_rays(sc, rng, n):
     return o.astype(np.float32), d.astype(np.float32)
 
 
-@pytest.mark.parametrize("which", ["spheres", "cornell", "hair", "bench"])
-def test_trace_parity(which, ctx, oracle, scenes, bench_scene):
+@pytest.mark.parametrize("which", ["spheres", "cornell", "hair", "bench", "spheres_plan", "bench_plan"])
+def test_trace_parity(which, pt, ctx, oracle, scenes, bench_scene):
     """Closest hits against the oracle's SAH BVH.  The triangle test rounds as
     the oracle's (bit-identical t, u, v), so a ray may disagree only where
     traversal decides: an equal-t tie between triangles, or a hit within
     1e-6 (barycentric) of an edge that one tree's box test grazes.  No other
     disagreement is allowed.  The bench scene's 1,310,720-triangle tree gets
-    2^20 rays, half from random points in space, half leaving its surfaces."""
+    2^20 rays, half from random points in space, half leaving its surfaces.
+    The *_plan cases build the 8-wide tree by the least-area plan, which
+    only trees larger than the L2 get by default (PT_DEBUG_WIDE_PLAN)."""
     rng = np.random.default_rng(47)
     n = 200000
+    plan = which.endswith("_plan")
+    which = which.replace("_plan", "")
     if which == "spheres":
         sc, _ = scenes.disney_spheres(32, 32, grid=3, slices=48, rings=25, env_w=16, env_h=8)
         lo, hi = -6.0, 6.0
@@ -418,7 +422,11 @@ def test_trace_parity(which, ctx, oracle, scenes, bench_scene):
         sc, _ = bench_scene
         n = 1 << 20
         lo, hi = sc.positions.min(0) - 1.0, sc.positions.max(0) + 1.0
-    ctx.upload(sc)
+    ctx.debug_set(pt.PT_DEBUG_WIDE_PLAN, 1 if plan else 0)
+    try:
+        ctx.upload(sc)
+    finally:
+        ctx.debug_set(pt.PT_DEBUG_WIDE_PLAN, 0)
     oracle.load(sc)
     o = rng.uniform(lo, hi, (n, 3)).astype(np.float32)
     d = scenes.sample_directions(n, 48)

@@ -33,11 +33,19 @@ SCENES = {
 }
 
 
-@pytest.mark.parametrize("name", ["cornell", "spheres"])
+@pytest.mark.parametrize("name", ["cornell", "spheres", "spheres_plan"])
 def test_per_path_parity(name, pt, scenes, ctx, oracle):
+    """Per-path equality with the oracle; spheres_plan renders over the 8-wide
+    tree of the least-area plan (PT_DEBUG_WIDE_PLAN)."""
+    plan = name.endswith("_plan")
+    name = name.replace("_plan", "")
     make, W, H, depth = SCENES[name]
     sc, cam = make(scenes)
-    ctx.upload(sc)
+    ctx.debug_set(pt.PT_DEBUG_WIDE_PLAN, 1 if plan else 0)
+    try:
+        ctx.upload(sc)
+    finally:
+        ctx.debug_set(pt.PT_DEBUG_WIDE_PLAN, 0)
     oracle.load(sc)
     P = pt.render_params(W, H, 1, cam, max_depth=depth, sample_offset=3)
     sg, _, st = ctx.render(P)
