@@ -529,6 +529,27 @@ __device__ __forceinline__ void put_bf16(uint8_t *img, int i, float x) {
     *reinterpret_cast<__nv_bfloat16 *>(img + rc_image_base(l) + rc_core_offset(o, in, rc_rows(l))) =
         __float2bfloat16_rn(x);
 }
+// One parameter's Adam update from its gradient sum over n records (3 outputs
+// each): FP32 master weight, moments and inference average, then both BF16
+// images.
+__device__ __forceinline__ void rc_adam_param(const RcAdamArgs &a, int i, float gradSum, uint32_t n,
+                                              uint32_t step) {
+    const float b1 = 0.9f, b2 = 0.99f, eps = 1e-8f;
+    const float gs = 1.0f / (3.0f * (float)n);
+    const float bc1 = 1.0f - powf(b1, (float)step), bc2 = 1.0f - powf(b2, (float)step);
+    float g = gradSum * gs;
+    if (!isfinite(g)) g = 0.0f;
+    float m = b1 * a.m[i] + (1.0f - b1) * g;
+    float v = b2 * a.v[i] + (1.0f - b2) * g * g;
+    a.m[i] = m;
+    a.v[i] = v;
+    float w = a.w[i] - a.lr * (m / bc1) / (sqrtf(v / bc2) + eps);
+    a.w[i] = w;
+    float e = (step == 1u || a.emaDecay == 0.0f) ? w : a.emaDecay * a.ema[i] + (1.0f - a.emaDecay) * w;
+    a.ema[i] = e;
+    put_bf16(a.imgTrain, i, w);
+    put_bf16(a.imgInfer, i, e);
+}
 __global__ void __launch_bounds__(1024) k_rc_adam(RcAdamArgs a) {
     __shared__ uint32_t sStep, sN;
     if (threadIdx.x == 0) {
@@ -546,23 +567,10 @@ __global__ void __launch_bounds__(1024) k_rc_adam(RcAdamArgs a) {
     __syncthreads();
     const uint32_t n = sN, step = sStep;
     if (n == 0) return;
-    const float b1 = 0.9f, b2 = 0.99f, eps = 1e-8f;
-    const float gs = 1.0f / (3.0f * (float)n);
-    const float bc1 = 1.0f - powf(b1, (float)step), bc2 = 1.0f - powf(b2, (float)step);
     for (int i = threadIdx.x; i < kRcParams; i += blockDim.x) {
-        float g = a.grad[i] * gs;
+        const float g = a.grad[i];
         a.grad[i] = 0.0f;
-        if (!isfinite(g)) g = 0.0f;
-        float m = b1 * a.m[i] + (1.0f - b1) * g;
-        float v = b2 * a.v[i] + (1.0f - b2) * g * g;
-        a.m[i] = m;
-        a.v[i] = v;
-        float w = a.w[i] - a.lr * (m / bc1) / (sqrtf(v / bc2) + eps);
-        a.w[i] = w;
-        float e = (step == 1u || a.emaDecay == 0.0f) ? w : a.emaDecay * a.ema[i] + (1.0f - a.emaDecay) * w;
-        a.ema[i] = e;
-        put_bf16(a.imgTrain, i, w);
-        put_bf16(a.imgInfer, i, e);
+        rc_adam_param(a, i, g, n, step);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -597,21 +605,7 @@ __global__ void __launch_bounds__(256) k_rc_adam_slots(RcAdamArgs a, const float
     if (i < kRcParams) {
         float sum = 0.0f;
         for (uint32_t k = 0; k < slots; k++) sum += __ldcs(part + (size_t)k * kRcParams + i);
-        const float b1 = 0.9f, b2 = 0.99f, eps = 1e-8f;
-        const float gs = 1.0f / (3.0f * (float)n);
-        const float bc1 = 1.0f - powf(b1, (float)step), bc2 = 1.0f - powf(b2, (float)step);
-        float g = sum * gs;
-        if (!isfinite(g)) g = 0.0f;
-        float m = b1 * a.m[i] + (1.0f - b1) * g;
-        float v = b2 * a.v[i] + (1.0f - b2) * g * g;
-        a.m[i] = m;
-        a.v[i] = v;
-        float w = a.w[i] - a.lr * (m / bc1) / (sqrtf(v / bc2) + eps);
-        a.w[i] = w;
-        float e = (step == 1u || a.emaDecay == 0.0f) ? w : a.emaDecay * a.ema[i] + (1.0f - a.emaDecay) * w;
-        a.ema[i] = e;
-        put_bf16(a.imgTrain, i, w);
-        put_bf16(a.imgInfer, i, e);
+        rc_adam_param(a, (int)i, sum, n, step);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
