@@ -621,6 +621,8 @@ __global__ void __launch_bounds__(256) k_rc_adam_slots(RcAdamArgs a, const float
     }
 }
 
+__global__ void k_rc_set_chance(float *chance, float p) { *chance = p; }
+
 // Images from the FP32 weights (initialisation, pt_cache_weights).
 __global__ void k_rc_images(const float *w, uint8_t *imgTrain, uint8_t *imgInfer, float *ema) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kRcParams; i += gridDim.x * blockDim.x) {
@@ -902,9 +904,8 @@ int rc_render_setup(pt_ctx *ctx, size_t waveCap, uint64_t callPaths) {
         // 1.5 x train_records / paths keeps the first call's records well
         // inside the buffers (twice the target) and their choice repeatable
         const float p = std::min(C.params.max_train_fraction, 1.5f * (float)C.params.train_records / (float)callPaths);
-        if (cudaMemcpyAsync(C.ctr + 7, &p, 4, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess ||
-            cudaStreamSynchronize(ctx->stream) != cudaSuccess)
-            return ctx->fail(PT_E_CUDA, "cache training chance");
+        k_rc_set_chance<<<1, 1, 0, ctx->stream>>>(reinterpret_cast<float *>(C.ctr + 7), p);  // stream-ordered, no sync
+        if (cudaGetLastError() != cudaSuccess) return ctx->fail(PT_E_CUDA, "cache training chance");
         C.firstCall = false;
     }
     // a path makes at most two queries per wave: at its cache vertex and, as a
