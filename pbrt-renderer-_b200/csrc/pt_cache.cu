@@ -671,27 +671,29 @@ __global__ void __launch_bounds__(256) k_rc_targets(RcRows<1> rec, float4 *beta,
 // ---- the records of a wave in a fixed order ------------------------------------
 // Records are appended by the shading kernels in whatever order their warps
 // run, and an Adam step's batch and its gradient sums follow record order.
-// Each wave's records are therefore put in path-slot order (a path leaves
-// at most one record per wave, so slots are distinct): counted into
-// kRcOrdBuckets buckets of consecutive slots, scanned, scattered with their
-// slots, and each record placed at its bucket's offset plus its rank by slot
+// Each wave's records are therefore put in the order of their key (rec[2].w:
+// sample x pixels + pixel position, from the wave's first sample group; a
+// path leaves at most one record per wave, so keys are distinct, and they do
+// not depend on the order in which the wave runs its paths): counted into
+// kRcOrdBuckets buckets of consecutive keys, scanned, scattered with their
+// keys, and each record placed at its bucket's offset plus its rank by key
 // among the bucket's few records; the training inputs and targets are copied
 // to recOrd there.  Training reads recOrd, and cached renders repeat bit for
 // bit.  The wave's records are [ctr[6], count) until k_rc_ord_scan records
 // that range in ctr[9], ctr[10] and moves ctr[6] on.
 constexpr uint32_t kRcOrdBuckets = 4096;
-__device__ __forceinline__ uint32_t rc_ord_slot(const float4 *r1, uint32_t r) {
-    return __float_as_uint(__ldg(reinterpret_cast<const float *>(r1 + r) + 3));
+__device__ __forceinline__ uint32_t rc_ord_key(const float4 *r2, uint32_t r) {
+    return __float_as_uint(__ldg(reinterpret_cast<const float *>(r2 + r) + 3));
 }
-__device__ __forceinline__ uint32_t rc_ord_bucket(uint32_t slot, uint32_t waveCount) {
-    // slots lie below waveCount; the clamp keeps any other value in bounds
-    return min((uint32_t)(((uint64_t)slot * kRcOrdBuckets) / waveCount), kRcOrdBuckets - 1u);
+__device__ __forceinline__ uint32_t rc_ord_bucket(uint32_t key, uint32_t keyRange) {
+    // keys lie below keyRange; the clamp keeps any other value in bounds
+    return min((uint32_t)(((uint64_t)key * kRcOrdBuckets) / max(keyRange, 1u)), kRcOrdBuckets - 1u);
 }
-__global__ void __launch_bounds__(256) k_rc_ord_count(RcRows<1> rec, const uint32_t *ctr, uint32_t waveCount,
+__global__ void __launch_bounds__(256) k_rc_ord_count(RcRows<1> rec, const uint32_t *ctr, uint32_t keyRange,
                                                       uint32_t *cnt) {
     const uint32_t s0 = ctr[6], s1 = rec.total();
     for (uint32_t r = s0 + blockIdx.x * blockDim.x + threadIdx.x; r < s1; r += gridDim.x * blockDim.x)
-        atomicAdd(cnt + rc_ord_bucket(rc_ord_slot(rec.r1, r), waveCount), 1u);
+        atomicAdd(cnt + rc_ord_bucket(rc_ord_key(rec.r2, r), keyRange), 1u);
 }
 // One block: exclusive scan of the bucket counts into off (kRcOrdBuckets + 1
 // entries) and the scatter cursors; then the wave's record range moves to
@@ -731,14 +733,14 @@ __global__ void __launch_bounds__(1024) k_rc_ord_scan(RcRows<1> rec, const uint3
         ctr[5] += ctr[1];
     }
 }
-// Record indices and their slots into bucket order (order within a bucket:
-// whatever the atomics give; the place kernel ranks by slot).
-__global__ void __launch_bounds__(256) k_rc_ord_scatter(const float4 *r1, const uint32_t *ctr, uint32_t waveCount,
+// Record indices and their keys into bucket order (order within a bucket:
+// whatever the atomics give; the place kernel ranks by key).
+__global__ void __launch_bounds__(256) k_rc_ord_scatter(const float4 *r2, const uint32_t *ctr, uint32_t keyRange,
                                                         uint32_t *cur, uint2 *tmp) {
     const uint32_t s0 = ctr[9], s1 = ctr[10];
     for (uint32_t r = s0 + blockIdx.x * blockDim.x + threadIdx.x; r < s1; r += gridDim.x * blockDim.x) {
-        const uint32_t slot = rc_ord_slot(r1, r);
-        tmp[atomicAdd(cur + rc_ord_bucket(slot, waveCount), 1u)] = make_uint2(r, slot);
+        const uint32_t key = rc_ord_key(r2, r);
+        tmp[atomicAdd(cur + rc_ord_bucket(key, keyRange), 1u)] = make_uint2(r, key);
     }
 }
 struct RcOrdCopy {
@@ -746,14 +748,14 @@ struct RcOrdCopy {
     float4 *dst[5];
 };
 // One thread per scattered record: its position is its bucket's offset plus
-// the number of the bucket's records with a smaller slot; the record's
+// the number of the bucket's records with a smaller key; the record's
 // training inputs and target are copied to ctr[9] + that position.
-__global__ void __launch_bounds__(256) k_rc_ord_place(RcOrdCopy a, const uint32_t *ctr, uint32_t waveCount,
+__global__ void __launch_bounds__(256) k_rc_ord_place(RcOrdCopy a, const uint32_t *ctr, uint32_t keyRange,
                                                       const uint32_t *off, const uint2 *tmp) {
     const uint32_t s0 = ctr[9], n = ctr[10] - s0;
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
         const uint2 e = tmp[j];
-        const uint32_t b = rc_ord_bucket(e.y, waveCount), lo = off[b], hi = off[b + 1];
+        const uint32_t b = rc_ord_bucket(e.y, keyRange), lo = off[b], hi = off[b + 1];
         uint32_t rank = 0;
         for (uint32_t i = lo; i < hi; i++) rank += tmp[i].y < e.y ? 1u : 0u;
         const uint32_t d = s0 + lo + rank;
@@ -852,7 +854,7 @@ cudaError_t rc_enqueue_resolve(pt_ctx *ctx, cudaStream_t st, float4 *lo_eta) {
     return cudaGetLastError();
 }
 cudaError_t rc_enqueue_targets(pt_ctx *ctx, cudaStream_t st, float4 *lo_eta, uint4 *rng, const float4 *pendA,
-                               const float4 *pendE, uint32_t waveCount) {
+                               const float4 *pendE, uint32_t keyRange) {
     const RadianceCache &C = ctx->cache;
     RcRows<1> rec{C.rec[0], C.rec[1], C.rec[2], C.rec[3], C.rec[6], C.ctr + 2, (uint32_t)C.recCap, 1u, 0u};
     k_rc_targets<<<(unsigned)ctx->numSMs, 256, 0, st>>>(rec, C.rec[4], C.rec[5], C.rec[6], C.rec[7], C.ctr, lo_eta,
@@ -863,12 +865,12 @@ cudaError_t rc_enqueue_targets(pt_ctx *ctx, cudaStream_t st, float4 *lo_eta, uin
     cudaError_t e = cudaMemsetAsync(cnt, 0, kRcOrdBuckets * sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
     const unsigned g = (unsigned)ctx->numSMs;
-    k_rc_ord_count<<<g, 256, 0, st>>>(rec, C.ctr, waveCount, cnt);
+    k_rc_ord_count<<<g, 256, 0, st>>>(rec, C.ctr, keyRange, cnt);
     k_rc_ord_scan<<<1, 1024, 0, st>>>(rec, cnt, off, cur, C.ctr);
-    k_rc_ord_scatter<<<g, 256, 0, st>>>(C.rec[1], C.ctr, waveCount, cur, tmp);
+    k_rc_ord_scatter<<<g, 256, 0, st>>>(C.rec[2], C.ctr, keyRange, cur, tmp);
     RcOrdCopy oc{{C.rec[0], C.rec[1], C.rec[2], C.rec[3], C.rec[6]},
                  {C.recOrd[0], C.recOrd[1], C.recOrd[2], C.recOrd[3], C.recOrd[4]}};
-    k_rc_ord_place<<<g, 256, 0, st>>>(oc, C.ctr, waveCount, off, tmp);
+    k_rc_ord_place<<<g, 256, 0, st>>>(oc, C.ctr, keyRange, off, tmp);
     return cudaGetLastError();
 }
 // kRcStepsPerCall (pt_internal.h) Adam steps per render call, step s on

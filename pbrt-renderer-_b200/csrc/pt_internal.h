@@ -293,9 +293,9 @@ void pt_cache_free(pt_ctx *ctx);
 int pt_cache_prepare(pt_ctx *ctx, size_t queryCap);  // query buffers for a cached render
 int rc_render_setup(pt_ctx *ctx, size_t waveCap, uint64_t callPaths);  // checks, bounds, query buffers
 cudaError_t rc_enqueue_resolve(pt_ctx *ctx, cudaStream_t st, float4 *lo_eta);
-// the wave's records: training targets, then their fixed order (waveCount: the wave's paths)
+// the wave's records: training targets, then their fixed order (keyRange: their order keys lie below it)
 cudaError_t rc_enqueue_targets(pt_ctx *ctx, cudaStream_t st, float4 *lo_eta, uint4 *rng, const float4 *pendA,
-                               const float4 *pendE, uint32_t waveCount);
+                               const float4 *pendE, uint32_t keyRange);
 // one training step s of kRcStepsPerCall: the network kernel (adam = false) or its Adam update (adam = true)
 cudaError_t rc_enqueue_train(pt_ctx *ctx, cudaStream_t st, uint32_t s, bool adam);
 constexpr uint32_t kRcStepsPerCall = 4;  // Adam steps per cached render call, on interleaved quarters of its records

@@ -52,6 +52,9 @@ struct ReqDev {
 struct WaveArgs {
     DevScene S;
     uint32_t width, height, npix;
+    uint32_t spp, spp8, fullTilePix;  // the call's samples, those in full groups of 8, pixels in full 8 x 4 tiles
+    uint64_t recKeyBase;  // a training record's order key: sample x npix + position - recKeyBase (this wave)
+    uint32_t recKeyRange; // keys of this wave's records lie in [0, recKeyRange)
     const uint32_t *sampleOffset;  // -> sample index of path id 0 of this render call
     uint32_t rngKind, envMode, maxDepth;
     uint64_t waveStart;      // first path id of the wave
@@ -139,6 +142,49 @@ __device__ __forceinline__ uint32_t find_request(const WaveArgs &A, uint64_t pid
     }
     return lo;
 }
+// Path order of a render call (path id -> pixel position of tile_pixel,
+// sample of the call).  Samples run one after the other over the pixel
+// positions, except the first spp8, which go in groups of 8: within a
+// group, each 8 x 4 tile's eight 2 x 2 pixel blocks in turn, a block's 32
+// paths being its 4 pixels x the group's 8 samples — a warp's camera rays
+// then lie within 2 x 2 pixels rather than 8 x 4.  Positions outside the
+// full tiles take the group's samples one after the other.  A bijection;
+// path_id is its inverse (the film sums each pixel's samples in sample
+// order through it).
+__host__ __device__ inline void path_pos_sample(const WaveArgs &A, uint64_t pid, uint32_t &p, uint32_t &s) {
+    const uint32_t npix = A.npix;
+    const uint64_t grouped = (uint64_t)A.spp8 * npix;
+    if (pid < grouped) {
+        const uint64_t gsz = 8ull * npix;
+        const uint32_t c = (uint32_t)(pid / gsz), r = (uint32_t)(pid % gsz), full = A.fullTilePix;
+        if (r < 8u * full) {
+            const uint32_t t = r >> 8, q = r & 255u, b = q >> 5, u = q & 31u, i = u & 3u;
+            p = 32u * t + ((2u * (b >> 2) + (i >> 1)) << 3) + 2u * (b & 3u) + (i & 1u);
+            s = 8u * c + (u >> 2);
+        } else {
+            const uint32_t r2 = r - 8u * full, rem = npix - full;
+            p = full + r2 % rem;
+            s = 8u * c + r2 / rem;
+        }
+    } else {
+        const uint64_t q = pid - grouped;
+        p = (uint32_t)(q % npix);
+        s = A.spp8 + (uint32_t)(q / npix);
+    }
+}
+__device__ __forceinline__ uint64_t path_id(const WaveArgs &A, uint32_t p, uint32_t s) {
+    const uint32_t npix = A.npix;
+    if (s < A.spp8) {
+        const uint64_t base = (uint64_t)(s >> 3) * 8u * npix;
+        const uint32_t si = s & 7u, full = A.fullTilePix;
+        if (p < full) {
+            const uint32_t t = p >> 5, w = p & 31u, row = w >> 3, col = w & 7u;
+            return base + 256ull * t + 32u * ((row >> 1) * 4u + (col >> 1)) + 4u * si + (row & 1u) * 2u + (col & 1u);
+        }
+        return base + 8ull * full + (uint64_t)si * (npix - full) + (p - full);
+    }
+    return (uint64_t)A.spp8 * npix + (uint64_t)(s - A.spp8) * npix + p;
+}
 __device__ __forceinline__ void path_coords(const WaveArgs &A, uint32_t slot, uint32_t &pix, uint32_t &frame) {
     if (A.batch) {
         uint2 si = A.slotInfo[slot];
@@ -146,9 +192,10 @@ __device__ __forceinline__ void path_coords(const WaveArgs &A, uint32_t slot, ui
         frame = si.y;
         return;
     }
-    uint64_t pid = A.waveStart + slot;
-    pix = tile_pixel(A, (uint32_t)(pid % A.npix));
-    frame = __ldg(A.sampleOffset) + (uint32_t)(pid / A.npix);
+    uint32_t p, s;
+    path_pos_sample(A, A.waveStart + slot, p, s);
+    pix = tile_pixel(A, p);
+    frame = __ldg(A.sampleOffset) + s;
 }
 // Per-request image size and depth of a path (the render's own without a batch).
 __device__ __forceinline__ uint32_t path_depth(const WaveArgs &A, uint32_t slot) {
@@ -281,6 +328,7 @@ __device__ __forceinline__ void bind_stack(TravStack &, uint2 *) {}
 // their traversal waits on DRAM in large scenes and wants the warps more than
 // those registers.
 constexpr int kTraversalBlocksPerSm = 4;
+
 
 // Persistent work-stealing over a ray queue: each warp claims the next 32
 // queue positions with one atomic (so a warp's rays stay neighbours in the
@@ -957,6 +1005,12 @@ __device__ __forceinline__ void shade_item(const WaveArgs &A, bool active, uint3
                         uint32_t r = warp_append(A.crCount, true);
                         if (r < A.recCap) {
                             cache_record(A.cr, r, hp, -rd, N, m, type, slot);
+                            {  // its order key, independent of the path order: sample-major
+                                uint32_t kp, ks;
+                                path_pos_sample(A, A.waveStart + slot, kp, ks);
+                                A.cr[2][r].w = __uint_as_float(
+                                    (uint32_t)((uint64_t)ks * A.npix + kp - A.recKeyBase));
+                            }
                             A.cr[4][r] = make_float4(thr.x, thr.y, thr.z, 0.0f);
                             A.cr[5][r] = make_float4(Lo.x, Lo.y, Lo.z, 0.0f);
                             st.w |= kFlagTrain | kFlagHasRec | (r << 8);
@@ -1339,14 +1393,30 @@ __device__ __forceinline__ void kahan(float &s, float &c, float x) {
     c = (t - s) - y;
     s = t;
 }
+// One thread per pixel position: the wave's samples of the pixel, in sample
+// order (path_id), Kahan-added to the film.
 __global__ void k_film(WaveArgs A, float4 *sum, float4 *comp) {
-    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t cover = min(A.waveCount, A.npix);
-    if (t >= cover) return;
-    uint64_t first = A.waveStart, last = A.waveStart + A.waveCount;
-    uint32_t pix = tile_pixel(A, (uint32_t)((first + t) % A.npix));
-    float4 s = sum[pix], c = comp[pix];
-    for (uint64_t pid = first + t; pid < last; pid += A.npix) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= A.npix) return;
+    const uint64_t first = A.waveStart, last = A.waveStart + A.waveCount;
+    // the samples the wave can hold: its first and last paths' samples, widened to their groups
+    uint32_t p0, s0, p1, s1;
+    path_pos_sample(A, first, p0, s0);
+    path_pos_sample(A, last - 1, p1, s1);
+    if (s0 < A.spp8) s0 &= ~7u;
+    if (s1 < A.spp8) s1 |= 7u;
+    s1 = min(s1, A.spp - 1u);
+    bool any = false;
+    float4 s = make_float4(0.0f, 0.0f, 0.0f, 0.0f), c = s;
+    const uint32_t pix = tile_pixel(A, p);
+    for (uint32_t smp = s0; smp <= s1; smp++) {
+        const uint64_t pid = path_id(A, p, smp);
+        if (pid < first || pid >= last) continue;
+        if (!any) {
+            s = sum[pix];
+            c = comp[pix];
+            any = true;
+        }
         uint32_t slot = (uint32_t)(pid - first);
         float4 le = A.lo_eta[slot];
         float3 L = make_float3(le.x, le.y, le.z);
@@ -1361,8 +1431,10 @@ __global__ void k_film(WaveArgs A, float4 *sum, float4 *comp) {
         kahan(s.z, c.z, L.z);
         kahan(s.w, c.w, 1.0f);
     }
-    sum[pix] = s;
-    comp[pix] = c;
+    if (any) {
+        sum[pix] = s;
+        comp[pix] = c;
+    }
 }
 
 // Film of request q for the paths of this wave (k_film's order: per pixel,
@@ -1601,6 +1673,16 @@ cudaError_t enqueue_render(const pt_ctx *ctx, Enqueue &E, WaveArgs A, const pt_r
     for (uint64_t ws = 0; ws < total; ws += cap) {
         A.waveStart = ws;
         A.waveCount = (uint32_t)std::min<uint64_t>(cap, total - ws);
+        {  // the samples this wave holds (whole groups of 8): its training records' key range
+            uint32_t p0, s0, p1, s1;
+            path_pos_sample(A, A.waveStart, p0, s0);
+            path_pos_sample(A, A.waveStart + A.waveCount - 1, p1, s1);
+            if (s0 < A.spp8) s0 &= ~7u;
+            if (s1 < A.spp8) s1 |= 7u;
+            s1 = std::min(s1, A.spp - 1u);
+            A.recKeyBase = (uint64_t)s0 * A.npix;
+            A.recKeyRange = (uint32_t)std::min<uint64_t>((uint64_t)(s1 - s0 + 1) * A.npix, 0xFFFFFFFFull);
+        }
         if (cached) chk(cudaMemsetAsync(A.cqCount, 0, 4, st));
         chk(enqueue_paths(ctx, E, A, P->max_depth, G));
         if (cached) {
@@ -1612,10 +1694,10 @@ cudaError_t enqueue_render(const pt_ctx *ctx, Enqueue &E, WaveArgs A, const pt_r
             // training targets from the suffixes, then the training paths' image
             // values (prefix + throughput x cache); counts the wave's queries
             E.begin(STG_CACHE);
-            chk(rc_enqueue_targets(const_cast<pt_ctx *>(ctx), st, A.lo_eta, A.rng, A.pendA, A.pendE, A.waveCount));
+            chk(rc_enqueue_targets(const_cast<pt_ctx *>(ctx), st, A.lo_eta, A.rng, A.pendA, A.pendE, A.recKeyRange));
             E.end();
         }
-        uint32_t cover = (uint32_t)std::min<uint64_t>(A.waveCount, npix);
+        uint32_t cover = (uint32_t)npix;  // k_film: one thread per pixel position
         if (ws == 0) {  // the film's contents (a host film's upload may still be in flight)
             cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
             chk(cudaStreamIsCapturing(st, &cs));
@@ -1708,6 +1790,9 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
     WaveArgs A;
     A.S = ctx->S;
     A.width = W; A.height = H; A.npix = (uint32_t)npix;
+    A.spp = P->spp;
+    A.spp8 = P->spp & ~7u;  // samples in groups of 8 (path_pos_sample)
+    A.fullTilePix = 32u * (W / 8u) * (H / 4u);
     A.sampleOffset = ctx->d_err + 1;
     A.rngKind = P->rng_kind; A.envMode = P->env_sampling; A.maxDepth = P->max_depth;
     A.cam = P->camera;
@@ -2066,6 +2151,9 @@ int render_batch(pt_ctx *ctx, const pt_request *R, uint32_t n, float *request_ms
     memset(&A, 0, sizeof(A));
     A.S = ctx->S;
     A.width = hostReqs[0].width; A.height = hostReqs[0].height; A.npix = hostReqs[0].npix;
+    A.spp = A.spp8 = A.fullTilePix = 0u;  // batches keep their own path order (slotInfo)
+    A.recKeyBase = 0u;
+    A.recKeyRange = 0u;
     A.sampleOffset = ctx->d_err + 1;
     A.rngKind = R[0].params.rng_kind; A.envMode = R[0].params.env_sampling; A.maxDepth = 0;
     A.thr_pdf = B.thr_pdf; A.lo_eta = B.lo_eta; A.pendA = B.pendA; A.pendE = B.pendE; A.rng = B.rng;
