@@ -142,10 +142,11 @@ def measured_peaks():
 
 
 # k_extend DRAM traffic per extension ray (dram__bytes_read.sum + dram__bytes_write.sum
-# from one ncu capture of this workload at 4 spp: 233.6 MB over the 3,686,400
-# camera rays of bounce 0).  The scene is L2-resident and the queues stream
-# once, so traffic scales with the rays a launch processes.
-EXTEND_DRAM_BYTES_PER_RAY = {"disney_envmap": 63.4}
+# from one ncu capture of this workload at 8 spp, the smallest case in the
+# grouped path order of the full frame: 383.3 MB over the 7,372,800 camera
+# rays of bounce 0).  The scene is L2-resident and the queues stream once, so
+# traffic scales with the rays a launch processes.
+EXTEND_DRAM_BYTES_PER_RAY = {"disney_envmap": 52.0}
 
 
 REF_SPP = 4096        # reference image: plain path tracing, samples [0, 4096)
