@@ -52,7 +52,7 @@ struct ReqDev {
 struct WaveArgs {
     DevScene S;
     uint32_t width, height, npix;
-    uint32_t spp, spp8, fullTilePix;  // the call's samples, those in full groups of 8, pixels in full 8 x 4 tiles
+    uint32_t spp, spp32, spp8, fullTilePix;  // the call's samples, those in groups of 32, then of 8; pixels in full 8 x 4 tiles
     uint64_t recKeyBase;  // a training record's order key: sample x npix + position - recKeyBase (this wave)
     uint32_t recKeyRange; // keys of this wave's records lie in [0, recKeyRange)
     const uint32_t *sampleOffset;  // -> sample index of path id 0 of this render call
@@ -143,47 +143,74 @@ __device__ __forceinline__ uint32_t find_request(const WaveArgs &A, uint64_t pid
     return lo;
 }
 // Path order of a render call (path id -> pixel position of tile_pixel,
-// sample of the call).  Samples run one after the other over the pixel
-// positions, except the first spp8, which go in groups of 8: within a
-// group, each 8 x 4 tile's eight 2 x 2 pixel blocks in turn, a block's 32
-// paths being its 4 pixels x the group's 8 samples — a warp's camera rays
-// then lie within 2 x 2 pixels rather than 8 x 4.  Positions outside the
-// full tiles take the group's samples one after the other.  A bijection;
-// path_id is its inverse (the film sums each pixel's samples in sample
-// order through it).
+// sample of the call).  The call's samples go in groups, so that a warp's
+// 32 paths are camera rays of few pixels: first as many groups of 32 as
+// fit (a warp = 32 samples of one pixel; consecutive warps follow the pixel
+// positions), then groups of 8 (within a group, each 8 x 4 tile's eight
+// 2 x 2 pixel blocks in turn, a block's 32 paths being its 4 pixels x the 8
+// samples; positions outside the full tiles take the group's samples one
+// after the other), and the remaining samples one after the other over the
+// pixel positions.  A bijection; path_id is its inverse (the film sums each
+// pixel's samples in sample order through it).  Measured on the 64-sphere
+// frame (Mpaths/s): one sample at a time 1849, groups of 8 1958, groups of
+// 32 2040; the 10 M-triangle scene at 16 spp per call: 466 -> 489 with 8.
 __host__ __device__ inline void path_pos_sample(const WaveArgs &A, uint64_t pid, uint32_t &p, uint32_t &s) {
     const uint32_t npix = A.npix;
-    const uint64_t grouped = (uint64_t)A.spp8 * npix;
-    if (pid < grouped) {
+    const uint64_t g32 = (uint64_t)A.spp32 * npix;
+    if (pid < g32) {
+        const uint64_t gsz = 32ull * npix;
+        const uint32_t c = (uint32_t)(pid / gsz), r = (uint32_t)(pid % gsz);
+        p = r >> 5;
+        s = 32u * c + (r & 31u);
+        return;
+    }
+    pid -= g32;
+    const uint64_t g8 = (uint64_t)A.spp8 * npix;
+    if (pid < g8) {
         const uint64_t gsz = 8ull * npix;
         const uint32_t c = (uint32_t)(pid / gsz), r = (uint32_t)(pid % gsz), full = A.fullTilePix;
         if (r < 8u * full) {
             const uint32_t t = r >> 8, q = r & 255u, b = q >> 5, u = q & 31u, i = u & 3u;
             p = 32u * t + ((2u * (b >> 2) + (i >> 1)) << 3) + 2u * (b & 3u) + (i & 1u);
-            s = 8u * c + (u >> 2);
+            s = A.spp32 + 8u * c + (u >> 2);
         } else {
             const uint32_t r2 = r - 8u * full, rem = npix - full;
             p = full + r2 % rem;
-            s = 8u * c + r2 / rem;
+            s = A.spp32 + 8u * c + r2 / rem;
         }
-    } else {
-        const uint64_t q = pid - grouped;
-        p = (uint32_t)(q % npix);
-        s = A.spp8 + (uint32_t)(q / npix);
+        return;
     }
+    const uint64_t q = pid - g8;
+    p = (uint32_t)(q % npix);
+    s = A.spp32 + A.spp8 + (uint32_t)(q / npix);
 }
 __device__ __forceinline__ uint64_t path_id(const WaveArgs &A, uint32_t p, uint32_t s) {
     const uint32_t npix = A.npix;
-    if (s < A.spp8) {
-        const uint64_t base = (uint64_t)(s >> 3) * 8u * npix;
-        const uint32_t si = s & 7u, full = A.fullTilePix;
+    if (s < A.spp32) return (uint64_t)(s >> 5) * 32u * npix + 32ull * p + (s & 31u);
+    const uint64_t base = (uint64_t)A.spp32 * npix;
+    const uint32_t s2 = s - A.spp32;
+    if (s2 < A.spp8) {
+        const uint64_t gbase = base + (uint64_t)(s2 >> 3) * 8u * npix;
+        const uint32_t si = s2 & 7u, full = A.fullTilePix;
         if (p < full) {
             const uint32_t t = p >> 5, w = p & 31u, row = w >> 3, col = w & 7u;
-            return base + 256ull * t + 32u * ((row >> 1) * 4u + (col >> 1)) + 4u * si + (row & 1u) * 2u + (col & 1u);
+            return gbase + 256ull * t + 32u * ((row >> 1) * 4u + (col >> 1)) + 4u * si + (row & 1u) * 2u + (col & 1u);
         }
-        return base + 8ull * full + (uint64_t)si * (npix - full) + (p - full);
+        return gbase + 8ull * full + (uint64_t)si * (npix - full) + (p - full);
     }
-    return (uint64_t)A.spp8 * npix + (uint64_t)(s - A.spp8) * npix + p;
+    return base + (uint64_t)A.spp8 * npix + (uint64_t)(s2 - A.spp8) * npix + p;
+}
+// The first and last sample of sample s's group.
+__host__ __device__ inline void path_group(const WaveArgs &A, uint32_t s, uint32_t &lo, uint32_t &hi) {
+    if (s < A.spp32) {
+        lo = s & ~31u;
+        hi = s | 31u;
+    } else if (s - A.spp32 < A.spp8) {
+        lo = A.spp32 + ((s - A.spp32) & ~7u);
+        hi = A.spp32 + ((s - A.spp32) | 7u);
+    } else {
+        lo = hi = s;
+    }
 }
 __device__ __forceinline__ void path_coords(const WaveArgs &A, uint32_t slot, uint32_t &pix, uint32_t &frame) {
     if (A.batch) {
@@ -1403,8 +1430,9 @@ __global__ void k_film(WaveArgs A, float4 *sum, float4 *comp) {
     uint32_t p0, s0, p1, s1;
     path_pos_sample(A, first, p0, s0);
     path_pos_sample(A, last - 1, p1, s1);
-    if (s0 < A.spp8) s0 &= ~7u;
-    if (s1 < A.spp8) s1 |= 7u;
+    uint32_t lo, hi;
+    path_group(A, s0, s0, hi);
+    path_group(A, s1, lo, s1);
     s1 = min(s1, A.spp - 1u);
     bool any = false;
     float4 s = make_float4(0.0f, 0.0f, 0.0f, 0.0f), c = s;
@@ -1677,8 +1705,9 @@ cudaError_t enqueue_render(const pt_ctx *ctx, Enqueue &E, WaveArgs A, const pt_r
             uint32_t p0, s0, p1, s1;
             path_pos_sample(A, A.waveStart, p0, s0);
             path_pos_sample(A, A.waveStart + A.waveCount - 1, p1, s1);
-            if (s0 < A.spp8) s0 &= ~7u;
-            if (s1 < A.spp8) s1 |= 7u;
+            uint32_t lo, hi;
+            path_group(A, s0, s0, hi);
+            path_group(A, s1, lo, s1);
             s1 = std::min(s1, A.spp - 1u);
             A.recKeyBase = (uint64_t)s0 * A.npix;
             A.recKeyRange = (uint32_t)std::min<uint64_t>((uint64_t)(s1 - s0 + 1) * A.npix, 0xFFFFFFFFull);
@@ -1791,7 +1820,8 @@ int pt_render_impl(pt_ctx *ctx, const pt_render_params *P, float *d_sum, float *
     A.S = ctx->S;
     A.width = W; A.height = H; A.npix = (uint32_t)npix;
     A.spp = P->spp;
-    A.spp8 = P->spp & ~7u;  // samples in groups of 8 (path_pos_sample)
+    A.spp32 = P->spp & ~31u;  // samples in groups of 32, then of 8 (path_pos_sample)
+    A.spp8 = (P->spp - A.spp32) & ~7u;
     A.fullTilePix = 32u * (W / 8u) * (H / 4u);
     A.sampleOffset = ctx->d_err + 1;
     A.rngKind = P->rng_kind; A.envMode = P->env_sampling; A.maxDepth = P->max_depth;
@@ -2151,7 +2181,7 @@ int render_batch(pt_ctx *ctx, const pt_request *R, uint32_t n, float *request_ms
     memset(&A, 0, sizeof(A));
     A.S = ctx->S;
     A.width = hostReqs[0].width; A.height = hostReqs[0].height; A.npix = hostReqs[0].npix;
-    A.spp = A.spp8 = A.fullTilePix = 0u;  // batches keep their own path order (slotInfo)
+    A.spp = A.spp32 = A.spp8 = A.fullTilePix = 0u;  // batches keep their own path order (slotInfo)
     A.recKeyBase = 0u;
     A.recKeyRange = 0u;
     A.sampleOffset = ctx->d_err + 1;
