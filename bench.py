@@ -143,9 +143,10 @@ def measured_peaks():
 
 # k_extend DRAM traffic per extension ray (dram__bytes_read.sum + dram__bytes_write.sum
 # from one ncu capture of this workload at 8 spp, the smallest case in the
-# grouped path order of the full frame: 383.3 MB over the 7,372,800 camera
-# rays of bounce 0).  The scene is L2-resident and the queues stream once, so
-# traffic scales with the rays a launch processes.
+# grouped path order (groups of 8 samples): 383.3 MB over the 7,372,800
+# camera rays of bounce 0; the full frame's groups of 32 are more coherent,
+# so this is an upper bound for it).  The scene is L2-resident and the
+# queues stream once, so traffic scales with the rays a launch processes.
 EXTEND_DRAM_BYTES_PER_RAY = {"disney_envmap": 52.0}
 
 
